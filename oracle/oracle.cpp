@@ -1,0 +1,720 @@
+// CPU restatement of the TideGBM training hot path — TEST INFRASTRUCTURE ONLY.
+//
+// Used by tests/, by __graft_entry__.smoke() as the checker and by bench.py's
+// cpu_baseline leg.  The product never links or calls it.  Single-threaded,
+// written for clarity; every function names the reference file:line it
+// restates (paths relative to the reference project root).  Compiled with
+// -ffp-contract=off so the FP64 arithmetic follows the reference's statement
+// order exactly.
+//
+// Library dependency: the reference draws its random samples with libstdc++'s
+// std::mt19937 + std::shuffle and orders GOSS candidates with std::sort; this
+// restatement calls the same library routines with the same arguments, so the
+// same libstdc++ (GCC 13 here) gives the same samples.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+struct OrcNode {
+    int is_leaf = 1;
+    int feature = -1;
+    int threshold_bin = -1;
+    int left = -1;
+    int right = -1;
+    int missing_go_left = 1;
+    double value = 0.0;
+    double gain = 0.0;
+    int n_samples = 0;
+    int depth = 0;
+};
+
+struct OrcTree {
+    std::vector<OrcNode> nodes;
+    std::vector<double> values;
+    std::vector<int> cover;
+    std::vector<double> prefix;
+};
+
+struct OrcModel {
+    orc_config cfg;
+    int n_f = 0;
+    int n_bins = 0;
+    int n_buckets = 1;
+    double init_score = 0.0;
+    std::vector<double> init_prefix;
+    std::vector<double> edges;  // n_f x 256
+    std::vector<int> n_edges;
+    std::vector<OrcTree> trees;
+    std::vector<double> evals;
+};
+
+inline bool is_nan(double v) { return !(v == v); }
+
+// cpp/src/binning.cpp:14-32
+std::vector<double> quantile_edges(std::vector<double>& vals, int n_bins) {
+    std::sort(vals.begin(), vals.end());
+    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    if (vals.empty()) return {0.0};
+    if (static_cast<int>(vals.size()) <= n_bins) return vals;
+    std::vector<double> e;
+    for (int i = 1; i < n_bins; ++i) {
+        const double q = static_cast<double>(i) / n_bins;
+        const double pos = q * (vals.size() - 1);
+        const size_t lo = static_cast<size_t>(pos);
+        const size_t hi = std::min(lo + 1, vals.size() - 1);
+        const double frac = pos - lo;
+        e.push_back(vals[lo] * (1 - frac) + vals[hi] * frac);
+    }
+    std::sort(e.begin(), e.end());
+    e.erase(std::unique(e.begin(), e.end()), e.end());
+    return e;
+}
+
+// cpp/include/tidegbm/tree.hpp:53-67 with l1 = 0 and max_delta_step = 0.
+inline double leaf_value(double G, double H, double l2) { return -G / (H + l2); }
+
+// cpp/src/histogram.cpp:126-134 with l1 = 0.
+inline double leaf_score(double G, double H, double lam) { return (G * G) / (H + lam); }
+
+// cpp/src/tree.cpp:15-41 for axis splits on uint8 codes.
+int apply_one(const OrcTree& t, const uint8_t* row) {
+    int nid = 0;
+    for (;;) {
+        const OrcNode& d = t.nodes[nid];
+        if (d.is_leaf) return nid;
+        const int b = row[d.feature];
+        const bool left = (b == 0) ? d.missing_go_left != 0 : b <= d.threshold_bin;
+        nid = left ? d.left : d.right;
+    }
+}
+
+// cpp/src/objective.cpp:18-39
+void group_runs(const int64_t* groups, int n, std::vector<int>& idx,
+                std::vector<std::pair<int, int>>& runs) {
+    idx.resize(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    bool sorted = true;
+    for (int i = 1; i < n; ++i)
+        if (groups[i] < groups[i - 1]) {
+            sorted = false;
+            break;
+        }
+    if (!sorted)
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return groups[a] < groups[b]; });
+    runs.clear();
+    int i = 0;
+    while (i < n) {
+        int j = i + 1;
+        while (j < n && groups[idx[j]] == groups[idx[i]]) ++j;
+        runs.emplace_back(i, j - i);
+        i = j;
+    }
+}
+
+// cpp/src/booster.cpp:36-58
+int auto_time_buckets(const int64_t* ts, int n, int64_t horizon, int uniq_cap) {
+    std::vector<int64_t> u(ts, ts + n);
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    int64_t step = 1;
+    if (u.size() >= 2) {
+        std::vector<int64_t> d;
+        for (size_t i = 1; i < u.size(); ++i)
+            if (u[i] - u[i - 1] > 0) d.push_back(u[i] - u[i - 1]);
+        if (!d.empty()) {
+            std::nth_element(d.begin(), d.begin() + d.size() / 2, d.end());
+            step = std::max<int64_t>(d[d.size() / 2], 1);
+        }
+    }
+    const int h_steps = static_cast<int>(std::max<int64_t>(horizon, 0) / step);
+    const int want = h_steps >= 8 ? 64 : 32;
+    return std::max(2, std::min(want, std::max(uniq_cap, 2)));
+}
+
+// cpp/src/tree.cpp:283-472, axis splits only (no colsample, groups, HALO, PAIR,
+// regime, interaction constraints, monotone).  Rows are sorted ascending first.
+OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const double* h,
+                  std::vector<int32_t> sample, int n_f, int n_bins, const orc_config& c) {
+    OrcTree tree;
+    std::sort(sample.begin(), sample.end());
+    const int nb_stride = n_bins;
+    OrcNode root;
+    root.n_samples = static_cast<int>(sample.size());
+    double sg = 0, sh = 0;
+    for (int32_t i : sample) {
+        sg += g[i];
+        sh += h[i];
+    }
+    root.value = leaf_value(sg, sh, c.l2);
+    tree.nodes.push_back(root);
+    std::vector<std::vector<int32_t>> leaf_idx(1, sample);
+    std::vector<std::vector<double>> leaf_hist(1);
+    leaf_hist[0].assign(static_cast<size_t>(n_f) * nb_stride * 3, 0.0);
+    orc_build_hist(codes, stride, n_f, sample.data(), static_cast<int>(sample.size()), g, h, n_bins,
+                   leaf_hist[0].data());
+    std::vector<orc_split> cached(1);
+    std::vector<char> ok(1, 0);
+
+    auto best_for_leaf = [&](int lid) {
+        // cpp/src/tree.cpp:106-166
+        orc_split best{-1e300, -1, -1, 1};
+        for (int f = 0; f < n_f; ++f) {
+            orc_split s = orc_best_numeric(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
+                                           c.min_samples_leaf, c.min_child_weight);
+            if (s.feature < 0 || s.gain < c.min_split_gain) continue;
+            if (s.gain > best.gain) best = s;
+        }
+        return best;
+    };
+
+    for (int iter = 0; iter < c.max_leaves - 1; ++iter) {
+        int best_leaf = -1;
+        orc_split best{-1e300, -1, -1, 1};
+        double best_score = c.min_split_gain;
+        for (int lid = 0; lid < static_cast<int>(tree.nodes.size()); ++lid) {
+            if (!tree.nodes[lid].is_leaf) continue;
+            if (tree.nodes[lid].depth >= c.max_depth) continue;
+            if (static_cast<int>(leaf_idx[lid].size()) < 2 * c.min_samples_leaf) continue;
+            if (!ok[lid]) {
+                cached[lid] = best_for_leaf(lid);
+                ok[lid] = 1;
+            }
+            const orc_split& rec = cached[lid];
+            if (rec.feature >= 0 && rec.gain >= c.min_split_gain && rec.gain > best_score) {
+                best_score = rec.gain;
+                best_leaf = lid;
+                best = rec;
+            }
+        }
+        if (best_leaf < 0) break;
+        OrcNode& p = tree.nodes[best_leaf];
+        p.is_leaf = 0;
+        p.feature = best.feature;
+        p.threshold_bin = best.threshold_bin;
+        p.missing_go_left = best.missing_go_left;
+        p.gain = best.gain;
+        ok[best_leaf] = 0;
+        // cpp/src/tree.cpp:68-91 stable partition
+        std::vector<int32_t> L, R;
+        for (int32_t i : leaf_idx[best_leaf]) {
+            const int b = codes[static_cast<size_t>(i) * stride + best.feature];
+            const bool left = (b == 0) ? best.missing_go_left != 0 : b <= best.threshold_bin;
+            (left ? L : R).push_back(i);
+        }
+        OrcNode nl, nr;
+        nl.depth = nr.depth = p.depth + 1;
+        nl.n_samples = static_cast<int>(L.size());
+        nr.n_samples = static_cast<int>(R.size());
+        auto fill_val = [&](OrcNode& nd, const std::vector<int32_t>& ix) {
+            double G = 0, H = 0;
+            for (int32_t i : ix) {
+                G += g[i];
+                H += h[i];
+            }
+            nd.value = leaf_value(G, H, c.l2);
+        };
+        fill_val(nl, L);
+        fill_val(nr, R);
+        // cpp/src/tree.cpp:418-436: build the smaller child, subtract for the other.
+        const bool left_small = L.size() <= R.size();
+        const std::vector<int32_t>& small_ix = left_small ? L : R;
+        std::vector<double> small(leaf_hist[best_leaf].size(), 0.0);
+        orc_build_hist(codes, stride, n_f, small_ix.data(), static_cast<int>(small_ix.size()), g, h,
+                       n_bins, small.data());
+        std::vector<double> big = std::move(leaf_hist[best_leaf]);
+        for (size_t k = 0; k < big.size(); ++k) big[k] -= small[k];
+        const int left_id = static_cast<int>(tree.nodes.size());
+        tree.nodes[best_leaf].left = left_id;
+        tree.nodes[best_leaf].right = left_id + 1;
+        tree.nodes.push_back(nl);
+        tree.nodes.push_back(nr);
+        leaf_idx.push_back(std::move(L));
+        leaf_idx.push_back(std::move(R));
+        if (left_small) {
+            leaf_hist.push_back(std::move(small));
+            leaf_hist.push_back(std::move(big));
+        } else {
+            leaf_hist.push_back(std::move(big));
+            leaf_hist.push_back(std::move(small));
+        }
+        leaf_hist[best_leaf].clear();
+        leaf_idx[best_leaf].clear();
+        cached.resize(tree.nodes.size());
+        ok.resize(tree.nodes.size(), 0);
+    }
+    const size_t nn = tree.nodes.size();
+    tree.values.resize(nn);
+    tree.cover.resize(nn);
+    for (size_t k = 0; k < nn; ++k) {
+        tree.values[k] = tree.nodes[k].value;
+        tree.cover[k] = tree.nodes[k].n_samples;
+    }
+    return tree;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+int orc_binner_fit(const double* X, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
+                   double* edges, int* n_edges, int* n_bins_col) {
+    // cpp/src/binning.cpp:34-102, numeric features, mask all ones.
+    int mx = 2;
+    for (int f = 0; f < n_f; ++f) {
+        std::vector<double> vals;
+        vals.reserve(n);
+        for (int i = 0; i < n; ++i) {
+            const double v = X[static_cast<size_t>(i) * n_f + f];
+            if (!is_nan(v)) vals.push_back(v);
+        }
+        if (bin_sample > 0 && static_cast<int>(vals.size()) > bin_sample) {
+            std::mt19937 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
+            std::shuffle(vals.begin(), vals.end(), rng);
+            vals.resize(static_cast<size_t>(bin_sample));
+        }
+        std::vector<double> e = quantile_edges(vals, max_bin - 1);
+        n_edges[f] = static_cast<int>(e.size());
+        std::memcpy(edges + static_cast<size_t>(f) * 256, e.data(), e.size() * sizeof(double));
+        n_bins_col[f] = static_cast<int>(e.size()) + 2;
+        mx = std::max(mx, n_bins_col[f]);
+    }
+    return std::max(mx, max_bin);  // binning.cpp:130-134
+}
+
+void orc_bin_transform(const double* X, int n, int n_f, const double* edges, const int* n_edges,
+                       uint8_t* codes, int stride) {
+    // cpp/src/binning.cpp:104-128: code = 1 + upper_bound(edges, v); NaN -> 0.
+    for (int i = 0; i < n; ++i)
+        for (int f = 0; f < n_f; ++f) {
+            const double v = X[static_cast<size_t>(i) * n_f + f];
+            int b = 0;
+            if (!is_nan(v)) {
+                const double* e = edges + static_cast<size_t>(f) * 256;
+                b = static_cast<int>(std::upper_bound(e, e + n_edges[f], v) - e) + 1;
+            }
+            codes[static_cast<size_t>(i) * stride + f] = static_cast<uint8_t>(b);
+        }
+}
+
+void orc_build_hist(const uint8_t* codes, int stride, int n_f, const int32_t* idx, int n_idx,
+                    const double* g, const double* h, int n_bins, double* out) {
+    // cpp/src/histogram.cpp:44-76 (per feature, rows in idx order).
+    std::memset(out, 0, sizeof(double) * 3 * static_cast<size_t>(n_f) * n_bins);
+    for (int f = 0; f < n_f; ++f) {
+        double* B = out + static_cast<size_t>(f) * n_bins * 3;
+        for (int k = 0; k < n_idx; ++k) {
+            const int32_t i = idx[k];
+            const int b = codes[static_cast<size_t>(i) * stride + f];
+            B[3 * b] += g[i];
+            B[3 * b + 1] += h[i];
+            B[3 * b + 2] += 1.0;
+        }
+    }
+}
+
+orc_split orc_best_numeric(const double* ghc, int n_bins, int f, double lam, double gamma,
+                           int min_leaf, double min_hess) {
+    // cpp/src/histogram.cpp:144-193 with l1 = 0 and monotone = 0.
+    orc_split best{-1e300, -1, -1, 1};
+    const double* B = ghc + static_cast<size_t>(f) * n_bins * 3;
+    double totG = 0, totH = 0;
+    int64_t totC = 0;
+    for (int b = 0; b < n_bins; ++b) {
+        totG += B[3 * b];
+        totH += B[3 * b + 1];
+        totC += static_cast<int64_t>(B[3 * b + 2]);
+    }
+    const double missG = B[0], missH = B[1];
+    const int64_t missC = static_cast<int64_t>(B[2]);
+    const double parent = leaf_score(totG, totH, lam);
+    double GL = 0, HL = 0;
+    int64_t CL = 0;
+    for (int b = 1; b < n_bins - 1; ++b) {
+        const int64_t cb = static_cast<int64_t>(B[3 * b + 2]);
+        GL += B[3 * b];
+        HL += B[3 * b + 1];
+        CL += cb;
+        if (cb == 0) continue;
+        for (int ml = 0; ml <= 1; ++ml) {
+            const double gL = GL + (ml ? missG : 0);
+            const double hL = HL + (ml ? missH : 0);
+            const int64_t cL = CL + (ml ? missC : 0);
+            const double gR = totG - gL, hR = totH - hL;
+            const int64_t cR = totC - cL;
+            if (cL < min_leaf || cR < min_leaf) continue;
+            if (hL < min_hess || hR < min_hess) continue;
+            const double gain =
+                0.5 * (leaf_score(gL, hL, lam) + leaf_score(gR, hR, lam) - parent) - gamma;
+            if (gain > best.gain) best = orc_split{gain, f, b, ml};
+        }
+    }
+    return best;
+}
+
+void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t* groups, int n,
+                   double* g, double* h) {
+    if (kind == 0) {  // objective.cpp:105-118, w = 1, no cost terms
+        for (int i = 0; i < n; ++i) {
+            g[i] = 1.0 * (pred[i] - y[i]);
+            h[i] = 1.0;
+        }
+        return;
+    }
+    // objective.cpp:179-219
+    std::fill(g, g + n, 0.0);
+    std::fill(h, h + n, 1e-6);
+    if (!groups) return;
+    std::vector<int> idx;
+    std::vector<std::pair<int, int>> runs;
+    group_runs(groups, n, idx, runs);
+    for (const auto& r : runs) {
+        const int* ix = idx.data() + r.first;
+        const int m = r.second;
+        if (m < 2) continue;
+        const int step = m > 48 ? std::max(1, m / 24) : 1;
+        for (int a = 0; a < m; ++a)
+            for (int b = a + step; b < m; b += step) {
+                const int i = ix[a], j = ix[b];
+                if (y[i] == y[j]) continue;
+                int hi = i, lo = j;
+                if (y[j] > y[i]) {
+                    hi = j;
+                    lo = i;
+                }
+                const double s = pred[hi] - pred[lo];
+                const double e = std::exp(std::clamp(1.0 * s, -30.0, 30.0));
+                const double dyw = std::max(std::abs(y[hi] - y[lo]), 1e-6);
+                const double lam = -1.0 / (1.0 + e) * dyw;
+                const double d2 = 1.0 * 1.0 * e / ((1 + e) * (1 + e)) * dyw;
+                g[hi] += 1.0 * lam;
+                g[lo] -= 1.0 * lam;
+                h[hi] += 1.0 * d2;
+                h[lo] += 1.0 * d2;
+            }
+    }
+}
+
+double orc_loss(int kind, const double* y, const double* pred, const int64_t* groups, int n) {
+    if (kind == 5 && groups) {  // objective.cpp:290-322
+        std::vector<int> idx;
+        std::vector<std::pair<int, int>> runs;
+        group_runs(groups, n, idx, runs);
+        double acc = 0;
+        int ng = 0;
+        for (const auto& r : runs) {
+            const int* ix = idx.data() + r.first;
+            const int m = r.second;
+            if (m < 3) continue;
+            double my = 0, mp = 0;
+            for (int k = 0; k < m; ++k) {
+                my += y[ix[k]];
+                mp += pred[ix[k]];
+            }
+            my /= m;
+            mp /= m;
+            double vy = 0, vp = 0, cc = 0;
+            for (int k = 0; k < m; ++k) {
+                const double dy = y[ix[k]] - my, dp = pred[ix[k]] - mp;
+                vy += dy * dy;
+                vp += dp * dp;
+                cc += dy * dp;
+            }
+            if (vy > 1e-18 && vp > 1e-18) {
+                acc += cc / std::sqrt(vy * vp);
+                ng += 1;
+            }
+        }
+        return ng > 0 ? -acc / ng : 0.0;
+    }
+    double s = 0, sw = 0;  // objective.cpp:323-328
+    for (int i = 0; i < n; ++i) {
+        const double d = pred[i] - y[i];
+        s += 1.0 * d * d;
+        sw += 1.0;
+    }
+    return sw > 0 ? s / sw : 0;
+}
+
+void orc_config_default(orc_config* c) {
+    // Defaults of cpp/include/tidegbm/config.hpp:13-113.
+    c->n_estimators = 100;
+    c->learning_rate = 0.1;
+    c->max_depth = 6;
+    c->max_leaves = 31;
+    c->min_samples_leaf = 20;
+    c->min_child_weight = 1e-3;
+    c->l2 = 1.0;
+    c->min_split_gain = 0.0;
+    c->max_bin = 255;
+    c->n_time_buckets = 0;
+    c->horizon = -1;
+    c->embargo = 0;
+    c->iid_mode = 0;
+    c->objective = 0;
+    c->random_state = 0;
+    c->goss = -1;
+    c->goss_top = 0.2;
+    c->goss_other = 0.1;
+    c->bin_sample = 262144;
+    c->torb_min_cover = 0.0;
+    c->finer_torb = 1;
+}
+
+void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, int n, int n_f,
+              const int64_t* ts_in, const int64_t* ent_in) {
+    // cpp/src/booster.cpp:231-742 for the supported subset.
+    try {
+        const orc_config c = *cfgp;
+        if (!c.iid_mode && c.horizon < 0) throw std::runtime_error("horizon is required in time mode");
+        if (!c.iid_mode && !ts_in) throw std::runtime_error("timestamp is required unless iid_mode");
+        auto* M = new OrcModel();
+        M->cfg = c;
+        M->n_f = n_f;
+        std::vector<double> X(X_in, X_in + static_cast<size_t>(n) * n_f), y(y_in, y_in + n);
+        std::vector<int64_t> ts;
+        if (ts_in) ts.assign(ts_in, ts_in + n);
+        // booster.cpp:264-309 stable sort by (ts, entity)
+        if (!c.iid_mode && n > 1) {
+            std::vector<int> ord(n);
+            std::iota(ord.begin(), ord.end(), 0);
+            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+                if (ts_in[a] != ts_in[b]) return ts_in[a] < ts_in[b];
+                if (ent_in) return ent_in[a] < ent_in[b];
+                return a < b;
+            });
+            for (int i = 0; i < n; ++i) {
+                const int s = ord[i];
+                std::memcpy(&X[static_cast<size_t>(i) * n_f], X_in + static_cast<size_t>(s) * n_f,
+                            sizeof(double) * n_f);
+                y[i] = y_in[s];
+                ts[i] = ts_in[s];
+            }
+        }
+        // booster.cpp:311-331 TORB buckets
+        std::vector<int32_t> bucket(n, 0);
+        int nbk = 1;
+        int64_t embargo = c.embargo;
+        if (!c.iid_mode) {
+            std::vector<int64_t> u(ts);
+            std::sort(u.begin(), u.end());
+            u.erase(std::unique(u.begin(), u.end()), u.end());
+            const int uniq_n = std::max(2, static_cast<int>(u.size()));
+            int want = c.n_time_buckets;
+            if (want <= 0) want = auto_time_buckets(ts.data(), n, std::max<int64_t>(c.horizon, 0), uniq_n);
+            nbk = c.finer_torb ? std::max(2, std::min(want, uniq_n)) : std::max(2, want);
+            // booster.cpp:60-72 on already-sorted rows: rank = row position.
+            for (int i = 0; i < n; ++i) {
+                int b = static_cast<int>(static_cast<double>(i) / std::max(n, 1) * nbk);
+                if (b >= nbk) b = nbk - 1;
+                bucket[i] = b;
+            }
+            embargo += std::max<int64_t>(c.horizon, 0);
+        }
+        M->n_buckets = nbk;
+        // booster.cpp:337-364 prefix cuts
+        std::vector<int> cut(nbk, 0);
+        if (!c.iid_mode && n > 0) {
+            std::vector<int> first(nbk, -1);
+            for (int i = 0; i < n; ++i)
+                if (first[bucket[i]] < 0) first[bucket[i]] = i;
+            int run = 0;
+            for (int b = 0; b < nbk; ++b) {
+                int ct = 0;
+                if (first[b] >= 0) {
+                    const int64_t lim = ts[first[b]] - embargo;
+                    ct = static_cast<int>(std::lower_bound(ts.begin(), ts.end(), lim) - ts.begin());
+                }
+                run = std::max(run, ct);
+                cut[b] = run;
+            }
+        }
+        // booster.cpp:378-383 binning
+        M->edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
+        M->n_edges.assign(n_f, 0);
+        std::vector<int> nbc(n_f);
+        M->n_bins = orc_binner_fit(X.data(), n, n_f, c.max_bin, c.bin_sample,
+                                   static_cast<uint32_t>(c.random_state), M->edges.data(),
+                                   M->n_edges.data(), nbc.data());
+        std::vector<uint8_t> codes(static_cast<size_t>(n) * n_f);
+        orc_bin_transform(X.data(), n, n_f, M->edges.data(), M->n_edges.data(), codes.data(), n_f);
+        // booster.cpp:399-457 initial predictions (Objective::init_score,
+        // objective.cpp:80-100: mean for MSE, 0 for ranking).
+        auto init_of = [&](int m) -> double {
+            if (c.objective == 5 || m <= 0) return 0.0;
+            double sw = 0, sy = 0;
+            for (int i = 0; i < m; ++i) {
+                sw += 1.0;
+                sy += 1.0 * y[i];
+            }
+            return sw > 0 ? sy / sw : 0;
+        };
+        std::vector<double> pred(n);
+        M->init_prefix.assign(nbk, 0.0);
+        if (c.iid_mode) {
+            M->init_score = init_of(n);
+            std::fill(pred.begin(), pred.end(), M->init_score);
+        } else {
+            for (int b = 0; b < nbk; ++b) M->init_prefix[b] = cut[b] > 0 ? init_of(cut[b]) : NAN;
+            M->init_score = init_of(n);
+            for (int b = 0; b < nbk; ++b)
+                if (!std::isfinite(M->init_prefix[b])) M->init_prefix[b] = M->init_score;
+            for (int i = 0; i < n; ++i) pred[i] = M->init_prefix[bucket[i]];
+        }
+        const int64_t* groups = (c.objective == 5) ? ts.data() : nullptr;
+        std::mt19937 rng(static_cast<uint32_t>(c.random_state));
+        std::vector<double> g(n), h(n);
+        for (int m = 0; m < c.n_estimators; ++m) {
+            orc_grad_hess(c.objective, y.data(), pred.data(), groups, n, g.data(), h.data());
+            // booster.cpp:519-585 sampling: subsample = 1 keeps all rows; GOSS.
+            std::vector<int32_t> sample(n);
+            std::iota(sample.begin(), sample.end(), 0);
+            std::vector<double> gg, hg;
+            const double* gu = g.data();
+            const double* hu = h.data();
+            const bool use_goss = (c.goss > 0) || (c.goss < 0 && n >= 250000);
+            if (use_goss && c.goss_top < 1.0 && sample.size() > 64) {
+                gg = g;
+                hg = h;
+                std::vector<int32_t> order = sample;
+                std::sort(order.begin(), order.end(),
+                          [&](int32_t a, int32_t b) { return std::abs(g[a]) > std::abs(g[b]); });
+                const int n_top = std::min(static_cast<int>(order.size()),
+                                           std::max(1, static_cast<int>(std::ceil(c.goss_top * sample.size()))));
+                std::vector<char> keep(n, 0);
+                for (int i = 0; i < n_top; ++i) keep[order[i]] = 1;
+                std::vector<int32_t> rest(order.begin() + n_top, order.end());
+                int n_other = static_cast<int>(std::ceil(c.goss_other * sample.size()));
+                n_other = std::min(n_other, static_cast<int>(rest.size()));
+                std::shuffle(rest.begin(), rest.end(), rng);
+                const double scale = (1.0 - c.goss_top) / std::max(c.goss_other, 1e-12);
+                for (int i = 0; i < n_other; ++i) {
+                    keep[rest[i]] = 1;
+                    gg[rest[i]] *= scale;
+                    hg[rest[i]] *= scale;
+                }
+                sample.clear();
+                for (int32_t i : order)
+                    if (keep[i]) sample.push_back(i);
+                std::sort(sample.begin(), sample.end());
+                gu = gg.data();
+                hu = hg.data();
+            }
+            OrcTree tree = grow_tree(codes.data(), n_f, gu, hu, sample, n_f, M->n_bins, c);
+            (void)rng();  // booster.cpp:588 seeds grow_tree's own generator
+            // booster.cpp:589-600 full-data leaf values from unscaled g, h
+            std::vector<int> nid(n);
+            for (int i = 0; i < n; ++i) nid[i] = apply_one(tree, codes.data() + static_cast<size_t>(i) * n_f);
+            const int nn = static_cast<int>(tree.nodes.size());
+            std::vector<double> Gs(nn, 0), Hs(nn, 0);
+            tree.cover.assign(nn, 0);
+            for (int i = 0; i < n; ++i) {
+                Gs[nid[i]] += g[i];
+                Hs[nid[i]] += h[i];
+                tree.cover[nid[i]] += 1;
+            }
+            for (int k = 0; k < nn; ++k) tree.values[k] = leaf_value(Gs[k], Hs[k], c.l2);
+            // booster.cpp:604-648 TORB prefix values
+            tree.prefix.assign(static_cast<size_t>(nbk) * nn, 0.0);
+            if (c.iid_mode) {
+                for (int b = 0; b < nbk; ++b)
+                    for (int k = 0; k < nn; ++k) tree.prefix[static_cast<size_t>(b) * nn + k] = tree.values[k];
+            } else {
+                const double min_cover = c.torb_min_cover > 0.0
+                                             ? c.torb_min_cover
+                                             : static_cast<double>(2 * std::max(c.min_samples_leaf, 1));
+                std::vector<double> pG(nn, 0), pH(nn, 0);
+                int swept = 0;
+                for (int b = 0; b < nbk; ++b) {
+                    for (; swept < cut[b]; ++swept) {
+                        pG[nid[swept]] += g[swept];
+                        pH[nid[swept]] += h[swept];
+                    }
+                    const double cover = static_cast<double>(cut[b]);
+                    const double alpha = cover <= 0.0 ? 0.0 : std::min(1.0, cover / std::max(min_cover, 1.0));
+                    for (int k = 0; k < nn; ++k) {
+                        const double full = tree.values[k];
+                        const double pref = cover > 0.0 ? leaf_value(pG[k], pH[k], c.l2) : full;
+                        tree.prefix[static_cast<size_t>(b) * nn + k] = alpha * pref + (1.0 - alpha) * full;
+                    }
+                }
+            }
+            // booster.cpp:655-664
+            for (int i = 0; i < n; ++i) {
+                if (c.iid_mode) pred[i] += c.learning_rate * tree.values[nid[i]];
+                else pred[i] += c.learning_rate * tree.prefix[static_cast<size_t>(bucket[i]) * nn + nid[i]];
+            }
+            M->trees.push_back(std::move(tree));
+            M->evals.push_back(orc_loss(c.objective, y.data(), pred.data(), groups, n));  // booster.cpp:704-706
+        }
+        return M;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+void orc_free(void* m) { delete static_cast<OrcModel*>(m); }
+int orc_n_trees(void* m) { return static_cast<int>(static_cast<OrcModel*>(m)->trees.size()); }
+int orc_n_bins(void* m) { return static_cast<OrcModel*>(m)->n_bins; }
+int orc_n_buckets(void* m) { return static_cast<OrcModel*>(m)->n_buckets; }
+double orc_init_score(void* m) { return static_cast<OrcModel*>(m)->init_score; }
+void orc_init_prefix(void* m, double* out) {
+    const auto& v = static_cast<OrcModel*>(m)->init_prefix;
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+void orc_evals_train(void* m, double* out) {
+    const auto& v = static_cast<OrcModel*>(m)->evals;
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+int orc_tree_n_nodes(void* m, int t) {
+    return static_cast<int>(static_cast<OrcModel*>(m)->trees[t].nodes.size());
+}
+void orc_tree_export(void* m, int t, int* inodes, double* fnodes, double* values, int* cover,
+                     double* prefix) {
+    const OrcTree& tr = static_cast<OrcModel*>(m)->trees[t];
+    for (size_t k = 0; k < tr.nodes.size(); ++k) {
+        const OrcNode& d = tr.nodes[k];
+        int* o = inodes + 8 * k;
+        o[0] = d.is_leaf;
+        o[1] = d.feature;
+        o[2] = d.threshold_bin;
+        o[3] = d.left;
+        o[4] = d.right;
+        o[5] = d.missing_go_left;
+        o[6] = d.n_samples;
+        o[7] = d.depth;
+        fnodes[2 * k] = d.value;
+        fnodes[2 * k + 1] = d.gain;
+        values[k] = tr.values[k];
+        cover[k] = tr.cover[k];
+    }
+    std::memcpy(prefix, tr.prefix.data(), tr.prefix.size() * sizeof(double));
+}
+
+void orc_predict_raw(void* mp, const double* X, int n, double* out) {
+    // booster.cpp:744-773 with tree_decay = 1 and best_iteration = n_estimators.
+    const OrcModel& M = *static_cast<OrcModel*>(mp);
+    std::vector<uint8_t> codes(static_cast<size_t>(n) * M.n_f);
+    orc_bin_transform(X, n, M.n_f, M.edges.data(), M.n_edges.data(), codes.data(), M.n_f);
+    for (int i = 0; i < n; ++i) {
+        double s = M.init_score;
+        for (const OrcTree& t : M.trees)
+            s += M.cfg.learning_rate * t.values[apply_one(t, codes.data() + static_cast<size_t>(i) * M.n_f)];
+        out[i] = s;
+    }
+}
+
+}  // extern "C"

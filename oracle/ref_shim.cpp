@@ -1,0 +1,229 @@
+// C-ABI shim over the reference TideGBM core, compiled together with the
+// reference's own sources (see oracle/Makefile) into oracle/_ref/libtgbref.so.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product links or loads this file;
+// tests/, bench.py's reference arm and the oracle pinning tests use it to run
+// the reference's CPU path on the same inputs as the CUDA path.
+//
+// It exposes:
+//   * the whole Booster::fit (cpp/src/booster.cpp:231) with a flat key/value
+//     config, and read-back of the fitted trees, init prefixes and evals;
+//   * Binner::fit / transform (cpp/src/binning.cpp:34-128);
+//   * build_hist_col (cpp/src/histogram.cpp:44-76);
+//   * best_numeric_missing (cpp/src/histogram.cpp:144-193);
+//   * Objective::grad_hess / loss (cpp/src/objective.cpp:102-329);
+//   * apply_all (cpp/src/tree.cpp:43-55).
+#include "tidegbm/booster.hpp"
+#include "tidegbm/histogram.hpp"
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace tidegbm;
+
+namespace {
+thread_local std::string g_err;
+
+ObjectiveKind objective_from_code(int code) {
+    switch (code) {
+        case 0: return ObjectiveKind::MSE;
+        case 5: return ObjectiveKind::RankPairwise;
+        default: return static_cast<ObjectiveKind>(code);
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_err.c_str(); }
+
+void* ref_create(void) { return new Booster(); }
+void ref_free(void* b) { delete static_cast<Booster*>(b); }
+
+// Sets one Config field.  Unknown keys return -1.
+int ref_set(void* hb, const char* key, double v) {
+    Config& c = static_cast<Booster*>(hb)->cfg;
+    const std::string k(key);
+    if (k == "n_estimators") c.n_estimators = static_cast<int>(v);
+    else if (k == "learning_rate") c.learning_rate = v;
+    else if (k == "max_depth") c.max_depth = static_cast<int>(v);
+    else if (k == "max_leaves") c.max_leaves = static_cast<int>(v);
+    else if (k == "min_samples_leaf") c.min_samples_leaf = static_cast<int>(v);
+    else if (k == "min_child_weight") c.min_child_weight = v;
+    else if (k == "l2") c.l2 = v;
+    else if (k == "min_split_gain") c.min_split_gain = v;
+    else if (k == "max_bin") c.max_bin = static_cast<int>(v);
+    else if (k == "n_time_buckets") c.n_time_buckets = static_cast<int>(v);
+    else if (k == "horizon") c.horizon = static_cast<i64>(v);
+    else if (k == "embargo") c.embargo = static_cast<i64>(v);
+    else if (k == "iid_mode") c.iid_mode = v != 0;
+    else if (k == "halo") c.halo = v != 0;
+    else if (k == "pair_splits") c.pair_splits = v != 0;
+    else if (k == "objective") c.objective = objective_from_code(static_cast<int>(v));
+    else if (k == "n_jobs") c.n_jobs = static_cast<int>(v);
+    else if (k == "random_state") c.random_state = static_cast<int>(v);
+    else if (k == "goss") c.goss = static_cast<int>(v);
+    else if (k == "goss_top") c.goss_top = v;
+    else if (k == "goss_other") c.goss_other = v;
+    else if (k == "bin_sample") c.bin_sample = static_cast<int>(v);
+    else if (k == "col_major_hist") c.col_major_hist = v != 0;
+    else if (k == "torb_min_cover") c.torb_min_cover = v;
+    else if (k == "finer_torb") c.finer_torb = v != 0;
+    else if (k == "ooc_bytes") c.ooc_bytes = static_cast<size_t>(v);
+    else {
+        g_err = "unknown key " + k;
+        return -1;
+    }
+    return 0;
+}
+
+int ref_fit(void* hb, const double* X, const double* y, int n, int n_f, const long long* ts,
+            const long long* rank_groups, const long long* entity) {
+    try {
+        static_cast<Booster*>(hb)->fit(X, y, n, n_f, reinterpret_cast<const i64*>(ts), nullptr,
+                                       nullptr, nullptr, nullptr,
+                                       reinterpret_cast<const i64*>(rank_groups), nullptr, nullptr,
+                                       nullptr, 0, reinterpret_cast<const i64*>(entity), nullptr);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_predict_raw(void* hb, const double* X, int n, int n_f, double* out) {
+    try {
+        static_cast<Booster*>(hb)->predict_raw(X, n, n_f, out);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_n_trees(void* hb) { return static_cast<int>(static_cast<Booster*>(hb)->trees.size()); }
+int ref_n_bins(void* hb) { return static_cast<Booster*>(hb)->n_bins; }
+int ref_n_time_buckets(void* hb) { return static_cast<Booster*>(hb)->n_time_buckets; }
+double ref_init_score(void* hb) { return static_cast<Booster*>(hb)->init_score; }
+int ref_n_evals(void* hb) { return static_cast<int>(static_cast<Booster*>(hb)->evals.train.size()); }
+
+void ref_evals_train(void* hb, double* out) {
+    const auto& v = static_cast<Booster*>(hb)->evals.train;
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+
+void ref_init_prefix(void* hb, double* out) {
+    const auto& v = static_cast<Booster*>(hb)->init_prefix;
+    std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+
+int ref_tree_n_nodes(void* hb, int t) {
+    return static_cast<int>(static_cast<Booster*>(hb)->trees[t].nodes.size());
+}
+
+// Node fields as int32 [is_leaf, feature, threshold_bin, left, right, missing_go_left,
+// n_samples, depth] and f64 [value, gain]; values/cover per node; prefix values
+// n_buckets * n_nodes.
+void ref_tree_export(void* hb, int t, int* inodes, double* fnodes, double* values, int* cover,
+                     double* prefix) {
+    const Tree& tr = static_cast<Booster*>(hb)->trees[t];
+    const int nn = static_cast<int>(tr.nodes.size());
+    for (int k = 0; k < nn; ++k) {
+        const Node& d = tr.nodes[k];
+        int* o = inodes + 8 * k;
+        o[0] = d.is_leaf ? 1 : 0;
+        o[1] = d.feature;
+        o[2] = d.threshold_bin;
+        o[3] = d.left;
+        o[4] = d.right;
+        o[5] = d.missing_go_left;
+        o[6] = d.n_samples;
+        o[7] = d.depth;
+        fnodes[2 * k] = d.value;
+        fnodes[2 * k + 1] = d.gain;
+        values[k] = tr.values[k];
+        cover[k] = tr.cover[k];
+    }
+    std::memcpy(prefix, tr.prefix_values.data(), tr.prefix_values.size() * sizeof(double));
+}
+
+int ref_edges(void* hb, int f, double* out) {
+    const auto& e = static_cast<Booster*>(hb)->binner.edges[f];
+    if (out) std::memcpy(out, e.data(), e.size() * sizeof(double));
+    return static_cast<int>(e.size());
+}
+
+// ---- component entry points -------------------------------------------------
+
+// Binner::fit on all rows (no mask) followed by transform into row-major u16 codes.
+// edges_out: F x 256 f64 (first n_edges[f] used).
+int ref_binner(const double* X, int n, int n_f, int max_bin, int bin_sample, unsigned seed,
+               double* edges_out, int* n_edges, int* n_bins_col, int* max_bins,
+               unsigned short* codes) {
+    try {
+        Binner b;
+        std::vector<int> is_cat(n_f, 0);
+        std::vector<u8> mask(n, 1);
+        b.fit(X, n, n_f, is_cat.data(), mask.data(), max_bin, 5, bin_sample, seed);
+        for (int f = 0; f < n_f; ++f) {
+            n_edges[f] = static_cast<int>(b.edges[f].size());
+            n_bins_col[f] = b.n_bins_col[f];
+            std::memcpy(edges_out + static_cast<size_t>(f) * 256, b.edges[f].data(),
+                        b.edges[f].size() * sizeof(double));
+        }
+        *max_bins = b.max_bins();
+        if (codes) b.transform(X, n, n_f, codes);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// build_hist_col; out is interleaved {g, h, c(as f64)} per (feature, bin).
+void ref_build_hist_col(const unsigned short* xcol, int n_rows, int n_f, const int* idx, int n_idx,
+                        const double* g, const double* h, int n_bins, int n_jobs, double* out) {
+    Hist hist;
+    hist.resize(n_f, n_bins);
+    build_hist_col(xcol, n_rows, n_f, idx, n_idx, g, h, hist, n_jobs);
+    for (size_t i = 0; i < hist.B.size(); ++i) {
+        out[3 * i] = hist.B[i].g;
+        out[3 * i + 1] = hist.B[i].h;
+        out[3 * i + 2] = static_cast<double>(hist.B[i].c);
+    }
+}
+
+// best_numeric_missing on one feature of an interleaved {g, h, c} histogram.
+// res: [gain], ires: [feature, threshold_bin, missing_go_left].
+void ref_best_numeric(const double* ghc, int n_f, int n_bins, int f, double lam, double gamma,
+                      int min_leaf, double min_hess, double* res, int* ires) {
+    Hist hist;
+    hist.resize(n_f, n_bins);
+    for (size_t i = 0; i < hist.B.size(); ++i) {
+        hist.B[i].g = ghc[3 * i];
+        hist.B[i].h = ghc[3 * i + 1];
+        hist.B[i].c = static_cast<i64>(ghc[3 * i + 2]);
+    }
+    SplitCand c = best_numeric_missing(hist, f, lam, gamma, min_leaf, min_hess, 0, 0.0);
+    res[0] = c.gain;
+    ires[0] = c.feature;
+    ires[1] = c.threshold_bin;
+    ires[2] = c.missing_go_left;
+}
+
+// Objective::grad_hess for MSE (kind 0) or RankPairwise (kind 5), unit weights.
+void ref_grad_hess(int kind, const double* y, const double* pred, const long long* groups, int n,
+                   double* g, double* h) {
+    Objective o;
+    o.kind = objective_from_code(kind);
+    o.grad_hess(y, pred, nullptr, reinterpret_cast<const i64*>(groups), n, g, h);
+}
+
+double ref_loss(int kind, const double* y, const double* pred, const long long* groups, int n) {
+    Objective o;
+    o.kind = objective_from_code(kind);
+    return o.loss(y, pred, nullptr, reinterpret_cast<const i64*>(groups), n);
+}
+
+}  // extern "C"
