@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the device="gpu" TideGBM training hot path on B200.
+
+Workload (default): the 10M-row panel — 5,000 dates x 2,000 entities, 128 float32
+features (N(0,1) and log-normal columns, 1% NaN), 255 bins, objective mse, GOSS auto
+(top 20% / other 10%), max_depth 8, max_leaves 31 (reference default), 100 trees,
+synthetic seeded data (tidegbm_b200.panels.panel_scale).
+
+A step is one boosting iteration (one tree: gradients, GOSS selection, histograms,
+split scans, partitions, post-tree TORB sweep, prediction update, loss).  One fit of
+max(100, W+K) trees is run through the C ABI (tgb_fit) from pinned host buffers:
+  value     trees/s over trees W..W+K-1, device time from CUDA events on the fit's
+            stream (inputs resident in HBM; the 1.28 GB code matrix exceeds L2)
+  e2e       trees/s of the whole tgb_fit call (host X/y in, trees out: binning,
+            H2D, transform, all trees, D2H) — wall clock
+A second, short fit with per-launch events around every histogram kernel gives the
+histogram GB/s (algorithmic bytes: rows x (F code bytes + 16 B of f64 g, h)).
+The reference's own CPU fit (oracle/_ref, built from its sources) is timed on a
+bounded 1M-row sample of the same workload and scaled to 10M rows; the reference's
+only GPU code (build_hist_gpu, compiled for sm_100a) is timed on the same root
+histogram as "plain GPU".
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "hist GB/s & trees/s (10M×128, 255 bins) vs plain GPU; serve p50/p99 at same IC"
+PARAMS = dict(n_estimators=100, learning_rate=0.1, max_depth=8, max_leaves=31, max_bin=255, horizon=1,
+              objective="mse", goss=-1, goss_top=0.2, goss_other=0.1, random_state=0, pair_splits=False)
+WORKLOAD = ("panel_scale: 10M rows (5000 dates x 2000 entities) x 128 f32 features, 1% NaN, 255 bins, mse, "
+            "GOSS auto (0.2/0.1), max_depth 8, max_leaves 31, 100 trees")
+
+
+def peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled every 200 ms during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:
+            pass
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for ln in open(self.path):
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx.append(float(p[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_panel(n_dates: int = 5000):
+    from tidegbm_b200 import panels
+
+    return panels.panel_scale(n_dates=n_dates)
+
+
+# ---------------------------------------------------------------- reference CPU
+def ref_cpu_trees_per_s(warmup: int, steps: int, n_dates: int = 500) -> dict:
+    """The reference's own CPU fit (oracle/_ref, all host cores, n_jobs = 0) on a
+    bounded sample of the workload: the first n_dates dates (n_dates x 2000 rows).
+    Per-tree time from the reference's per-iteration hook; scaled by rows to 10M."""
+    from oracle import bind
+
+    L = bind.ref_lib()
+    L.ref_fit_timed.argtypes = [C.c_void_p] + [np.ctypeslib.ndpointer(np.float64, flags="C")] * 2 + \
+        [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, np.ctypeslib.ndpointer(np.float64, flags="C")]
+    p = make_panel(n_dates)
+    X = np.ascontiguousarray(p.X, dtype=np.float64)
+    h = L.ref_create()
+    n_est = warmup + steps
+    cfg = dict(PARAMS, n_estimators=n_est, n_jobs=0, halo=0)
+    for k, v in cfg.items():
+        if k == "objective":
+            v = 0
+        if L.ref_set(h, k.encode(), float(v)) != 0:
+            raise KeyError(k)
+    t_iter = np.zeros(n_est)
+    ts = np.ascontiguousarray(p.ts)
+    ent = np.ascontiguousarray(p.entity.astype(np.int64))
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(2)
+    os.dup2(devnull, 2)  # the reference prints one line per iteration with verbose = 1
+    try:
+        t0 = time.perf_counter()
+        rc = L.ref_fit_timed(h, X, np.ascontiguousarray(p.y), p.n, p.n_features, ts.ctypes.data_as(C.c_void_p),
+                             None, ent.ctypes.data_as(C.c_void_p), t_iter)
+        wall = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 2)
+        os.close(devnull)
+        os.close(saved)
+    L.ref_free(h)
+    if rc != 0:
+        raise RuntimeError(L.ref_last_error().decode())
+    per_tree = (t_iter[n_est - 1] - (t_iter[warmup - 1] if warmup > 0 else 0.0)) / steps
+    scale = 10_000_000 / p.n
+    return {"value": 1.0 / (per_tree * scale), "unit": "trees/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"reference Booster::fit (oracle/_ref, -O3 -fopenmp, n_jobs=0) on {p.n} rows "
+                      f"({n_dates} dates x 2000) x 128 of the same generator; {warmup} warm-up + {steps} timed trees "
+                      f"via its per-iteration hook ({per_tree:.3f} s/tree), scaled x{scale:g} rows to 10M; "
+                      f"fit wall {wall:.1f} s incl. binning",
+            "per_tree_s_sample": per_tree}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    try:
+        from oracle import bind
+
+        if not bind.ref_available():
+            raise RuntimeError("reference core not built (oracle/_ref)")
+        r = ref_cpu_trees_per_s(max(1, args.warmup), max(1, args.steps))
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"{type(e).__name__}: {e}"}))
+        return
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "trees/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / r["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host OpenMP"},
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": r["value"], "unit": "trees/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- plain GPU
+def plain_gpu_hist(native, X32, edges, n_edges, idx, g, h, n_bins) -> dict | None:
+    """The reference's build_hist_gpu (cpp/src/histogram_cuda.cu:81-167, built for
+    sm_100a) on one root histogram, against this library's kernel on the same rows."""
+    import torch
+    from oracle import bind
+
+    if not os.path.exists(bind.REF_CUDA_SO):
+        return None
+    R = C.CDLL(bind.REF_CUDA_SO)
+    R.refgpu_build_hist.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_int, C.c_void_p]
+    n, nf = X32.shape
+    stride = (nf + 15) // 16 * 16
+    # codes via this library's transform (bit-identical to the reference's Binner::transform)
+    E = np.full((nf, 256), np.inf, dtype=np.float32)
+    for f in range(nf):
+        e = edges[f, : n_edges[f]]
+        e32 = e.astype(np.float32)
+        low = e32.astype(np.float64) < e
+        e32[low] = np.nextafter(e32[low], np.float32(np.inf))
+        E[f, : n_edges[f]] = e32
+    Xd = torch.from_numpy(X32).cuda()
+    Ed = torch.from_numpy(E).cuda()
+    ned = torch.from_numpy(n_edges.astype(np.int32)).cuda()
+    codes = torch.empty((n, stride), dtype=torch.uint8, device="cuda")
+    native.check(native.lib().tgb_bin_transform(C.c_void_p(Xd.data_ptr()), 0, n, nf, C.c_void_p(Ed.data_ptr()),
+                                                C.c_void_p(ned.data_ptr()), C.c_void_p(codes.data_ptr()), stride,
+                                                None))
+    del Xd
+    torch.cuda.synchronize()
+    xb16 = np.ascontiguousarray(codes[:, :nf].cpu().numpy().astype(np.uint16))
+    out = np.zeros(nf * n_bins * 3)
+    bytes_alg = idx.size * (nf + 16)
+    args = (xb16.ctypes.data_as(C.c_void_p), nf, idx.ctypes.data_as(C.c_void_p), idx.size,
+            g.ctypes.data_as(C.c_void_p), h.ctypes.data_as(C.c_void_p), n_bins, n, out.ctypes.data_as(C.c_void_p))
+    if R.refgpu_build_hist(*args) != 0:  # first call uploads the code matrix once
+        return None
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        R.refgpu_build_hist(*args)
+    ref_s = (time.perf_counter() - t0) / reps
+    # this library's kernel on the same rows, inputs resident
+    rt = torch.from_numpy(idx).cuda()
+    gt, ht = torch.from_numpy(g).cuda(), torch.from_numpy(h).cuda()
+    G = torch.zeros((nf, 256), dtype=torch.int64, device="cuda")
+    H = torch.zeros_like(G)
+    Cn = torch.zeros((nf, 256), dtype=torch.int32, device="cuda")
+    gs = 61 - (int(np.floor(np.log2(np.abs(g[idx]).max()))) + 1) - int(np.ceil(np.log2(idx.size)))
+    hs = 61 - (int(np.floor(np.log2(np.abs(h[idx]).max()))) + 1) - int(np.ceil(np.log2(idx.size)))
+    L = native.lib()
+    def ours():
+        L.tgb_hist_build(C.c_void_p(codes.data_ptr()), stride, nf, C.c_void_p(rt.data_ptr()), idx.size,
+                         C.c_void_p(gt.data_ptr()), C.c_void_p(ht.data_ptr()), gs, hs, C.c_void_p(G.data_ptr()),
+                         C.c_void_p(H.data_ptr()), C.c_void_p(Cn.data_ptr()), None)
+    for _ in range(3):
+        ours()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.default_stream())  # launches go to the legacy default stream (NULL)
+    for _ in range(10):
+        ours()
+    e1.record(torch.cuda.default_stream())
+    torch.cuda.synchronize()
+    ours_s = e0.elapsed_time(e1) / 10 / 1e3
+    # cross-check: both give the same counts
+    cnt = Cn.cpu().numpy()[:, :n_bins] // 13
+    same = bool(np.array_equal(cnt, out.reshape(nf, n_bins, 3)[:, :, 2].astype(np.int64)))
+    return {"rows": int(idx.size), "features": nf, "plain_gpu_call_s": ref_s,
+            "plain_gpu_gbs": bytes_alg / ref_s / 1e9, "ours_kernel_s": ours_s, "ours_gbs": bytes_alg / ours_s / 1e9,
+            "counts_match": same,
+            "note": "plain GPU = reference build_hist_gpu call as shipped (H2D of g/h/idx, FP64 global atomics "
+                    "over u16 row-major codes, D2H); ours = tgb_hist_build kernel on resident inputs"}
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args) -> None:
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from tidegbm_b200 import native
+
+    native.lib()
+    W, K = max(3, args.warmup), max(1, args.steps)
+    p = make_panel(args.dates)
+    n, nf = p.X.shape
+    # pinned host buffers for the end-to-end call
+    cudart = torch.cuda.cudart()
+    for arr in (p.X, p.y):
+        cudart.cudaHostRegister(arr.ctypes.data, arr.nbytes, 0)
+
+    # Warm-up fit (context, module load, allocator) on a small slice.
+    wb = native.Booster(device=local, **dict(PARAMS, n_estimators=3))
+    m = min(n, 400_000)
+    wb.fit(p.X[:m], p.y[:m], timestamps=p.ts[:m], entity=p.entity[:m])
+    del wb
+
+    n_est = max(PARAMS["n_estimators"], W + K)
+    b = native.Booster(device=local, **dict(PARAMS, n_estimators=n_est, timing_from=W))
+    launches0 = native.kernel_launches()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        b.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+        e2e_wall = time.perf_counter() - t0
+    st = b.fit_stats()
+    timed_ms = st["timed_ms"]
+    # timed trees are trees W .. n_est-1; K of them are the bench's steps
+    ms_per_tree = timed_ms / st["timed_trees"]
+    times = torch.tensor([ms_per_tree], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    ms_max = float(times.item())
+    value = world * 1000.0 / ms_max
+    info = b.info()
+    trees = b.trees()
+    d2h = sum(t.is_leaf.size * (8 * 4 + 2 * 8) + t.values.nbytes + t.cover.nbytes + t.prefix.nbytes for t in trees)
+    h2d = p.X.nbytes + p.y.nbytes
+    e2e = {"value": world * n_est / e2e_wall, "unit": "trees/s", "h2d_bytes_per_step": int(h2d / n_est),
+           "d2h_bytes_per_step": int(d2h / n_est), "fit_wall_s": e2e_wall, "trees": n_est,
+           "breakdown_s": {k: st[k] for k in ("sort", "bin_fit", "upload_transform", "trees", "download",
+                                              "host_rng")}}
+    # Histogram GB/s: short fit with events around every histogram launch.
+    bp = native.Booster(device=local, **dict(PARAMS, n_estimators=W + 2, timing_from=W, profile_hist=1))
+    bp.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+    sp = bp.fit_stats()
+    del bp
+    hist_bytes = sp["hist_rows"] * (nf + 16)
+    hist_gbs = hist_bytes / (sp["hist_ms"] / 1e3) / 1e9 if sp["hist_ms"] > 0 else None
+    pk = peaks()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "hist_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "achieved": hist_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": (hist_gbs / pk["hbm_gbs"]) if hist_gbs else None, "traffic": traffic,
+            "peak_source": pk["source"], "kernel": "hist_node_kernel<16>",
+            "launches": sp["hist_launches"], "avg_launch_ms": sp["hist_ms"] / max(1, sp["hist_launches"]),
+            "algorithmic_bytes": "rows x (128 code bytes + 16 B f64 g,h) per built node"}
+    line = {"metric": METRIC, "value": value, "unit": "trees/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (int64 fixed-point histograms)", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_rows": n, "n_features": nf, "n_bins": info["n_bins"],
+                       "timed_trees": int(st["timed_trees"]), "l2": "inputs larger than L2 (1.28 GB codes)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "hist_gbs": hist_gbs, "roofline": roof, "e2e": e2e,
+            "gpu_launches": int(st["timed_launches"] * K / max(1, st["timed_trees"])),
+            "gpu_launches_note": "this library's kernels per K timed trees (+ CUB radix-sort passes inside GOSS)",
+            "clocks": clk.summary()}
+    if rank == 0 and not args.no_baselines:
+        try:
+            line["cpu_baseline"] = {k: v for k, v in ref_cpu_trees_per_s(1, 3).items() if k != "per_tree_s_sample"}
+        except Exception as e:
+            line["cpu_baseline"] = {"unavailable": f"{type(e).__name__}: {e}"}
+        try:
+            edges = np.stack([np.pad(b.edges(f), (0, 256 - b.edges(f).size)) for f in range(nf)])
+            n_edges = np.array([b.edges(f).size for f in range(nf)])
+            rng = np.random.default_rng(0)
+            idx = np.sort(rng.choice(n, 3_000_000, replace=False)).astype(np.int32)
+            g = rng.standard_normal(n)
+            h = np.ones(n)
+            line["plain_gpu"] = plain_gpu_hist(native, p.X, edges, n_edges, idx, g, h, info["n_bins"])
+        except Exception as e:
+            line["plain_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dates", type=int, default=5000, help="panel dates (x 2000 rows); default 10M rows")
+    ap.add_argument("--no-baselines", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/* tidegbm_b200 — C ABI of the B200 (sm_100a) implementation of TideGBM's GBDT
+ * training hot path: quantile binning to uint8 codes, per-node gradient/hessian
+ * histograms, best-split scan, stable row partitioning, MSE and within-date
+ * pairwise gradients, and the per-tree TORB sweep.
+ *
+ * Conventions (those of the reference C API, cpp/include/tidegbm/c_api.h:9-28 and
+ * cpp/src/c_api.cpp:12-18): every function returns 0 on success and -1 on error,
+ * with the message in thread-local storage read by tgb_last_error(); no C++
+ * exception crosses the ABI; the caller owns every buffer it passes.  Host
+ * pointers are plain host memory (pinned memory is faster for the fit upload);
+ * "device" pointers are CUDA device memory of the current device and `stream` is
+ * a cudaStream_t (NULL = legacy default stream).
+ *
+ * x_dtype: 0 = float32, 1 = float64, row-major n x n_features.
+ */
+#ifndef TIDEGBM_B200_H
+#define TIDEGBM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define TGB_API __attribute__((visibility("default")))
+#else
+#define TGB_API
+#endif
+
+typedef struct tgb_booster tgb_booster;
+
+/* Message of the last failed call on this thread (tide_last_error, c_api.cpp:220). */
+TGB_API const char* tgb_last_error(void);
+
+/* Number of kernel launches issued by this library in this process (for audits). */
+TGB_API long long tgb_kernel_launches(void);
+
+/* ---- Booster level: the device="gpu" Booster (cpp/include/tidegbm/booster.hpp:22-72) ---- */
+
+/* tide_create (c_api.cpp:22-30); one booster owns one CUDA stream and its device
+ * buffers on `device` — no process-global state (unlike GpuHistState,
+ * cpp/src/histogram_cuda.cu:76-79). */
+TGB_API int tgb_booster_create(int device, tgb_booster** out);
+/* tide_free (c_api.cpp:232). */
+TGB_API void tgb_booster_free(tgb_booster* b);
+
+/* tide_set_int / tide_set_double (c_api.cpp:234-272), extended to every Config key the
+ * GPU path reads (cpp/include/tidegbm/config.hpp:49-113).  Unknown keys return -1. */
+TGB_API int tgb_set_int(tgb_booster* b, const char* key, long long value);
+TGB_API int tgb_set_double(tgb_booster* b, const char* key, double value);
+/* String keys the reference only sets through pybind (bindings.cpp:78, 115-125):
+ * "objective" in {"mse","l2","regression","auto","pairwise","lambdarank"}, "device". */
+TGB_API int tgb_set_str(tgb_booster* b, const char* key, const char* value);
+
+/* Booster::fit (cpp/src/booster.cpp:231-742) with device=="gpu", the entry
+ * tide_fit (c_api.cpp:274-288) reaches.  X: host, row-major; y: host f64 [n];
+ * timestamps: host int64 [n] (required unless iid_mode; rank groups of the pairwise
+ * objective); entity: host int64 [n] or NULL (sort key after the timestamp). */
+TGB_API int tgb_fit(tgb_booster* b, const void* X, int x_dtype, const double* y, int n, int n_features,
+            const long long* timestamps, const long long* entity);
+
+/* Booster::predict_raw (cpp/src/booster.cpp:805-811): init_score + lr * sum of tree
+ * values, computed on the device.  X host, out host f64 [n]. */
+TGB_API int tgb_predict_raw(tgb_booster* b, const void* X, int x_dtype, int n, int n_features, double* out);
+
+/* Fitted model read-back: the Tree / Node fields the .tgbm format serialises
+ * (cpp/src/serialize.cpp:120-143) and the booster fields around them. */
+TGB_API int tgb_model_info(tgb_booster* b, int* n_trees, int* n_bins, int* n_buckets, double* init_score);
+TGB_API int tgb_init_prefix(tgb_booster* b, double* out);  /* n_buckets values */
+TGB_API int tgb_evals_train(tgb_booster* b, double* out);  /* n_trees values (evals.train) */
+TGB_API int tgb_tree_n_nodes(tgb_booster* b, int tree);
+/* inodes[8k] = {is_leaf, feature, threshold_bin, left, right, missing_go_left, n_samples,
+ * depth}; fnodes[2k] = {value, gain}; values/cover per node; prefix n_buckets x n_nodes. */
+TGB_API int tgb_tree_export(tgb_booster* b, int tree, int* inodes, double* fnodes, double* values, int* cover,
+                    double* prefix);
+/* Bin edges of feature f (Binner::edges, cpp/include/tidegbm/binning.hpp:15); returns
+ * the count, copies them when out != NULL. */
+TGB_API int tgb_edges(tgb_booster* b, int f, double* out);
+/* Breakdown of the last fit (14 values): wall seconds {total, sort, bin_fit,
+ * upload+transform, trees, download, host_rng}, kernel_launches, then the timed range
+ * set by the int keys "timing_from" (first timed tree) and "profile_hist":
+ * {device ms (CUDA events), trees, kernel launches, histogram-kernel ms, histogram
+ * launches, rows histogrammed}. */
+TGB_API int tgb_fit_stats(tgb_booster* b, double* out14);
+
+/* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:
+ * quantile edges from the bin_sample values std::shuffle(mt19937(seed + f*2654435761))
+ * keeps, bit-identical to the reference.  X host row-major; edges_out [n_features][256],
+ * n_edges_out [n_features].  Returns Binner::max_bins() (binning.cpp:130-134) or -1. */
+TGB_API int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
+                           unsigned seed, double* edges_out, int* n_edges_out);
+
+/* The first `keep` elements of std::shuffle(iota(m), std::mt19937(seed)) (libstdc++),
+ * computed without materialising the range — the GOSS and bin-sample draw
+ * (cpp/src/booster.cpp:572, cpp/src/binning.cpp:95). */
+TGB_API int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out);
+
+/* ---- Kernel level: one reference function each, on device memory ---- */
+
+/* Binner::transform (cpp/src/binning.cpp:104-128): codes[i*stride + f] = 1 + #{edges <= x},
+ * NaN -> 0.  edges: device [n_features][256] of x_dtype, padded with +inf; for float32 X
+ * pass ceil_f32 of the f64 edges (smallest float >= edge) to reproduce the f64 compare.
+ * stride >= n_features, multiple of 16; padding bytes are zeroed. */
+TGB_API int tgb_bin_transform(const void* X, int x_dtype, int n, int n_features, const void* edges,
+                      const int* n_edges, unsigned char* codes, int stride, void* stream);
+
+/* build_hist_col (cpp/src/histogram.cpp:44-76) and the build_hist_gpu kernel it replaces
+ * (cpp/src/histogram_cuda.cu:28-44): for rows[0..n_rows), accumulate
+ * G[f][code] += rint(g * 2^gshift), H[f][code] += rint(h * 2^hshift), C[f][code] += 1.
+ * G, H: device int64 [n_features][256]; C: device int32 [n_features][256]; all must be
+ * zeroed (or hold a partial sum to add to).  Exact integer sums: pick the shifts so
+ * that n_rows * max|v| * 2^shift < 2^62. */
+TGB_API int tgb_hist_build(const unsigned char* codes, int stride, int n_features, const int* rows, int n_rows,
+                   const double* g, const double* h, int gshift, int hshift, long long* G, long long* H,
+                   int* C, void* stream);
+
+/* best_numeric_missing (cpp/src/histogram.cpp:144-193, l1 = 0, no monotone) for every
+ * feature of one fixed-point histogram: gain[f], thr[f] (-1 = none), ml[f]. */
+TGB_API int tgb_split_scan(const long long* G, const long long* H, const int* C, int n_features, int n_bins,
+                   int gshift, int hshift, double l2, double min_split_gain, int min_samples_leaf,
+                   double min_child_weight, double* gain, int* thr, int* missing_left, void* stream);
+
+/* split_indices (cpp/src/tree.cpp:68-91): stable partition of rows[0..n_rows) into
+ * out[0..n_left) (code == 0 ? missing_left : code <= threshold) and out[n_left..n_rows).
+ * n_left_out: device int.  workspace: device scratch of tgb_partition_workspace_bytes(n_rows). */
+TGB_API size_t tgb_partition_workspace_bytes(int n_rows);
+TGB_API int tgb_partition(const unsigned char* codes, int stride, const int* rows, int n_rows, int feature,
+                  int threshold, int missing_left, int* out, int* n_left_out, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* Objective::grad_hess (cpp/src/objective.cpp:102-219), unit weights, device f64 arrays.
+ * MSE: g = pred - y, h = 1.  Pairwise: date groups given as runs of consecutive rows
+ * (run_start/run_len device int [n_runs]; rows of a run are order[run_start..] when
+ * order != NULL, else consecutive). */
+TGB_API int tgb_grad_mse(const double* y, const double* pred, int n, double* g, double* h, void* stream);
+TGB_API int tgb_grad_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len,
+                      const int* order, int n_runs, int n, double* g, double* h, void* stream);
+
+/* Literal drop-in for the reference seam build_hist_gpu (cpp/include/tidegbm/histogram.hpp:
+ * 57-58, cpp/src/histogram_cuda.cu:81-167): host row-major uint16 codes (kept resident
+ * on the booster's device across calls with the same pointer), host idx/g/h, result
+ * written as the interleaved FP64 {g, h, c} Hist layout (histogram.hpp:14-46),
+ * n_features x n_bins. */
+TGB_API int tgb_build_hist_gpu(tgb_booster* b, const unsigned short* xb, int n_features, const int* idx, int n_idx,
+                       const double* g, const double* h, int n_bins, int n_rows, double* out_ghc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

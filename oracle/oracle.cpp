@@ -364,6 +364,14 @@ orc_split orc_best_numeric(const double* ghc, int n_bins, int f, double lam, dou
     return best;
 }
 
+void orc_shuffle_prefix(int64_t m, int64_t keep, uint32_t seed, int32_t* out) {
+    std::vector<int32_t> v(static_cast<size_t>(m));
+    std::iota(v.begin(), v.end(), 0);
+    std::mt19937 rng(seed);
+    std::shuffle(v.begin(), v.end(), rng);
+    std::copy(v.begin(), v.begin() + keep, out);
+}
+
 void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t* groups, int n,
                    double* g, double* h) {
     if (kind == 0) {  // objective.cpp:105-118, w = 1, no cost terms

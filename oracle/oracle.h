@@ -48,6 +48,10 @@ void orc_build_hist(const uint8_t* codes, int stride, int n_f, const int32_t* id
 orc_split orc_best_numeric(const double* ghc, int n_bins, int f, double lam, double gamma,
                            int min_leaf, double min_hess);
 
+/* First `keep` elements of std::shuffle(iota(m), std::mt19937(seed)) — the draw the
+ * reference makes in Binner::fit (binning.cpp:93-97) and GOSS (booster.cpp:572). */
+void orc_shuffle_prefix(int64_t m, int64_t keep, uint32_t seed, int32_t* out);
+
 /* Objective::grad_hess for MSE (objective.cpp:105-118) and RankPairwise
  * (objective.cpp:179-219), unit weights.  kind: 0 = MSE, 5 = RankPairwise. */
 void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t* groups, int n,

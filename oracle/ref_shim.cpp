@@ -16,6 +16,7 @@
 #include "tidegbm/booster.hpp"
 #include "tidegbm/histogram.hpp"
 
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -90,6 +91,25 @@ int ref_fit(void* hb, const double* X, const double* y, int n, int n_f, const lo
         g_err = e.what();
         return -1;
     }
+}
+
+// Booster::fit with the reference's own per-iteration hook (log_fn, called from
+// booster.cpp:733-737 when verbose > 0): iter_seconds[m] = steady-clock seconds at the
+// end of boosting iteration m, relative to the call.  The hook prints one line per
+// iteration to stderr, as the reference does with verbose = 1.
+int ref_fit_timed(void* hb, const double* X, const double* y, int n, int n_f, const long long* ts,
+                  const long long* rank_groups, const long long* entity, double* iter_seconds) {
+    auto* b = static_cast<Booster*>(hb);
+    const auto t0 = std::chrono::steady_clock::now();
+    b->cfg.verbose = 1;
+    b->log_fn = [&](int iter, f64, f64) {
+        iter_seconds[iter - 1] =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    };
+    const int rc = ref_fit(hb, X, y, n, n_f, ts, rank_groups, entity);
+    b->log_fn = nullptr;
+    b->cfg.verbose = 0;
+    return rc;
 }
 
 int ref_predict_raw(void* hb, const double* X, int n, int n_f, double* out) {

@@ -1,0 +1,66 @@
+"""CPU-only checks: the C-ABI library loads and exports every declared symbol, the
+host-side samplers reproduce libstdc++'s std::shuffle, and the host binner's edges
+are bit-identical to the oracle's Binner::fit."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "tidegbm_b200.h")).read()
+    return sorted(set(re.findall(r"TGB_API[^;(]*?\b(tgb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(native):
+    L = C.CDLL(native.LIB_PATH)
+    names = _declared_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(L, name), name
+
+
+def test_no_internal_symbols_exported(native):
+    out = os.popen(f"nm -D --defined-only {native.LIB_PATH}").read()
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert exported == set(_declared_symbols())
+
+
+@pytest.mark.parametrize("m,keep,seed", [(1, 1, 0), (10, 3, 1), (1000, 1000, 2), (65535, 100, 3), (65536, 100, 4),
+                                         (65537, 65537, 5), (300000, 26214, 6), (1_000_000, 100_000, 7)])
+def test_shuffled_prefix_equals_std_shuffle(native, oracle, m, keep, seed):
+    got = np.zeros(keep, np.int32)
+    native.check(native.lib().tgb_shuffled_prefix(m, keep, seed, got.ctypes.data_as(C.c_void_p)))
+    ref = np.zeros(keep, np.int32)
+    L = oracle.oracle_lib()
+    L.orc_shuffle_prefix.argtypes = [C.c_int64, C.c_int64, C.c_uint32, C.c_void_p]
+    L.orc_shuffle_prefix(m, keep, seed, ref.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("dtype,bin_sample", [(np.float32, 3000), (np.float64, 0), (np.float64, 70000)])
+def test_host_binner_matches_oracle(native, oracle, dtype, bin_sample):
+    rng = np.random.default_rng(11)
+    n, nf = 80000, 12
+    X = rng.standard_normal((n, nf)).astype(dtype)
+    X[:, 1] = np.round(X[:, 1])  # few uniques: edges = values
+    X[:, 2] = np.exp(X[:, 2] * 2)
+    X[:, 4] = np.nan  # all missing -> edges {0.0}
+    X[rng.random((n, nf)) < 0.02] = np.nan
+    e1 = np.zeros(nf * 256)
+    n1 = np.zeros(nf, np.int32)
+    nb1 = native.lib().tgb_binner_fit(X.ctypes.data_as(C.c_void_p), 0 if dtype == np.float32 else 1, n, nf, 255,
+                                      bin_sample, 42, e1.ctypes.data_as(C.c_void_p), n1.ctypes.data_as(C.c_void_p))
+    assert nb1 > 0, native.lib().tgb_last_error()
+    e2 = np.zeros(nf * 256)
+    n2 = np.zeros(nf, np.int32)
+    nbc = np.zeros(nf, np.int32)
+    nb2 = oracle.oracle_lib().orc_binner_fit(np.ascontiguousarray(X, dtype=np.float64), n, nf, 255, bin_sample, 42,
+                                             e2, n2, nbc)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1, e2)

@@ -1,0 +1,129 @@
+"""End-to-end parity of the device="gpu" fit (tgb_fit through the C ABI) against the
+oracle restatement of Booster::fit (oracle/oracle.cpp, pinned bit-exact to the
+reference core).
+
+Bar: tree structure (feature, threshold, missing direction, children, n_samples,
+depth) identical; node values, full-data leaf values, TORB prefix values and
+predictions within 1e-9 absolute (the bar is 1e-5); training loss within 1e-9.
+Histogram sums are exact 64-bit fixed point, so the only differences from the FP64
+oracle are its own summation rounding.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare(gpu, ref, atol=1e-9):
+    trees_g = gpu.trees()
+    assert len(trees_g) == len(ref.trees)
+    for t, (a, b) in enumerate(zip(trees_g, ref.trees)):
+        for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth"):
+            assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        assert np.array_equal(a.cover, b.cover), t
+        np.testing.assert_allclose(a.value, b.value, rtol=0, atol=atol, err_msg=f"tree {t} node value")
+        np.testing.assert_allclose(a.gain, b.gain, rtol=1e-9, atol=atol, err_msg=f"tree {t} gain")
+        np.testing.assert_allclose(a.values, b.values, rtol=0, atol=atol, err_msg=f"tree {t} values")
+        np.testing.assert_allclose(a.prefix, b.prefix, rtol=0, atol=atol, err_msg=f"tree {t} prefix")
+    info = gpu.info()
+    assert info["n_bins"] == ref.n_bins and info["n_buckets"] == ref.n_buckets
+    assert abs(info["init_score"] - ref.init_score) <= 1e-12
+    np.testing.assert_allclose(gpu.init_prefix(), ref.init_prefix, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(gpu.evals_result()["train"], ref.evals_train, rtol=1e-9, atol=1e-9)
+
+
+def _fit_both(native, oracle, params, p, x_f64=False):
+    X = p.X.astype(np.float64) if x_f64 else p.X
+    gpu = native.Booster(**params)
+    gpu.fit(X, p.y, timestamps=p.ts, entity=p.entity)
+    ref, h = oracle.oracle_fit(params, p.X.astype(np.float64), p.y, p.ts, p.entity)
+    return gpu, ref, h
+
+
+def test_fit_small_mse_matches_oracle(native, oracle):
+    """Plain method, small: 400 dates x 250 entities, 32 features, mse, depth 6, 80 trees."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_small()
+    params = dict(n_estimators=80, learning_rate=0.08, max_depth=6, horizon=1, objective="mse", goss=0,
+                  random_state=0, pair_splits=False)
+    gpu, ref, h = _fit_both(native, oracle, params, p)
+    try:
+        _compare(gpu, ref)
+        Xq = p.X[:5000]
+        np.testing.assert_allclose(gpu.raw_predict(Xq), oracle.oracle_predict(h, Xq.astype(np.float64)),
+                                   rtol=0, atol=1e-9)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_pairwise_uneven_dates(native, oracle):
+    """Pairwise objective over uneven cross-sections (Uniform{50..800} per date), 2% NaN."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_pairwise(n_dates=120)
+    params = dict(n_estimators=12, learning_rate=0.08, max_depth=6, horizon=1, objective="pairwise",
+                  random_state=0, pair_splits=False)
+    gpu, ref, h = _fit_both(native, oracle, params, p)
+    try:
+        _compare(gpu, ref)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_goss_lognormal_nan(native, oracle):
+    """GOSS on (top 20% / 10% sampled, x8 scale), log-normal columns, 1% NaN, horizon 5."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_scale(n_dates=60, n_entities=1500, n_features=20)
+    params = dict(n_estimators=10, learning_rate=0.1, max_depth=8, horizon=5, objective="mse", goss=1,
+                  random_state=1, bin_sample=20000, pair_splits=False)
+    gpu, ref, h = _fit_both(native, oracle, params, p)
+    try:
+        _compare(gpu, ref)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_iid_float64_input(native, oracle):
+    """iid mode (no TORB), float64 X, max_leaves 15, depth 4."""
+    rng = np.random.default_rng(5)
+    n = 30000
+    X = rng.standard_normal((n, 9))
+    y = X[:, 0] - 0.5 * X[:, 1] + 0.1 * rng.standard_normal(n)
+    params = dict(n_estimators=15, learning_rate=0.1, max_depth=4, max_leaves=15, iid_mode=1, objective="mse",
+                  goss=0, pair_splits=False)
+    gpu = native.Booster(**params)
+    gpu.fit(X, y)
+    ref, h = oracle.oracle_fit(params, X, y)
+    try:
+        _compare(gpu, ref)
+        np.testing.assert_allclose(gpu.raw_predict(X[:2000]), oracle.oracle_predict(h, X[:2000]), rtol=0, atol=1e-9)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_unsorted_rows_match_sorted(native):
+    """Row order invariance (reference test_unsorted_rows_match_sorted, tests/test_tidegbm.py:282-291)."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_small(n_dates=60, n_entities=100, n_features=8)
+    params = dict(n_estimators=6, learning_rate=0.1, max_depth=5, horizon=1, goss=0, pair_splits=False)
+    a = native.Booster(**params).fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+    perm = np.random.default_rng(0).permutation(p.n)
+    b = native.Booster(**params).fit(p.X[perm], p.y[perm], timestamps=p.ts[perm], entity=p.entity[perm])
+    np.testing.assert_array_equal(a.raw_predict(p.X), b.raw_predict(p.X))
+
+
+def test_gpu_rejects_unsupported_options(native):
+    """No CPU fallback: options the GPU path lacks raise (config_from_kwargs names)."""
+    X = np.zeros((100, 3), np.float32)
+    y = np.zeros(100)
+    with pytest.raises(native.TideError, match="pair_splits"):
+        native.Booster(iid_mode=1, pair_splits=True).fit(X, y)
+    with pytest.raises(native.TideError, match="objective"):
+        native.Booster(iid_mode=1, objective="huber")
+    with pytest.raises(native.TideError, match="horizon"):
+        native.Booster(pair_splits=False).fit(X, y, timestamps=np.arange(100))
+    with pytest.raises(native.TideError, match="colsample"):
+        native.Booster(iid_mode=1, pair_splits=False, colsample=0.5).fit(X, y)

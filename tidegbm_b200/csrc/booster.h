@@ -1,0 +1,129 @@
+// GPU booster: the device="gpu" implementation of TideGBM's Booster::fit
+// (cpp/src/booster.cpp:231-742) for the hot-path subset, plus predict_raw.
+#pragma once
+
+#include <cstdint>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace tgb {
+
+struct TideError : std::runtime_error {
+    explicit TideError(const std::string& m) : std::runtime_error(m) {}
+};
+
+// The Config fields (cpp/include/tidegbm/config.hpp:12-113) the GPU path reads.  Every
+// other option keeps its default; options the GPU path does not implement are
+// rejected by validate() with a TideError instead of falling back to the CPU.
+struct Config {
+    int n_estimators = 100;
+    double learning_rate = 0.1;
+    int max_depth = 6;
+    int max_leaves = 31;
+    int min_samples_leaf = 20;
+    double min_child_weight = 1e-3;
+    double l2 = 1.0;
+    double min_split_gain = 0.0;
+    int max_bin = 255;
+    int n_time_buckets = 0;
+    int64_t horizon = -1;
+    int64_t embargo = 0;
+    bool iid_mode = false;
+    int objective = 0;  // 0 mse, 5 pairwise (ObjectiveKind, cpp/include/tidegbm/types.hpp:26-35)
+    int random_state = 0;
+    int goss = -1;
+    double goss_top = 0.2;
+    double goss_other = 0.1;
+    int bin_sample = 262144;
+    double torb_min_cover = 0.0;
+    bool finer_torb = true;
+    int n_jobs = 0;
+    std::string device = "gpu";
+    // Options that exist in the reference but are not implemented on the GPU path.
+    // pair_splits defaults to true as in the reference (config.hpp:31); the fit
+    // rejects it unless n >= 1M, where the reference itself turns it off.
+    bool pair_splits = true;
+    bool halo = false;
+    double subsample = 1.0;
+    double colsample = 1.0;
+    double colsample_bynode = 1.0;
+    double l1 = 0.0;
+    double max_delta_step = 0.0;
+    double time_decay = 1.0;
+    bool causal_bins = false;
+    bool causal_structure = false;
+    double structure_frac = 1.0;
+    double entity_subsample = 1.0;
+    // Measurement hooks (no effect on results): CUDA events from tree `timing_from` to
+    // the last tree, and per-launch events around every histogram kernel in that range.
+    int timing_from = -1;
+    bool profile_hist = false;
+
+    void validate() const;
+};
+
+struct HostNode {
+    int is_leaf, feature, threshold, left, right, missing_left, n_samples, depth;
+    double value, gain;
+};
+
+struct HostTree {
+    std::vector<HostNode> nodes;
+    std::vector<double> values;
+    std::vector<int> cover;
+    std::vector<double> prefix;  // n_buckets x n_nodes
+};
+
+struct FitStats {
+    double t_total = 0, t_sort = 0, t_binfit = 0, t_upload = 0, t_transform = 0, t_trees = 0, t_download = 0;
+    double t_rng = 0;
+    int gpu_launches = 0;
+    // timed range (cfg.timing_from .. last tree), device time from CUDA events
+    double timed_ms = 0;
+    int timed_trees = 0;
+    long long timed_launches = 0;
+    double hist_ms = 0;       // sum of histogram-kernel durations in the timed range
+    int hist_launches = 0;
+    long long hist_rows = 0;  // rows histogrammed in the timed range
+};
+
+struct DeviceState;  // device buffers of one fit
+
+class GpuBooster {
+public:
+    explicit GpuBooster(int device);
+    ~GpuBooster();
+    GpuBooster(const GpuBooster&) = delete;
+    GpuBooster& operator=(const GpuBooster&) = delete;
+
+    Config cfg;
+    int device = 0;
+    // fitted model
+    bool fitted = false;
+    int n_features = 0;
+    int n_bins = 0;
+    int n_buckets = 1;
+    double init_score = 0.0;
+    std::vector<double> init_prefix;
+    std::vector<double> edges;  // n_features x 256 (first n_edges[f] used)
+    std::vector<int> n_edges;
+    std::vector<HostTree> trees;
+    std::vector<double> evals_train;
+    FitStats stats;
+
+    void fit(const void* X, int x_dtype, const double* y, int n, int n_f, const int64_t* ts,
+             const int64_t* entity);
+    void predict_raw(const void* X, int x_dtype, int n, int n_f, double* out);
+
+private:
+    DeviceState* ds_ = nullptr;
+};
+
+// Host part of Binner::fit (cpp/src/binning.cpp:14-102) for numeric features: the
+// sampled values per feature and their quantile edges.  Returns max_bins().
+int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
+               std::vector<double>& edges, std::vector<int>& n_edges, int n_threads);
+
+}  // namespace tgb

@@ -1,0 +1,457 @@
+// extern "C" boundary (include/tidegbm_b200.h).  Every entry catches all exceptions
+// and reports -1 + a thread-local message, like the reference C API
+// (cpp/src/c_api.cpp:12-18, 21-157).
+#include "tidegbm_b200.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "booster.h"
+#include "sampling.h"
+#include "tgb_internal.h"
+
+namespace tgb {
+extern std::atomic<long long> g_kernel_launches;
+}
+
+struct tgb_booster {
+    tgb::GpuBooster* b = nullptr;
+    // state of the build_hist_gpu drop-in (per booster, not process-global)
+    const unsigned short* host_xb = nullptr;
+    int xb_rows = 0, xb_f = 0, xb_stride = 0;
+    unsigned char* d_codes = nullptr;
+    int* d_idx = nullptr;
+    double *d_g = nullptr, *d_h = nullptr;
+    long long *d_G = nullptr, *d_H = nullptr;
+    int* d_C = nullptr;
+    size_t cap_idx = 0, cap_rows = 0, cap_hist = 0;
+    ~tgb_booster() {
+        cudaFree(d_codes);
+        cudaFree(d_idx);
+        cudaFree(d_g);
+        cudaFree(d_h);
+        cudaFree(d_G);
+        cudaFree(d_H);
+        cudaFree(d_C);
+        delete b;
+    }
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    } catch (...) {
+        g_err = "unknown error";
+        return -1;
+    }
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+void need(bool ok, const char* msg) {
+    if (!ok) throw tgb::TideError(msg);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tgb_last_error(void) { return g_err.c_str(); }
+
+long long tgb_kernel_launches(void) { return tgb::g_kernel_launches.load(); }
+
+int tgb_booster_create(int device, tgb_booster** out) {
+    return guard([&] {
+        need(out != nullptr, "out is NULL");
+        auto* h = new tgb_booster();
+        try {
+            h->b = new tgb::GpuBooster(device);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+void tgb_booster_free(tgb_booster* b) { delete b; }
+
+int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
+    return guard([&] {
+        need(hb && key, "NULL argument");
+        tgb::Config& c = hb->b->cfg;
+        const std::string k(key);
+        if (k == "n_estimators") c.n_estimators = static_cast<int>(v);
+        else if (k == "max_depth") c.max_depth = static_cast<int>(v);
+        else if (k == "max_leaves") c.max_leaves = static_cast<int>(v);
+        else if (k == "min_samples_leaf") c.min_samples_leaf = static_cast<int>(v);
+        else if (k == "max_bin") c.max_bin = static_cast<int>(v);
+        else if (k == "n_time_buckets") c.n_time_buckets = static_cast<int>(v);
+        else if (k == "random_state") c.random_state = static_cast<int>(v);
+        else if (k == "n_jobs") c.n_jobs = static_cast<int>(v);
+        else if (k == "iid_mode") c.iid_mode = v != 0;
+        else if (k == "halo") c.halo = v != 0;
+        else if (k == "pair_splits") c.pair_splits = v != 0;
+        else if (k == "horizon") c.horizon = v;
+        else if (k == "embargo") c.embargo = v;
+        else if (k == "goss") c.goss = static_cast<int>(v);
+        else if (k == "bin_sample") c.bin_sample = static_cast<int>(v);
+        else if (k == "finer_torb") c.finer_torb = v != 0;
+        else if (k == "objective") c.objective = static_cast<int>(v);
+        else if (k == "causal_bins") c.causal_bins = v != 0;
+        else if (k == "causal_structure") c.causal_structure = v != 0;
+        else if (k == "timing_from") c.timing_from = static_cast<int>(v);
+        else if (k == "profile_hist") c.profile_hist = v != 0;
+        else if (k == "verbose" || k == "col_major_hist" || k == "cat_min_count") { /* no effect on GPU path */ }
+        else throw tgb::TideError("unknown int key");
+    });
+}
+
+int tgb_set_double(tgb_booster* hb, const char* key, double v) {
+    return guard([&] {
+        need(hb && key, "NULL argument");
+        tgb::Config& c = hb->b->cfg;
+        const std::string k(key);
+        if (k == "learning_rate") c.learning_rate = v;
+        else if (k == "l2") c.l2 = v;
+        else if (k == "l1") c.l1 = v;
+        else if (k == "min_child_weight") c.min_child_weight = v;
+        else if (k == "min_split_gain") c.min_split_gain = v;
+        else if (k == "subsample") c.subsample = v;
+        else if (k == "colsample") c.colsample = v;
+        else if (k == "colsample_bynode") c.colsample_bynode = v;
+        else if (k == "goss_top") c.goss_top = v;
+        else if (k == "goss_other") c.goss_other = v;
+        else if (k == "torb_min_cover") c.torb_min_cover = v;
+        else if (k == "max_delta_step") c.max_delta_step = v;
+        else if (k == "time_decay") c.time_decay = v;
+        else if (k == "structure_frac") c.structure_frac = v;
+        else if (k == "entity_subsample") c.entity_subsample = v;
+        else throw tgb::TideError("unknown double key");
+    });
+}
+
+int tgb_set_str(tgb_booster* hb, const char* key, const char* value) {
+    return guard([&] {
+        need(hb && key && value, "NULL argument");
+        tgb::Config& c = hb->b->cfg;
+        const std::string k(key), v(value);
+        if (k == "objective") {
+            // bindings.cpp:115-125 names
+            if (v == "mse" || v == "auto" || v == "l2" || v == "regression") c.objective = 0;
+            else if (v == "pairwise" || v == "lambdarank") c.objective = 5;
+            else if (v == "huber" || v == "quantile" || v == "pinball" || v == "logloss" || v == "binary" ||
+                     v == "classification" || v == "rank" || v == "listnet" || v == "multiclass" || v == "custom")
+                throw tgb::TideError("GPU path: objective '" + v + "' is not supported (mse or pairwise)");
+            else throw tgb::TideError("unknown objective: " + v);
+        } else if (k == "device") {
+            c.device = v;
+        } else {
+            throw tgb::TideError("unknown string key");
+        }
+    });
+}
+
+int tgb_fit(tgb_booster* hb, const void* X, int x_dtype, const double* y, int n, int n_features,
+            const long long* timestamps, const long long* entity) {
+    return guard([&] {
+        need(hb && X && y, "NULL argument");
+        hb->b->fit(X, x_dtype, y, n, n_features, reinterpret_cast<const int64_t*>(timestamps),
+                   reinterpret_cast<const int64_t*>(entity));
+    });
+}
+
+int tgb_predict_raw(tgb_booster* hb, const void* X, int x_dtype, int n, int n_features, double* out) {
+    return guard([&] {
+        need(hb && X && out, "NULL argument");
+        hb->b->predict_raw(X, x_dtype, n, n_features, out);
+    });
+}
+
+int tgb_model_info(tgb_booster* hb, int* n_trees, int* n_bins, int* n_buckets, double* init_score) {
+    return guard([&] {
+        need(hb != nullptr, "NULL booster");
+        const auto& b = *hb->b;
+        if (n_trees) *n_trees = static_cast<int>(b.trees.size());
+        if (n_bins) *n_bins = b.n_bins;
+        if (n_buckets) *n_buckets = b.n_buckets;
+        if (init_score) *init_score = b.init_score;
+    });
+}
+
+int tgb_init_prefix(tgb_booster* hb, double* out) {
+    return guard([&] {
+        need(hb && out, "NULL argument");
+        std::copy(hb->b->init_prefix.begin(), hb->b->init_prefix.end(), out);
+    });
+}
+
+int tgb_evals_train(tgb_booster* hb, double* out) {
+    return guard([&] {
+        need(hb && out, "NULL argument");
+        std::copy(hb->b->evals_train.begin(), hb->b->evals_train.end(), out);
+    });
+}
+
+int tgb_tree_n_nodes(tgb_booster* hb, int t) {
+    if (!hb || t < 0 || t >= static_cast<int>(hb->b->trees.size())) {
+        g_err = "tree index out of range";
+        return -1;
+    }
+    return static_cast<int>(hb->b->trees[t].nodes.size());
+}
+
+int tgb_tree_export(tgb_booster* hb, int t, int* inodes, double* fnodes, double* values, int* cover, double* prefix) {
+    return guard([&] {
+        need(hb != nullptr, "NULL booster");
+        need(t >= 0 && t < static_cast<int>(hb->b->trees.size()), "tree index out of range");
+        const tgb::HostTree& tr = hb->b->trees[t];
+        for (size_t k = 0; k < tr.nodes.size(); ++k) {
+            const tgb::HostNode& d = tr.nodes[k];
+            if (inodes) {
+                int* o = inodes + 8 * k;
+                o[0] = d.is_leaf;
+                o[1] = d.feature;
+                o[2] = d.threshold;
+                o[3] = d.left;
+                o[4] = d.right;
+                o[5] = d.missing_left;
+                o[6] = d.n_samples;
+                o[7] = d.depth;
+            }
+            if (fnodes) {
+                fnodes[2 * k] = d.value;
+                fnodes[2 * k + 1] = d.gain;
+            }
+        }
+        if (values) std::copy(tr.values.begin(), tr.values.end(), values);
+        if (cover) std::copy(tr.cover.begin(), tr.cover.end(), cover);
+        if (prefix) std::copy(tr.prefix.begin(), tr.prefix.end(), prefix);
+    });
+}
+
+int tgb_edges(tgb_booster* hb, int f, double* out) {
+    if (!hb || f < 0 || f >= hb->b->n_features) {
+        g_err = "feature index out of range";
+        return -1;
+    }
+    const int ne = hb->b->n_edges[f];
+    if (out) std::copy(hb->b->edges.begin() + static_cast<size_t>(f) * 256,
+                       hb->b->edges.begin() + static_cast<size_t>(f) * 256 + ne, out);
+    return ne;
+}
+
+int tgb_fit_stats(tgb_booster* hb, double* o) {
+    return guard([&] {
+        need(hb && o, "NULL argument");
+        const tgb::FitStats& s = hb->b->stats;
+        o[0] = s.t_total;
+        o[1] = s.t_sort;
+        o[2] = s.t_binfit;
+        o[3] = s.t_upload;
+        o[4] = s.t_trees;
+        o[5] = s.t_download;
+        o[6] = s.t_rng;
+        o[7] = s.gpu_launches;
+        o[8] = s.timed_ms;
+        o[9] = s.timed_trees;
+        o[10] = static_cast<double>(s.timed_launches);
+        o[11] = s.hist_ms;
+        o[12] = s.hist_launches;
+        o[13] = static_cast<double>(s.hist_rows);
+    });
+}
+
+int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample, unsigned seed,
+                   double* edges_out, int* n_edges_out) {
+    int nb = -1;
+    const int rc = guard([&] {
+        need(X && edges_out && n_edges_out, "NULL argument");
+        need(x_dtype == 0 || x_dtype == 1, "x_dtype must be 0 or 1");
+        need(max_bin >= 8 && max_bin <= 256, "max_bin must be in [8, 256]");
+        std::vector<double> e;
+        std::vector<int> ne;
+        nb = tgb::binner_fit(X, x_dtype, n, n_features, max_bin, bin_sample, seed, e, ne,
+                             static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+        std::copy(e.begin(), e.end(), edges_out);
+        std::copy(ne.begin(), ne.end(), n_edges_out);
+    });
+    return rc == 0 ? nb : -1;
+}
+
+int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out) {
+    return guard([&] {
+        need(m >= 0 && m < (1ll << 31) && keep >= 0 && keep <= m, "bad sizes");
+        std::mt19937 rng(seed);
+        tgb::shuffled_prefix(m, keep, rng, out);
+    });
+}
+
+int tgb_bin_transform(const void* X, int x_dtype, int n, int n_features, const void* edges, const int* n_edges,
+                      unsigned char* codes, int stride, void* stream) {
+    return guard([&] {
+        need(stride >= n_features && stride % 16 == 0, "stride must be >= n_features and a multiple of 16");
+        need(x_dtype == 0 || x_dtype == 1, "x_dtype must be 0 or 1");
+        if (x_dtype == 0)
+            tgb::launch_bin_transform_f32(static_cast<const float*>(X), n, n_features, static_cast<const float*>(edges),
+                                          n_edges, codes, stride, as_stream(stream));
+        else
+            tgb::launch_bin_transform_f64(static_cast<const double*>(X), n, n_features,
+                                          static_cast<const double*>(edges), n_edges, codes, stride,
+                                          as_stream(stream));
+    });
+}
+
+int tgb_hist_build(const unsigned char* codes, int stride, int n_features, const int* rows, int n_rows,
+                   const double* g, const double* h, int gshift, int hshift, long long* G, long long* H, int* C,
+                   void* stream) {
+    return guard([&] {
+        need(stride >= n_features && stride % 16 == 0, "stride must be >= n_features and a multiple of 16");
+        tgb::launch_hist_rows(codes, stride, n_features, rows, n_rows, g, h, gshift, hshift, G, H, C,
+                              as_stream(stream));
+    });
+}
+
+int tgb_split_scan(const long long* G, const long long* H, const int* C, int n_features, int n_bins, int gshift,
+                   int hshift, double l2, double min_split_gain, int min_samples_leaf, double min_child_weight,
+                   double* gain, int* thr, int* missing_left, void* stream) {
+    return guard([&] {
+        need(n_bins >= 2 && n_bins <= 256, "n_bins must be in [2, 256]");
+        tgb::launch_scan_hist(G, H, C, n_features, n_bins, std::ldexp(1.0, -gshift), std::ldexp(1.0, -hshift), l2,
+                              min_split_gain, min_samples_leaf, min_child_weight, gain, thr, missing_left,
+                              as_stream(stream));
+    });
+}
+
+size_t tgb_partition_workspace_bytes(int n_rows) {
+    const size_t tiles = static_cast<size_t>(std::max(0, n_rows) + tgb::kPartTile - 1) / tgb::kPartTile;
+    return 256 + (tiles + 1) * sizeof(int);
+}
+
+int tgb_partition(const unsigned char* codes, int stride, const int* rows, int n_rows, int feature, int threshold,
+                  int missing_left, int* out, int* n_left_out, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+    return guard([&] {
+        need(workspace_bytes >= tgb_partition_workspace_bytes(n_rows), "workspace too small");
+        need(feature >= 0 && feature < stride, "feature out of range");
+        need(sizeof(tgb::PartJob) <= 256, "job layout");
+        char* ws = static_cast<char*>(workspace);
+        tgb::launch_partition_rows(codes, stride, rows, n_rows, feature, threshold, missing_left, out, n_left_out,
+                                   reinterpret_cast<int*>(ws + 256), ws, as_stream(stream));
+    });
+}
+
+int tgb_grad_mse(const double* y, const double* pred, int n, double* g, double* h, void* stream) {
+    return guard([&] { tgb::launch_grad_mse(y, pred, n, g, h, as_stream(stream)); });
+}
+
+int tgb_grad_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len, const int* order,
+                      int n_runs, int n, double* g, double* h, void* stream) {
+    return guard([&] {
+        tgb::launch_grad_pairwise(y, pred, run_start, run_len, order, n_runs, n, g, h, as_stream(stream));
+    });
+}
+
+int tgb_build_hist_gpu(tgb_booster* hb, const unsigned short* xb, int n_f, const int* idx, int n_idx, const double* g,
+                       const double* h, int n_bins, int n_rows, double* out) {
+    return guard([&] {
+        need(hb && xb && out, "NULL argument");
+        need(n_bins >= 1 && n_bins <= 256, "GPU path: n_bins must be <= 256 (uint8 codes)");
+        tgb::check(cudaSetDevice(hb->b->device), "cudaSetDevice");
+        const size_t hist_sz = static_cast<size_t>(n_f) * n_bins;
+        std::fill(out, out + 3 * hist_sz, 0.0);
+        if (n_idx <= 0) return;
+        if (n_rows <= 0) n_rows = n_idx;  // histogram_cuda.cu:85-88
+        const int stride = (n_f + 15) / 16 * 16;
+        if (hb->host_xb != xb || hb->xb_rows != n_rows || hb->xb_f != n_f) {
+            std::vector<unsigned char> c8(static_cast<size_t>(n_rows) * stride, 0);
+            for (size_t i = 0; i < static_cast<size_t>(n_rows); ++i)
+                for (int f = 0; f < n_f; ++f) {
+                    const unsigned short v = xb[i * n_f + f];
+                    if (v > 255) throw tgb::TideError("GPU path: bin code > 255");
+                    c8[i * stride + f] = static_cast<unsigned char>(v);
+                }
+            cudaFree(hb->d_codes);
+            hb->d_codes = nullptr;
+            tgb::check(cudaMalloc(&hb->d_codes, c8.size()), "cudaMalloc codes");
+            tgb::check(cudaMemcpy(hb->d_codes, c8.data(), c8.size(), cudaMemcpyHostToDevice), "H2D codes");
+            hb->host_xb = xb;
+            hb->xb_rows = n_rows;
+            hb->xb_f = n_f;
+            hb->xb_stride = stride;
+        }
+        if (hb->cap_rows < static_cast<size_t>(n_rows)) {
+            cudaFree(hb->d_g);
+            cudaFree(hb->d_h);
+            tgb::check(cudaMalloc(&hb->d_g, sizeof(double) * n_rows), "cudaMalloc g");
+            tgb::check(cudaMalloc(&hb->d_h, sizeof(double) * n_rows), "cudaMalloc h");
+            hb->cap_rows = n_rows;
+        }
+        if (hb->cap_idx < static_cast<size_t>(n_idx)) {
+            cudaFree(hb->d_idx);
+            tgb::check(cudaMalloc(&hb->d_idx, sizeof(int) * n_idx), "cudaMalloc idx");
+            hb->cap_idx = n_idx;
+        }
+        const size_t full = static_cast<size_t>(n_f) * tgb::kBins;
+        if (hb->cap_hist < full) {
+            cudaFree(hb->d_G);
+            cudaFree(hb->d_H);
+            cudaFree(hb->d_C);
+            tgb::check(cudaMalloc(&hb->d_G, sizeof(long long) * full), "cudaMalloc G");
+            tgb::check(cudaMalloc(&hb->d_H, sizeof(long long) * full), "cudaMalloc H");
+            tgb::check(cudaMalloc(&hb->d_C, sizeof(int) * full), "cudaMalloc C");
+            hb->cap_hist = full;
+        }
+        tgb::check(cudaMemcpy(hb->d_g, g, sizeof(double) * n_rows, cudaMemcpyHostToDevice), "H2D g");
+        tgb::check(cudaMemcpy(hb->d_h, h, sizeof(double) * n_rows, cudaMemcpyHostToDevice), "H2D h");
+        tgb::check(cudaMemcpy(hb->d_idx, idx, sizeof(int) * n_idx, cudaMemcpyHostToDevice), "H2D idx");
+        tgb::check(cudaMemset(hb->d_G, 0, sizeof(long long) * full), "memset");
+        tgb::check(cudaMemset(hb->d_H, 0, sizeof(long long) * full), "memset");
+        tgb::check(cudaMemset(hb->d_C, 0, sizeof(int) * full), "memset");
+        double mg = 0, mh = 0;
+        for (int k = 0; k < n_idx; ++k) {
+            mg = std::max(mg, std::fabs(g[idx[k]]));
+            mh = std::max(mh, std::fabs(h[idx[k]]));
+        }
+        auto shift = [&](double mx) {
+            if (!(mx > 0)) return 0;
+            int clog = 0;
+            while ((1ll << clog) < static_cast<long long>(n_idx)) ++clog;
+            return std::max(-1000, std::min(1000, 61 - (std::ilogb(mx) + 1) - clog));
+        };
+        const int gs = shift(mg), hs = shift(mh);
+        tgb::launch_hist_rows(hb->d_codes, stride, n_f, hb->d_idx, n_idx, hb->d_g, hb->d_h, gs, hs, hb->d_G, hb->d_H,
+                              hb->d_C, nullptr);
+        std::vector<long long> G(full), H(full);
+        std::vector<int> C(full);
+        tgb::check(cudaMemcpy(G.data(), hb->d_G, sizeof(long long) * full, cudaMemcpyDeviceToHost), "D2H G");
+        tgb::check(cudaMemcpy(H.data(), hb->d_H, sizeof(long long) * full, cudaMemcpyDeviceToHost), "D2H H");
+        tgb::check(cudaMemcpy(C.data(), hb->d_C, sizeof(int) * full, cudaMemcpyDeviceToHost), "D2H C");
+        const double ig = std::ldexp(1.0, -gs), ih = std::ldexp(1.0, -hs);
+        for (int f = 0; f < n_f; ++f)
+            for (int b = 0; b < n_bins; ++b) {
+                const size_t o = static_cast<size_t>(f) * n_bins + b;
+                const size_t q = static_cast<size_t>(f) * tgb::kBins + b;
+                out[3 * o] = static_cast<double>(G[q]) * ig;
+                out[3 * o + 1] = static_cast<double>(H[q]) * ih;
+                out[3 * o + 2] = static_cast<double>(C[q]);
+            }
+    });
+}
+
+}  // extern "C"

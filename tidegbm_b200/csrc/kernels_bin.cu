@@ -1,0 +1,103 @@
+// Quantile-bin transform: X (row-major f32 or f64) -> uint8 codes, row-major
+// [n][stride].  Restates Binner::transform (cpp/src/binning.cpp:104-128):
+// code = 1 + #{edges <= v}, NaN -> 0 (kMissingBin, cpp/include/tidegbm/types.hpp:20).
+//
+// For f32 input the edges arrive as ceil_f32(edge) (the smallest float >= the f64
+// edge): for a float v, v >= e  <=>  v >= ceil_f32(e), so the float compare gives
+// the reference's f64 upper_bound exactly.  f64 input compares against f64 edges.
+//
+// Launch shape: one CTA = 8 warps x a group of 32 features; lane = feature, so a
+// warp reads one row's 32 consecutive values (coalesced) and writes 32 code bytes.
+// Edges of the group sit in shared memory with a 257-element feature stride so the
+// first probes of the 32 lanes fall in 32 different banks.
+#include "tgb_internal.h"
+
+#include <cmath>
+
+namespace tgb {
+
+namespace {
+
+constexpr int kBinWarps = 8;
+constexpr int kEdgeStride = 257;
+
+template <typename T>
+__global__ void __launch_bounds__(kBinWarps * 32)
+    bin_transform_kernel(const T* __restrict__ X, int n, int n_f, const T* __restrict__ edges,
+                         const int* __restrict__ n_edges, uint8_t* __restrict__ codes, int stride,
+                         int rows_per_cta) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* se = reinterpret_cast<T*>(smem_raw);
+    __shared__ int sne[32];
+    const int f0 = blockIdx.y * 32;
+    const int nf_here = min(32, n_f - f0);
+    for (int k = threadIdx.x; k < 32 * 256; k += blockDim.x) {
+        const int ff = k >> 8, b = k & 255;
+        T v = T(INFINITY);
+        if (ff < nf_here) v = edges[static_cast<size_t>(f0 + ff) * 256 + b];
+        se[ff * kEdgeStride + b] = v;
+    }
+    if (threadIdx.x < 32) sne[threadIdx.x] = threadIdx.x < nf_here ? n_edges[f0 + threadIdx.x] : 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane >= nf_here) return;
+    const T* e = se + lane * kEdgeStride;
+    const int ne = sne[lane];
+    const int r0 = blockIdx.x * rows_per_cta;
+    const int r1 = min(n, r0 + rows_per_cta);
+    for (int r = r0 + warp; r < r1; r += kBinWarps) {
+        const T v = X[static_cast<size_t>(r) * n_f + f0 + lane];
+        int code = 0;
+        if (!(v != v)) {
+            int pos = 0;
+#pragma unroll
+            for (int step = 128; step >= 1; step >>= 1)
+                if (e[pos + step - 1] <= v) pos += step;
+            code = min(pos, ne) + 1;
+        }
+        codes[static_cast<size_t>(r) * stride + f0 + lane] = static_cast<uint8_t>(code);
+    }
+}
+
+// Zero the padding bytes [n_f, stride) of every row so gathers of whole rows see 0.
+__global__ void zero_pad_kernel(uint8_t* codes, int n, int n_f, int stride) {
+    const int pad = stride - n_f;
+    const size_t total = static_cast<size_t>(n) * pad;
+    for (size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; k < total;
+         k += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t r = k / pad;
+        codes[r * stride + n_f + (k % pad)] = 0;
+    }
+}
+
+template <typename T>
+void launch_bin(const T* X, int n, int n_f, const T* edges, const int* n_edges, uint8_t* codes,
+                int stride, cudaStream_t s) {
+    if (n <= 0 || n_f <= 0) return;
+    const int rows_per_cta = 512;
+    dim3 grid((n + rows_per_cta - 1) / rows_per_cta, (n_f + 31) / 32);
+    const size_t smem = sizeof(T) * 32 * kEdgeStride;
+    auto kern = bin_transform_kernel<T>;
+    check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+          "bin smem attr");
+    kern<<<grid, kBinWarps * 32, smem, s>>>(X, n, n_f, edges, n_edges, codes, stride, rows_per_cta);
+    check(cudaGetLastError(), "bin_transform launch");
+    if (stride > n_f) {
+        zero_pad_kernel<<<1184, 256, 0, s>>>(codes, n, n_f, stride);
+        check(cudaGetLastError(), "zero_pad launch");
+    }
+}
+
+}  // namespace
+
+void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
+                              uint8_t* codes, int stride, cudaStream_t s) {
+    launch_bin<float>(X, n, n_f, edges, n_edges, codes, stride, s);
+}
+
+void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edges, const int* n_edges,
+                              uint8_t* codes, int stride, cudaStream_t s) {
+    launch_bin<double>(X, n, n_f, edges, n_edges, codes, stride, s);
+}
+
+}  // namespace tgb

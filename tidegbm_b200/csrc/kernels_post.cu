@@ -1,0 +1,279 @@
+// Per-tree sweep over all rows after a tree is grown.  Restates
+// Booster::fit's grow_head tail (cpp/src/booster.cpp:589-664):
+//   apply_all (cpp/src/tree.cpp:43-55)           leaf id of every row
+//   full-data leaf values                        leaf_value(sum g, sum h) over ALL rows,
+//                                                unscaled g and h (booster.cpp:594-600)
+//   TORB prefix values                           per time bucket b, leaf values from the
+//                                                rows [0, cut_b) of its causal past,
+//                                                blended toward the full value when the
+//                                                past is short (booster.cpp:604-648)
+//   prediction update                            pred += lr * prefix[bucket][leaf]
+//                                                (booster.cpp:655-664)
+//
+// Rows are sorted by time, so every cut is a row position and the rows between two
+// consecutive distinct cuts form a segment.  apply_accum sums (g, h, 1) per
+// (segment, leaf) in exact 64-bit fixed point (one shift per tree from max |g|,
+// max h over all rows); finalize turns segment sums into prefix sums per bucket.
+// CTAs own segment-aligned row chunks, so each CTA accumulates into one segment: the
+// chunk's rows are staged into shared memory with coalesced 16-byte loads (one
+// contiguous block of rows x stride bytes) and each thread walks one row.
+#include "tgb_internal.h"
+
+namespace tgb {
+
+namespace {
+
+constexpr int kApplyThreads = 256;
+
+__device__ int shift_for_all(double max_abs, long long count) {
+    if (!(max_abs > 0.0) || count <= 0) return 0;
+    int clog = 0;
+    while ((1ll << clog) < count) ++clog;
+    const int e = ilogb(max_abs);
+    return max(-1000, min(1000, 61 - (e + 1) - clog));
+}
+
+__global__ void max_abs_kernel(const double* __restrict__ g, const double* __restrict__ h, int n,
+                               AllScale* __restrict__ sc) {
+    double mg = 0.0, mh = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        mg = fmax(mg, fabs(g[i]));
+        mh = fmax(mh, fabs(h[i]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+        mh = fmax(mh, __shfl_xor_sync(0xffffffffu, mh, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&sc->maxg_bits, static_cast<unsigned long long>(__double_as_longlong(mg)));
+        atomicMax(&sc->maxh_bits, static_cast<unsigned long long>(__double_as_longlong(mh)));
+    }
+}
+
+__global__ void all_scale_finalize_kernel(AllScale* sc, int n) {
+    const double mg = __longlong_as_double(static_cast<long long>(sc->maxg_bits));
+    const double mh = __longlong_as_double(static_cast<long long>(sc->maxh_bits));
+    sc->gshift = shift_for_all(mg, n);
+    sc->hshift = shift_for_all(mh, n);
+    sc->gscale = ldexp(1.0, sc->gshift);
+    sc->hscale = ldexp(1.0, sc->hshift);
+    sc->inv_gscale = ldexp(1.0, -sc->gshift);
+    sc->inv_hscale = ldexp(1.0, -sc->hshift);
+}
+
+__global__ void __launch_bounds__(kApplyThreads)
+    apply_accum_kernel(const uint8_t* __restrict__ codes, int stride, const DevNode* __restrict__ nodes,
+                       const DevTreeState* __restrict__ st, const double* __restrict__ g,
+                       const double* __restrict__ h, const int4* __restrict__ chunks,
+                       const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
+                       unsigned long long* __restrict__ seg_sums) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
+    __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes];
+    __shared__ unsigned long long acc[kMaxNodes][3];
+    const int nn = st->n_nodes;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        const DevNode& N = nodes[k];
+        s_feat[k] = static_cast<int16_t>(N.feature);
+        s_left[k] = static_cast<int16_t>(N.left);
+        s_right[k] = static_cast<int16_t>(N.right);
+        s_thr[k] = static_cast<uint8_t>(N.threshold < 0 ? 0 : N.threshold);
+        s_ml[k] = static_cast<uint8_t>(N.missing_left);
+        s_leaf[k] = static_cast<uint8_t>(N.is_leaf);
+        acc[k][0] = acc[k][1] = acc[k][2] = 0ull;
+    }
+    const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
+    const double gs = sc->gscale, hs = sc->hscale;
+    uint8_t* tile = smem_raw;
+    const int vec_per_row = stride / 16;
+    __syncthreads();
+    for (int t0 = ch.y; t0 < ch.z; t0 += kApplyThreads) {
+        const int rows_here = min(kApplyThreads, ch.z - t0);
+        const uint4* src = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(t0) * stride);
+        uint4* dst = reinterpret_cast<uint4*>(tile);
+        for (int v = threadIdx.x; v < rows_here * vec_per_row; v += blockDim.x) dst[v] = __ldg(src + v);
+        __syncthreads();
+        if (threadIdx.x < rows_here) {
+            const int r = t0 + threadIdx.x;
+            const uint8_t* row = tile + threadIdx.x * stride;
+            int k = 0;
+            while (!s_leaf[k]) {
+                const int b = row[s_feat[k]];
+                const bool left = b == 0 ? s_ml[k] != 0 : b <= s_thr[k];
+                k = left ? s_left[k] : s_right[k];
+            }
+            nid[r] = static_cast<int16_t>(k);
+            atomicAdd(&acc[k][0], static_cast<unsigned long long>(__double2ll_rn(g[r] * gs)));
+            atomicAdd(&acc[k][1], static_cast<unsigned long long>(__double2ll_rn(h[r] * hs)));
+            atomicAdd(&acc[k][2], 1ull);
+        }
+        __syncthreads();
+    }
+    unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        if (acc[k][2] == 0ull) continue;
+        atomicAdd(out + 3 * k, acc[k][0]);
+        atomicAdd(out + 3 * k + 1, acc[k][1]);
+        atomicAdd(out + 3 * k + 2, acc[k][2]);
+    }
+}
+
+__device__ __forceinline__ double leaf_value(double G, double H, double l2) { return -G / (H + l2); }
+
+__global__ void finalize_tree_kernel(PostParams pp, const DevTreeState* __restrict__ st,
+                                     const unsigned long long* __restrict__ seg_sums,
+                                     const int* __restrict__ bucket_seg_end, const int* __restrict__ cuts,
+                                     const AllScale* __restrict__ sc, double* __restrict__ values,
+                                     int* __restrict__ cover, double* __restrict__ prefix) {
+    const int nn = st->n_nodes;
+    const double ig = sc->inv_gscale, ih = sc->inv_hscale;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        long long G = 0, H = 0, Cn = 0;
+        for (int s = 0; s < pp.n_segments; ++s) {
+            const unsigned long long* e = seg_sums + (static_cast<size_t>(s) * kMaxNodes + k) * 3;
+            G += static_cast<long long>(e[0]);
+            H += static_cast<long long>(e[1]);
+            Cn += static_cast<long long>(e[2]);
+        }
+        values[k] = leaf_value(static_cast<double>(G) * ig, static_cast<double>(H) * ih, pp.l2);
+        cover[k] = static_cast<int>(Cn);
+    }
+    __syncthreads();
+    const int nb = pp.n_buckets;
+    for (int q = threadIdx.x; q < nb * nn; q += blockDim.x) {
+        const int b = q / nn, k = q % nn;
+        const double full = values[k];
+        double v;
+        if (pp.iid_mode) {
+            v = full;
+        } else {
+            long long pG = 0, pH = 0;
+            for (int s = 0; s < bucket_seg_end[b]; ++s) {
+                const unsigned long long* e = seg_sums + (static_cast<size_t>(s) * kMaxNodes + k) * 3;
+                pG += static_cast<long long>(e[0]);
+                pH += static_cast<long long>(e[1]);
+            }
+            const double cov = static_cast<double>(cuts[b]);
+            const double alpha = cov <= 0.0 ? 0.0 : fmin(1.0, cov / fmax(pp.min_cover, 1.0));
+            const double pref = cov > 0.0 ? leaf_value(static_cast<double>(pG) * ig, static_cast<double>(pH) * ih, pp.l2)
+                                          : full;
+            v = alpha * pref + (1.0 - alpha) * full;
+        }
+        prefix[static_cast<size_t>(b) * nn + k] = v;
+    }
+}
+
+__global__ void pred_update_kernel(PostParams pp, const int16_t* __restrict__ nid,
+                                   const double* __restrict__ prefix, const DevTreeState* __restrict__ st,
+                                   double* __restrict__ pred) {
+    const int nn = st->n_nodes;
+    const int n = pp.n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = 0;
+        if (!pp.iid_mode) {
+            // time_buckets on time-sorted rows (cpp/src/booster.cpp:60-72): rank = row.
+            b = static_cast<int>(static_cast<double>(i) / max(n, 1) * pp.n_buckets);
+            if (b >= pp.n_buckets) b = pp.n_buckets - 1;
+        }
+        pred[i] += pp.learning_rate * prefix[static_cast<size_t>(b) * nn + nid[i]];
+    }
+}
+
+__global__ void fill_pred_kernel(const double* __restrict__ init_prefix, int n, int n_buckets, int iid_mode,
+                                 double* __restrict__ pred) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = 0;
+        if (!iid_mode) {
+            b = static_cast<int>(static_cast<double>(i) / max(n, 1) * n_buckets);
+            if (b >= n_buckets) b = n_buckets - 1;
+        }
+        pred[i] = init_prefix[b];
+    }
+}
+
+// Booster::predict_raw_binned (cpp/src/booster.cpp:744-773): base + sum over trees
+// of lr * values[leaf], accumulated per row in tree order.
+__global__ void predict_trees_kernel(const uint8_t* __restrict__ codes, int stride, int n,
+                                     const int16_t* __restrict__ feat, const int16_t* __restrict__ left,
+                                     const int16_t* __restrict__ right, const uint8_t* __restrict__ thr,
+                                     const uint8_t* __restrict__ ml, const double* __restrict__ val,
+                                     const int* __restrict__ off, int n_trees, double base, double lr,
+                                     double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint8_t* row = codes + static_cast<size_t>(i) * stride;
+        double s = base;
+        for (int t = 0; t < n_trees; ++t) {
+            const int o = off[t];
+            int k = 0;
+            while (feat[o + k] >= 0) {
+                const int b = row[feat[o + k]];
+                const bool go_left = b == 0 ? ml[o + k] != 0 : b <= thr[o + k];
+                k = go_left ? left[o + k] : right[o + k];
+            }
+            s += lr * val[o + k];
+        }
+        out[i] = s;
+    }
+}
+
+}  // namespace
+
+void launch_fill_pred(const double* init_prefix, int n, int n_buckets, int iid_mode, double* pred,
+                      cudaStream_t s) {
+    fill_pred_kernel<<<std::max(1, std::min(2368, (n + 255) / 256)), 256, 0, s>>>(init_prefix, n, n_buckets,
+                                                                                  iid_mode, pred);
+    check(cudaGetLastError(), "fill_pred launch");
+}
+
+void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t* tree_feat,
+                          const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
+                          const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
+                          double base, double lr, double* out, cudaStream_t s) {
+    if (n <= 0) return;
+    predict_trees_kernel<<<std::max(1, std::min(4736, (n + 127) / 128)), 128, 0, s>>>(
+        codes, stride, n, tree_feat, tree_left, tree_right, tree_thr, tree_ml, tree_val, tree_off, n_trees, base,
+        lr, out);
+    check(cudaGetLastError(), "predict_trees launch");
+}
+
+void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s) {
+    check(cudaMemsetAsync(sc, 0, 2 * sizeof(unsigned long long), s), "all scale reset");
+    max_abs_kernel<<<std::max(1, std::min(1184, (n + 255) / 256)), 256, 0, s>>>(g, h, n, sc);
+    check(cudaGetLastError(), "max_abs launch");
+    all_scale_finalize_kernel<<<1, 1, 0, s>>>(sc, n);
+    check(cudaGetLastError(), "all_scale_finalize launch");
+}
+
+void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, const DevTreeState* st,
+                        const double* g, const double* h, const int4* chunks, int n_chunks,
+                        const AllScale* sc, int16_t* nid, unsigned long long* seg_sums, int n_segments,
+                        cudaStream_t s) {
+    check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
+          "seg sums reset");
+    const size_t smem = static_cast<size_t>(kApplyThreads) * stride;
+    static int configured = 0;
+    if (static_cast<int>(smem) > configured) {
+        check(cudaFuncSetAttribute(apply_accum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)),
+              "apply smem attr");
+        configured = static_cast<int>(smem);
+    }
+    apply_accum_kernel<<<n_chunks, kApplyThreads, smem, s>>>(codes, stride, nodes, st, g, h, chunks, sc, nid,
+                                                             seg_sums);
+    check(cudaGetLastError(), "apply_accum launch");
+}
+
+void launch_finalize_tree(const PostParams& pp, const DevTreeState* st, const unsigned long long* seg_sums,
+                          const int* bucket_seg_end, const int* cuts, const AllScale* sc, double* values,
+                          int* cover, double* prefix, cudaStream_t s) {
+    finalize_tree_kernel<<<1, 1024, 0, s>>>(pp, st, seg_sums, bucket_seg_end, cuts, sc, values, cover, prefix);
+    check(cudaGetLastError(), "finalize_tree launch");
+}
+
+void launch_pred_update(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
+                        double* pred, cudaStream_t s) {
+    pred_update_kernel<<<std::max(1, std::min(2368, (pp.n + 255) / 256)), 256, 0, s>>>(pp, nid, prefix, st, pred);
+    check(cudaGetLastError(), "pred_update launch");
+}
+
+}  // namespace tgb

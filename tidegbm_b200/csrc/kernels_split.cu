@@ -1,0 +1,278 @@
+// Best-split scan and best-first leaf selection.
+//
+// split_scan restates best_numeric_missing (cpp/src/histogram.cpp:126-193, l1 = 0,
+// no monotone) for every feature of a node and best_for_leaf's axis reduction
+// (cpp/src/tree.cpp:120-166): gain = 0.5 (GL^2/(HL+l2) + GR^2/(HR+l2) - G^2/(H+l2)) - gamma,
+// thresholds b = 1 .. n_bins-2 with a non-empty bin b, missing (bin 0) sent left or
+// right, min_samples_leaf on counts and min_child_weight on hessians, and ties broken
+// exactly as the reference's strict '>' does: lowest (feature, threshold,
+// missing_left) wins.  Prefix sums run in exact 64-bit integers (warp-shuffle scan,
+// 8 bins per lane); only the gain is FP64.  This file is compiled with -fmad=false
+// so the gain arithmetic follows the reference's statement order.
+//
+// select restates the leaf choice of grow_tree (cpp/src/tree.cpp:343-383): among
+// leaves with depth < max_depth and at least 2*min_samples_leaf rows, the largest
+// cached gain above min_split_gain, lowest node id on ties.
+#include "tgb_internal.h"
+
+namespace tgb {
+
+namespace {
+
+constexpr int kScanWarps = 16;
+
+struct Cand {
+    double gain;
+    int key;  // feature * 512 + threshold * 2 + missing_left
+};
+
+__device__ __forceinline__ bool better(const Cand& a, const Cand& b) {
+    return a.gain > b.gain || (a.gain == b.gain && a.key < b.key);
+}
+
+__device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ long long warp_sum(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One warp scans one feature of a histogram; returns the warp's best candidate
+// (identical in every lane) and the node totals.
+__device__ Cand scan_feature(const long long* __restrict__ Gf, const long long* __restrict__ Hf,
+                             const int* __restrict__ Cf, int f, int n_bins, double inv_gs,
+                             double inv_hs, double lam, double gamma, int min_leaf, double min_hess,
+                             long long& Gt, long long& Ht, long long& Ct) {
+    const int lane = threadIdx.x & 31;
+    long long g[8], hh[8];
+    int c[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        g[i] = Gf[lane * 8 + i];
+        hh[i] = Hf[lane * 8 + i];
+        c[i] = Cf[lane * 8 + i];
+    }
+    long long sg = 0, sh = 0, sc = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        sg += g[i];
+        sh += hh[i];
+        sc += c[i];
+    }
+    const long long ig = warp_incl_scan(sg, lane), ih = warp_incl_scan(sh, lane),
+                    ic = warp_incl_scan(sc, lane);
+    Gt = __shfl_sync(0xffffffffu, ig, 31);
+    Ht = __shfl_sync(0xffffffffu, ih, 31);
+    Ct = __shfl_sync(0xffffffffu, ic, 31);
+    const long long G0 = __shfl_sync(0xffffffffu, g[0], 0);
+    const long long H0 = __shfl_sync(0xffffffffu, hh[0], 0);
+    const long long C0 = __shfl_sync(0xffffffffu, static_cast<long long>(c[0]), 0);
+    const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
+    const double parent = (dGt * dGt) / (dHt + lam);
+    long long pg = ig - sg, ph = ih - sh, pc = ic - sc;  // exclusive prefix of this lane
+    Cand best{-1e300, 0x7fffffff};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        pg += g[i];
+        ph += hh[i];
+        pc += c[i];
+        const int b = lane * 8 + i;
+        if (b < 1 || b > n_bins - 2 || c[i] == 0) continue;
+        const long long GL = pg - G0, HL = ph - H0, CL = pc - C0;
+#pragma unroll
+        for (int ml = 0; ml <= 1; ++ml) {
+            const long long gL = GL + (ml ? G0 : 0), hL = HL + (ml ? H0 : 0), cL = CL + (ml ? C0 : 0);
+            const long long cR = Ct - cL;
+            if (cL < min_leaf || cR < min_leaf) continue;
+            const double dgL = static_cast<double>(gL) * inv_gs, dhL = static_cast<double>(hL) * inv_hs;
+            const double dgR = static_cast<double>(Gt - gL) * inv_gs,
+                         dhR = static_cast<double>(Ht - hL) * inv_hs;
+            if (dhL < min_hess || dhR < min_hess) continue;
+            const double gain =
+                0.5 * ((dgL * dgL) / (dhL + lam) + (dgR * dgR) / (dhR + lam) - parent) - gamma;
+            const Cand cand{gain, f * 512 + b * 2 + ml};
+            if (better(cand, best)) best = cand;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        Cand other{__shfl_xor_sync(0xffffffffu, best.gain, o), __shfl_xor_sync(0xffffffffu, best.key, o)};
+        if (better(other, best)) best = other;
+    }
+    return best;
+}
+
+__global__ void __launch_bounds__(kScanWarps * 32)
+    split_scan_kernel(GrowParams p, HistSlotPtrs hs, DevNode* __restrict__ nodes,
+                      DevSplit* __restrict__ splits, const DevTreeState* __restrict__ st, int mode,
+                      int node) {
+    if (st->done) return;
+    int nd = node;
+    if (mode == 1) {
+        const DevNode& par = nodes[st->parent];
+        nd = blockIdx.x == 0 ? par.left : par.right;
+    }
+    const long long* G = hs.G + nd * hs.slot_elems;
+    const long long* H = hs.H + nd * hs.slot_elems;
+    const int* C = hs.C + nd * hs.slot_elems;
+    const double inv_gs = st->inv_gscale, inv_hs = st->inv_hscale;
+    DevNode& N = nodes[nd];
+    const bool eligible = N.depth < p.max_depth && N.count >= 2 * p.min_samples_leaf;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ Cand sbest[kScanWarps];
+    Cand best{-1e300, 0x7fffffff};
+    if (eligible) {
+        for (int f = warp; f < p.n_features; f += kScanWarps) {
+            long long Gt, Ht, Ct;
+            const Cand c = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
+                                        C + static_cast<size_t>(f) * kBins, f, p.n_bins, inv_gs, inv_hs, p.l2,
+                                        p.min_split_gain, p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
+            if (c.gain > best.gain) best = c;  // ascending f: strict '>' keeps the lowest feature
+        }
+    }
+    if (lane == 0) sbest[warp] = best;
+    if (warp == 0) {
+        // Node totals from feature 0 (every feature's bins sum to the same exact integers).
+        long long g = 0, h = 0, c = 0;
+        for (int b = lane; b < kBins; b += 32) {
+            g += G[b];
+            h += H[b];
+            c += C[b];
+        }
+        g = warp_sum(g);
+        h = warp_sum(h);
+        c = warp_sum(c);
+        if (lane == 0) {
+            N.G = g;
+            N.H = h;
+            N.C = c;
+            const double dg = static_cast<double>(g) * inv_gs, dh = static_cast<double>(h) * inv_hs;
+            N.value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Cand b = sbest[0];
+        for (int w = 1; w < kScanWarps; ++w)
+            if (better(sbest[w], b)) b = sbest[w];
+        DevSplit s;
+        s.gain = b.gain;
+        s.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
+        s.feature = s.valid ? b.key / 512 : -1;
+        s.threshold = s.valid ? (b.key % 512) / 2 : -1;
+        s.missing_left = s.valid ? (b.key & 1) : 1;
+        splits[nd] = s;
+    }
+}
+
+__global__ void select_kernel(GrowParams p, DevNode* __restrict__ nodes, DevSplit* __restrict__ splits,
+                              DevTreeState* __restrict__ st) {
+    if (st->done) return;
+    const int lane = threadIdx.x;
+    const int nn = st->n_nodes;
+    double best_gain = p.min_split_gain;
+    int best_id = 0x7fffffff;
+    for (int k = lane; k < nn; k += 32) {
+        const DevNode& N = nodes[k];
+        if (!N.is_leaf || N.depth >= p.max_depth || N.count < 2 * p.min_samples_leaf) continue;
+        const DevSplit& s = splits[k];
+        if (!s.valid || !(s.gain >= p.min_split_gain)) continue;
+        if (s.gain > best_gain) {
+            best_gain = s.gain;
+            best_id = k;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double og = __shfl_xor_sync(0xffffffffu, best_gain, o);
+        const int oid = __shfl_xor_sync(0xffffffffu, best_id, o);
+        if (og > best_gain || (og == best_gain && oid < best_id)) {
+            best_gain = og;
+            best_id = oid;
+        }
+    }
+    if (lane != 0) return;
+    if (best_id == 0x7fffffff) {
+        st->done = 1;
+        return;
+    }
+    DevNode& P = nodes[best_id];
+    const DevSplit& s = splits[best_id];
+    P.is_leaf = 0;
+    P.feature = s.feature;
+    P.threshold = s.threshold;
+    P.missing_left = s.missing_left;
+    P.gain = s.gain;
+    const int l = nn, r = nn + 1;
+    P.left = l;
+    P.right = r;
+    for (int c = 0; c < 2; ++c) {
+        DevNode ch{};
+        ch.start = P.start;
+        ch.count = 0;
+        ch.buf = 1 - P.buf;
+        ch.depth = P.depth + 1;
+        ch.is_leaf = 1;
+        ch.feature = -1;
+        ch.threshold = -1;
+        ch.missing_left = 1;
+        ch.left = ch.right = -1;
+        ch.parent = best_id;
+        nodes[nn + c] = ch;
+        splits[nn + c].valid = 0;
+    }
+    st->parent = best_id;
+    st->n_nodes = nn + 2;
+}
+
+__global__ void __launch_bounds__(kScanWarps * 32)
+    scan_hist_kernel(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
+                     double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
+                     double min_hess, double* gain, int* thr, int* ml) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int f = blockIdx.x * kScanWarps + warp;
+    if (f >= n_f) return;
+    long long Gt, Ht, Ct;
+    const Cand c = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
+                                C + static_cast<size_t>(f) * kBins, f, n_bins, inv_gs, inv_hs, lam, gamma,
+                                min_leaf, min_hess, Gt, Ht, Ct);
+    if (lane == 0) {
+        const bool ok = c.key != 0x7fffffff;
+        gain[f] = c.gain;
+        thr[f] = ok ? (c.key % 512) / 2 : -1;
+        ml[f] = ok ? (c.key & 1) : 1;
+    }
+}
+
+}  // namespace
+
+void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
+                       const DevTreeState* st, int mode, int node, cudaStream_t s) {
+    split_scan_kernel<<<mode == 1 ? 2 : 1, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node);
+    check(cudaGetLastError(), "split_scan launch");
+}
+
+void launch_select(const GrowParams& p, DevNode* nodes, DevSplit* splits, DevTreeState* st,
+                   cudaStream_t s) {
+    select_kernel<<<1, 32, 0, s>>>(p, nodes, splits, st);
+    check(cudaGetLastError(), "select launch");
+}
+
+void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
+                      double inv_gscale, double inv_hscale, double lam, double gamma, int min_leaf,
+                      double min_hess, double* gain, int* thr, int* ml, cudaStream_t s) {
+    if (n_f <= 0) return;
+    scan_hist_kernel<<<(n_f + kScanWarps - 1) / kScanWarps, kScanWarps * 32, 0, s>>>(
+        G, H, C, n_f, n_bins, inv_gscale, inv_hscale, lam, gamma, min_leaf, min_hess, gain, thr, ml);
+    check(cudaGetLastError(), "scan_hist launch");
+}
+
+}  // namespace tgb

@@ -1,0 +1,184 @@
+// Internal declarations shared by the CUDA kernels (.cu) and the host runtime.
+//
+// Device data layout of one fit context (all resident in HBM):
+//   codes       uint8 row-major [n][stride], stride = round_up(F, 16): one 16-byte
+//               aligned row per sample, gathered whole by the histogram kernel
+//   y, pred, g, h         f64 [n]
+//   rows[2]     int32 [n] ping-pong row lists; every tree node owns a contiguous
+//               segment [start, start+count) of one of them
+//   hist slot per node: G int64 [F][256], H int64 [F][256], C int32 [F][256]
+//               fixed-point sums (value * 2^shift), exact and order independent
+//   nodes       DevNode[kMaxNodes], splits DevSplit[kMaxNodes], DevTreeState
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tgb {
+
+constexpr int kBins = 256;       // histogram width (codes are uint8)
+constexpr int kMaxNodes = 511;   // max_leaves <= 256
+constexpr int kPartTile = 2048;  // rows per partition tile
+
+struct DevNode {
+    int32_t start, count, buf, depth;
+    int32_t is_leaf, feature, threshold, missing_left;
+    int32_t left, right, parent, pad0;
+    double gain;        // split gain (internal nodes)
+    double value;       // leaf value from the node's sample sums (Node::value)
+    long long G, H, C;  // fixed-point sample sums
+    long long pad1;
+};
+
+struct DevSplit {
+    double gain;
+    int feature, threshold, missing_left, valid;
+};
+
+struct DevTreeState {
+    int n_nodes;
+    int done;
+    int parent;  // node split in the current iteration
+    int small_node, large_node;
+    int n_left;
+    int gshift, hshift;
+    double gscale, hscale, inv_gscale, inv_hscale;
+    unsigned long long max_abs_g_bits, max_h_bits;  // reductions for the scales
+    int n_sample;
+    int pad;
+};
+
+// Fixed-point scale for sums over all rows (post-tree leaf values).
+struct AllScale {
+    unsigned long long maxg_bits, maxh_bits;
+    int gshift, hshift;
+    double gscale, hscale, inv_gscale, inv_hscale;
+};
+
+struct PartJob {
+    const int32_t* in;    // row list (nullptr: rows 0..count-1)
+    int32_t* out;
+    const uint8_t* flag;  // compaction mode: keep rows with flag != 0
+    int* n_left_out;      // optional copy of n_left
+    int count;
+    int feature, threshold, missing_left;
+    int n_tiles;
+    int n_left;
+    int left_only;
+    int pad;
+};
+
+struct GrowParams {
+    int n_features;
+    int stride;
+    int n_bins;  // Binner::max_bins()
+    int max_depth;
+    int max_leaves;
+    int min_samples_leaf;
+    double min_child_weight;
+    double l2;
+    double min_split_gain;
+};
+
+struct PostParams {
+    int n;
+    int n_buckets;
+    int iid_mode;
+    int n_segments;
+    double learning_rate;
+    double l2;
+    double min_cover;
+};
+
+struct HistSlotPtrs {
+    long long* G;
+    long long* H;
+    int* C;
+    size_t slot_elems;  // F * kBins
+};
+
+struct GossWork {
+    unsigned long long* keys_in;
+    unsigned long long* keys_out;
+    int32_t* vals_in;
+    int32_t* vals_out;
+    void* cub_tmp;
+    size_t cub_tmp_bytes;
+};
+
+void check(cudaError_t e, const char* what);
+
+// binning (kernels_bin.cu)
+void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
+                              uint8_t* codes, int stride, cudaStream_t s);
+void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edges, const int* n_edges,
+                              uint8_t* codes, int stride, cudaStream_t s);
+
+// histograms + tree state (kernels_hist.cu)
+void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows, const DevNode* nodes,
+                      const DevTreeState* st, int node, const double* g, const double* h,
+                      const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs, int grid_rows,
+                      unsigned long long* rows_counter, cudaStream_t s);
+void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* rows, int n_rows,
+                      const double* g, const double* h, int gshift, int hshift, long long* G, long long* H,
+                      int* C, cudaStream_t s);
+void launch_hist_subtract(const DevTreeState* st, HistSlotPtrs hs, cudaStream_t s);
+void launch_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_sample_host, int use_dev_count,
+                      cudaStream_t s);
+void launch_iota_rows(int32_t* rows, int n, cudaStream_t s);
+void launch_scales(const int32_t* rows, const double* g, const double* h, const uint8_t* goss_flag,
+                   double goss_scale, DevTreeState* st, int max_rows, cudaStream_t s);
+int hist_grid_rows(int n_f, int max_rows);
+
+// split scan + selection (kernels_split.cu); mode 0 = node `node`, 1 = children of st->parent
+void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
+                       const DevTreeState* st, int mode, int node, cudaStream_t s);
+void launch_select(const GrowParams& p, DevNode* nodes, DevSplit* splits, DevTreeState* st, cudaStream_t s);
+void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
+                      double inv_gscale, double inv_hscale, double lam, double gamma, int min_leaf,
+                      double min_hess, double* gain, int* thr, int* ml, cudaStream_t s);
+
+// partition (kernels_part.cu); job_mem: device PartJob
+void launch_partition(const uint8_t* codes, int stride, int32_t* const* rows, DevNode* nodes, DevTreeState* st,
+                      int* tile_counts, int max_tiles, void* job_mem, cudaStream_t s);
+void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
+                           int threshold, int missing_left, int32_t* out, int* n_left_dev, int* tile_counts,
+                           void* job_mem, cudaStream_t s);
+void launch_compact_flagged(const uint8_t* flag, int n, int32_t* out, int* n_out_dev, int* tile_counts,
+                            void* job_mem, cudaStream_t s);
+
+// objectives (kernels_obj.cu)
+void launch_grad_mse(const double* y, const double* pred, int n, double* g, double* h, cudaStream_t s);
+void launch_grad_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len,
+                          const int* order, int n_runs, int n, double* g, double* h, cudaStream_t s);
+void launch_loss_mse(const double* y, const double* pred, int n, double* partials, int n_part, cudaStream_t s);
+void launch_loss_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len,
+                          const int* order, int n_runs, double* corr, int* valid, cudaStream_t s);
+void launch_loss_finalize(int kind, const double* partials, const int* valid, int n_part, int n,
+                          double* out, cudaStream_t s);
+
+// GOSS (kernels_goss.cu)
+size_t goss_cub_bytes(int n);
+void launch_goss_select(const double* g, int n, int n_top, int n_other, const int32_t* rest_pos, GossWork& w,
+                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, void* job_mem, DevTreeState* st,
+                        cudaStream_t s);
+
+// post-tree sweep (kernels_post.cu)
+void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s);
+void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, const DevTreeState* st,
+                        const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
+                        int16_t* nid, unsigned long long* seg_sums, int n_segments, cudaStream_t s);
+void launch_finalize_tree(const PostParams& pp, const DevTreeState* st, const unsigned long long* seg_sums,
+                          const int* bucket_seg_end, const int* cuts, const AllScale* sc, double* values,
+                          int* cover, double* prefix, cudaStream_t s);
+void launch_pred_update(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
+                        double* pred, cudaStream_t s);
+void launch_fill_pred(const double* init_prefix, int n, int n_buckets, int iid_mode, double* pred,
+                      cudaStream_t s);
+void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t* tree_feat,
+                          const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
+                          const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
+                          double base, double lr, double* out, cudaStream_t s);
+
+}  // namespace tgb
