@@ -129,6 +129,21 @@ TGB_API int tgb_partition(const unsigned char* codes, int stride, const int* row
                   int threshold, int missing_left, int* out, int* n_left_out, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* tgb_partition for callers that cannot allocate device memory (this entry point has no
+ * counterpart in the reference).  Some callers have no way to provide the workspace
+ * tgb_partition asks for: a serving process that reserves all device memory at start-up
+ * and must not call cudaMalloc later (it can block the device and fail under memory
+ * pressure), or a binding that passes only a call's inputs and outputs.  This variant
+ * allocates nothing: its scratch is a fixed device array inside the library (about
+ * 33 KB, held on every GPU that loads the library until the process exits), so n_rows
+ * is limited to 16,777,216 (larger calls return -1 with a message).  The first call on a
+ * device looks up that array's device address; make the first call on each device
+ * before any stream capture.  All calls on a device share the array: calls whose
+ * kernels may overlap on the GPU (other streams or host threads) race and must be
+ * serialised by the caller.  Results equal tgb_partition's. */
+TGB_API int tgb_partition_noalloc(const unsigned char* codes, int stride, const int* rows, int n_rows, int feature,
+                                  int threshold, int missing_left, int* out, int* n_left_out, void* stream);
+
 /* Objective::grad_hess (cpp/src/objective.cpp:102-219), unit weights, device f64 arrays.
  * MSE: g = pred - y, h = 1.  Pairwise: date groups given as runs of consecutive rows
  * (run_start/run_len device int [n_runs]; rows of a run are order[run_start..] when

@@ -356,6 +356,15 @@ int tgb_partition(const unsigned char* codes, int stride, const int* rows, int n
     });
 }
 
+int tgb_partition_noalloc(const unsigned char* codes, int stride, const int* rows, int n_rows, int feature,
+                          int threshold, int missing_left, int* out, int* n_left_out, void* stream) {
+    return guard([&] {
+        need(feature >= 0 && feature < stride, "feature out of range");
+        tgb::launch_partition_rows_noalloc(codes, stride, rows, n_rows, feature, threshold, missing_left, out,
+                                           n_left_out, as_stream(stream));
+    });
+}
+
 int tgb_grad_mse(const double* y, const double* pred, int n, double* g, double* h, void* stream) {
     return guard([&] { tgb::launch_grad_mse(y, pred, n, g, h, as_stream(stream)); });
 }

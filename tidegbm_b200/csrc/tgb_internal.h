@@ -147,6 +147,10 @@ void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows
                            void* job_mem, cudaStream_t s);
 void launch_compact_flagged(const uint8_t* flag, int n, int32_t* out, int* n_out_dev, int* tile_counts,
                             void* job_mem, cudaStream_t s);
+// Same partition with its scratch in a fixed device array of kernels_part.cu (no allocation).
+int partition_noalloc_max_rows();
+void launch_partition_rows_noalloc(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
+                                   int threshold, int missing_left, int32_t* out, int* n_left_dev, cudaStream_t s);
 
 // objectives (kernels_obj.cu)
 void launch_grad_mse(const double* y, const double* pred, int n, double* g, double* h, cudaStream_t s);

@@ -64,6 +64,7 @@ def lib() -> C.CDLL:
         "tgb_split_scan": ([vp, vp, vp, i, i, i, i, d, d, i, d, vp, vp, vp, vp], i),
         "tgb_partition_workspace_bytes": ([i], C.c_size_t),
         "tgb_partition": ([vp, i, vp, i, i, i, i, vp, vp, vp, C.c_size_t, vp], i),
+        "tgb_partition_noalloc": ([vp, i, vp, i, i, i, i, vp, vp, vp], i),
         "tgb_grad_mse": ([vp, vp, i, vp, vp, vp], i),
         "tgb_grad_pairwise": ([vp, vp, vp, vp, vp, i, i, vp, vp, vp], i),
         "tgb_build_hist_gpu": ([vp, vp, i, vp, i, vp, vp, i, i, vp], i),
