@@ -94,7 +94,7 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
         for (int f = 0; f < n_f; ++f) m[f] += counts[static_cast<size_t>(c) * n_f + f];
     parallel_for(n_f, n_threads, [&](int f) {
         if (bin_sample > 0 && m[f] > bin_sample) {
-            std::mt19937 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
+            Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);  // std::mt19937's stream
             keep[f].resize(static_cast<size_t>(bin_sample));
             shuffled_prefix(m[f], bin_sample, rng, keep[f].data());
             std::sort(keep[f].begin(), keep[f].end());

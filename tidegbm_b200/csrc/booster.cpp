@@ -19,6 +19,9 @@
 #include <numeric>
 #include <thread>
 
+#include <memory>
+
+#include "goss_sampler.h"
 #include "sampling.h"
 #include "tgb_internal.h"
 
@@ -110,7 +113,7 @@ int auto_time_buckets(const std::vector<int64_t>& uniq, int64_t horizon, int uni
 
 struct DeviceState {
     cudaStream_t stream = nullptr;
-    DBuf<uint8_t> codes;
+    DBuf<uint8_t> codes, codes_col;
     DBuf<double> y, pred, g, h;
     DBuf<int32_t> rows0, rows1;
     DBuf<long long> histG, histH;
@@ -120,6 +123,8 @@ struct DeviceState {
     DBuf<DevTreeState> st, st_all;
     DBuf<int> tile_counts;
     DBuf<PartJob> job;
+    DBuf<double> scan_gain;
+    DBuf<int> scan_key, scan_ticket;
     DBuf<unsigned long long> keys_in, keys_out;
     DBuf<int32_t> vals_in, vals_out, rest_pos;
     DBuf<unsigned char> cub_tmp;
@@ -314,6 +319,10 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     const int max_tiles = (n + kPartTile - 1) / kPartTile;
     D.tile_counts.alloc(max_tiles + 1);
     D.job.alloc(1);
+    D.scan_gain.alloc(2 * scan_ctas_per_node(n_f));
+    D.scan_key.alloc(2 * scan_ctas_per_node(n_f));
+    D.scan_ticket.alloc(2);
+    check(cudaMemsetAsync(D.scan_ticket.p, 0, 2 * sizeof(int), s), "ticket reset");
     D.nid.alloc(n);
     D.all_scale.alloc(1);
     D.init_prefix.alloc(nbk);
@@ -355,6 +364,10 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
             check(cudaStreamSynchronize(s), "transform");
         }
     }
+    // Column-major copy for the partition's reads of one feature over a row list.
+    D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n));
+    launch_codes_transpose(D.codes.p, stride, n, n_f, D.codes_col.p, s);
+    check(cudaStreamSynchronize(s), "transpose");
     stats.t_upload = now() - tb;
 
     // TORB segments: distinct cuts split the time-sorted rows into segments; CTAs of the
@@ -432,8 +445,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     int n_top = 0, n_other = 0;
     int64_t m_rest = 0;
     const double goss_scale = (1.0 - c.goss_top) / std::max(c.goss_other, 1e-12);
-    int32_t* pinned_pos[2] = {nullptr, nullptr};
-    cudaEvent_t pos_done[2] = {nullptr, nullptr};
+    std::unique_ptr<GossSampler> sampler;
     if (use_goss) {
         n_top = std::min(n, std::max(1, static_cast<int>(std::ceil(c.goss_top * static_cast<double>(n)))));
         m_rest = n - n_top;
@@ -446,11 +458,10 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         D.rest_pos.alloc(std::max(1, n_other));
         const size_t cb = goss_cub_bytes(n);
         D.cub_tmp.alloc(cb);
-        for (int k = 0; k < 2; ++k) {
-            check(cudaMallocHost(reinterpret_cast<void**>(&pinned_pos[k]), sizeof(int32_t) * std::max(1, n_other)),
-                  "pinned positions");
-            check(cudaEventCreateWithFlags(&pos_done[k], cudaEventDisableTiming), "event");
-        }
+        // The booster's generator (booster.cpp:483) is only used by GOSS and grow_tree's
+        // seed draw, so the sampler owns the whole stream.
+        sampler = std::make_unique<GossSampler>(static_cast<uint32_t>(c.random_state), m_rest, n_other, T, 8,
+                                                std::max(1, std::min(8, n_threads - 2)));
     }
     GossWork gw{D.keys_in.p, D.keys_out.p, D.vals_in.p, D.vals_out.p, D.cub_tmp.p, D.cub_tmp.n};
 
@@ -459,9 +470,9 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     PostParams pp{n, nbk, c.iid_mode ? 1 : 0, n_segments, c.learning_rate, c.l2,
                   c.torb_min_cover > 0.0 ? c.torb_min_cover : static_cast<double>(2 * std::max(c.min_samples_leaf, 1))};
     HistSlotPtrs hs{D.histG.p, D.histH.p, D.histC.p, slot};
+    ScanScratch scs{D.scan_gain.p, D.scan_key.p, D.scan_ticket.p};
     int32_t* rows[2] = {D.rows0.p, D.rows1.p};
     const int grid_rows = hist_grid_rows(n_f, n);
-    std::mt19937 rng(static_cast<uint32_t>(c.random_state));
     const double ttree = now();
 
     // Measurement hooks: events bracket the timed trees; optional event pairs bracket
@@ -486,7 +497,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         const bool prof = in_timed && c.profile_hist && hist_ev_used + 2 <= hist_ev.size();
         if (prof) check(cudaEventRecord(hist_ev[hist_ev_used], s), "event record");
         launch_hist_node(D.codes.p, stride, n_f, rows, D.nodes.p, D.st.p, node, D.g.p, D.h.p, flag, goss_scale, hs,
-                         grid_rows, in_timed ? rows_counter.p : nullptr, s);
+                         grid_rows, in_timed ? rows_counter.p : nullptr, c.objective == 0, s);
         if (prof) {
             check(cudaEventRecord(hist_ev[hist_ev_used + 1], s), "event record");
             hist_ev_used += 2;
@@ -505,15 +516,12 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         launch_all_scale(D.g.p, D.h.p, n, D.all_scale.p, s);
         // sample
         if (use_goss) {
-            const int slot_k = t & 1;
             const double tr = now();
-            check(cudaEventSynchronize(pos_done[slot_k]), "positions slot");
-            shuffled_prefix(m_rest, n_other, rng, pinned_pos[slot_k]);
+            const int32_t* pos = sampler->wait(t);  // host time spent waiting for the draw
             stats.t_rng += now() - tr;
-            check(cudaMemcpyAsync(D.rest_pos.p, pinned_pos[slot_k], sizeof(int32_t) * std::max(1, n_other),
-                                  cudaMemcpyHostToDevice, s),
+            check(cudaMemcpyAsync(D.rest_pos.p, pos, sizeof(int32_t) * std::max(1, n_other), cudaMemcpyHostToDevice, s),
                   "positions upload");
-            check(cudaEventRecord(pos_done[slot_k], s), "event record");
+            sampler->release(t, s);
             launch_goss_select(D.g.p, n, n_top, n_other, D.rest_pos.p, gw, D.goss_flag.p, D.rows0.p, D.tile_counts.p,
                                D.job.p, D.st.p, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, 0, 1, s);
@@ -521,7 +529,6 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
             launch_iota_rows(D.rows0.p, n, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, n, 0, s);
         }
-        (void)rng();  // booster.cpp:588 draws grow_tree's seed from the same generator
         const uint8_t* flag = use_goss ? D.goss_flag.p : nullptr;
         launch_scales(D.rows0.p, D.g.p, D.h.p, flag, goss_scale, D.st.p, n, s);
         check(cudaMemsetAsync(D.histG.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
@@ -529,13 +536,14 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         check(cudaMemsetAsync(D.histC.p, 0, sizeof(int) * slot * max_nodes, s), "hist reset");
         // grow_tree (cpp/src/tree.cpp:283-472)
         hist_launch(0, flag, in_timed);
-        launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 0, 0, s);
+        launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 0, 0, scs, s);
         for (int it = 0; it < c.max_leaves - 1; ++it) {
             launch_select(gp, D.nodes.p, D.splits.p, D.st.p, s);
-            launch_partition(D.codes.p, stride, rows, D.nodes.p, D.st.p, D.tile_counts.p, max_tiles, D.job.p, s);
+            launch_partition(D.codes.p, stride, D.codes_col.p, codes_col_pitch(n), rows, D.nodes.p, D.st.p,
+                             D.tile_counts.p, max_tiles, D.job.p, s);
             hist_launch(-1, flag, in_timed);
             launch_hist_subtract(D.st.p, hs, s);
-            launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 1, 0, s);
+            launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 1, 0, scs, s);
         }
         // post-tree sweep (booster.cpp:589-664), outputs straight into tree slot t
         double* values_t = D.values_all.p + static_cast<size_t>(t) * max_nodes;
@@ -584,10 +592,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         cudaEventDestroy(ev_end);
         for (auto& e : hist_ev) cudaEventDestroy(e);
     }
-    for (int k = 0; k < 2; ++k) {
-        if (pinned_pos[k]) cudaFreeHost(pinned_pos[k]);
-        if (pos_done[k]) cudaEventDestroy(pos_done[k]);
-    }
+    sampler.reset();
 
     // ---- read back the trees ----
     const double td = now();

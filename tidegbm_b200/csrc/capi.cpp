@@ -297,7 +297,7 @@ int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bi
 int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out) {
     return guard([&] {
         need(m >= 0 && m < (1ll << 31) && keep >= 0 && keep <= m, "bad sizes");
-        std::mt19937 rng(seed);
+        tgb::Mt32 rng(seed);
         tgb::shuffled_prefix(m, keep, rng, out);
     });
 }

@@ -1,0 +1,131 @@
+// Host pipeline that produces each tree's GOSS draw positions ahead of the GPU.
+//
+// Per tree the booster's generator makes one std::shuffle of the m-row GOSS remainder
+// (cpp/src/booster.cpp:572) and one draw for grow_tree's seed (booster.cpp:588).  The
+// positions a tree needs depend only on the generator state at the tree's start, so:
+//   producer  walks the stream once (skip_shuffle: exact, no positions) and snapshots
+//             the generator at every tree start;
+//   workers   take trees in order, restart from the snapshot and compute the kept
+//             positions (shuffled_prefix) into a pinned slot, in parallel;
+//   consumer  (the fit loop) waits for tree t, enqueues the H2D copy, records an event
+//             and releases the slot; a worker reuses a slot only after that copy ends.
+#pragma once
+
+#include <condition_variable>
+#include <cuda_runtime.h>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "sampling.h"
+
+namespace tgb {
+
+class GossSampler {
+public:
+    GossSampler(uint32_t seed, int64_t m, int64_t keep, int n_trees, int n_slots, int n_workers)
+        : m_(m), keep_(std::max<int64_t>(1, keep)), T_(n_trees), S_(std::max(1, n_slots)),
+          snaps_(n_trees), produced_(n_trees, 0), ready_(n_trees, 0), released_(n_trees, 0),
+          slot_(S_, nullptr), slot_ev_(S_, nullptr) {
+        for (int k = 0; k < S_; ++k) {
+            if (cudaMallocHost(reinterpret_cast<void**>(&slot_[k]), sizeof(int32_t) * keep_) != cudaSuccess)
+                throw std::runtime_error("cudaMallocHost (GOSS positions)");
+            if (cudaEventCreateWithFlags(&slot_ev_[k], cudaEventDisableTiming) != cudaSuccess)
+                throw std::runtime_error("cudaEventCreate (GOSS positions)");
+        }
+        threads_.emplace_back([this, seed] { produce(seed); });
+        for (int w = 0; w < std::max(1, n_workers); ++w) threads_.emplace_back([this] { work(); });
+    }
+
+    ~GossSampler() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            abort_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : threads_) t.join();
+        for (int k = 0; k < S_; ++k) {
+            if (slot_[k]) cudaFreeHost(slot_[k]);
+            if (slot_ev_[k]) cudaEventDestroy(slot_ev_[k]);
+        }
+    }
+
+    // Blocks until tree t's positions are ready; returns the pinned slot holding them.
+    const int32_t* wait(int t) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return ready_[t] || abort_ || !error_.empty(); });
+        if (!error_.empty()) throw std::runtime_error(error_);
+        return slot_[t % S_];
+    }
+
+    // After the consumer enqueued the copy of tree t's slot on `stream`.
+    void release(int t, cudaStream_t stream) {
+        if (cudaEventRecord(slot_ev_[t % S_], stream) != cudaSuccess) throw std::runtime_error("cudaEventRecord");
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            released_[t] = 1;
+        }
+        cv_.notify_all();
+    }
+
+private:
+    void produce(uint32_t seed) {
+        Mt32 rng(seed);
+        for (int t = 0; t < T_; ++t) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (abort_) return;
+                snaps_[t] = rng;
+                produced_[t] = 1;
+            }
+            cv_.notify_all();
+            skip_shuffle(m_, rng);
+            (void)rng();  // grow_tree's seed draw
+        }
+    }
+
+    void work() {
+        for (;;) {
+            int t;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (next_ >= T_ || abort_) return;
+                t = next_++;
+                cv_.wait(lk, [&] { return abort_ || (produced_[t] && (t < S_ || released_[t - S_])); });
+                if (abort_) return;
+            }
+            const int k = t % S_;
+            if (t >= S_ && cudaEventSynchronize(slot_ev_[k]) != cudaSuccess) {
+                std::lock_guard<std::mutex> lk(mu_);
+                error_ = "cudaEventSynchronize (GOSS positions)";
+                cv_.notify_all();
+                return;
+            }
+            Mt32 rng = snaps_[t];
+            shuffled_prefix(m_, keep_, rng, slot_[k]);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ready_[t] = 1;
+            }
+            cv_.notify_all();
+        }
+    }
+
+    int64_t m_, keep_;
+    int T_, S_;
+    std::vector<Mt32> snaps_;
+    std::vector<char> produced_, ready_, released_;
+    std::vector<int32_t*> slot_;
+    std::vector<cudaEvent_t> slot_ev_;
+    std::vector<std::thread> threads_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    int next_ = 0;
+    bool abort_ = false;
+    std::string error_;
+};
+
+}  // namespace tgb

@@ -70,6 +70,41 @@ __global__ void zero_pad_kernel(uint8_t* codes, int n, int n_f, int stride) {
     }
 }
 
+// Column-major copy for the partition's single-feature reads: a CTA moves a tile of
+// 128 rows x 32 features through shared memory (16-byte loads of row chunks, 16-byte
+// stores of column runs).
+// col has a row pitch of round_up(n, 16) bytes, so every 16-row run is 16-byte aligned.
+__global__ void __launch_bounds__(256)
+    codes_transpose_kernel(const uint8_t* __restrict__ codes, int stride, int n, int n_f, uint8_t* __restrict__ col,
+                           long long pitch) {
+    __shared__ uint8_t tile[128][33];
+    const int r0 = blockIdx.x * 128, f0 = blockIdx.y * 32;
+    {
+        const int r = threadIdx.x >> 1, half = threadIdx.x & 1;  // 2 x 16 bytes per row
+        const int fb = f0 + half * 16;
+        if (r0 + r < n && fb < stride) {
+            const uint4 v = *reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r0 + r) * stride + fb);
+            const uint8_t* b = reinterpret_cast<const uint8_t*>(&v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) tile[r][half * 16 + i] = b[i];
+        }
+    }
+    __syncthreads();
+    const int fl = threadIdx.x >> 3, q = threadIdx.x & 7;  // feature, run of 16 rows
+    const int f = f0 + fl;
+    if (f >= n_f) return;
+    const int rb = r0 + q * 16;
+    if (rb + 16 <= n) {
+        uint4 v;
+        uint8_t* b = reinterpret_cast<uint8_t*>(&v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) b[i] = tile[q * 16 + i][fl];
+        *reinterpret_cast<uint4*>(col + static_cast<size_t>(f) * pitch + rb) = v;
+    } else {
+        for (int i = 0; i < 16 && rb + i < n; ++i) col[static_cast<size_t>(f) * pitch + rb + i] = tile[q * 16 + i][fl];
+    }
+}
+
 template <typename T>
 void launch_bin(const T* X, int n, int n_f, const T* edges, const int* n_edges, uint8_t* codes,
                 int stride, cudaStream_t s) {
@@ -89,6 +124,13 @@ void launch_bin(const T* X, int n, int n_f, const T* edges, const int* n_edges, 
 }
 
 }  // namespace
+
+void launch_codes_transpose(const uint8_t* codes, int stride, int n, int n_f, uint8_t* col, cudaStream_t s) {
+    if (n <= 0 || n_f <= 0) return;
+    dim3 grid((n + 127) / 128, (n_f + 31) / 32);
+    codes_transpose_kernel<<<grid, 256, 0, s>>>(codes, stride, n, n_f, col, codes_col_pitch(n));
+    check(cudaGetLastError(), "codes_transpose launch");
+}
 
 void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
                               uint8_t* codes, int stride, cudaStream_t s) {

@@ -9,12 +9,23 @@
 // subtraction is exact.  The error against an FP64 sum is at most
 // rows * 2^-(shift+1) (about 1e-12 relative at 10M rows).
 //
-// Launch shape: CTA = (feature group of FG features) x (contiguous chunk of the
-// node's row list).  Each thread takes one row at a time, loads the FG code bytes of
-// that row with 128-bit loads (rows are 16-byte aligned), and adds (g, h, 1) to a
-// CTA-private shared-memory histogram (FG x 256 x {i64, i64, u32}).  The private
-// histogram is flushed to the node's global slot with one 64-bit atomic per
-// non-empty bin.
+// Launch shape: CTA = (group of 32 features) x (contiguous chunk of the node's row
+// list), one CTA per SM.  A warp takes one row at a time and lane l owns feature l of
+// the group: the warp reads the row's 32 code bytes with one coalesced 32-byte access,
+// g and h are warp-uniform broadcasts, and each lane adds into bin (code_l, l) of the
+// CTA-private shared histogram, stored at b*32 + l: every lane of a warp access owns its
+// own bank whatever the codes are, and the features being distinct there are no
+// same-address collisions either.
+//
+// Shared atomics are 32-bit only (the 64-bit shared add is not a single instruction):
+// a 64-bit fixed-point value is added as two words, the low word with atomicAdd, whose
+// returned old value tells whether this addition wrapped, then (high + carry) to the
+// high word.  The words end up holding the exact 64-bit sum modulo 2^64.  For objectives
+// with a constant hessian (mse with unit weights: h = 1, or 1 * goss_scale for sampled
+// GOSS rows) the hessian and count sums are two 32-bit row counters, c1 (unscaled rows)
+// and c2 (scaled rows): H = c1 * rint(2^hs) + c2 * rint(goss_scale * 2^hs), C = c1 + c2,
+// the same integers the per-row sums give.  The private histogram is flushed to the
+// node's global slot with one 64-bit global atomic per non-empty bin and value.
 #include "tgb_internal.h"
 
 #include <cmath>
@@ -23,10 +34,23 @@ namespace tgb {
 
 namespace {
 
-constexpr int kHistThreads = 512;
+constexpr int kHistThreads = 1024;
+constexpr int kHistWarps = kHistThreads / 32;
 constexpr int kMinRowsPerCta = 2048;
+constexpr int kFG = 32;      // features per CTA (one per lane)
+constexpr int kUnroll = 8;   // code loads in flight per warp
+constexpr int kPlane = kFG * kBins;  // 32-bit words per plane
 
-template <int FG>
+// Exact 64-bit add into a (low, high) pair of 32-bit shared words.
+__device__ __forceinline__ void add64(unsigned int* lo, unsigned int* hi, int slot, unsigned long long v) {
+    const unsigned int vlo = static_cast<unsigned int>(v);
+    const unsigned int vhi = static_cast<unsigned int>(v >> 32);
+    const unsigned int old = atomicAdd(&lo[slot], vlo);
+    const unsigned int up = vhi + (old + vlo < old ? 1u : 0u);
+    if (up != 0u) atomicAdd(&hi[slot], up);
+}
+
+template <bool kConstH>
 __device__ __forceinline__ void hist_body(const uint8_t* __restrict__ codes, int stride, int n_f,
                                           const int32_t* __restrict__ rows, int count,
                                           const double* __restrict__ g, const double* __restrict__ h,
@@ -34,9 +58,13 @@ __device__ __forceinline__ void hist_body(const uint8_t* __restrict__ codes, int
                                           double gscale, double hscale, long long* G, long long* H,
                                           int* C) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned long long* sG = reinterpret_cast<unsigned long long*>(smem_raw);
-    unsigned long long* sH = sG + FG * kBins;
-    unsigned int* sC = reinterpret_cast<unsigned int*>(sH + FG * kBins);
+    unsigned int* gLo = reinterpret_cast<unsigned int*>(smem_raw);
+    unsigned int* gHi = gLo + kPlane;
+    // kConstH: c1, c2 row counters; otherwise hLo, hHi, count.
+    unsigned int* p2 = gHi + kPlane;
+    unsigned int* p3 = p2 + kPlane;
+    unsigned int* p4 = p3 + kPlane;
+    constexpr int n_planes = kConstH ? 4 : 5;
 
     // Row chunk of this CTA.
     const int need = (count + kMinRowsPerCta - 1) / kMinRowsPerCta;
@@ -46,52 +74,93 @@ __device__ __forceinline__ void hist_body(const uint8_t* __restrict__ codes, int
     const int r0 = blockIdx.y * chunk;
     const int r1 = min(count, r0 + chunk);
     if (r0 >= r1) return;
-    const int fg0 = blockIdx.x * FG;
 
-    for (int k = threadIdx.x; k < FG * kBins; k += blockDim.x) {
-        sG[k] = 0ull;
-        sH[k] = 0ull;
-        sC[k] = 0u;
+    {
+        uint4* z = reinterpret_cast<uint4*>(smem_raw);
+        for (int k = threadIdx.x; k < n_planes * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
     }
     __syncthreads();
 
-    for (int k = r0 + threadIdx.x; k < r1; k += blockDim.x) {
-        const int32_t r = rows[k];
-        const uint8_t* src = codes + static_cast<size_t>(r) * stride + fg0;
-        uint4 v[FG / 16];
-#pragma unroll
-        for (int q = 0; q < FG / 16; ++q) v[q] = __ldg(reinterpret_cast<const uint4*>(src) + q);
-        double gv = g[r], hv = h[r];
-        if (goss_flag != nullptr && goss_flag[r] == 2) {
-            gv *= goss_scale;
-            hv *= goss_scale;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int f = blockIdx.x * kFG + lane;
+    const bool active = f < n_f;
+    const int fo = active ? f : 0;  // in-bounds byte for idle lanes
+    // A warp takes 32 rows at a time: lane j loads row j's index, g and h (one gather each),
+    // then the warp walks the 32 rows, kBatch code loads in flight, with the row's index
+    // and fixed-point values broadcast by shuffles.
+    for (int base = r0 + warp * 32; base < r1; base += kHistWarps * 32) {
+        const int nrow = min(32, r1 - base);
+        const bool own = lane < nrow;
+        const int rid = own ? rows[base + lane] : 0;
+        unsigned long long gq = 0ull, hq = 0ull;
+        int sc = 0;
+        if (own) {
+            double gv = g[rid];
+            sc = goss_flag != nullptr && goss_flag[rid] == 2;
+            if (sc) gv *= goss_scale;
+            gq = static_cast<unsigned long long>(__double2ll_rn(gv * gscale));
+            if (!kConstH) {
+                double hv = h[rid];
+                if (sc) hv *= goss_scale;
+                hq = static_cast<unsigned long long>(__double2ll_rn(hv * hscale));
+            }
         }
-        const unsigned long long gq = static_cast<unsigned long long>(__double2ll_rn(gv * gscale));
-        const unsigned long long hq = static_cast<unsigned long long>(__double2ll_rn(hv * hscale));
-        const uint8_t* bytes = reinterpret_cast<const uint8_t*>(v);
+        for (int j0 = 0; j0 < nrow; j0 += kUnroll) {
+            unsigned int cc[kUnroll];
 #pragma unroll
-        for (int j = 0; j < FG; ++j) {
-            const int slot = j * kBins + bytes[j];
-            atomicAdd(&sG[slot], gq);
-            atomicAdd(&sH[slot], hq);
-            atomicAdd(&sC[slot], 1u);
+            for (int u = 0; u < kUnroll; ++u) {
+                const int j = j0 + u;
+                const int rj = __shfl_sync(0xffffffffu, rid, j & 31);
+                cc[u] = j < nrow ? codes[static_cast<size_t>(rj) * stride + fo] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                const int j = j0 + u;
+                const unsigned long long gj = __shfl_sync(0xffffffffu, gq, j & 31);
+                const int sj = __shfl_sync(0xffffffffu, sc, j & 31);
+                const unsigned long long hj = kConstH ? 0ull : __shfl_sync(0xffffffffu, hq, j & 31);
+                if (j >= nrow || !active) continue;
+                const int slot = static_cast<int>(cc[u]) * 32 + lane;
+                add64(gLo, gHi, slot, gj);
+                if (kConstH) {
+                    atomicAdd(sj ? &p3[slot] : &p2[slot], 1u);
+                } else {
+                    add64(p2, p3, slot, hj);
+                    atomicAdd(&p4[slot], 1u);
+                }
+            }
         }
     }
     __syncthreads();
 
-    for (int k = threadIdx.x; k < FG * kBins; k += blockDim.x) {
-        const int f = fg0 + k / kBins;
-        if (f >= n_f) break;
-        const size_t o = static_cast<size_t>(f) * kBins + (k % kBins);
-        const unsigned int c = sC[k];
+    // Flush: warp w takes bins w, w + 32, ...; lane l = feature l (conflict-free reads).
+    const int ff = blockIdx.x * kFG + lane;
+    if (ff >= n_f) return;
+    const unsigned long long hq1 = kConstH ? static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale)) : 0ull;
+    const unsigned long long hq2 =
+        kConstH ? static_cast<unsigned long long>(__double2ll_rn(1.0 * goss_scale * hscale)) : 0ull;
+    for (int b = warp; b < kBins; b += kHistWarps) {
+        const int slot = b * 32 + lane;
+        unsigned long long hsum;
+        unsigned int c;
+        if (kConstH) {
+            const unsigned int c1 = p2[slot], c2 = p3[slot];
+            c = c1 + c2;
+            hsum = static_cast<unsigned long long>(c1) * hq1 + static_cast<unsigned long long>(c2) * hq2;
+        } else {
+            c = p4[slot];
+            hsum = (static_cast<unsigned long long>(p3[slot]) << 32) | p2[slot];
+        }
         if (c == 0u) continue;
-        atomicAdd(reinterpret_cast<unsigned long long*>(G) + o, sG[k]);
-        atomicAdd(reinterpret_cast<unsigned long long*>(H) + o, sH[k]);
+        const unsigned long long gsum = (static_cast<unsigned long long>(gHi[slot]) << 32) | gLo[slot];
+        const size_t o = static_cast<size_t>(ff) * kBins + b;
+        atomicAdd(reinterpret_cast<unsigned long long*>(G) + o, gsum);
+        atomicAdd(reinterpret_cast<unsigned long long*>(H) + o, hsum);
         atomicAdd(C + o, static_cast<int>(c));
     }
 }
 
-template <int FG>
+template <bool kConstH>
 __global__ void __launch_bounds__(kHistThreads)
     hist_node_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0,
                      int32_t* rows1, const DevNode* __restrict__ nodes,
@@ -105,18 +174,15 @@ __global__ void __launch_bounds__(kHistThreads)
     // Rows histogrammed, for the algorithmic-bytes figure of the benchmark.
     if (rows_counter != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         atomicAdd(rows_counter, static_cast<unsigned long long>(N.count));
-    hist_body<FG>(codes, stride, n_f, rows, N.count, g, h, goss_flag, goss_scale, st->gscale,
-                  st->hscale, hs.G + nd * hs.slot_elems, hs.H + nd * hs.slot_elems,
-                  hs.C + nd * hs.slot_elems);
+    hist_body<kConstH>(codes, stride, n_f, rows, N.count, g, h, goss_flag, goss_scale, st->gscale, st->hscale,
+                       hs.G + nd * hs.slot_elems, hs.H + nd * hs.slot_elems, hs.C + nd * hs.slot_elems);
 }
 
-template <int FG>
 __global__ void __launch_bounds__(kHistThreads)
-    hist_rows_kernel(const uint8_t* __restrict__ codes, int stride, int n_f,
-                     const int32_t* __restrict__ rows, int count, const double* __restrict__ g,
-                     const double* __restrict__ h, double gscale, double hscale, long long* G,
-                     long long* H, int* C) {
-    hist_body<FG>(codes, stride, n_f, rows, count, g, h, nullptr, 1.0, gscale, hscale, G, H, C);
+    hist_rows_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, const int32_t* __restrict__ rows,
+                     int count, const double* __restrict__ g, const double* __restrict__ h, double gscale,
+                     double hscale, long long* G, long long* H, int* C) {
+    hist_body<false>(codes, stride, n_f, rows, count, g, h, nullptr, 1.0, gscale, hscale, G, H, C);
 }
 
 __global__ void hist_subtract_kernel(const DevTreeState* __restrict__ st, HistSlotPtrs hs) {
@@ -207,55 +273,49 @@ __global__ void scales_finalize_kernel(DevTreeState* st) {
     st->inv_hscale = ldexp(1.0, -st->hshift);
 }
 
-template <int FG>
-size_t hist_smem() {
-    return static_cast<size_t>(FG) * kBins * (8 + 8 + 4);
-}
+constexpr size_t hist_smem(bool const_h) { return static_cast<size_t>(kPlane) * 4 * (const_h ? 4 : 5); }
 
-template <int FG, typename K>
-void set_smem(K kern) {
-    check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(hist_smem<FG>())),
+template <typename K>
+void set_smem(K kern, size_t bytes) {
+    check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)),
           "hist smem attr");
 }
 
 }  // namespace
 
-constexpr int kFG = 16;
+int hist_grid_rows(int n_f, int max_rows) {
+    const int groups = (n_f + kFG - 1) / kFG;
+    const int need = (max_rows + kMinRowsPerCta - 1) / kMinRowsPerCta;
+    return std::max(1, std::min(need, (148 + groups - 1) / groups));
+}
 
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows,
                       const DevNode* nodes, const DevTreeState* st, int node, const double* g,
                       const double* h, const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs,
-                      int grid_rows, unsigned long long* rows_counter, cudaStream_t s) {
-    set_smem<kFG>(hist_node_kernel<kFG>);
+                      int grid_rows, unsigned long long* rows_counter, bool const_h, cudaStream_t s) {
     dim3 grid((n_f + kFG - 1) / kFG, max(1, grid_rows));
-    hist_node_kernel<kFG><<<grid, kHistThreads, hist_smem<kFG>(), s>>>(
-        codes, stride, n_f, rows[0], rows[1], nodes, st, node, g, h, goss_flag, goss_scale, hs, rows_counter);
+    if (const_h) {
+        set_smem(hist_node_kernel<true>, hist_smem(true));
+        hist_node_kernel<true><<<grid, kHistThreads, hist_smem(true), s>>>(
+            codes, stride, n_f, rows[0], rows[1], nodes, st, node, g, h, goss_flag, goss_scale, hs, rows_counter);
+    } else {
+        set_smem(hist_node_kernel<false>, hist_smem(false));
+        hist_node_kernel<false><<<grid, kHistThreads, hist_smem(false), s>>>(
+            codes, stride, n_f, rows[0], rows[1], nodes, st, node, g, h, goss_flag, goss_scale, hs, rows_counter);
+    }
     check(cudaGetLastError(), "hist_node launch");
 }
 
 void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* rows, int n_rows,
                       const double* g, const double* h, int gshift, int hshift, long long* G,
                       long long* H, int* C, cudaStream_t s) {
-    static bool init = false;
-    if (!init) {
-        set_smem<kFG>(hist_rows_kernel<kFG>);
-        init = true;
-    }
     if (n_rows <= 0) return;
-    const int need = (n_rows + kMinRowsPerCta - 1) / kMinRowsPerCta;
-    const int groups = (n_f + kFG - 1) / kFG;
-    const int grid_rows = max(1, min(need, (148 * 4 + groups - 1) / groups));
-    dim3 grid(groups, grid_rows);
-    hist_rows_kernel<kFG><<<grid, kHistThreads, hist_smem<kFG>(), s>>>(
-        codes, stride, n_f, rows, n_rows, g, h, std::ldexp(1.0, gshift), std::ldexp(1.0, hshift), G, H, C);
+    set_smem(hist_rows_kernel, hist_smem(false));
+    dim3 grid((n_f + kFG - 1) / kFG, hist_grid_rows(n_f, n_rows));
+    hist_rows_kernel<<<grid, kHistThreads, hist_smem(false), s>>>(codes, stride, n_f, rows, n_rows, g, h,
+                                                           std::ldexp(1.0, gshift), std::ldexp(1.0, hshift), G, H,
+                                                           C);
     check(cudaGetLastError(), "hist_rows launch");
-}
-
-int hist_grid_rows(int n_f, int max_rows) {
-    const int groups = (n_f + kFG - 1) / kFG;
-    const int need = (max_rows + kMinRowsPerCta - 1) / kMinRowsPerCta;
-    return std::max(1, std::min(need, (148 * 4 + groups - 1) / groups));
 }
 
 void launch_hist_subtract(const DevTreeState* st, HistSlotPtrs hs, cudaStream_t s) {

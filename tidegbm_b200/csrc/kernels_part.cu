@@ -31,13 +31,17 @@ __device__ __forceinline__ int32_t job_row(const PartJob& j, int k) { return j.i
 __device__ __forceinline__ bool goes_left(const uint8_t* __restrict__ codes, int stride, int32_t r,
                                           const PartJob& j) {
     if (j.flag) return j.flag[r] != 0;
-    const int b = codes[static_cast<size_t>(r) * stride + j.feature];
+    const int b = j.col ? j.col[static_cast<size_t>(j.feature) * j.col_n + r]
+                        : codes[static_cast<size_t>(r) * stride + j.feature];
     return b == 0 ? j.missing_left != 0 : b <= j.threshold;
 }
 
 __global__ void part_setup_tree_kernel(const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st,
-                                       int32_t* rows0, int32_t* rows1, PartJob* job) {
+                                       int32_t* rows0, int32_t* rows1, const uint8_t* col, long long col_n,
+                                       PartJob* job) {
     PartJob j{};
+    j.col = col;
+    j.col_n = col_n;
     if (!st->done) {
         const DevNode& P = nodes[st->parent];
         j.in = (P.buf ? rows1 : rows0) + P.start;
@@ -188,10 +192,11 @@ void run_partition(const uint8_t* codes, int stride, PartJob* job, int* tile_cou
 
 }  // namespace
 
-void launch_partition(const uint8_t* codes, int stride, int32_t* const* rows, DevNode* nodes,
-                      DevTreeState* st, int* tile_counts, int max_tiles, void* job_mem, cudaStream_t s) {
+void launch_partition(const uint8_t* codes, int stride, const uint8_t* codes_col, long long n_rows_total,
+                      int32_t* const* rows, DevNode* nodes, DevTreeState* st, int* tile_counts, int max_tiles,
+                      void* job_mem, cudaStream_t s) {
     PartJob* job = static_cast<PartJob*>(job_mem);
-    part_setup_tree_kernel<<<1, 1, 0, s>>>(nodes, st, rows[0], rows[1], job);
+    part_setup_tree_kernel<<<1, 1, 0, s>>>(nodes, st, rows[0], rows[1], codes_col, n_rows_total, job);
     check(cudaGetLastError(), "part_setup launch");
     run_partition(codes, stride, job, tile_counts, max_tiles, nodes, st, 1, s);
 }

@@ -61,6 +61,15 @@ __global__ void all_scale_finalize_kernel(AllScale* sc, int n) {
     sc->inv_hscale = ldexp(1.0, -sc->hshift);
 }
 
+// Exact 64-bit add into (low, high) 32-bit shared words: the low word's returned old
+// value says whether this addition wrapped; the carry goes to the high word.
+__device__ __forceinline__ void add64s(unsigned int* lo, unsigned int* hi, int k, unsigned long long v) {
+    const unsigned int vlo = static_cast<unsigned int>(v);
+    const unsigned int old = atomicAdd(&lo[k], vlo);
+    const unsigned int up = static_cast<unsigned int>(v >> 32) + (old + vlo < old ? 1u : 0u);
+    if (up != 0u) atomicAdd(&hi[k], up);
+}
+
 __global__ void __launch_bounds__(kApplyThreads)
     apply_accum_kernel(const uint8_t* __restrict__ codes, int stride, const DevNode* __restrict__ nodes,
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
@@ -70,7 +79,8 @@ __global__ void __launch_bounds__(kApplyThreads)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
     __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes];
-    __shared__ unsigned long long acc[kMaxNodes][3];
+    // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
+    __shared__ unsigned int aGl[kMaxNodes], aGh[kMaxNodes], aHl[kMaxNodes], aHh[kMaxNodes], aC[kMaxNodes];
     const int nn = st->n_nodes;
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         const DevNode& N = nodes[k];
@@ -80,22 +90,31 @@ __global__ void __launch_bounds__(kApplyThreads)
         s_thr[k] = static_cast<uint8_t>(N.threshold < 0 ? 0 : N.threshold);
         s_ml[k] = static_cast<uint8_t>(N.missing_left);
         s_leaf[k] = static_cast<uint8_t>(N.is_leaf);
-        acc[k][0] = acc[k][1] = acc[k][2] = 0ull;
+        aGl[k] = aGh[k] = aHl[k] = aHh[k] = aC[k] = 0u;
     }
     const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
     const double gs = sc->gscale, hs = sc->hscale;
     uint8_t* tile = smem_raw;
     const int vec_per_row = stride / 16;
+    // Shared pitch of stride + 4 bytes: (stride/4 + 1) is odd, so the 32 lanes walking 32
+    // consecutive rows read 32 different banks at any feature offset.
+    const int pitch = stride + 4;
     __syncthreads();
     for (int t0 = ch.y; t0 < ch.z; t0 += kApplyThreads) {
         const int rows_here = min(kApplyThreads, ch.z - t0);
         const uint4* src = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(t0) * stride);
-        uint4* dst = reinterpret_cast<uint4*>(tile);
-        for (int v = threadIdx.x; v < rows_here * vec_per_row; v += blockDim.x) dst[v] = __ldg(src + v);
+        for (int v = threadIdx.x; v < rows_here * vec_per_row; v += blockDim.x) {
+            const uint4 val = __ldg(src + v);
+            uint32_t* d = reinterpret_cast<uint32_t*>(tile + (v / vec_per_row) * pitch + (v % vec_per_row) * 16);
+            d[0] = val.x;
+            d[1] = val.y;
+            d[2] = val.z;
+            d[3] = val.w;
+        }
         __syncthreads();
         if (threadIdx.x < rows_here) {
             const int r = t0 + threadIdx.x;
-            const uint8_t* row = tile + threadIdx.x * stride;
+            const uint8_t* row = tile + threadIdx.x * pitch;
             int k = 0;
             while (!s_leaf[k]) {
                 const int b = row[s_feat[k]];
@@ -103,18 +122,18 @@ __global__ void __launch_bounds__(kApplyThreads)
                 k = left ? s_left[k] : s_right[k];
             }
             nid[r] = static_cast<int16_t>(k);
-            atomicAdd(&acc[k][0], static_cast<unsigned long long>(__double2ll_rn(g[r] * gs)));
-            atomicAdd(&acc[k][1], static_cast<unsigned long long>(__double2ll_rn(h[r] * hs)));
-            atomicAdd(&acc[k][2], 1ull);
+            add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(g[r] * gs)));
+            add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(h[r] * hs)));
+            atomicAdd(&aC[k], 1u);
         }
         __syncthreads();
     }
     unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
-        if (acc[k][2] == 0ull) continue;
-        atomicAdd(out + 3 * k, acc[k][0]);
-        atomicAdd(out + 3 * k + 1, acc[k][1]);
-        atomicAdd(out + 3 * k + 2, acc[k][2]);
+        if (aC[k] == 0u) continue;
+        atomicAdd(out + 3 * k, (static_cast<unsigned long long>(aGh[k]) << 32) | aGl[k]);
+        atomicAdd(out + 3 * k + 1, (static_cast<unsigned long long>(aHh[k]) << 32) | aHl[k]);
+        atomicAdd(out + 3 * k + 2, static_cast<unsigned long long>(aC[k]));
     }
 }
 
@@ -250,7 +269,7 @@ void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, 
                         cudaStream_t s) {
     check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
           "seg sums reset");
-    const size_t smem = static_cast<size_t>(kApplyThreads) * stride;
+    const size_t smem = static_cast<size_t>(kApplyThreads) * (stride + 4);
     static int configured = 0;
     if (static_cast<int>(smem) > configured) {
         check(cudaFuncSetAttribute(apply_accum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -110,15 +110,18 @@ __device__ Cand scan_feature(const long long* __restrict__ Gf, const long long* 
     return best;
 }
 
+// grid = (ceil(F / kScanWarps), nodes): one warp per (node, feature).  Each CTA reduces
+// its warps' candidates and stores one per CTA; the last CTA of a node to finish
+// (ticket counter, no waiting) reduces the per-CTA candidates, lowest feature on ties.
 __global__ void __launch_bounds__(kScanWarps * 32)
     split_scan_kernel(GrowParams p, HistSlotPtrs hs, DevNode* __restrict__ nodes,
                       DevSplit* __restrict__ splits, const DevTreeState* __restrict__ st, int mode,
-                      int node) {
+                      int node, ScanScratch sc) {
     if (st->done) return;
     int nd = node;
     if (mode == 1) {
         const DevNode& par = nodes[st->parent];
-        nd = blockIdx.x == 0 ? par.left : par.right;
+        nd = blockIdx.y == 0 ? par.left : par.right;
     }
     const long long* G = hs.G + nd * hs.slot_elems;
     const long long* H = hs.H + nd * hs.slot_elems;
@@ -127,19 +130,7 @@ __global__ void __launch_bounds__(kScanWarps * 32)
     DevNode& N = nodes[nd];
     const bool eligible = N.depth < p.max_depth && N.count >= 2 * p.min_samples_leaf;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ Cand sbest[kScanWarps];
-    Cand best{-1e300, 0x7fffffff};
-    if (eligible) {
-        for (int f = warp; f < p.n_features; f += kScanWarps) {
-            long long Gt, Ht, Ct;
-            const Cand c = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
-                                        C + static_cast<size_t>(f) * kBins, f, p.n_bins, inv_gs, inv_hs, p.l2,
-                                        p.min_split_gain, p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
-            if (c.gain > best.gain) best = c;  // ascending f: strict '>' keeps the lowest feature
-        }
-    }
-    if (lane == 0) sbest[warp] = best;
-    if (warp == 0) {
+    if (blockIdx.x == 0 && warp == 0) {
         // Node totals from feature 0 (every feature's bins sum to the same exact integers).
         long long g = 0, h = 0, c = 0;
         for (int b = lane; b < kBins; b += 32) {
@@ -156,20 +147,64 @@ __global__ void __launch_bounds__(kScanWarps * 32)
             N.C = c;
             const double dg = static_cast<double>(g) * inv_gs, dh = static_cast<double>(h) * inv_hs;
             N.value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
+            if (!eligible) {
+                DevSplit s{};
+                s.gain = -1e300;
+                s.valid = 0;
+                s.feature = s.threshold = -1;
+                s.missing_left = 1;
+                splits[nd] = s;
+            }
         }
     }
+    if (!eligible) return;
+    __shared__ Cand sbest[kScanWarps];
+    __shared__ int last;
+    Cand best{-1e300, 0x7fffffff};
+    const int f = blockIdx.x * kScanWarps + warp;
+    if (f < p.n_features) {
+        long long Gt, Ht, Ct;
+        best = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
+                            C + static_cast<size_t>(f) * kBins, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
+                            p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
+    }
+    if (lane == 0) sbest[warp] = best;
     __syncthreads();
     if (threadIdx.x == 0) {
         Cand b = sbest[0];
         for (int w = 1; w < kScanWarps; ++w)
             if (better(sbest[w], b)) b = sbest[w];
-        DevSplit s;
-        s.gain = b.gain;
-        s.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
-        s.feature = s.valid ? b.key / 512 : -1;
-        s.threshold = s.valid ? (b.key % 512) / 2 : -1;
-        s.missing_left = s.valid ? (b.key & 1) : 1;
-        splits[nd] = s;
+        const int slot = blockIdx.y * gridDim.x + blockIdx.x;
+        sc.gain[slot] = b.gain;
+        sc.key[slot] = b.key;
+        __threadfence();
+        last = atomicAdd(&sc.ticket[blockIdx.y], 1) == static_cast<int>(gridDim.x) - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    if (warp == 0) {
+        __threadfence();
+        Cand b{-1e300, 0x7fffffff};
+        for (int k = lane; k < static_cast<int>(gridDim.x); k += 32) {
+            const int slot = blockIdx.y * gridDim.x + k;
+            const Cand c{static_cast<volatile double*>(sc.gain)[slot], static_cast<volatile int*>(sc.key)[slot]};
+            if (better(c, b)) b = c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            Cand other{__shfl_xor_sync(0xffffffffu, b.gain, o), __shfl_xor_sync(0xffffffffu, b.key, o)};
+            if (better(other, b)) b = other;
+        }
+        if (lane == 0) {
+            DevSplit s;
+            s.gain = b.gain;
+            s.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
+            s.feature = s.valid ? b.key / 512 : -1;
+            s.threshold = s.valid ? (b.key % 512) / 2 : -1;
+            s.missing_left = s.valid ? (b.key & 1) : 1;
+            splits[nd] = s;
+            sc.ticket[blockIdx.y] = 0;  // ready for the next launch
+        }
     }
 }
 
@@ -254,9 +289,12 @@ __global__ void __launch_bounds__(kScanWarps * 32)
 
 }  // namespace
 
+int scan_ctas_per_node(int n_f) { return (n_f + kScanWarps - 1) / kScanWarps; }
+
 void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
-                       const DevTreeState* st, int mode, int node, cudaStream_t s) {
-    split_scan_kernel<<<mode == 1 ? 2 : 1, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node);
+                       const DevTreeState* st, int mode, int node, ScanScratch sc, cudaStream_t s) {
+    dim3 grid(scan_ctas_per_node(p.n_features), mode == 1 ? 2 : 1);
+    split_scan_kernel<<<grid, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc);
     check(cudaGetLastError(), "split_scan launch");
 }
 

@@ -14,6 +14,13 @@
 // draws: O(keep) memory instead of O(m), and no value traffic.  Shorter ranges take
 // libstdc++'s two-draws-per-call path, so they call std::shuffle itself on an index
 // range.  The generator is left in exactly the state std::shuffle leaves it.
+//
+// Mt32 is MT19937 (Matsumoto & Nishimura, ACM TOMACS 8(1), 1998) on 32-bit words,
+// generating a block of 624 outputs per refill: the same output stream as
+// std::mt19937, at a fraction of libstdc++'s per-call cost.  bounded() is Lemire's
+// nearly divisionless method (ACM TOMACS 29(1), 2019, arXiv:1805.10941), the
+// algorithm libstdc++'s uniform_int_distribution uses for 32-bit generators; both are
+// checked against the standard library by the tests.
 #pragma once
 
 #include <algorithm>
@@ -24,14 +31,90 @@
 
 namespace tgb {
 
-// out[p] = index (in [0, m)) of the element that std::shuffle puts at position p, p < keep.
-inline void shuffled_prefix(int64_t m, int64_t keep, std::mt19937& rng, int32_t* out) {
+// One MT19937 block: twist the 624-word state in place, write the 624 tempered
+// outputs.  Compiled for several x86 vector ISAs and picked at load time (the three
+// loops carry no dependence shorter than 227 words, so they vectorise).
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
+__attribute__((target_clones("avx512f", "avx2", "default")))
+#endif
+inline void mt_refill(uint32_t* __restrict__ st, uint32_t* __restrict__ out) {
+    constexpr uint32_t UM = 0x80000000u, LM = 0x7fffffffu, A = 0x9908b0dfu;
+    for (int k = 0; k < 227; ++k) {
+        const uint32_t y = (st[k] & UM) | (st[k + 1] & LM);
+        st[k] = st[k + 397] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+    }
+    for (int k = 227; k < 623; ++k) {
+        const uint32_t y = (st[k] & UM) | (st[k + 1] & LM);
+        st[k] = st[k - 227] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+    }
+    {
+        const uint32_t y = (st[623] & UM) | (st[0] & LM);
+        st[623] = st[396] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+    }
+    for (int k = 0; k < 624; ++k) {
+        uint32_t v = st[k];
+        v ^= v >> 11;
+        v ^= (v << 7) & 0x9d2c5680u;
+        v ^= (v << 15) & 0xefc60000u;
+        v ^= v >> 18;
+        out[k] = v;
+    }
+}
+
+struct Mt32 {
+    using result_type = uint32_t;
+    static constexpr result_type min() { return 0u; }
+    static constexpr result_type max() { return 0xffffffffu; }
+
+    uint32_t st[624];
+    uint32_t out[624];
+    int pos = 624;
+
+    explicit Mt32(uint32_t seed = 5489u) {
+        st[0] = seed;
+        for (uint32_t i = 1; i < 624; ++i) st[i] = 1812433253u * (st[i - 1] ^ (st[i - 1] >> 30)) + i;
+        pos = 624;
+    }
+
+    void refill() {
+        mt_refill(st, out);
+        pos = 0;
+    }
+
+    result_type operator()() {
+        if (pos >= 624) refill();
+        return out[pos++];
+    }
+};
+
+// Uniform draw in [0, range), range in [1, 2^32): Lemire's method.
+template <class G>
+inline uint32_t bounded(G& g, uint32_t range) {
+    uint64_t m = static_cast<uint64_t>(g()) * range;
+    uint32_t low = static_cast<uint32_t>(m);
+    if (low < range) {
+        const uint32_t t = (0u - range) % range;
+        while (low < t) {
+            m = static_cast<uint64_t>(g()) * range;
+            low = static_cast<uint32_t>(m);
+        }
+    }
+    return static_cast<uint32_t>(m >> 32);
+}
+
+// True when libstdc++'s std::shuffle takes its two-positions-per-draw path for a
+// range of m elements with a 32-bit generator.
+inline bool shuffle_pairs(int64_t m) {
+    const unsigned long urngrange = 0xffffffffUL;
+    return m > 0 && urngrange / static_cast<unsigned long>(m) >= static_cast<unsigned long>(m);
+}
+
+// out[p] = index (in [0, m)) of the element std::shuffle(iota(m), rng) puts at p < keep.
+template <class G>
+inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
     if (m <= 0) return;  // std::shuffle of an empty range draws nothing
     keep = std::max<int64_t>(0, std::min(keep, m));
-    const unsigned long urngrange = static_cast<unsigned long>(rng.max() - rng.min());
-    const unsigned long urange = static_cast<unsigned long>(m);
-    if (urngrange / urange >= urange) {
-        // libstdc++ pairs two swap positions per generator call here: run it for real.
+    if (shuffle_pairs(m)) {
         std::vector<int32_t> v(static_cast<size_t>(m));
         std::iota(v.begin(), v.end(), 0);
         std::shuffle(v.begin(), v.end(), rng);
@@ -39,16 +122,64 @@ inline void shuffled_prefix(int64_t m, int64_t keep, std::mt19937& rng, int32_t*
         return;
     }
     std::iota(out, out + keep, 0);
-    std::uniform_int_distribution<unsigned long> d;
-    using P = std::uniform_int_distribution<unsigned long>::param_type;
-    for (int64_t i = 1; i < m; ++i) {
-        const unsigned long j = d(rng, P(0, static_cast<unsigned long>(i)));
-        if (i < keep) {
-            std::swap(out[i], out[j]);
-        } else if (static_cast<int64_t>(j) < keep) {
-            out[j] = static_cast<int32_t>(i);
-        }
+    int64_t i = 1;
+    for (; i < keep; ++i) {
+        const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
+        std::swap(out[i], out[j]);
     }
+    for (; i < m; ++i) {
+        const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
+        if (static_cast<int64_t>(j) < keep) out[j] = static_cast<int32_t>(i);
+    }
+}
+
+// Advances rng exactly as std::shuffle of m elements does, without producing positions.
+// A draw consumes extra words only when its first product's low half is below the
+// range (probability range / 2^32), so whole groups of 8 consecutive words are tested
+// at once and only a group containing such a word is replayed draw by draw.
+inline void skip_shuffle(int64_t m, Mt32& rng) {
+    if (m <= 0) return;
+    if (shuffle_pairs(m)) {
+        std::vector<int32_t> v(static_cast<size_t>(m));
+        std::shuffle(v.begin(), v.end(), rng);
+        return;
+    }
+    int64_t i = 1;  // next draw uses range i + 1
+    while (i < m) {
+        if (rng.pos >= 624) rng.refill();
+        const int avail = 624 - rng.pos;
+        const int64_t left = m - i;
+        int k = static_cast<int>(std::min<int64_t>(avail, left));
+        int done = 0;
+        while (done + 8 <= k) {
+            const uint32_t* w = rng.out + rng.pos + done;
+            const uint32_t r0 = static_cast<uint32_t>(i + done + 1);
+            uint32_t flag = 0;
+            for (int l = 0; l < 8; ++l) {
+                const uint32_t r = r0 + static_cast<uint32_t>(l);
+                flag |= static_cast<uint32_t>(static_cast<uint32_t>(static_cast<uint64_t>(w[l]) * r) < r);
+            }
+            if (flag) break;
+            done += 8;
+        }
+        rng.pos += done;
+        i += done;
+        if (done == k) continue;  // block exhausted or m reached
+        // Replay up to 8 draws exactly (one of them may consume extra words).
+        const int64_t stop = std::min<int64_t>(m, i + 8);
+        for (; i < stop; ++i) (void)bounded(rng, static_cast<uint32_t>(i + 1));
+    }
+}
+
+template <class G>
+inline void skip_shuffle(int64_t m, G& rng) {
+    if (m <= 0) return;
+    if (shuffle_pairs(m)) {
+        std::vector<int32_t> v(static_cast<size_t>(m));
+        std::shuffle(v.begin(), v.end(), rng);
+        return;
+    }
+    for (int64_t i = 1; i < m; ++i) (void)bounded(rng, static_cast<uint32_t>(i + 1));
 }
 
 }  // namespace tgb

@@ -61,6 +61,8 @@ struct PartJob {
     int32_t* out;
     const uint8_t* flag;  // compaction mode: keep rows with flag != 0
     int* n_left_out;      // optional copy of n_left
+    const uint8_t* col;   // column-major codes [F][col_n] (nullptr: read the row-major codes)
+    long long col_n;
     int count;
     int feature, threshold, missing_left;
     int n_tiles;
@@ -119,7 +121,7 @@ void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edg
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows, const DevNode* nodes,
                       const DevTreeState* st, int node, const double* g, const double* h,
                       const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs, int grid_rows,
-                      unsigned long long* rows_counter, cudaStream_t s);
+                      unsigned long long* rows_counter, bool const_h, cudaStream_t s);
 void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* rows, int n_rows,
                       const double* g, const double* h, int gshift, int hshift, long long* G, long long* H,
                       int* C, cudaStream_t s);
@@ -131,17 +133,29 @@ void launch_scales(const int32_t* rows, const double* g, const double* h, const 
                    double goss_scale, DevTreeState* st, int max_rows, cudaStream_t s);
 int hist_grid_rows(int n_f, int max_rows);
 
-// split scan + selection (kernels_split.cu); mode 0 = node `node`, 1 = children of st->parent
+// split scan + selection (kernels_split.cu); mode 0 = node `node`, 1 = children of st->parent.
+// ScanScratch: per-CTA candidates (2 x scan_ctas_per_node) and 2 ticket counters that
+// must start at zero (the kernel leaves them at zero).
+struct ScanScratch {
+    double* gain;
+    int* key;
+    int* ticket;
+};
+int scan_ctas_per_node(int n_f);
 void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
-                       const DevTreeState* st, int mode, int node, cudaStream_t s);
+                       const DevTreeState* st, int mode, int node, ScanScratch sc, cudaStream_t s);
 void launch_select(const GrowParams& p, DevNode* nodes, DevSplit* splits, DevTreeState* st, cudaStream_t s);
 void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
                       double inv_gscale, double inv_hscale, double lam, double gamma, int min_leaf,
                       double min_hess, double* gain, int* thr, int* ml, cudaStream_t s);
 
 // partition (kernels_part.cu); job_mem: device PartJob
-void launch_partition(const uint8_t* codes, int stride, int32_t* const* rows, DevNode* nodes, DevTreeState* st,
-                      int* tile_counts, int max_tiles, void* job_mem, cudaStream_t s);
+void launch_partition(const uint8_t* codes, int stride, const uint8_t* codes_col, long long n_rows_total,
+                      int32_t* const* rows, DevNode* nodes, DevTreeState* st, int* tile_counts, int max_tiles,
+                      void* job_mem, cudaStream_t s);
+// Column-major copy of the row-major codes: col[f * codes_col_pitch(n) + r] = codes[r][f].
+inline long long codes_col_pitch(int n) { return (static_cast<long long>(n) + 15) / 16 * 16; }
+void launch_codes_transpose(const uint8_t* codes, int stride, int n, int n_f, uint8_t* col, cudaStream_t s);
 void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
                            int threshold, int missing_left, int32_t* out, int* n_left_dev, int* tile_counts,
                            void* job_mem, cudaStream_t s);
