@@ -322,8 +322,8 @@ def run_ours(args) -> None:
     h2d = p.X.nbytes + p.y.nbytes
     e2e = {"value": world * n_est / e2e_wall, "unit": "trees/s", "h2d_bytes_per_step": int(h2d / n_est),
            "d2h_bytes_per_step": int(d2h / n_est), "fit_wall_s": e2e_wall, "trees": n_est,
-           "breakdown_s": {k: st[k] for k in ("sort", "bin_fit", "upload_transform", "trees", "download",
-                                              "host_rng")}}
+           "breakdown_s": {k: st[k] for k in ("sort", "bin_fit", "upload_transform", "alloc", "h2d", "transpose",
+                                              "trees", "download", "host_rng", "goss_producer")}}
     # Histogram GB/s: short fit with events around every histogram launch.
     bp = native.Booster(device=local, **dict(PARAMS, n_estimators=W + 2, timing_from=W, profile_hist=1))
     bp.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)

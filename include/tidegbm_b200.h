@@ -77,12 +77,13 @@ TGB_API int tgb_tree_export(tgb_booster* b, int tree, int* inodes, double* fnode
 /* Bin edges of feature f (Binner::edges, cpp/include/tidegbm/binning.hpp:15); returns
  * the count, copies them when out != NULL. */
 TGB_API int tgb_edges(tgb_booster* b, int f, double* out);
-/* Breakdown of the last fit (14 values): wall seconds {total, sort, bin_fit,
+/* Breakdown of the last fit (17 values): wall seconds {total, sort, bin_fit,
  * upload+transform, trees, download, host_rng}, kernel_launches, then the timed range
  * set by the int keys "timing_from" (first timed tree) and "profile_hist":
  * {device ms (CUDA events), trees, kernel launches, histogram-kernel ms, histogram
- * launches, rows histogrammed}. */
-TGB_API int tgb_fit_stats(tgb_booster* b, double* out14);
+ * launches, rows histogrammed}, then wall seconds {device allocation, X/y H2D,
+ * column-major copy, GOSS draw producer}. */
+TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
 
 /* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:
  * quantile edges from the bin_sample values std::shuffle(mt19937(seed + f*2654435761))

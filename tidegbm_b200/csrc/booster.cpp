@@ -336,10 +336,13 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
 
     // X upload + transform, then X is released.
     {
+        stats.t_alloc = now() - tb;
         DBuf<unsigned char> Xd;
         Xd.alloc(static_cast<size_t>(n) * n_f * xsz);
         check(cudaMemcpyAsync(Xd.p, X, static_cast<size_t>(n) * n_f * xsz, cudaMemcpyHostToDevice, s), "X upload");
         check(cudaMemcpyAsync(D.y.p, y, sizeof(double) * n, cudaMemcpyHostToDevice, s), "y upload");
+        check(cudaStreamSynchronize(s), "X upload");
+        stats.t_h2d = now() - tb - stats.t_alloc;
         DBuf<int> ne;
         ne.alloc(n_f);
         check(cudaMemcpyAsync(ne.p, n_edges.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "edges upload");
@@ -365,9 +368,11 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         }
     }
     // Column-major copy for the partition's reads of one feature over a row list.
+    const double ttr = now();
     D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n));
     launch_codes_transpose(D.codes.p, stride, n, n_f, D.codes_col.p, s);
     check(cudaStreamSynchronize(s), "transpose");
+    stats.t_transpose = now() - ttr;
     stats.t_upload = now() - tb;
 
     // TORB segments: distinct cuts split the time-sorted rows into segments; CTAs of the
@@ -592,7 +597,11 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         cudaEventDestroy(ev_end);
         for (auto& e : hist_ev) cudaEventDestroy(e);
     }
-    sampler.reset();
+    if (sampler) {
+        sampler->stop();
+        stats.t_producer = sampler->producer_seconds();
+        sampler.reset();
+    }
 
     // ---- read back the trees ----
     const double td = now();

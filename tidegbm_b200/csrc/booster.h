@@ -79,6 +79,7 @@ struct HostTree {
 struct FitStats {
     double t_total = 0, t_sort = 0, t_binfit = 0, t_upload = 0, t_transform = 0, t_trees = 0, t_download = 0;
     double t_rng = 0;
+    double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
     int gpu_launches = 0;
     // timed range (cfg.timing_from .. last tree), device time from CUDA events
     double timed_ms = 0;

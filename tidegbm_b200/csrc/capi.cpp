@@ -274,6 +274,10 @@ int tgb_fit_stats(tgb_booster* hb, double* o) {
         o[11] = s.hist_ms;
         o[12] = s.hist_launches;
         o[13] = static_cast<double>(s.hist_rows);
+        o[14] = s.t_alloc;
+        o[15] = s.t_h2d;
+        o[16] = s.t_transpose;
+        o[17] = s.t_producer;
     });
 }
 

@@ -11,6 +11,7 @@
 //             and releases the slot; a worker reuses a slot only after that copy ends.
 #pragma once
 
+#include <chrono>
 #include <condition_variable>
 #include <cuda_runtime.h>
 #include <memory>
@@ -40,13 +41,19 @@ public:
         for (int w = 0; w < std::max(1, n_workers); ++w) threads_.emplace_back([this] { work(); });
     }
 
-    ~GossSampler() {
+    // Stops the threads (all trees consumed, or an error path) and joins them.
+    void stop() {
         {
             std::lock_guard<std::mutex> lk(mu_);
             abort_ = true;
         }
         cv_.notify_all();
-        for (auto& t : threads_) t.join();
+        for (auto& t : threads_)
+            if (t.joinable()) t.join();
+    }
+
+    ~GossSampler() {
+        stop();
         for (int k = 0; k < S_; ++k) {
             if (slot_[k]) cudaFreeHost(slot_[k]);
             if (slot_ev_[k]) cudaEventDestroy(slot_ev_[k]);
@@ -82,10 +89,19 @@ private:
                 produced_[t] = 1;
             }
             cv_.notify_all();
+            const auto t0 = std::chrono::steady_clock::now();
             skip_shuffle(m_, rng);
             (void)rng();  // grow_tree's seed draw
+            producer_s_ += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         }
     }
+
+public:
+    // Seconds the producer spent walking the stream (its per-tree cost bounds throughput).
+    double producer_seconds() const { return producer_s_; }
+
+private:
+    double producer_s_ = 0.0;
 
     void work() {
         for (;;) {

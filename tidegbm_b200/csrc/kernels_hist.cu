@@ -160,6 +160,140 @@ __device__ __forceinline__ void hist_body(const uint8_t* __restrict__ codes, int
     }
 }
 
+// ---- constant-hessian histogram (mse with unit weights, the GOSS workloads) ----------
+//
+// Lane = row.  A warp takes 32 rows, one per lane; each lane loads its row's 32 code
+// bytes of the feature group once (8 x 4-byte loads, word order rotated by lane / 4,
+// then a byte funnel-shift by lane % 4), so that step j of the 32-step loop reads byte j
+// of the rotated array = the code of feature (j + lane) & 31.  All 32 lanes therefore
+// touch 32 different features, i.e. 32 different banks of the [bin][feature] layout, at
+// every step, and the row's g, GOSS flag and count increment stay in the lane's registers.
+//
+// Each row's fixed-point g (|v| < 2^37, enforced by the per-tree shift) is split into a
+// 19-bit unsigned low part and a signed high part (v >> 19).  Over at most kSub = 8192
+// rows a bin's low sum stays below 2^32 and its high sum inside int32, so three
+// fire-and-forget 32-bit shared reductions per code (low, high, packed counts c1 + c2<<16)
+// are exact.  After every kSub rows the CTA folds the three planes into per-thread 64-bit
+// register accumulators (each thread owns 8 fixed cells) and clears them.
+constexpr int kSub = 8192;
+constexpr int kLoBits = 19;
+constexpr int kCells = kFG * kBins / kHistThreads;  // cells owned per thread (8)
+constexpr size_t kConstSmem = static_cast<size_t>(kPlane) * 4 * 3;
+
+__device__ __forceinline__ void hist_const_body(const uint8_t* __restrict__ codes, int stride, int n_f,
+                                                const int32_t* __restrict__ rows, int count,
+                                                const double* __restrict__ g, const uint8_t* __restrict__ goss_flag,
+                                                double goss_scale, double gscale, double hscale, long long* G,
+                                                long long* H, int* C) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);
+    unsigned int* pHi = pLo + kPlane;
+    unsigned int* pCn = pHi + kPlane;
+
+    const int need = (count + kMinRowsPerCta - 1) / kMinRowsPerCta;
+    const int n_chunks = max(1, min(static_cast<int>(gridDim.y), need));
+    if (static_cast<int>(blockIdx.y) >= n_chunks) return;
+    const int chunk = (count + n_chunks - 1) / n_chunks;
+    const int r0 = blockIdx.y * chunk;
+    const int r1 = min(count, r0 + chunk);
+    if (r0 >= r1) return;
+
+    {
+        uint4* z = reinterpret_cast<uint4*>(smem_raw);
+        for (int k = threadIdx.x; k < 3 * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
+    }
+    long long accG[kCells];
+    unsigned int accC1[kCells], accC2[kCells];
+#pragma unroll
+    for (int c = 0; c < kCells; ++c) {
+        accG[c] = 0;
+        accC1[c] = accC2[c] = 0u;
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int fg0 = blockIdx.x * kFG;
+    const int nf_here = min(kFG, n_f - fg0);
+    const int q = lane >> 2, sh = (lane & 3) * 8;
+    for (int s0 = r0; s0 < r1; s0 += kSub) {
+        const int s1 = min(r1, s0 + kSub);
+        for (int base = s0 + warp * 32; base < s1; base += kHistWarps * 32) {
+            const int k = base + lane;
+            if (k < s1) {
+                const int r = rows[k];
+                double gv = g[r];
+                const bool sc = goss_flag != nullptr && goss_flag[r] == 2;
+                if (sc) gv *= goss_scale;
+                const long long v = __double2ll_rn(gv * gscale);
+                const unsigned int lo = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
+                const unsigned int hi = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
+                const unsigned int inc = sc ? 0x10000u : 1u;
+                const uint8_t* src = codes + static_cast<size_t>(r) * stride + fg0;
+                const int lim = stride - fg0;  // bytes of this group inside the row
+                unsigned int w[8], R[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const int off = ((t + q) & 7) * 4;
+                    w[t] = off < lim ? __ldg(reinterpret_cast<const unsigned int*>(src + off)) : 0u;
+                }
+#pragma unroll
+                for (int t = 0; t < 8; ++t) R[t] = __funnelshift_r(w[t], w[(t + 1) & 7], sh);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int f = (j + lane) & 31;
+                    if (f >= nf_here) continue;
+                    const unsigned int code = (R[j >> 2] >> ((j & 3) * 8)) & 0xffu;
+                    const int cell = static_cast<int>(code) * 32 + f;
+                    atomicAdd(&pLo[cell], lo);
+                    atomicAdd(&pHi[cell], hi);
+                    atomicAdd(&pCn[cell], inc);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < kCells; ++c) {
+            const int cell = threadIdx.x + c * kHistThreads;
+            accG[c] += static_cast<long long>(static_cast<int>(pHi[cell])) * (1ll << kLoBits) + pLo[cell];
+            const unsigned int cn = pCn[cell];
+            accC1[c] += cn & 0xffffu;
+            accC2[c] += cn >> 16;
+            pLo[cell] = pHi[cell] = pCn[cell] = 0u;
+        }
+        __syncthreads();
+    }
+
+    const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale));
+    const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * goss_scale * hscale));
+#pragma unroll
+    for (int c = 0; c < kCells; ++c) {
+        const int cell = threadIdx.x + c * kHistThreads;
+        const int b = cell >> 5, f = cell & 31;
+        const unsigned int cn = accC1[c] + accC2[c];
+        if (f >= nf_here || cn == 0u) continue;
+        const size_t o = static_cast<size_t>(fg0 + f) * kBins + b;
+        atomicAdd(reinterpret_cast<unsigned long long*>(G) + o, static_cast<unsigned long long>(accG[c]));
+        atomicAdd(reinterpret_cast<unsigned long long*>(H) + o,
+                  static_cast<unsigned long long>(accC1[c]) * hq1 + static_cast<unsigned long long>(accC2[c]) * hq2);
+        atomicAdd(C + o, static_cast<int>(cn));
+    }
+}
+
+__global__ void __launch_bounds__(kHistThreads)
+    hist_node_const_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0, int32_t* rows1,
+                           const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st, int node,
+                           const double* __restrict__ g, const uint8_t* __restrict__ goss_flag, double goss_scale,
+                           HistSlotPtrs hs, unsigned long long* rows_counter) {
+    if (st->done) return;
+    const int nd = node >= 0 ? node : st->small_node;
+    const DevNode& N = nodes[nd];
+    const int32_t* rows = (N.buf ? rows1 : rows0) + N.start;
+    if (rows_counter != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        atomicAdd(rows_counter, static_cast<unsigned long long>(N.count));
+    hist_const_body(codes, stride, n_f, rows, N.count, g, goss_flag, goss_scale, st->gscale, st->hscale,
+                    hs.G + nd * hs.slot_elems, hs.H + nd * hs.slot_elems, hs.C + nd * hs.slot_elems);
+}
+
 template <bool kConstH>
 __global__ void __launch_bounds__(kHistThreads)
     hist_node_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0,
@@ -253,12 +387,15 @@ __global__ void scales_reduce_kernel(const int32_t* __restrict__ rows, const dou
     }
 }
 
+// Largest shift with count * max_abs * 2^s < 2^62 (no sum can overflow) and
+// max_abs * 2^s < 2^37 (one row's value fits the split low/high words of
+// hist_const_body); the per-row resolution is then 2^-37 of the largest |value| or finer.
 __device__ int shift_for(double max_abs, int count) {
     if (!(max_abs > 0.0) || count <= 0) return 0;
     int clog = 0;
     while ((1ll << clog) < static_cast<long long>(count)) ++clog;
     const int e = ilogb(max_abs);
-    int s = 61 - (e + 1) - clog;
+    int s = min(61 - (e + 1) - clog, 36 - e);
     return max(-1000, min(1000, s));
 }
 
@@ -295,9 +432,9 @@ void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const*
                       int grid_rows, unsigned long long* rows_counter, bool const_h, cudaStream_t s) {
     dim3 grid((n_f + kFG - 1) / kFG, max(1, grid_rows));
     if (const_h) {
-        set_smem(hist_node_kernel<true>, hist_smem(true));
-        hist_node_kernel<true><<<grid, kHistThreads, hist_smem(true), s>>>(
-            codes, stride, n_f, rows[0], rows[1], nodes, st, node, g, h, goss_flag, goss_scale, hs, rows_counter);
+        set_smem(hist_node_const_kernel, kConstSmem);
+        hist_node_const_kernel<<<grid, kHistThreads, kConstSmem, s>>>(codes, stride, n_f, rows[0], rows[1], nodes, st,
+                                                                      node, g, goss_flag, goss_scale, hs, rows_counter);
     } else {
         set_smem(hist_node_kernel<false>, hist_smem(false));
         hist_node_kernel<false><<<grid, kHistThreads, hist_smem(false), s>>>(

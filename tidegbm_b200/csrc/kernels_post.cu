@@ -14,9 +14,9 @@
 // consecutive distinct cuts form a segment.  apply_accum sums (g, h, 1) per
 // (segment, leaf) in exact 64-bit fixed point (one shift per tree from max |g|,
 // max h over all rows); finalize turns segment sums into prefix sums per bucket.
-// CTAs own segment-aligned row chunks, so each CTA accumulates into one segment: the
-// chunk's rows are staged into shared memory with coalesced 16-byte loads (one
-// contiguous block of rows x stride bytes) and each thread walks one row.
+// CTAs own segment-aligned row chunks, so each CTA accumulates into one segment in
+// shared memory (32-bit atomics) and adds its totals to the segment with one global
+// 64-bit atomic per leaf and value.
 #include "tgb_internal.h"
 
 namespace tgb {
@@ -76,7 +76,6 @@ __global__ void __launch_bounds__(kApplyThreads)
                        const double* __restrict__ h, const int4* __restrict__ chunks,
                        const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
                        unsigned long long* __restrict__ seg_sums) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
     __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes];
     // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
@@ -94,40 +93,25 @@ __global__ void __launch_bounds__(kApplyThreads)
     }
     const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
     const double gs = sc->gscale, hs = sc->hscale;
-    uint8_t* tile = smem_raw;
-    const int vec_per_row = stride / 16;
-    // Shared pitch of stride + 4 bytes: (stride/4 + 1) is odd, so the 32 lanes walking 32
-    // consecutive rows read 32 different banks at any feature offset.
-    const int pitch = stride + 4;
     __syncthreads();
-    for (int t0 = ch.y; t0 < ch.z; t0 += kApplyThreads) {
-        const int rows_here = min(kApplyThreads, ch.z - t0);
-        const uint4* src = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(t0) * stride);
-        for (int v = threadIdx.x; v < rows_here * vec_per_row; v += blockDim.x) {
-            const uint4 val = __ldg(src + v);
-            uint32_t* d = reinterpret_cast<uint32_t*>(tile + (v / vec_per_row) * pitch + (v % vec_per_row) * 16);
-            d[0] = val.x;
-            d[1] = val.y;
-            d[2] = val.z;
-            d[3] = val.w;
+    // Each thread walks its rows straight from the row-major codes: a row is one 128-byte
+    // line at most, so the walk's byte loads hit the same line (L1) after the first
+    // touch; g and h are loaded before the walk so their latency overlaps it.
+    for (int r = ch.y + threadIdx.x; r < ch.z; r += blockDim.x) {
+        const double gv = g[r], hv = h[r];
+        const uint8_t* row = codes + static_cast<size_t>(r) * stride;
+        int k = 0;
+        while (!s_leaf[k]) {
+            const int b = __ldg(row + s_feat[k]);
+            const bool left = b == 0 ? s_ml[k] != 0 : b <= s_thr[k];
+            k = left ? s_left[k] : s_right[k];
         }
-        __syncthreads();
-        if (threadIdx.x < rows_here) {
-            const int r = t0 + threadIdx.x;
-            const uint8_t* row = tile + threadIdx.x * pitch;
-            int k = 0;
-            while (!s_leaf[k]) {
-                const int b = row[s_feat[k]];
-                const bool left = b == 0 ? s_ml[k] != 0 : b <= s_thr[k];
-                k = left ? s_left[k] : s_right[k];
-            }
-            nid[r] = static_cast<int16_t>(k);
-            add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(g[r] * gs)));
-            add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(h[r] * hs)));
-            atomicAdd(&aC[k], 1u);
-        }
-        __syncthreads();
+        nid[r] = static_cast<int16_t>(k);
+        add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
+        add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
+        atomicAdd(&aC[k], 1u);
     }
+    __syncthreads();
     unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         if (aC[k] == 0u) continue;
@@ -269,16 +253,8 @@ void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, 
                         cudaStream_t s) {
     check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
           "seg sums reset");
-    const size_t smem = static_cast<size_t>(kApplyThreads) * (stride + 4);
-    static int configured = 0;
-    if (static_cast<int>(smem) > configured) {
-        check(cudaFuncSetAttribute(apply_accum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(smem)),
-              "apply smem attr");
-        configured = static_cast<int>(smem);
-    }
-    apply_accum_kernel<<<n_chunks, kApplyThreads, smem, s>>>(codes, stride, nodes, st, g, h, chunks, sc, nid,
-                                                             seg_sums);
+    apply_accum_kernel<<<n_chunks, kApplyThreads, 0, s>>>(codes, stride, nodes, st, g, h, chunks, sc, nid,
+                                                          seg_sums);
     check(cudaGetLastError(), "apply_accum launch");
 }
 

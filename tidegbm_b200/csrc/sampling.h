@@ -133,9 +133,29 @@ inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
     }
 }
 
+// Number of leading words of w[0..k) (a multiple of 16) whose draws take Lemire's fast
+// path: word j paired with range r0 + j has (w * r mod 2^32) >= r, so it consumes no
+// extra word.  One wrapping 32-bit multiply and compare per word; vectorised.
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
+__attribute__((target_clones("avx512f", "avx2", "default")))
+#endif
+inline int clean_prefix(const uint32_t* __restrict__ w, uint32_t r0, int k) {
+    int done = 0;
+    while (done + 16 <= k) {
+        uint32_t flag = 0;
+        for (int l = 0; l < 16; ++l) {
+            const uint32_t r = r0 + static_cast<uint32_t>(done + l);
+            flag |= static_cast<uint32_t>(w[done + l] * r < r);
+        }
+        if (flag) break;
+        done += 16;
+    }
+    return done;
+}
+
 // Advances rng exactly as std::shuffle of m elements does, without producing positions.
 // A draw consumes extra words only when its first product's low half is below the
-// range (probability range / 2^32), so whole groups of 8 consecutive words are tested
+// range (probability range / 2^32), so whole groups of 16 consecutive words are tested
 // at once and only a group containing such a word is replayed draw by draw.
 inline void skip_shuffle(int64_t m, Mt32& rng) {
     if (m <= 0) return;
@@ -149,24 +169,13 @@ inline void skip_shuffle(int64_t m, Mt32& rng) {
         if (rng.pos >= 624) rng.refill();
         const int avail = 624 - rng.pos;
         const int64_t left = m - i;
-        int k = static_cast<int>(std::min<int64_t>(avail, left));
-        int done = 0;
-        while (done + 8 <= k) {
-            const uint32_t* w = rng.out + rng.pos + done;
-            const uint32_t r0 = static_cast<uint32_t>(i + done + 1);
-            uint32_t flag = 0;
-            for (int l = 0; l < 8; ++l) {
-                const uint32_t r = r0 + static_cast<uint32_t>(l);
-                flag |= static_cast<uint32_t>(static_cast<uint32_t>(static_cast<uint64_t>(w[l]) * r) < r);
-            }
-            if (flag) break;
-            done += 8;
-        }
+        const int k = static_cast<int>(std::min<int64_t>(avail, left));
+        const int done = clean_prefix(rng.out + rng.pos, static_cast<uint32_t>(i + 1), k);
         rng.pos += done;
         i += done;
         if (done == k) continue;  // block exhausted or m reached
-        // Replay up to 8 draws exactly (one of them may consume extra words).
-        const int64_t stop = std::min<int64_t>(m, i + 8);
+        // Replay up to 16 draws exactly (one of them may consume extra words).
+        const int64_t stop = std::min<int64_t>(m, i + 16);
         for (; i < stop; ++i) (void)bounded(rng, static_cast<uint32_t>(i + 1));
     }
 }

@@ -222,10 +222,11 @@ class Booster:
         return out
 
     def fit_stats(self) -> dict:
-        o = np.zeros(14)
+        o = np.zeros(18)
         check(lib().tgb_fit_stats(self._h, _ptr(o)))
         keys = ["total", "sort", "bin_fit", "upload_transform", "trees", "download", "host_rng", "kernel_launches",
-                "timed_ms", "timed_trees", "timed_launches", "hist_ms", "hist_launches", "hist_rows"]
+                "timed_ms", "timed_trees", "timed_launches", "hist_ms", "hist_launches", "hist_rows", "alloc", "h2d",
+                "transpose", "goss_producer"]
         return dict(zip(keys, o.tolist()))
 
     def build_hist_gpu(self, xb: np.ndarray, idx: np.ndarray, g: np.ndarray, h: np.ndarray, n_bins: int) -> np.ndarray:
