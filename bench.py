@@ -219,8 +219,8 @@ def plain_gpu_hist(native, X32, edges, n_edges, idx, g, h, n_bins) -> dict | Non
     native.check(native.lib().tgb_bin_transform(C.c_void_p(Xd.data_ptr()), 0, n, nf, C.c_void_p(Ed.data_ptr()),
                                                 C.c_void_p(ned.data_ptr()), C.c_void_p(codes.data_ptr()), stride,
                                                 None))
-    del Xd
     torch.cuda.synchronize()
+    del Xd
     xb16 = np.ascontiguousarray(codes[:, :nf].cpu().numpy().astype(np.uint16))
     out = np.zeros(nf * n_bins * 3)
     bytes_alg = idx.size * (nf + 16)

@@ -64,3 +64,19 @@ def test_host_binner_matches_oracle(native, oracle, dtype, bin_sample):
     assert nb1 == nb2
     assert np.array_equal(n1, n2)
     assert np.array_equal(e1, e2)
+
+
+def test_host_binner_matches_reference_fixture(native):
+    """tgb_binner_fit (the host part of binning) against the reference's own edges."""
+    import os
+
+    d = np.load(os.path.join(ROOT, "tests", "golden", "binner.npz"))
+    X = np.ascontiguousarray(d["X"])
+    n, nf = X.shape
+    e = np.zeros(nf * 256)
+    ne = np.zeros(nf, np.int32)
+    nb = native.lib().tgb_binner_fit(X.ctypes.data_as(C.c_void_p), 1, n, nf, int(d["max_bin"]), int(d["bin_sample"]),
+                                     int(d["seed"]), e.ctypes.data_as(C.c_void_p), ne.ctypes.data_as(C.c_void_p))
+    assert nb == int(d["max_bins"])
+    assert np.array_equal(ne, d["n_edges"])
+    assert np.array_equal(e.reshape(nf, 256), d["edges"])

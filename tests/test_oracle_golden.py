@@ -1,0 +1,98 @@
+"""The oracle restatement (oracle/oracle.cpp) against golden fixtures produced by the
+reference core itself (tests/golden/make_golden.py).  Everything is bit-exact: the
+oracle follows the reference's FP64 statement order and calls the same libstdc++
+sampling routines."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name), allow_pickle=False)
+
+
+def test_binner_matches_reference(oracle):
+    d = load("binner.npz")
+    X = np.ascontiguousarray(d["X"])
+    n, nf = X.shape
+    edges = np.zeros(nf * 256)
+    ne = np.zeros(nf, np.int32)
+    nbc = np.zeros(nf, np.int32)
+    L = oracle.oracle_lib()
+    mb = L.orc_binner_fit(X, n, nf, int(d["max_bin"]), int(d["bin_sample"]), int(d["seed"]), edges, ne, nbc)
+    assert mb == int(d["max_bins"])
+    assert np.array_equal(ne, d["n_edges"])
+    assert np.array_equal(nbc, d["n_bins_col"])
+    assert np.array_equal(edges.reshape(nf, 256), d["edges"])
+    codes = np.zeros(n * nf, np.uint8)
+    L.orc_bin_transform(X, n, nf, edges, ne, codes, nf)
+    assert np.array_equal(codes.reshape(n, nf), d["codes"].astype(np.uint8))
+
+
+def test_histogram_matches_reference(oracle):
+    d = load("hist.npz")
+    codes = np.ascontiguousarray(d["codes"].astype(np.uint8))
+    n, nf = codes.shape
+    nb = int(d["n_bins"])
+    out = np.zeros(nf * nb * 3)
+    oracle.oracle_lib().orc_build_hist(codes, nf, nf, d["idx"], d["idx"].size, d["g"], d["h"], nb, out)
+    assert np.array_equal(out.reshape(nf, nb, 3), d["hist"])
+
+
+def test_split_scan_matches_reference(oracle):
+    d = load("hist.npz")
+    s = load("split.npz")
+    hist = np.ascontiguousarray(d["hist"].reshape(-1))
+    nf = d["hist"].shape[0]
+
+    class S(C.Structure):
+        _fields_ = [("gain", C.c_double), ("feature", C.c_int), ("threshold_bin", C.c_int),
+                    ("missing_go_left", C.c_int)]
+
+    L = oracle.oracle_lib()
+    L.orc_best_numeric.restype = S
+    L.orc_best_numeric.argtypes = [np.ctypeslib.ndpointer(np.float64, flags="C"), C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_int, C.c_double]
+    for f in range(nf):
+        r = L.orc_best_numeric(hist, int(d["n_bins"]), f, float(s["l2"]), float(s["gamma"]), int(s["min_leaf"]),
+                               float(s["min_hess"]))
+        assert r.threshold_bin == s["threshold"][f]
+        assert r.missing_go_left == s["missing_left"][f]
+        assert r.gain == s["gain"][f]
+
+
+def test_pairwise_gradients_match_reference(oracle):
+    d = load("pairwise.npz")
+    m = d["y"].size
+    g = np.zeros(m)
+    h = np.zeros(m)
+    grp = np.ascontiguousarray(d["groups"])
+    L = oracle.oracle_lib()
+    L.orc_grad_hess(5, d["y"], d["pred"], grp.ctypes.data_as(C.c_void_p), m, g, h)
+    assert np.array_equal(g, d["g"]) and np.array_equal(h, d["h"])
+    assert L.orc_loss(5, d["y"], d["pred"], grp.ctypes.data_as(C.c_void_p), m) == float(d["loss"])
+
+
+@pytest.mark.parametrize("name", ["fit_mse", "fit_pair"])
+def test_fit_matches_reference(oracle, name):
+    d = load(f"{name}.npz")
+    params = eval(str(d["params"]))  # the fixture's own dict literal
+    res, h = oracle.oracle_fit(params, d["X"].astype(np.float64), d["y"], d["ts"], d["entity"])
+    try:
+        assert len(res.trees) == int(d["n_trees"])
+        assert res.n_bins == int(d["n_bins"]) and res.n_buckets == int(d["n_buckets"])
+        assert res.init_score == float(d["init_score"])
+        assert np.array_equal(res.init_prefix, d["init_prefix"])
+        assert np.array_equal(res.evals_train, d["evals"])
+        for t, tr in enumerate(res.trees):
+            for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
+                        "value", "gain", "values", "cover", "prefix"):
+                assert np.array_equal(getattr(tr, fld), d[f"t{t}_{fld}"]), (t, fld)
+        pr = oracle.oracle_predict(h, d["X"][:500].astype(np.float64))
+        assert np.array_equal(pr, d["pred"])
+    finally:
+        oracle.oracle_free(h)

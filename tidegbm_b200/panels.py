@@ -120,8 +120,9 @@ def panel_scale(n_dates: int = 5000, n_entities: int = 2000, n_features: int = 1
     """Scale: N(0,1) columns mixed with log-normal (sigma = 1) columns (every fourth
     column), 1% NaN; y = 16-sparse linear + 0.1 sin(x_k) + N(0,1), demeaned."""
     rng0 = np.random.default_rng([seed, 10**6])
-    support = rng0.choice(n_features, 16, replace=False)
-    w = rng0.standard_normal(16)
+    n_support = min(16, n_features)
+    support = rng0.choice(n_features, n_support, replace=False)
+    w = rng0.standard_normal(n_support)
     k_sin = int(rng0.integers(n_features))
     lognorm = (np.arange(n_features) % 4) == 3
     sizes = np.full(n_dates, n_entities, dtype=np.int64)
