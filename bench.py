@@ -297,7 +297,7 @@ def run_ours(args) -> None:
     del wb
 
     n_est = max(PARAMS["n_estimators"], W + K)
-    b = native.Booster(device=local, **dict(PARAMS, n_estimators=n_est, timing_from=W))
+    b = native.Booster(device=local, **dict(PARAMS, n_estimators=n_est, timing_from=W, timing_to=W + K))
     launches0 = native.kernel_launches()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
@@ -306,7 +306,8 @@ def run_ours(args) -> None:
         e2e_wall = time.perf_counter() - t0
     st = b.fit_stats()
     timed_ms = st["timed_ms"]
-    # timed trees are trees W .. n_est-1; K of them are the bench's steps
+    # timed trees are exactly trees W .. W+K-1 (the bench's K steps)
+    assert int(st["timed_trees"]) == K, st
     ms_per_tree = timed_ms / st["timed_trees"]
     times = torch.tensor([ms_per_tree], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -325,7 +326,8 @@ def run_ours(args) -> None:
            "breakdown_s": {k: st[k] for k in ("sort", "bin_fit", "upload_transform", "alloc", "h2d", "transpose",
                                               "trees", "download", "host_rng", "goss_producer")}}
     # Histogram GB/s: short fit with events around every histogram launch.
-    bp = native.Booster(device=local, **dict(PARAMS, n_estimators=W + 2, timing_from=W, profile_hist=1))
+    bp = native.Booster(device=local, **dict(PARAMS, n_estimators=W + 2, timing_from=W, timing_to=W + 2,
+                                             profile_hist=1))
     bp.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
     sp = bp.fit_stats()
     del bp
@@ -341,7 +343,7 @@ def run_ours(args) -> None:
             traffic = None
     roof = {"bound": "hbm", "achieved": hist_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": (hist_gbs / pk["hbm_gbs"]) if hist_gbs else None, "traffic": traffic,
-            "peak_source": pk["source"], "kernel": "hist_node_kernel<16>",
+            "peak_source": pk["source"], "kernel": "hist_node_const_kernel",
             "launches": sp["hist_launches"], "avg_launch_ms": sp["hist_ms"] / max(1, sp["hist_launches"]),
             "algorithmic_bytes": "rows x (128 code bytes + 16 B f64 g,h) per built node"}
     line = {"metric": METRIC, "value": value, "unit": "trees/s", "n_gpus": world, "steps": K, "warmup": W,
@@ -351,7 +353,7 @@ def run_ours(args) -> None:
                        "timed_trees": int(st["timed_trees"]), "l2": "inputs larger than L2 (1.28 GB codes)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "hist_gbs": hist_gbs, "roofline": roof, "e2e": e2e,
-            "gpu_launches": int(st["timed_launches"] * K / max(1, st["timed_trees"])),
+            "gpu_launches": int(st["timed_launches"]),
             "gpu_launches_note": "this library's kernels per K timed trees (+ CUB radix-sort passes inside GOSS)",
             "clocks": clk.summary()}
     if rank == 0 and not args.no_baselines:

@@ -77,13 +77,18 @@ TGB_API int tgb_tree_export(tgb_booster* b, int tree, int* inodes, double* fnode
 /* Bin edges of feature f (Binner::edges, cpp/include/tidegbm/binning.hpp:15); returns
  * the count, copies them when out != NULL. */
 TGB_API int tgb_edges(tgb_booster* b, int f, double* out);
-/* Breakdown of the last fit (17 values): wall seconds {total, sort, bin_fit,
+/* Breakdown of the last fit (18 values): wall seconds {total, sort, bin_fit,
  * upload+transform, trees, download, host_rng}, kernel_launches, then the timed range
- * set by the int keys "timing_from" (first timed tree) and "profile_hist":
+ * set by the int keys "timing_from" / "timing_to" (trees [from, to); to < 0: through the
+ * last tree) and "profile_hist":
  * {device ms (CUDA events), trees, kernel launches, histogram-kernel ms, histogram
  * launches, rows histogrammed}, then wall seconds {device allocation, X/y H2D,
  * column-major copy, GOSS draw producer}. */
 TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
+/* One value of the last fit's breakdown by name (wall seconds): "total", "bin_fit",
+ * "bin_counts", "bin_draws", "bin_edges" (the device binner's stages), "h2d", "alloc",
+ * "transpose", "trees".  Unknown names return -1. */
+TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);
 
 /* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:
  * quantile edges from the bin_sample values std::shuffle(mt19937(seed + f*2654435761))
@@ -91,6 +96,14 @@ TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
  * n_edges_out [n_features].  Returns Binner::max_bins() (binning.cpp:130-134) or -1. */
 TGB_API int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
                            unsigned seed, double* edges_out, int* n_edges_out);
+
+/* Binner::fit on X in device memory (row-major n x n_features of x_dtype, on `stream`):
+ * the same edges as tgb_binner_fit, with the non-NaN counts, the value gather, the
+ * sample sort and the edge arithmetic as kernels; only the kept ranks of the shuffle are
+ * drawn on the host.  edges_out / n_edges_out are host arrays as in tgb_binner_fit.
+ * Requires n_features * min(bin_sample, n) < 2^31.  Returns max_bins() or -1. */
+TGB_API int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
+                                  unsigned seed, double* edges_out, int* n_edges_out, void* stream);
 
 /* The first `keep` elements of std::shuffle(iota(m), std::mt19937(seed)) (libstdc++),
  * computed without materialising the range — the GOSS and bin-sample draw

@@ -31,7 +31,8 @@ def test_no_internal_symbols_exported(native):
 
 
 @pytest.mark.parametrize("m,keep,seed", [(1, 1, 0), (10, 3, 1), (1000, 1000, 2), (65535, 100, 3), (65536, 100, 4),
-                                         (65537, 65537, 5), (300000, 26214, 6), (1_000_000, 100_000, 7)])
+                                         (65537, 65537, 5), (300000, 26214, 6), (1_000_000, 100_000, 7),
+                                         (3_000_000, 262_144, 8), (100_000, 0, 9), (2_000_000, 1, 10)])
 def test_shuffled_prefix_equals_std_shuffle(native, oracle, m, keep, seed):
     got = np.zeros(keep, np.int32)
     native.check(native.lib().tgb_shuffled_prefix(m, keep, seed, got.ctypes.data_as(C.c_void_p)))

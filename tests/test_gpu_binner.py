@@ -1,0 +1,101 @@
+"""Device quantile binning (tgb_binner_fit_device) against the oracle's Binner::fit
+and the reference's own edges (tests/golden/binner.npz).  Bit-exact edges.
+
+Cases follow the branches of Binner::fit / quantile_edges (cpp/src/binning.cpp:14-102):
+  more non-NaN values than bin_sample (the shuffled sample; both the libstdc++
+  pairs path below 2^16 values and the one-draw path above), at most bin_sample
+  (every value), a column with no values (edges {0.0}), few distinct values (the
+  values are the edges), heavy duplicates, and bin_sample <= 0 (no sampling).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _device_edges(native, X, max_bin, bin_sample, seed):
+    n, nf = X.shape
+    Xt = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    torch.cuda.synchronize()
+    e = np.zeros(nf * 256)
+    ne = np.zeros(nf, np.int32)
+    nb = native.lib().tgb_binner_fit_device(C.c_void_p(Xt.data_ptr()), 0 if X.dtype == np.float32 else 1, n, nf,
+                                            max_bin, bin_sample, seed, e.ctypes.data_as(C.c_void_p),
+                                            ne.ctypes.data_as(C.c_void_p), None)
+    torch.cuda.synchronize()
+    del Xt
+    assert nb > 0, native.lib().tgb_last_error()
+    return nb, e.reshape(nf, 256), ne
+
+
+def _oracle_edges(oracle, X, max_bin, bin_sample, seed):
+    n, nf = X.shape
+    e = np.zeros(nf * 256)
+    ne = np.zeros(nf, np.int32)
+    nbc = np.zeros(nf, np.int32)
+    nb = oracle.oracle_lib().orc_binner_fit(np.ascontiguousarray(X, dtype=np.float64), n, nf, max_bin, bin_sample,
+                                            seed, e, ne, nbc)
+    return nb, e.reshape(nf, 256), ne
+
+
+def _panel(n, nf, seed, dtype):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, nf)).astype(dtype)
+    X[:, 1] = np.round(X[:, 1])            # few distinct values: edges = the values
+    X[:, 2] = np.exp(X[:, 2] * 2)          # skewed
+    if nf > 4:
+        X[:, 4] = np.nan                   # no values: edges {0.0}
+    if nf > 5:
+        X[:, 5] = np.round(X[:, 5] * 40)   # ~300 distinct values, heavy duplicates
+    if nf > 6:
+        X[: n // 2, 6] = np.nan            # half missing: fewer values than bin_sample for small n
+    X[rng.random((n, nf)) < 0.02] = np.nan
+    return X
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("n,bin_sample", [(80000, 20000), (30000, 12000), (5000, 262144), (120000, 0),
+                                          (300000, 262144)])
+def test_device_binner_matches_oracle(oracle, native, dtype, n, bin_sample):
+    X = _panel(n, 12, 11 + n % 7, dtype)
+    nb1, e1, n1 = _device_edges(native, X, 255, bin_sample, 42)
+    nb2, e2, n2 = _oracle_edges(oracle, X, 255, bin_sample, 42)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1, e2)
+
+
+@pytest.mark.parametrize("max_bin", [8, 64, 256])
+def test_device_binner_max_bin(oracle, native, max_bin):
+    X = _panel(70000, 7, 3, np.float32)
+    nb1, e1, n1 = _device_edges(native, X, max_bin, 50000, 5)
+    nb2, e2, n2 = _oracle_edges(oracle, X, max_bin, 50000, 5)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1, e2)
+
+
+def test_device_binner_matches_reference_fixture(native):
+    d = np.load(os.path.join(ROOT, "tests", "golden", "binner.npz"))
+    X = np.ascontiguousarray(d["X"])
+    nb, e, ne = _device_edges(native, X, int(d["max_bin"]), int(d["bin_sample"]), int(d["seed"]))
+    assert nb == int(d["max_bins"])
+    assert np.array_equal(ne, d["n_edges"])
+    assert np.array_equal(e, d["edges"])
+
+
+def test_device_binner_wide_features(oracle, native):
+    """More features than one CTA's 128 threads (grid y > 1) and a ragged row count."""
+    X = _panel(9001, 300, 8, np.float32)
+    nb1, e1, n1 = _device_edges(native, X, 255, 4000, 77)
+    nb2, e2, n2 = _oracle_edges(oracle, X, 255, 4000, 77)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1, e2)

@@ -85,6 +85,37 @@ def test_fit_goss_lognormal_nan(native, oracle):
         oracle.oracle_free(h)
 
 
+def test_fit_goss_two_feature_groups_ragged(native, oracle):
+    """GOSS mse with 40 features: two 32-feature histogram groups, the second holding 8
+    features in a 16-byte tail of the 48-byte code row; row count not a multiple of 32."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_scale(n_dates=41, n_entities=1333, n_features=40, seed=7)
+    params = dict(n_estimators=6, learning_rate=0.1, max_depth=7, max_leaves=40, horizon=3, objective="mse", goss=1,
+                  random_state=3, bin_sample=30000, pair_splits=False)
+    gpu, ref, h = _fit_both(native, oracle, params, p)
+    try:
+        _compare(gpu, ref)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_min_samples_leaf_stops_growth(native, oracle):
+    """Nodes too small to split (min_samples_leaf) end growth before max_leaves; the root
+    of the second fit cannot split at all (every tree is one leaf)."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_small(n_dates=50, n_entities=80, n_features=12)
+    for msl in (400, 3000):
+        params = dict(n_estimators=4, learning_rate=0.1, max_depth=6, horizon=1, objective="mse", goss=0,
+                      min_samples_leaf=msl, random_state=0, pair_splits=False)
+        gpu, ref, h = _fit_both(native, oracle, params, p)
+        try:
+            _compare(gpu, ref)
+        finally:
+            oracle.oracle_free(h)
+
+
 def test_fit_iid_float64_input(native, oracle):
     """iid mode (no TORB), float64 X, max_leaves 15, depth 4."""
     rng = np.random.default_rng(5)

@@ -4,7 +4,7 @@
 
 Objects go to tidegbm_b200/_build/; the shared library to tidegbm_b200/.
 Files whose FP64 arithmetic must follow the reference's statement order
-(split gains, pairwise gradients) are compiled with -fmad=false; host code with
+(split gains, pairwise gradients, quantile edges) are compiled with -fmad=false; host code with
 -ffp-contract=off.
 """
 from __future__ import annotations
@@ -21,7 +21,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtidegbm_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NO_FMA = {"kernels_split.cu", "kernels_obj.cu", "kernels_post.cu"}
+NO_FMA = {"kernels_split.cu", "kernels_obj.cu", "kernels_post.cu", "kernels_binfit.cu"}
 
 
 def _cuda_home() -> str:

@@ -13,8 +13,13 @@
 //   edges   (features in parallel)    quantile_edges, same FP64 statement order
 // The result is bit-identical to the reference's edges.  The device transform
 // (kernels_bin.cu) then maps X to codes.
+//
+// binner_fit_device runs the same steps on X already in device memory: the two
+// passes, the sample sort and the edge arithmetic run as kernels (kernels_binfit.cu);
+// the host only turns the non-NaN counts into kept ranks.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -22,6 +27,7 @@
 
 #include "booster.h"
 #include "sampling.h"
+#include "tgb_internal.h"
 
 namespace tgb {
 
@@ -44,6 +50,10 @@ void parallel_for(int n, int n_threads, F&& fn) {
 }
 
 inline bool is_nan(double v) { return !(v == v); }
+
+double wall_now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 template <typename T>
 inline double at(const void* X, size_t k) {
@@ -153,6 +163,120 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
 }
 
 }  // namespace
+
+bool binner_fits_device(int n, int n_f, int bin_sample) {
+    const long long cap = bin_sample > 0 ? std::min<long long>(bin_sample, n) : n;
+    return static_cast<long long>(n_f) * std::max(1LL, cap) < (1LL << 31) - 1;
+}
+
+int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
+                      std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
+                      BinFitTimes* tm) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const double t0 = wall_now();
+    const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
+    const size_t nc = static_cast<size_t>(n_chunks) * n_f;
+    DBuf<int> counts;
+    counts.alloc(nc);
+    launch_nonnan_counts(Xd, x_dtype, n, n_f, counts.p, s);
+    std::vector<int> ch(nc);
+    check(cudaMemcpyAsync(ch.data(), counts.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
+    check(cudaStreamSynchronize(s), "non-NaN counts");
+    const double t1 = wall_now();
+    // per-feature totals and the first non-NaN rank of every (chunk, feature)
+    std::vector<int64_t> m(n_f, 0);
+    std::vector<long long> base(nc);
+    for (int c = 0; c < n_chunks; ++c)
+        for (int f = 0; f < n_f; ++f) {
+            base[static_cast<size_t>(c) * n_f + f] = m[f];
+            m[f] += ch[static_cast<size_t>(c) * n_f + f];
+        }
+    std::vector<uint8_t> take_all(n_f, 1);
+    std::vector<int> kept(n_f, 0);
+    int64_t max_sampled = 0;
+    long long cap = 1;
+    for (int f = 0; f < n_f; ++f) {
+        take_all[f] = (bin_sample > 0 && m[f] > bin_sample) ? 0 : 1;
+        kept[f] = take_all[f] ? static_cast<int>(m[f]) : bin_sample;
+        if (!take_all[f]) max_sampled = std::max(max_sampled, m[f]);
+        cap = std::max<long long>(cap, kept[f]);
+    }
+    // kept ranks: the exact prefix of std::shuffle(mt19937(seed + f * 2654435761)), binning.cpp:93-97
+    std::vector<int32_t> keep;
+    if (max_sampled > 0) {
+        keep.resize(static_cast<size_t>(n_f) * bin_sample);
+        parallel_for(n_f, n_threads, [&](int f) {
+            if (take_all[f]) return;
+            Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
+            shuffled_prefix(m[f], bin_sample, rng, keep.data() + static_cast<size_t>(f) * bin_sample);
+        });
+    }
+    const double t2 = wall_now();
+    DBuf<long long> base_d;
+    base_d.alloc(nc);
+    check(cudaMemcpyAsync(base_d.p, base.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, s), "bases upload");
+    DBuf<uint8_t> take_d;
+    take_d.alloc(n_f);
+    check(cudaMemcpyAsync(take_d.p, take_all.data(), n_f, cudaMemcpyHostToDevice, s), "flags upload");
+    const long long words = max_sampled > 0 ? (max_sampled + 31) / 32 : 1;
+    DBuf<uint32_t> bits;
+    bits.alloc(static_cast<size_t>(n_f) * words);
+    DBuf<int32_t> keep_d;
+    if (max_sampled > 0) {
+        check(cudaMemsetAsync(bits.p, 0, sizeof(uint32_t) * bits.n, s), "bits reset");
+        keep_d.alloc(keep.size());
+        check(cudaMemcpyAsync(keep_d.p, keep.data(), sizeof(int32_t) * keep.size(), cudaMemcpyHostToDevice, s),
+              "kept ranks upload");
+        launch_keep_bits(keep_d.p, bin_sample, n_f, take_d.p, bits.p, words, s);
+    }
+    DBuf<int> fill;
+    fill.alloc(n_f);
+    check(cudaMemsetAsync(fill.p, 0, sizeof(int) * n_f, s), "fill reset");
+    const size_t esz = x_dtype == 0 ? sizeof(float) : sizeof(double);
+    const long long total = static_cast<long long>(n_f) * cap;
+    DBuf<unsigned char> smp_a, smp_b;
+    smp_a.alloc(static_cast<size_t>(total) * esz);
+    smp_b.alloc(static_cast<size_t>(total) * esz);
+    launch_sample_gather(Xd, x_dtype, n, n_f, base_d.p, bits.p, words, take_d.p, smp_a.p, cap, fill.p, s);
+    std::vector<int> seg(2 * static_cast<size_t>(n_f));
+    for (int f = 0; f < n_f; ++f) {
+        seg[f] = static_cast<int>(f * cap);
+        seg[n_f + f] = static_cast<int>(f * cap + kept[f]);
+    }
+    DBuf<int> seg_d, kept_d;
+    seg_d.alloc(seg.size());
+    kept_d.alloc(n_f);
+    check(cudaMemcpyAsync(seg_d.p, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice, s), "segs upload");
+    check(cudaMemcpyAsync(kept_d.p, kept.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "kept upload");
+    DBuf<unsigned char> tmp;
+    const size_t tmp_bytes = sample_sort_bytes(x_dtype, total, n_f);
+    tmp.alloc(std::max<size_t>(tmp_bytes, 16));
+    launch_sample_sort(x_dtype, smp_a.p, smp_b.p, total, n_f, seg_d.p, seg_d.p + n_f, tmp.p, tmp_bytes, s);
+    DBuf<double> ed;
+    DBuf<int> ne;
+    ed.alloc(static_cast<size_t>(n_f) * 256);
+    ne.alloc(n_f);
+    check(cudaMemsetAsync(ed.p, 0, sizeof(double) * ed.n, s), "edges reset");
+    launch_quantile_edges(x_dtype, smp_b.p, smp_a.p, cap, kept_d.p, n_f, max_bin - 1, ed.p, ne.p, s);
+    edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
+    n_edges.assign(n_f, 0);
+    std::vector<int> fill_h(n_f);
+    check(cudaMemcpyAsync(edges.data(), ed.p, sizeof(double) * edges.size(), cudaMemcpyDeviceToHost, s),
+          "edges download");
+    check(cudaMemcpyAsync(n_edges.data(), ne.p, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "edges download");
+    check(cudaMemcpyAsync(fill_h.data(), fill.p, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "fill download");
+    check(cudaStreamSynchronize(s), "quantile edges");
+    for (int f = 0; f < n_f; ++f)
+        if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");
+    if (tm) {
+        tm->counts = t1 - t0;
+        tm->draws = t2 - t1;
+        tm->edges = wall_now() - t2;
+    }
+    int mx = 2;
+    for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + 2);
+    return std::max(mx, max_bin);  // Binner::max_bins, binning.cpp:130-134
+}
 
 int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                std::vector<double>& edges, std::vector<int>& n_edges, int n_threads) {

@@ -68,23 +68,6 @@ double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-template <class T>
-struct DBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    void alloc(size_t k) {
-        release();
-        if (k) check(cudaMalloc(reinterpret_cast<void**>(&p), k * sizeof(T)), "cudaMalloc");
-        n = k;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    ~DBuf() { release(); }
-};
-
 float ceil_f32(double e) {
     float f = static_cast<float>(e);
     if (static_cast<double>(f) < e) f = std::nextafter(f, INFINITY);
@@ -115,6 +98,7 @@ struct DeviceState {
     cudaStream_t stream = nullptr;
     DBuf<uint8_t> codes, codes_col;
     DBuf<double> y, pred, g, h;
+    DBuf<long long> gq;  // per-tree packed fixed-point g (constant-hessian histograms)
     DBuf<int32_t> rows0, rows1;
     DBuf<long long> histG, histH;
     DBuf<int> histC;
@@ -122,7 +106,6 @@ struct DeviceState {
     DBuf<DevSplit> splits;
     DBuf<DevTreeState> st, st_all;
     DBuf<int> tile_counts;
-    DBuf<PartJob> job;
     DBuf<double> scan_gain;
     DBuf<int> scan_key, scan_ticket;
     DBuf<unsigned long long> keys_in, keys_out;
@@ -222,6 +205,25 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     }
     stats.t_sort = now() - t0;
 
+    // GOSS: booster.cpp:554-585 (sample = all rows since subsample = 1).  The draw
+    // positions depend only on n and the config, so the sampler's producer starts now and
+    // walks the generator while the data are uploaded and binned.
+    const int T = c.n_estimators;
+    const bool use_goss = ((c.goss > 0) || (c.goss < 0 && n >= 250000)) && c.goss_top < 1.0 && n > 64;
+    int n_top = 0, n_other = 0;
+    int64_t m_rest = 0;
+    const double goss_scale = (1.0 - c.goss_top) / std::max(c.goss_other, 1e-12);
+    std::unique_ptr<GossSampler> sampler;
+    if (use_goss) {
+        n_top = std::min(n, std::max(1, static_cast<int>(std::ceil(c.goss_top * static_cast<double>(n)))));
+        m_rest = n - n_top;
+        n_other = std::min(static_cast<int>(std::ceil(c.goss_other * static_cast<double>(n))), static_cast<int>(m_rest));
+        // The booster's generator (booster.cpp:483) is only used by GOSS and grow_tree's
+        // seed draw, so the sampler owns the whole stream.
+        sampler = std::make_unique<GossSampler>(static_cast<uint32_t>(c.random_state), m_rest, n_other, T, 8,
+                                                std::max(1, std::min(8, n_threads - 2)));
+    }
+
     // ---- TORB buckets + prefix cuts: booster.cpp:311-364 ----
     int nbk = 1;
     int64_t embargo = c.embargo;
@@ -252,13 +254,6 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         }
     }
     n_buckets = nbk;
-
-    // ---- quantile edges (host sample) ----
-    double tb = now();
-    n_bins = binner_fit(X, x_dtype, n, n_f, c.max_bin, c.bin_sample, static_cast<uint32_t>(c.random_state), edges,
-                        n_edges, n_threads);
-    n_features = n_f;
-    stats.t_binfit = now() - tb;
 
     // ---- initial predictions: booster.cpp:399-457 ----
     init_prefix.assign(nbk, 0.0);
@@ -299,7 +294,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     }
 
     // ---- device buffers ----
-    tb = now();
+    double tb = now();
     const int stride = (n_f + 15) / 16 * 16;
     const int max_nodes = 2 * c.max_leaves - 1;
     const size_t slot = static_cast<size_t>(n_f) * kBins;
@@ -308,6 +303,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     D.pred.alloc(n);
     D.g.alloc(n);
     D.h.alloc(n);
+    if (c.objective == 0) D.gq.alloc(n);
     D.rows0.alloc(n);
     D.rows1.alloc(n);
     D.histG.alloc(slot * max_nodes);
@@ -318,15 +314,13 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     D.st.alloc(1);
     const int max_tiles = (n + kPartTile - 1) / kPartTile;
     D.tile_counts.alloc(max_tiles + 1);
-    D.job.alloc(1);
     D.scan_gain.alloc(2 * scan_ctas_per_node(n_f));
     D.scan_key.alloc(2 * scan_ctas_per_node(n_f));
-    D.scan_ticket.alloc(2);
-    check(cudaMemsetAsync(D.scan_ticket.p, 0, 2 * sizeof(int), s), "ticket reset");
+    D.scan_ticket.alloc(3);
+    check(cudaMemsetAsync(D.scan_ticket.p, 0, 3 * sizeof(int), s), "ticket reset");
     D.nid.alloc(n);
     D.all_scale.alloc(1);
     D.init_prefix.alloc(nbk);
-    const int T = c.n_estimators;
     D.nodes_all.alloc(static_cast<size_t>(T) * max_nodes);
     D.st_all.alloc(T);
     D.values_all.alloc(static_cast<size_t>(T) * max_nodes);
@@ -343,6 +337,20 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         check(cudaMemcpyAsync(D.y.p, y, sizeof(double) * n, cudaMemcpyHostToDevice, s), "y upload");
         check(cudaStreamSynchronize(s), "X upload");
         stats.t_h2d = now() - tb - stats.t_alloc;
+        // ---- quantile edges: Binner::fit (binning.cpp:34-102) on the uploaded X ----
+        const double tbf = now();
+        BinFitTimes bt;
+        if (binner_fits_device(n, n_f, c.bin_sample))
+            n_bins = binner_fit_device(Xd.p, x_dtype, n, n_f, c.max_bin, c.bin_sample,
+                                       static_cast<uint32_t>(c.random_state), edges, n_edges, n_threads, s, &bt);
+        else
+            n_bins = binner_fit(X, x_dtype, n, n_f, c.max_bin, c.bin_sample, static_cast<uint32_t>(c.random_state),
+                                edges, n_edges, n_threads);
+        n_features = n_f;
+        stats.t_binfit = now() - tbf;
+        stats.t_bin_counts = bt.counts;
+        stats.t_bin_draws = bt.draws;
+        stats.t_bin_edges = bt.edges;
         DBuf<int> ne;
         ne.alloc(n_f);
         check(cudaMemcpyAsync(ne.p, n_edges.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "edges upload");
@@ -373,7 +381,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     launch_codes_transpose(D.codes.p, stride, n, n_f, D.codes_col.p, s);
     check(cudaStreamSynchronize(s), "transpose");
     stats.t_transpose = now() - ttr;
-    stats.t_upload = now() - tb;
+    stats.t_upload = now() - tb - stats.t_binfit;
 
     // TORB segments: distinct cuts split the time-sorted rows into segments; CTAs of the
     // post-tree sweep own segment-aligned chunks.
@@ -445,16 +453,8 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         D.loss_part.alloc(592);
     }
 
-    // GOSS: booster.cpp:554-585 (sample = all rows since subsample = 1).
-    const bool use_goss = ((c.goss > 0) || (c.goss < 0 && n >= 250000)) && c.goss_top < 1.0 && n > 64;
-    int n_top = 0, n_other = 0;
-    int64_t m_rest = 0;
-    const double goss_scale = (1.0 - c.goss_top) / std::max(c.goss_other, 1e-12);
-    std::unique_ptr<GossSampler> sampler;
+    // GOSS device buffers (the sample itself is set up with the sampler, above).
     if (use_goss) {
-        n_top = std::min(n, std::max(1, static_cast<int>(std::ceil(c.goss_top * static_cast<double>(n)))));
-        m_rest = n - n_top;
-        n_other = std::min(static_cast<int>(std::ceil(c.goss_other * static_cast<double>(n))), static_cast<int>(m_rest));
         D.keys_in.alloc(n);
         D.keys_out.alloc(n);
         D.vals_in.alloc(n);
@@ -463,10 +463,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         D.rest_pos.alloc(std::max(1, n_other));
         const size_t cb = goss_cub_bytes(n);
         D.cub_tmp.alloc(cb);
-        // The booster's generator (booster.cpp:483) is only used by GOSS and grow_tree's
-        // seed draw, so the sampler owns the whole stream.
-        sampler = std::make_unique<GossSampler>(static_cast<uint32_t>(c.random_state), m_rest, n_other, T, 8,
-                                                std::max(1, std::min(8, n_threads - 2)));
+        sampler->start_workers();
     }
     GossWork gw{D.keys_in.p, D.keys_out.p, D.vals_in.p, D.vals_out.p, D.cub_tmp.p, D.cub_tmp.n};
 
@@ -477,12 +474,13 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     HistSlotPtrs hs{D.histG.p, D.histH.p, D.histC.p, slot};
     ScanScratch scs{D.scan_gain.p, D.scan_key.p, D.scan_ticket.p};
     int32_t* rows[2] = {D.rows0.p, D.rows1.p};
-    const int grid_rows = hist_grid_rows(n_f, n);
+    const int grid_rows = hist_grid_rows(n_f, n, c.objective == 0);
     const double ttree = now();
 
     // Measurement hooks: events bracket the timed trees; optional event pairs bracket
     // every histogram launch in that range; a device counter adds up the rows.
     const bool timing = c.timing_from >= 0 && c.timing_from < T;
+    const int timing_end = (c.timing_to < 0 || c.timing_to > T) ? T : std::max(c.timing_to, c.timing_from + 1);
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     std::vector<cudaEvent_t> hist_ev;
     DBuf<unsigned long long> rows_counter;
@@ -493,7 +491,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         rows_counter.alloc(1);
         check(cudaMemsetAsync(rows_counter.p, 0, sizeof(unsigned long long), s), "counter reset");
         if (c.profile_hist) {
-            hist_ev.resize(static_cast<size_t>(2) * (T - c.timing_from) * c.max_leaves);
+            hist_ev.resize(static_cast<size_t>(2) * (timing_end - c.timing_from) * c.max_leaves);
             for (auto& e : hist_ev) check(cudaEventCreate(&e), "event");
         }
     }
@@ -501,7 +499,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     auto hist_launch = [&](int node, const uint8_t* flag, bool in_timed) {
         const bool prof = in_timed && c.profile_hist && hist_ev_used + 2 <= hist_ev.size();
         if (prof) check(cudaEventRecord(hist_ev[hist_ev_used], s), "event record");
-        launch_hist_node(D.codes.p, stride, n_f, rows, D.nodes.p, D.st.p, node, D.g.p, D.h.p, flag, goss_scale, hs,
+        launch_hist_node(D.codes.p, stride, n_f, rows, D.nodes.p, D.st.p, node, D.g.p, D.h.p, D.gq.p, flag, goss_scale, hs,
                          grid_rows, in_timed ? rows_counter.p : nullptr, c.objective == 0, s);
         if (prof) {
             check(cudaEventRecord(hist_ev[hist_ev_used + 1], s), "event record");
@@ -509,11 +507,16 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         }
     };
 
+    long long launches_end = 0;
     for (int t = 0; t < T; ++t) {
-        const bool in_timed = timing && t >= c.timing_from;
+        const bool in_timed = timing && t >= c.timing_from && t < timing_end;
         if (timing && t == c.timing_from) {
             check(cudaEventRecord(ev_begin, s), "event record");
             launches_begin = g_kernel_launches.load();
+        }
+        if (timing && t == timing_end) {
+            check(cudaEventRecord(ev_end, s), "event record");
+            launches_end = g_kernel_launches.load();
         }
         // gradients (booster.cpp:701)
         if (c.objective == 0) launch_grad_mse(D.y.p, D.pred.p, n, D.g.p, D.h.p, s);
@@ -528,7 +531,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
                   "positions upload");
             sampler->release(t, s);
             launch_goss_select(D.g.p, n, n_top, n_other, D.rest_pos.p, gw, D.goss_flag.p, D.rows0.p, D.tile_counts.p,
-                               D.job.p, D.st.p, s);
+                               D.st.p, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, 0, 1, s);
         } else {
             launch_iota_rows(D.rows0.p, n, s);
@@ -536,19 +539,19 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         }
         const uint8_t* flag = use_goss ? D.goss_flag.p : nullptr;
         launch_scales(D.rows0.p, D.g.p, D.h.p, flag, goss_scale, D.st.p, n, s);
+        if (c.objective == 0) launch_quantize(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, D.gq.p, n, s);
         check(cudaMemsetAsync(D.histG.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histH.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histC.p, 0, sizeof(int) * slot * max_nodes, s), "hist reset");
         // grow_tree (cpp/src/tree.cpp:283-472)
+        // Every scan launch ends with the choice of the next leaf to split, except the last.
         hist_launch(0, flag, in_timed);
-        launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 0, 0, scs, s);
+        launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 0, 0, scs, c.max_leaves > 1, s);
         for (int it = 0; it < c.max_leaves - 1; ++it) {
-            launch_select(gp, D.nodes.p, D.splits.p, D.st.p, s);
             launch_partition(D.codes.p, stride, D.codes_col.p, codes_col_pitch(n), rows, D.nodes.p, D.st.p,
-                             D.tile_counts.p, max_tiles, D.job.p, s);
+                             D.tile_counts.p, max_tiles, s);
             hist_launch(-1, flag, in_timed);
-            launch_hist_subtract(D.st.p, hs, s);
-            launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 1, 0, scs, s);
+            launch_split_scan(gp, hs, D.nodes.p, D.splits.p, D.st.p, 1, 0, scs, it < c.max_leaves - 2, s);
         }
         // post-tree sweep (booster.cpp:589-664), outputs straight into tree slot t
         double* values_t = D.values_all.p + static_cast<size_t>(t) * max_nodes;
@@ -574,15 +577,17 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         check(cudaMemcpyAsync(D.st_all.p + t, D.st.p, sizeof(DevTreeState), cudaMemcpyDeviceToDevice, s),
               "state snapshot");
     }
-    long long launches_end = g_kernel_launches.load();
-    if (timing) check(cudaEventRecord(ev_end, s), "event record");
+    if (timing && timing_end == T) {
+        check(cudaEventRecord(ev_end, s), "event record");
+        launches_end = g_kernel_launches.load();
+    }
     check(cudaStreamSynchronize(s), "tree loop");
     stats.t_trees = now() - ttree;
     if (timing) {
         float ms = 0.f;
         check(cudaEventElapsedTime(&ms, ev_begin, ev_end), "event time");
         stats.timed_ms = ms;
-        stats.timed_trees = T - c.timing_from;
+        stats.timed_trees = timing_end - c.timing_from;
         stats.timed_launches = launches_end - launches_begin;
         for (size_t k = 0; k + 1 < hist_ev_used; k += 2) {
             float hm = 0.f;

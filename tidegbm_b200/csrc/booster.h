@@ -56,9 +56,11 @@ struct Config {
     bool causal_structure = false;
     double structure_frac = 1.0;
     double entity_subsample = 1.0;
-    // Measurement hooks (no effect on results): CUDA events from tree `timing_from` to
-    // the last tree, and per-launch events around every histogram kernel in that range.
+    // Measurement hooks (no effect on results): CUDA events around trees
+    // [timing_from, timing_to) (timing_to < 0: through the last tree), and per-launch
+    // events around every histogram kernel in that range.
     int timing_from = -1;
+    int timing_to = -1;
     bool profile_hist = false;
 
     void validate() const;
@@ -80,6 +82,7 @@ struct FitStats {
     double t_total = 0, t_sort = 0, t_binfit = 0, t_upload = 0, t_transform = 0, t_trees = 0, t_download = 0;
     double t_rng = 0;
     double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
+    double t_bin_counts = 0, t_bin_draws = 0, t_bin_edges = 0;  // stages of the device binner
     int gpu_launches = 0;
     // timed range (cfg.timing_from .. last tree), device time from CUDA events
     double timed_ms = 0;
@@ -126,5 +129,15 @@ private:
 // sampled values per feature and their quantile edges.  Returns max_bins().
 int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                std::vector<double>& edges, std::vector<int>& n_edges, int n_threads);
+// The same edges from X in device memory (row-major n x n_f, stream `stream`, a
+// cudaStream_t).  binner_fits_device says whether one feature-major sample buffer of
+// the sizes involved stays under 2^31 values (else use binner_fit).
+struct BinFitTimes {
+    double counts = 0, draws = 0, edges = 0;  // wall seconds of the three stages
+};
+bool binner_fits_device(int n, int n_f, int bin_sample);
+int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
+                      std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
+                      BinFitTimes* tm);
 
 }  // namespace tgb

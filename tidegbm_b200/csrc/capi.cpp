@@ -116,6 +116,7 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "causal_bins") c.causal_bins = v != 0;
         else if (k == "causal_structure") c.causal_structure = v != 0;
         else if (k == "timing_from") c.timing_from = static_cast<int>(v);
+        else if (k == "timing_to") c.timing_to = static_cast<int>(v);
         else if (k == "profile_hist") c.profile_hist = v != 0;
         else if (k == "verbose" || k == "col_major_hist" || k == "cat_min_count") { /* no effect on GPU path */ }
         else throw tgb::TideError("unknown int key");
@@ -298,6 +299,45 @@ int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bi
     return rc == 0 ? nb : -1;
 }
 
+int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
+                          unsigned seed, double* edges_out, int* n_edges_out, void* stream) {
+    int nb = -1;
+    const int rc = guard([&] {
+        need(X && edges_out && n_edges_out, "NULL argument");
+        need(n > 0 && n_features > 0, "empty input");
+        need(x_dtype == 0 || x_dtype == 1, "x_dtype must be 0 or 1");
+        need(max_bin >= 8 && max_bin <= 256, "max_bin must be in [8, 256]");
+        need(tgb::binner_fits_device(n, n_features, bin_sample),
+             "n_features x min(bin_sample, n) must stay below 2^31 values (use tgb_binner_fit)");
+        std::vector<double> e;
+        std::vector<int> ne;
+        nb = tgb::binner_fit_device(X, x_dtype, n, n_features, max_bin, bin_sample, seed, e, ne,
+                                    static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), stream,
+                                    nullptr);
+        std::copy(e.begin(), e.end(), edges_out);
+        std::copy(ne.begin(), ne.end(), n_edges_out);
+    });
+    return rc == 0 ? nb : -1;
+}
+
+int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
+    return guard([&] {
+        need(hb && key && out, "NULL argument");
+        const tgb::FitStats& s = hb->b->stats;
+        const std::string k(key);
+        if (k == "bin_counts") *out = s.t_bin_counts;
+        else if (k == "bin_draws") *out = s.t_bin_draws;
+        else if (k == "bin_edges") *out = s.t_bin_edges;
+        else if (k == "bin_fit") *out = s.t_binfit;
+        else if (k == "h2d") *out = s.t_h2d;
+        else if (k == "alloc") *out = s.t_alloc;
+        else if (k == "transpose") *out = s.t_transpose;
+        else if (k == "trees") *out = s.t_trees;
+        else if (k == "total") *out = s.t_total;
+        else throw tgb::TideError("unknown fit stat: " + k);
+    });
+}
+
 int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out) {
     return guard([&] {
         need(m >= 0 && m < (1ll << 31) && keep >= 0 && keep <= m, "bad sizes");
@@ -353,10 +393,9 @@ int tgb_partition(const unsigned char* codes, int stride, const int* rows, int n
     return guard([&] {
         need(workspace_bytes >= tgb_partition_workspace_bytes(n_rows), "workspace too small");
         need(feature >= 0 && feature < stride, "feature out of range");
-        need(sizeof(tgb::PartJob) <= 256, "job layout");
-        char* ws = static_cast<char*>(workspace);
+        char* ws = static_cast<char*>(workspace);  // 256-byte header (reserved), then the tile counts
         tgb::launch_partition_rows(codes, stride, rows, n_rows, feature, threshold, missing_left, out, n_left_out,
-                                   reinterpret_cast<int*>(ws + 256), ws, as_stream(stream));
+                                   reinterpret_cast<int*>(ws + 256), as_stream(stream));
     });
 }
 

@@ -9,6 +9,8 @@
 //             positions (shuffled_prefix) into a pinned slot, in parallel;
 //   consumer  (the fit loop) waits for tree t, enqueues the H2D copy, records an event
 //             and releases the slot; a worker reuses a slot only after that copy ends.
+// The producer starts with the object, so it runs ahead while the fit uploads and bins
+// the data; the workers start on start_workers() (or the first wait).
 #pragma once
 
 #include <chrono>
@@ -37,8 +39,17 @@ public:
             if (cudaEventCreateWithFlags(&slot_ev_[k], cudaEventDisableTiming) != cudaSuccess)
                 throw std::runtime_error("cudaEventCreate (GOSS positions)");
         }
+        n_workers_ = std::max(1, n_workers);
         threads_.emplace_back([this, seed] { produce(seed); });
-        for (int w = 0; w < std::max(1, n_workers); ++w) threads_.emplace_back([this] { work(); });
+    }
+
+    // Starts the workers.  The producer runs from construction (it walks the stream
+    // sequentially and is the long pole); the workers can start once the host has
+    // finished its other parallel work.
+    void start_workers() {
+        if (workers_started_) return;
+        workers_started_ = true;
+        for (int w = 0; w < n_workers_; ++w) threads_.emplace_back([this] { work(); });
     }
 
     // Stops the threads (all trees consumed, or an error path) and joins them.
@@ -62,6 +73,7 @@ public:
 
     // Blocks until tree t's positions are ready; returns the pinned slot holding them.
     const int32_t* wait(int t) {
+        start_workers();
         std::unique_lock<std::mutex> lk(mu_);
         cv_.wait(lk, [&] { return ready_[t] || abort_ || !error_.empty(); });
         if (!error_.empty()) throw std::runtime_error(error_);
@@ -140,6 +152,8 @@ private:
     std::mutex mu_;
     std::condition_variable cv_;
     int next_ = 0;
+    int n_workers_ = 1;
+    bool workers_started_ = false;
     bool abort_ = false;
     std::string error_;
 };

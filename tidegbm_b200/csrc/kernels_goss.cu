@@ -51,8 +51,7 @@ size_t goss_cub_bytes(int n) {
 }
 
 void launch_goss_select(const double* g, int n, int n_top, int n_other, const int32_t* rest_pos, GossWork& w,
-                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, void* job_mem, DevTreeState* st,
-                        cudaStream_t s) {
+                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, DevTreeState* st, cudaStream_t s) {
     const int blocks = std::max(1, std::min(2368, (n + 255) / 256));
     goss_keys_kernel<<<blocks, 256, 0, s>>>(g, n, w.keys_in, w.vals_in);
     check(cudaGetLastError(), "goss_keys launch");
@@ -64,7 +63,7 @@ void launch_goss_select(const double* g, int n, int n_top, int n_other, const in
     goss_mark_kernel<<<std::max(1, std::min(2368, (n_top + n_other + 255) / 256)), 256, 0, s>>>(
         w.vals_out, n_top, n_other, rest_pos, goss_flag);
     check(cudaGetLastError(), "goss_mark launch");
-    launch_compact_flagged(goss_flag, n, rows0, &st->n_sample, tile_counts, job_mem, s);
+    launch_compact_flagged(goss_flag, n, rows0, &st->n_sample, tile_counts, s);
 }
 
 }  // namespace tgb

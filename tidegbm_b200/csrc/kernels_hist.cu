@@ -29,8 +29,11 @@
 #include "tgb_internal.h"
 
 #include <cmath>
+#include <cooperative_groups.h>
 
 namespace tgb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -162,41 +165,79 @@ __device__ __forceinline__ void hist_body(const uint8_t* __restrict__ codes, int
 
 // ---- constant-hessian histogram (mse with unit weights, the GOSS workloads) ----------
 //
-// Lane = row.  A warp takes 32 rows, one per lane; each lane loads its row's 32 code
-// bytes of the feature group once (8 x 4-byte loads, word order rotated by lane / 4,
-// then a byte funnel-shift by lane % 4), so that step j of the 32-step loop reads byte j
-// of the rotated array = the code of feature (j + lane) & 31.  All 32 lanes therefore
-// touch 32 different features, i.e. 32 different banks of the [bin][feature] layout, at
-// every step, and the row's g, GOSS flag and count increment stay in the lane's registers.
+// Lane = row.  A warp takes 32 rows, one per lane.  Each lane loads its row's 32 code
+// bytes of the feature group with two 16-byte loads and rotates them in registers by
+// `lane` bytes (a 3-stage word rotation by lane / 4, then a byte funnel-shift by
+// lane % 4), so that step j of the 32-step loop reads the code of feature
+// (j + lane) & 31.  All 32 lanes therefore touch 32 different features, i.e. 32
+// different banks of the [bin][feature] layout, at every step.  Features past the end
+// of the row read code 0 and add into cells that are never flushed, so the step loop
+// has no bounds test.
 //
-// Each row's fixed-point g (|v| < 2^37, enforced by the per-tree shift) is split into a
-// 19-bit unsigned low part and a signed high part (v >> 19).  Over at most kSub = 8192
-// rows a bin's low sum stays below 2^32 and its high sum inside int32, so three
-// fire-and-forget 32-bit shared reductions per code (low, high, packed counts c1 + c2<<16)
-// are exact.  After every kSub rows the CTA folds the three planes into per-thread 64-bit
-// register accumulators (each thread owns 8 fixed cells) and clears them.
+// Per row the kernel gathers one int64 prepared by quantize_kernel for the tree:
+// (v << 1) | s with v = rint(g * goss_factor * 2^gshift) and s = 1 for GOSS-scaled
+// rows.  v (|v| < 2^37, enforced by the per-tree shift) is split into a 19-bit unsigned
+// low part and a signed high part (v >> 19).  Over at most kSub = 8192 rows a bin's low
+// sum stays below 2^32 and its high sum inside int32, so three fire-and-forget 32-bit
+// shared reductions per code (low, high, packed counts c1 + c2<<16) are exact.  After
+// every kSub rows the CTA folds the three planes into per-thread 64-bit register
+// accumulators (each thread owns 8 fixed cells) and clears them.
 constexpr int kSub = 8192;
 constexpr int kLoBits = 19;
 constexpr int kCells = kFG * kBins / kHistThreads;  // cells owned per thread (8)
-constexpr size_t kConstSmem = static_cast<size_t>(kPlane) * 4 * 3;
 
-__device__ __forceinline__ void hist_const_body(const uint8_t* __restrict__ codes, int stride, int n_f,
-                                                const int32_t* __restrict__ rows, int count,
-                                                const double* __restrict__ g, const uint8_t* __restrict__ goss_flag,
-                                                double goss_scale, double gscale, double hscale, long long* G,
-                                                long long* H, int* C) {
+// out[t] = in[(t + k) & 7] for a lane-dependent k in [0, 8): three conditional rotations.
+__device__ __forceinline__ void rotate_words(unsigned int (&w)[8], int k) {
+    unsigned int t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = (k & 1) ? w[(i + 1) & 7] : w[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = (k & 2) ? t[(i + 2) & 7] : t[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = (k & 4) ? w[(i + 4) & 7] : w[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = t[i];
+}
+
+// The CTAs of a cluster (kCluster consecutive row chunks of one feature group) add
+// their partial histograms through distributed shared memory before the flush: each
+// CTA writes its totals (G as two words, c1, c2) into its own shared memory, and after a
+// cluster barrier CTA rank k sums cells [k, k+1) * kPlane / kCluster over the cluster and
+// issues the global atomics for them, so a launch makes kCluster times fewer global
+// atomics.  Every CTA of a cluster passes both cluster barriers: the only early exits
+// (tree done, whole cluster past the node's chunk count) are uniform over a cluster.
+constexpr int kCluster = 4;
+constexpr size_t kConstSmem = static_cast<size_t>(kPlane) * 4 * 4;  // 3 accumulation planes, then 4 total planes
+
+__global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
+    hist_node_const_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0, int32_t* rows1,
+                           const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st, int node,
+                           const long long* __restrict__ gq, double goss_scale, HistSlotPtrs hs,
+                           unsigned long long* rows_counter) {
+    if (st->done || (node < 0 && st->small_node < 0)) return;  // uniform over the grid
+    const int nd = node >= 0 ? node : st->small_node;
+    const DevNode& N = nodes[nd];
+    const int32_t* rows = (N.buf ? rows1 : rows0) + N.start;
+    const int count = N.count;
+    if (rows_counter != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        atomicAdd(rows_counter, static_cast<unsigned long long>(count));
+    long long* G = hs.G + nd * hs.slot_elems;
+    long long* H = hs.H + nd * hs.slot_elems;
+    int* C = hs.C + nd * hs.slot_elems;
+    const double hscale = st->hscale;
+
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);
     unsigned int* pHi = pLo + kPlane;
     unsigned int* pCn = pHi + kPlane;
 
+    // Row chunks: a multiple of kCluster, so whole clusters are active or idle.
     const int need = (count + kMinRowsPerCta - 1) / kMinRowsPerCta;
-    const int n_chunks = max(1, min(static_cast<int>(gridDim.y), need));
-    if (static_cast<int>(blockIdx.y) >= n_chunks) return;
+    const int n_chunks = min(static_cast<int>(gridDim.y), (max(1, need) + kCluster - 1) / kCluster * kCluster);
+    if (static_cast<int>(blockIdx.y) >= n_chunks) return;  // uniform over the cluster
     const int chunk = (count + n_chunks - 1) / n_chunks;
-    const int r0 = blockIdx.y * chunk;
+    const int r0 = min(count, static_cast<int>(blockIdx.y) * chunk);
     const int r1 = min(count, r0 + chunk);
-    if (r0 >= r1) return;
 
     {
         uint4* z = reinterpret_cast<uint4*>(smem_raw);
@@ -214,6 +255,8 @@ __device__ __forceinline__ void hist_const_body(const uint8_t* __restrict__ code
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int fg0 = blockIdx.x * kFG;
     const int nf_here = min(kFG, n_f - fg0);
+    // stride and fg0 are multiples of 16 and 32: the group has 16 or >= 32 bytes in a row
+    const bool two_chunks = stride - fg0 >= 32;
     const int q = lane >> 2, sh = (lane & 3) * 8;
     for (int s0 = r0; s0 < r1; s0 += kSub) {
         const int s1 = min(r1, s0 + kSub);
@@ -221,27 +264,22 @@ __device__ __forceinline__ void hist_const_body(const uint8_t* __restrict__ code
             const int k = base + lane;
             if (k < s1) {
                 const int r = rows[k];
-                double gv = g[r];
-                const bool sc = goss_flag != nullptr && goss_flag[r] == 2;
-                if (sc) gv *= goss_scale;
-                const long long v = __double2ll_rn(gv * gscale);
+                const long long p = gq[r];
+                const long long v = p >> 1;
                 const unsigned int lo = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
                 const unsigned int hi = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
-                const unsigned int inc = sc ? 0x10000u : 1u;
-                const uint8_t* src = codes + static_cast<size_t>(r) * stride + fg0;
-                const int lim = stride - fg0;  // bytes of this group inside the row
-                unsigned int w[8], R[8];
-#pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const int off = ((t + q) & 7) * 4;
-                    w[t] = off < lim ? __ldg(reinterpret_cast<const unsigned int*>(src + off)) : 0u;
-                }
+                const unsigned int inc = (p & 1) ? 0x10000u : 1u;
+                const uint4* src = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r) * stride + fg0);
+                const uint4 a = __ldg(src);
+                const uint4 b = two_chunks ? __ldg(src + 1) : make_uint4(0, 0, 0, 0);
+                unsigned int w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+                rotate_words(w, q);
+                unsigned int R[8];
 #pragma unroll
                 for (int t = 0; t < 8; ++t) R[t] = __funnelshift_r(w[t], w[(t + 1) & 7], sh);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int f = (j + lane) & 31;
-                    if (f >= nf_here) continue;
                     const unsigned int code = (R[j >> 2] >> ((j & 3) * 8)) & 0xffu;
                     const int cell = static_cast<int>(code) * 32 + f;
                     atomicAdd(&pLo[cell], lo);
@@ -263,35 +301,60 @@ __device__ __forceinline__ void hist_const_body(const uint8_t* __restrict__ code
         __syncthreads();
     }
 
-    const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale));
-    const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * goss_scale * hscale));
+    // This CTA's totals -> 4 planes of its shared memory.
+    unsigned int* tot = reinterpret_cast<unsigned int*>(smem_raw);
 #pragma unroll
     for (int c = 0; c < kCells; ++c) {
         const int cell = threadIdx.x + c * kHistThreads;
+        tot[cell] = static_cast<unsigned int>(accG[c]);
+        tot[kPlane + cell] = static_cast<unsigned int>(static_cast<unsigned long long>(accG[c]) >> 32);
+        tot[2 * kPlane + cell] = accC1[c];
+        tot[3 * kPlane + cell] = accC2[c];
+    }
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    // Rank k flushes its share of the cells, summed over the cluster.
+    const unsigned int rank = cluster.block_rank();
+    const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale));
+    const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * goss_scale * hscale));
+    constexpr int kShare = kPlane / kCluster;
+    for (int cell = rank * kShare + threadIdx.x; cell < static_cast<int>(rank + 1) * kShare; cell += kHistThreads) {
+        unsigned long long g = 0;
+        unsigned int c1 = 0, c2 = 0;
+#pragma unroll
+        for (int k = 0; k < kCluster; ++k) {
+            const unsigned int* rt = cluster.map_shared_rank(tot, k);
+            g += (static_cast<unsigned long long>(rt[kPlane + cell]) << 32) | rt[cell];
+            c1 += rt[2 * kPlane + cell];
+            c2 += rt[3 * kPlane + cell];
+        }
         const int b = cell >> 5, f = cell & 31;
-        const unsigned int cn = accC1[c] + accC2[c];
+        const unsigned int cn = c1 + c2;
         if (f >= nf_here || cn == 0u) continue;
         const size_t o = static_cast<size_t>(fg0 + f) * kBins + b;
-        atomicAdd(reinterpret_cast<unsigned long long*>(G) + o, static_cast<unsigned long long>(accG[c]));
+        atomicAdd(reinterpret_cast<unsigned long long*>(G) + o, g);
         atomicAdd(reinterpret_cast<unsigned long long*>(H) + o,
-                  static_cast<unsigned long long>(accC1[c]) * hq1 + static_cast<unsigned long long>(accC2[c]) * hq2);
+                  static_cast<unsigned long long>(c1) * hq1 + static_cast<unsigned long long>(c2) * hq2);
         atomicAdd(C + o, static_cast<int>(cn));
     }
+    cluster.sync();  // no CTA leaves while others read its shared memory
 }
 
-__global__ void __launch_bounds__(kHistThreads)
-    hist_node_const_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0, int32_t* rows1,
-                           const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st, int node,
-                           const double* __restrict__ g, const uint8_t* __restrict__ goss_flag, double goss_scale,
-                           HistSlotPtrs hs, unsigned long long* rows_counter) {
-    if (st->done) return;
-    const int nd = node >= 0 ? node : st->small_node;
-    const DevNode& N = nodes[nd];
-    const int32_t* rows = (N.buf ? rows1 : rows0) + N.start;
-    if (rows_counter != nullptr && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
-        atomicAdd(rows_counter, static_cast<unsigned long long>(N.count));
-    hist_const_body(codes, stride, n_f, rows, N.count, g, goss_flag, goss_scale, st->gscale, st->hscale,
-                    hs.G + nd * hs.slot_elems, hs.H + nd * hs.slot_elems, hs.C + nd * hs.slot_elems);
+// gq[r] = (rint(g[r] * goss_factor * 2^gshift) << 1) | (GOSS-scaled ? 1 : 0) for the rows
+// of the tree's sample: the same fixed-point value the general kernel computes per code.
+__global__ void quantize_kernel(const int32_t* __restrict__ rows, const double* __restrict__ g,
+                                const uint8_t* __restrict__ goss_flag, double goss_scale,
+                                const DevTreeState* __restrict__ st, long long* __restrict__ gq) {
+    const int count = st->n_sample;
+    const double gscale = st->gscale;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const int r = rows[k];
+        double gv = g[r];
+        const bool sc = goss_flag != nullptr && goss_flag[r] == 2;
+        if (sc) gv *= goss_scale;
+        const long long v = __double2ll_rn(gv * gscale);
+        gq[r] = static_cast<long long>((static_cast<unsigned long long>(v) << 1) | (sc ? 1ull : 0ull));
+    }
 }
 
 template <bool kConstH>
@@ -301,7 +364,7 @@ __global__ void __launch_bounds__(kHistThreads)
                      const DevTreeState* __restrict__ st, int node, const double* __restrict__ g,
                      const double* __restrict__ h, const uint8_t* __restrict__ goss_flag,
                      double goss_scale, HistSlotPtrs hs, unsigned long long* rows_counter) {
-    if (st->done) return;
+    if (st->done || (node < 0 && st->small_node < 0)) return;
     const int nd = node >= 0 ? node : st->small_node;
     const DevNode& N = nodes[nd];
     const int32_t* rows = (N.buf ? rows1 : rows0) + N.start;
@@ -317,20 +380,6 @@ __global__ void __launch_bounds__(kHistThreads)
                      int count, const double* __restrict__ g, const double* __restrict__ h, double gscale,
                      double hscale, long long* G, long long* H, int* C) {
     hist_body<false>(codes, stride, n_f, rows, count, g, h, nullptr, 1.0, gscale, hscale, G, H, C);
-}
-
-__global__ void hist_subtract_kernel(const DevTreeState* __restrict__ st, HistSlotPtrs hs) {
-    if (st->done) return;
-    const size_t e = hs.slot_elems;
-    const size_t p = static_cast<size_t>(st->parent) * e;
-    const size_t sm = static_cast<size_t>(st->small_node) * e;
-    const size_t lg = static_cast<size_t>(st->large_node) * e;
-    for (size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; k < e;
-         k += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        hs.G[lg + k] = hs.G[p + k] - hs.G[sm + k];
-        hs.H[lg + k] = hs.H[p + k] - hs.H[sm + k];
-        hs.C[lg + k] = hs.C[p + k] - hs.C[sm + k];
-    }
 }
 
 __global__ void tree_init_kernel(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_sample,
@@ -420,21 +469,36 @@ void set_smem(K kern, size_t bytes) {
 
 }  // namespace
 
-int hist_grid_rows(int n_f, int max_rows) {
+int hist_grid_rows(int n_f, int max_rows, bool const_h) {
     const int groups = (n_f + kFG - 1) / kFG;
     const int need = (max_rows + kMinRowsPerCta - 1) / kMinRowsPerCta;
-    return std::max(1, std::min(need, (148 + groups - 1) / groups));
+    if (!const_h) return std::max(1, std::min(need, (148 + groups - 1) / groups));
+    // Clusters that fit on the device at once, shared among the feature groups.
+    set_smem(hist_node_const_kernel, kConstSmem);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(groups, kCluster, 1);
+    cfg.blockDim = dim3(kHistThreads, 1, 1);
+    cfg.dynamicSmemBytes = kConstSmem;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, hist_node_const_kernel, &cfg) != cudaSuccess || clusters <= 0) {
+        (void)cudaGetLastError();
+        clusters = 148 / kCluster;
+    }
+    const int per_group = std::max(1, clusters / groups);
+    const int need_c = std::max(1, (need + kCluster - 1) / kCluster);
+    return std::min(per_group, need_c) * kCluster;
 }
 
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows,
                       const DevNode* nodes, const DevTreeState* st, int node, const double* g,
-                      const double* h, const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs,
-                      int grid_rows, unsigned long long* rows_counter, bool const_h, cudaStream_t s) {
+                      const double* h, const long long* gq, const uint8_t* goss_flag, double goss_scale,
+                      HistSlotPtrs hs, int grid_rows, unsigned long long* rows_counter, bool const_h,
+                      cudaStream_t s) {
     dim3 grid((n_f + kFG - 1) / kFG, max(1, grid_rows));
     if (const_h) {
         set_smem(hist_node_const_kernel, kConstSmem);
         hist_node_const_kernel<<<grid, kHistThreads, kConstSmem, s>>>(codes, stride, n_f, rows[0], rows[1], nodes, st,
-                                                                      node, g, goss_flag, goss_scale, hs, rows_counter);
+                                                                      node, gq, goss_scale, hs, rows_counter);
     } else {
         set_smem(hist_node_kernel<false>, hist_smem(false));
         hist_node_kernel<false><<<grid, kHistThreads, hist_smem(false), s>>>(
@@ -443,22 +507,23 @@ void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const*
     check(cudaGetLastError(), "hist_node launch");
 }
 
+void launch_quantize(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
+                     const DevTreeState* st, long long* gq, int max_rows, cudaStream_t s) {
+    const int blocks = std::max(1, std::min(1184, (max_rows + 255) / 256));
+    quantize_kernel<<<blocks, 256, 0, s>>>(rows, g, goss_flag, goss_scale, st, gq);
+    check(cudaGetLastError(), "quantize launch");
+}
+
 void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* rows, int n_rows,
                       const double* g, const double* h, int gshift, int hshift, long long* G,
                       long long* H, int* C, cudaStream_t s) {
     if (n_rows <= 0) return;
     set_smem(hist_rows_kernel, hist_smem(false));
-    dim3 grid((n_f + kFG - 1) / kFG, hist_grid_rows(n_f, n_rows));
+    dim3 grid((n_f + kFG - 1) / kFG, hist_grid_rows(n_f, n_rows, false));
     hist_rows_kernel<<<grid, kHistThreads, hist_smem(false), s>>>(codes, stride, n_f, rows, n_rows, g, h,
                                                            std::ldexp(1.0, gshift), std::ldexp(1.0, hshift), G, H,
                                                            C);
     check(cudaGetLastError(), "hist_rows launch");
-}
-
-void launch_hist_subtract(const DevTreeState* st, HistSlotPtrs hs, cudaStream_t s) {
-    const int blocks = static_cast<int>(std::min<size_t>(296, (hs.slot_elems + 255) / 256));
-    hist_subtract_kernel<<<blocks, 256, 0, s>>>(st, hs);
-    check(cudaGetLastError(), "hist_subtract launch");
 }
 
 void launch_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_sample_host,

@@ -3,16 +3,20 @@
 // 0 (missing) and missing_go_left, or when 0 < code <= threshold; both children
 // keep the parent's (ascending) row order.
 //
-// Three launches over fixed 2048-row tiles:
-//   count   per-tile number of left rows (warp ballot + popc)
-//   scan    one CTA: exclusive scan of the tile counts -> tile offsets, n_left;
-//           in tree mode it also fills the children's segments and picks the
-//           smaller child (left on ties, cpp/src/tree.cpp:423)
-//   scatter per tile: in-tile stable rank from ballots + a shared-memory scan over
-//           the 8 warps, rows written to the other ping-pong buffer
-// Grids are fixed (sized for the largest node) and read the job from device memory,
-// so the sequence can run without host synchronisation.  The same kernels compact
-// flagged rows (GOSS sample) in index order.
+// Two launches over fixed 2048-row tiles:
+//   count    per-tile number of left rows
+//   scatter  per tile: the tile's left offset and the node's left total from the tile
+//            counts (a block reduction; no separate scan pass), in-tile stable ranks
+//            from ballots, rows written to the other ping-pong buffer.  Block 0 also
+//            records n_left and, in tree mode, fills the children's segments and picks
+//            the smaller child (left on ties, cpp/src/tree.cpp:423).
+// A thread owns 8 rows of a tile (rows base + i*256 + tid), so each of the kernels
+// issues all its row-id loads, then all its code loads, before it waits: two memory
+// round trips per tile rather than one per 256 rows.
+// In tree mode the job (row segment, feature, threshold, missing direction) is read
+// from the node table at st->parent, so the sequence runs without host
+// synchronisation; grids are sized for the largest node and exit early.  The same
+// kernels compact flagged rows (GOSS sample) in index order.
 #include "tgb_internal.h"
 
 #include <mutex>
@@ -25,168 +29,171 @@ namespace {
 
 constexpr int kPartThreads = 256;
 constexpr int kPartWarps = kPartThreads / 32;
+constexpr int kPartPer = kPartTile / kPartThreads;  // rows per thread per tile (8)
+static_assert(kPartTile == kPartPer * kPartThreads, "tile shape");
 
-__device__ __forceinline__ int32_t job_row(const PartJob& j, int k) { return j.in ? j.in[k] : k; }
-
-__device__ __forceinline__ bool goes_left(const uint8_t* __restrict__ codes, int stride, int32_t r,
-                                          const PartJob& j) {
-    if (j.flag) return j.flag[r] != 0;
-    const int b = j.col ? j.col[static_cast<size_t>(j.feature) * j.col_n + r]
-                        : codes[static_cast<size_t>(r) * stride + j.feature];
-    return b == 0 ? j.missing_left != 0 : b <= j.threshold;
+// Resolves the job: tree mode (st != nullptr) from the node table, else the given one.
+__device__ __forceinline__ bool resolve_job(const PartJob& given, const DevNode* __restrict__ nodes,
+                                            const DevTreeState* __restrict__ st, int32_t* rows0, int32_t* rows1,
+                                            PartJob& j) {
+    j = given;
+    if (st == nullptr) return true;
+    if (st->done || st->parent < 0) return false;
+    const DevNode& P = nodes[st->parent];
+    j.in = (P.buf ? rows1 : rows0) + P.start;
+    j.out = (P.buf ? rows0 : rows1) + P.start;
+    j.count = P.count;
+    j.feature = P.feature;
+    j.threshold = P.threshold;
+    j.missing_left = P.missing_left;
+    return true;
 }
 
-__global__ void part_setup_tree_kernel(const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st,
-                                       int32_t* rows0, int32_t* rows1, const uint8_t* col, long long col_n,
-                                       PartJob* job) {
-    PartJob j{};
-    j.col = col;
-    j.col_n = col_n;
-    if (!st->done) {
-        const DevNode& P = nodes[st->parent];
-        j.in = (P.buf ? rows1 : rows0) + P.start;
-        j.out = (P.buf ? rows0 : rows1) + P.start;
-        j.count = P.count;
-        j.feature = P.feature;
-        j.threshold = P.threshold;
-        j.missing_left = P.missing_left;
+// Loads the tile's rows (8 per thread) and their left/right decisions.
+__device__ __forceinline__ void load_tile(const uint8_t* __restrict__ codes, int stride, const PartJob& j, int base,
+                                          int end, int32_t (&row)[kPartPer], bool (&left)[kPartPer]) {
+#pragma unroll
+    for (int i = 0; i < kPartPer; ++i) {
+        const int k = base + i * kPartThreads + threadIdx.x;
+        row[i] = k < end ? (j.in ? j.in[k] : k) : -1;
     }
-    j.n_tiles = (j.count + kPartTile - 1) / kPartTile;
-    *job = j;
+    int b[kPartPer];
+#pragma unroll
+    for (int i = 0; i < kPartPer; ++i) {
+        b[i] = 0;
+        if (row[i] < 0) continue;
+        if (j.flag) b[i] = j.flag[row[i]];
+        else if (j.col) b[i] = j.col[static_cast<size_t>(j.feature) * j.col_n + row[i]];
+        else b[i] = codes[static_cast<size_t>(row[i]) * stride + j.feature];
+    }
+#pragma unroll
+    for (int i = 0; i < kPartPer; ++i) {
+        if (row[i] < 0) left[i] = false;
+        else if (j.flag) left[i] = b[i] != 0;
+        else left[i] = b[i] == 0 ? j.missing_left != 0 : b[i] <= j.threshold;
+    }
+}
+
+__device__ __forceinline__ int block_sum(int v, int* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    int t = 0;
+#pragma unroll
+    for (int w = 0; w < kPartWarps; ++w) t += red[w];
+    return t;
 }
 
 __global__ void __launch_bounds__(kPartThreads)
-    part_count_kernel(const uint8_t* __restrict__ codes, int stride, const PartJob* __restrict__ jp,
+    part_count_kernel(const uint8_t* __restrict__ codes, int stride, PartJob given, const DevNode* __restrict__ nodes,
+                      const DevTreeState* __restrict__ st, int32_t* rows0, int32_t* rows1,
                       int* __restrict__ tile_counts) {
-    const PartJob j = *jp;
-    __shared__ int wsum[kPartWarps];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int t = blockIdx.x; t < j.n_tiles; t += gridDim.x) {
+    PartJob j;
+    if (!resolve_job(given, nodes, st, rows0, rows1, j)) return;
+    __shared__ int red[kPartWarps];
+    const int n_tiles = (j.count + kPartTile - 1) / kPartTile;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const int base = t * kPartTile;
         const int end = min(base + kPartTile, j.count);
+        int32_t row[kPartPer];
+        bool left[kPartPer];
+        load_tile(codes, stride, j, base, end, row, left);
         int cnt = 0;
-        for (int k = base + threadIdx.x; k < end; k += kPartThreads)
-            cnt += goes_left(codes, stride, job_row(j, k), j) ? 1 : 0;
-        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        if (lane == 0) wsum[warp] = cnt;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int s = 0;
-            for (int w = 0; w < kPartWarps; ++w) s += wsum[w];
-            tile_counts[t] = s;
-        }
-        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kPartPer; ++i) cnt += left[i] ? 1 : 0;
+        cnt = block_sum(cnt, red);
+        if (threadIdx.x == 0) tile_counts[t] = cnt;
     }
-}
-
-// One CTA of 1024 threads: exclusive scan of tile_counts in place.
-__global__ void __launch_bounds__(1024)
-    part_scan_kernel(PartJob* jp, int* __restrict__ tile_counts, DevNode* nodes, DevTreeState* st,
-                     int tree_mode) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
-    const int nt = jp->n_tiles;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < nt; base += 1024) {
-        const int k = base + threadIdx.x;
-        const int v = k < nt ? tile_counts[k] : 0;
-        int incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) warp_tot[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int w = warp_tot[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += t;
-            }
-            warp_tot[lane] = w;  // inclusive over warps
-        }
-        __syncthreads();
-        const int warp_excl = warp == 0 ? 0 : warp_tot[warp - 1];
-        if (k < nt) tile_counts[k] = carry + warp_excl + incl - v;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_tot[31];
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
-    const int n_left = carry;
-    jp->n_left = n_left;
-    if (jp->n_left_out) *jp->n_left_out = n_left;
-    if (!tree_mode || st->done) return;
-    DevNode& P = nodes[st->parent];
-    DevNode& L = nodes[P.left];
-    DevNode& R = nodes[P.right];
-    L.start = P.start;
-    L.count = n_left;
-    R.start = P.start + n_left;
-    R.count = P.count - n_left;
-    st->n_left = n_left;
-    const bool left_small = L.count <= R.count;  // cpp/src/tree.cpp:423
-    st->small_node = left_small ? P.left : P.right;
-    st->large_node = left_small ? P.right : P.left;
 }
 
 __global__ void __launch_bounds__(kPartThreads)
-    part_scatter_kernel(const uint8_t* __restrict__ codes, int stride, const PartJob* __restrict__ jp,
-                        const int* __restrict__ tile_offsets) {
-    const PartJob j = *jp;
-    __shared__ int wcnt[kPartWarps];
+    part_scatter_kernel(const uint8_t* __restrict__ codes, int stride, PartJob given, DevNode* __restrict__ nodes,
+                        DevTreeState* __restrict__ st, int32_t* rows0, int32_t* rows1,
+                        const int* __restrict__ tile_counts) {
+    PartJob j;
+    if (!resolve_job(given, nodes, st, rows0, rows1, j)) return;
+    __shared__ int red[kPartWarps];
+    __shared__ int wc[kPartPer * kPartWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    for (int t = blockIdx.x; t < j.n_tiles; t += gridDim.x) {
+    const int n_tiles = (j.count + kPartTile - 1) / kPartTile;
+    if (static_cast<int>(blockIdx.x) >= n_tiles && blockIdx.x != 0) return;
+    // node total of left rows
+    int tot = 0;
+    for (int k = threadIdx.x; k < n_tiles; k += kPartThreads) tot += tile_counts[k];
+    const int n_left = block_sum(tot, red);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (j.n_left_out) *j.n_left_out = n_left;
+        if (st != nullptr) {
+            DevNode& P = nodes[st->parent];
+            DevNode& L = nodes[P.left];
+            DevNode& R = nodes[P.right];
+            L.start = P.start;
+            L.count = n_left;
+            R.start = P.start + n_left;
+            R.count = P.count - n_left;
+            st->n_left = n_left;
+            const bool left_small = L.count <= R.count;  // cpp/src/tree.cpp:423
+            st->small_node = left_small ? P.left : P.right;
+            st->large_node = left_small ? P.right : P.left;
+        }
+    }
+    int prev_tiles = 0, left0 = 0;  // running prefix over this block's tiles
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        int part = 0;
+        for (int k = prev_tiles + threadIdx.x; k < t; k += kPartThreads) part += tile_counts[k];
+        left0 += block_sum(part, red);
+        prev_tiles = t;
         const int base = t * kPartTile;
         const int end = min(base + kPartTile, j.count);
-        const int left0 = tile_offsets[t];  // lefts before this tile
-        int run_left = 0;                   // lefts earlier in this tile
-        for (int r0 = base; r0 < end; r0 += kPartThreads) {
-            const int k = r0 + threadIdx.x;
-            const bool valid = k < end;
-            int32_t row = 0;
-            bool left = false;
-            if (valid) {
-                row = job_row(j, k);
-                left = goes_left(codes, stride, row, j);
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, left);
-            if (lane == 0) wcnt[warp] = __popc(bal);
-            __syncthreads();
-            int wexcl = 0, rtot = 0;
-            for (int w = 0; w < kPartWarps; ++w) {
-                const int c = wcnt[w];
-                if (w < warp) wexcl += c;
-                rtot += c;
-            }
-            if (valid) {
-                const int lrank = run_left + wexcl + __popc(bal & lt_mask);  // lefts before k in tile
-                if (left) {
-                    j.out[left0 + lrank] = row;
-                } else if (!j.left_only) {
-                    const int rrank = (k - base) - lrank;
-                    j.out[j.n_left + (base - left0) + rrank] = row;
-                }
-            }
-            run_left += rtot;
-            __syncthreads();
+        int32_t row[kPartPer];
+        bool left[kPartPer];
+        load_tile(codes, stride, j, base, end, row, left);
+        unsigned bal[kPartPer];
+#pragma unroll
+        for (int i = 0; i < kPartPer; ++i) {
+            bal[i] = __ballot_sync(0xffffffffu, left[i]);
+            if (lane == 0) wc[i * kPartWarps + warp] = __popc(bal[i]);
         }
+        __syncthreads();
+        // exclusive prefix of left rows over (i, warp) in tile order
+        int before = 0;
+        int excl[kPartPer];
+#pragma unroll
+        for (int i = 0; i < kPartPer; ++i) {
+            int e = before;
+            for (int w = 0; w < kPartWarps; ++w) {
+                const int c = wc[i * kPartWarps + w];
+                if (w < warp) e += c;
+                before += c;
+            }
+            excl[i] = e;
+        }
+#pragma unroll
+        for (int i = 0; i < kPartPer; ++i) {
+            if (row[i] < 0) continue;
+            const int k = base + i * kPartThreads + threadIdx.x;
+            const int lrank = excl[i] + __popc(bal[i] & lt_mask);  // lefts before k in the tile
+            if (left[i]) {
+                j.out[left0 + lrank] = row[i];
+            } else if (!j.left_only) {
+                const int rrank = (k - base) - lrank;
+                j.out[n_left + (base - left0) + rrank] = row[i];
+            }
+        }
+        __syncthreads();  // wc reuse
     }
 }
 
-__global__ void part_setup_const_kernel(PartJob j, PartJob* job) { *job = j; }
-
-void run_partition(const uint8_t* codes, int stride, PartJob* job, int* tile_counts, int max_tiles,
-                   DevNode* nodes, DevTreeState* st, int tree_mode, cudaStream_t s) {
+void run_partition(const uint8_t* codes, int stride, const PartJob& j, DevNode* nodes, DevTreeState* st,
+                   int32_t* rows0, int32_t* rows1, int* tile_counts, int max_tiles, cudaStream_t s) {
     const int grid = max(1, min(max_tiles, 148 * 8));
-    part_count_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, job, tile_counts);
+    part_count_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, j, nodes, st, rows0, rows1, tile_counts);
     check(cudaGetLastError(), "part_count launch");
-    part_scan_kernel<<<1, 1024, 0, s>>>(job, tile_counts, nodes, st, tree_mode);
-    check(cudaGetLastError(), "part_scan launch");
-    part_scatter_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, job, tile_counts);
+    part_scatter_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, j, nodes, st, rows0, rows1, tile_counts);
     check(cudaGetLastError(), "part_scatter launch");
 }
 
@@ -194,16 +201,16 @@ void run_partition(const uint8_t* codes, int stride, PartJob* job, int* tile_cou
 
 void launch_partition(const uint8_t* codes, int stride, const uint8_t* codes_col, long long n_rows_total,
                       int32_t* const* rows, DevNode* nodes, DevTreeState* st, int* tile_counts, int max_tiles,
-                      void* job_mem, cudaStream_t s) {
-    PartJob* job = static_cast<PartJob*>(job_mem);
-    part_setup_tree_kernel<<<1, 1, 0, s>>>(nodes, st, rows[0], rows[1], codes_col, n_rows_total, job);
-    check(cudaGetLastError(), "part_setup launch");
-    run_partition(codes, stride, job, tile_counts, max_tiles, nodes, st, 1, s);
+                      cudaStream_t s) {
+    PartJob j{};
+    j.col = codes_col;
+    j.col_n = n_rows_total;
+    run_partition(codes, stride, j, nodes, st, rows[0], rows[1], tile_counts, max_tiles, s);
 }
 
 void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
                            int threshold, int missing_left, int32_t* out, int* n_left_dev, int* tile_counts,
-                           void* job_mem, cudaStream_t s) {
+                           cudaStream_t s) {
     PartJob j{};
     j.in = rows;
     j.out = out;
@@ -211,28 +218,25 @@ void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows
     j.feature = feature;
     j.threshold = threshold;
     j.missing_left = missing_left;
-    j.n_tiles = (n_rows + kPartTile - 1) / kPartTile;
     j.n_left_out = n_left_dev;
-    PartJob* job = static_cast<PartJob*>(job_mem);
-    part_setup_const_kernel<<<1, 1, 0, s>>>(j, job);
-    check(cudaGetLastError(), "part_setup launch");
-    run_partition(codes, stride, job, tile_counts, j.n_tiles, nullptr, nullptr, 0, s);
+    if (n_rows <= 0) {
+        if (n_left_dev) check(cudaMemsetAsync(n_left_dev, 0, sizeof(int), s), "n_left reset");
+        return;
+    }
+    run_partition(codes, stride, j, nullptr, nullptr, nullptr, nullptr, tile_counts,
+                  (n_rows + kPartTile - 1) / kPartTile, s);
 }
 
 void launch_compact_flagged(const uint8_t* flag, int n, int32_t* out, int* n_out_dev, int* tile_counts,
-                            void* job_mem, cudaStream_t s) {
+                            cudaStream_t s) {
     PartJob j{};
     j.in = nullptr;  // rows are 0..n-1
     j.out = out;
     j.count = n;
     j.flag = flag;
     j.left_only = 1;
-    j.n_tiles = (n + kPartTile - 1) / kPartTile;
     j.n_left_out = n_out_dev;
-    PartJob* job = static_cast<PartJob*>(job_mem);
-    part_setup_const_kernel<<<1, 1, 0, s>>>(j, job);
-    check(cudaGetLastError(), "compact_setup launch");
-    run_partition(nullptr, 0, job, tile_counts, j.n_tiles, nullptr, nullptr, 0, s);
+    run_partition(nullptr, 0, j, nullptr, nullptr, nullptr, nullptr, tile_counts, (n + kPartTile - 1) / kPartTile, s);
 }
 
 // ---- partition without caller-provided scratch -------------------------------------
@@ -286,7 +290,7 @@ void launch_partition_rows_noalloc(const uint8_t* codes, int stride, const int32
                                  std::to_string(kNoAllocMaxRows) + "], got " + std::to_string(n_rows));
     unsigned char* base = partition_scratch_address();
     launch_partition_rows(codes, stride, rows, n_rows, feature, threshold, missing_left, out, n_left_dev,
-                          reinterpret_cast<int*>(base + kNoAllocJobBytes), base, s);
+                          reinterpret_cast<int*>(base + kNoAllocJobBytes), s);
 }
 
 }  // namespace tgb

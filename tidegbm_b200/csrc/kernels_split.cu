@@ -12,14 +12,15 @@
 //
 // select restates the leaf choice of grow_tree (cpp/src/tree.cpp:343-383): among
 // leaves with depth < max_depth and at least 2*min_samples_leaf rows, the largest
-// cached gain above min_split_gain, lowest node id on ties.
+// cached gain above min_split_gain, lowest node id on ties.  It runs at the end of the
+// scan launch, in the CTA that finishes last (a ticket counter; nothing waits).
 #include "tgb_internal.h"
 
 namespace tgb {
 
 namespace {
 
-constexpr int kScanWarps = 16;
+constexpr int kScanWarps = 2;  // 2 warps per CTA: 64 CTAs per node at 128 features
 
 struct Cand {
     double gain;
@@ -46,19 +47,42 @@ __device__ __forceinline__ long long warp_sum(long long v) {
 }
 
 // One warp scans one feature of a histogram; returns the warp's best candidate
-// (identical in every lane) and the node totals.
-__device__ Cand scan_feature(const long long* __restrict__ Gf, const long long* __restrict__ Hf,
-                             const int* __restrict__ Cf, int f, int n_bins, double inv_gs,
-                             double inv_hs, double lam, double gamma, int min_leaf, double min_hess,
-                             long long& Gt, long long& Ht, long long& Ct) {
+// (identical in every lane) and the node totals.  With Pp / Ps set the histogram is
+// derived first: hist = parent - small sibling (subtract_hist_inplace,
+// cpp/src/histogram.cpp:108-117, exact in fixed point) and stored to Gf / Hf / Cf.
+// scan = false only derives and totals (a node that cannot split).
+__device__ Cand scan_feature(long long* __restrict__ Gf, long long* __restrict__ Hf, int* __restrict__ Cf,
+                             const long long* __restrict__ PGf, const long long* __restrict__ PHf,
+                             const int* __restrict__ PCf, const long long* __restrict__ SGf,
+                             const long long* __restrict__ SHf, const int* __restrict__ SCf, bool derive, bool scan,
+                             int f, int n_bins, double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
+                             double min_hess, long long& Gt, long long& Ht, long long& Ct) {
     const int lane = threadIdx.x & 31;
     long long g[8], hh[8];
     int c[8];
+    if (derive) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        g[i] = Gf[lane * 8 + i];
-        hh[i] = Hf[lane * 8 + i];
-        c[i] = Cf[lane * 8 + i];
+        for (int i = 0; i < 8; ++i) {
+            const int b = lane * 8 + i;
+            g[i] = PGf[b] - SGf[b];
+            hh[i] = PHf[b] - SHf[b];
+            c[i] = PCf[b] - SCf[b];
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+            const int b = lane * 8 + i;
+            *reinterpret_cast<longlong2*>(Gf + b) = make_longlong2(g[i], g[i + 1]);
+            *reinterpret_cast<longlong2*>(Hf + b) = make_longlong2(hh[i], hh[i + 1]);
+        }
+        *reinterpret_cast<int4*>(Cf + lane * 8) = make_int4(c[0], c[1], c[2], c[3]);
+        *reinterpret_cast<int4*>(Cf + lane * 8 + 4) = make_int4(c[4], c[5], c[6], c[7]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            g[i] = Gf[lane * 8 + i];
+            hh[i] = Hf[lane * 8 + i];
+            c[i] = Cf[lane * 8 + i];
+        }
     }
     long long sg = 0, sh = 0, sc = 0;
 #pragma unroll
@@ -72,13 +96,14 @@ __device__ Cand scan_feature(const long long* __restrict__ Gf, const long long* 
     Gt = __shfl_sync(0xffffffffu, ig, 31);
     Ht = __shfl_sync(0xffffffffu, ih, 31);
     Ct = __shfl_sync(0xffffffffu, ic, 31);
+    Cand best{-1e300, 0x7fffffff};
+    if (!scan) return best;
     const long long G0 = __shfl_sync(0xffffffffu, g[0], 0);
     const long long H0 = __shfl_sync(0xffffffffu, hh[0], 0);
     const long long C0 = __shfl_sync(0xffffffffu, static_cast<long long>(c[0]), 0);
     const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
     const double parent = (dGt * dGt) / (dHt + lam);
     long long pg = ig - sg, ph = ih - sh, pc = ic - sc;  // exclusive prefix of this lane
-    Cand best{-1e300, 0x7fffffff};
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         pg += g[i];
@@ -110,64 +135,58 @@ __device__ Cand scan_feature(const long long* __restrict__ Gf, const long long* 
     return best;
 }
 
+__device__ void select_body(const GrowParams& p, DevNode* __restrict__ nodes, DevSplit* __restrict__ splits,
+                            DevTreeState* __restrict__ st);
+
 // grid = (ceil(F / kScanWarps), nodes): one warp per (node, feature).  Each CTA reduces
 // its warps' candidates and stores one per CTA; the last CTA of a node to finish
 // (ticket counter, no waiting) reduces the per-CTA candidates, lowest feature on ties.
+// mode 1 (the two children of st->parent): the large child's histogram is derived from
+// the parent's and the small child's on the way (no separate subtraction pass).
 __global__ void __launch_bounds__(kScanWarps * 32)
     split_scan_kernel(GrowParams p, HistSlotPtrs hs, DevNode* __restrict__ nodes,
-                      DevSplit* __restrict__ splits, const DevTreeState* __restrict__ st, int mode,
-                      int node, ScanScratch sc) {
-    if (st->done) return;
+                      DevSplit* __restrict__ splits, DevTreeState* __restrict__ st, int mode,
+                      int node, ScanScratch sc, int do_select) {
+    if (st->done || (mode == 1 && st->parent < 0)) return;
     int nd = node;
+    bool derive = false;
     if (mode == 1) {
         const DevNode& par = nodes[st->parent];
         nd = blockIdx.y == 0 ? par.left : par.right;
+        derive = nd == st->large_node;
     }
-    const long long* G = hs.G + nd * hs.slot_elems;
-    const long long* H = hs.H + nd * hs.slot_elems;
-    const int* C = hs.C + nd * hs.slot_elems;
+    const size_t e = hs.slot_elems;
+    long long* G = hs.G + nd * e;
+    long long* H = hs.H + nd * e;
+    int* C = hs.C + nd * e;
+    const size_t po = derive ? static_cast<size_t>(st->parent) * e : 0;
+    const size_t so = derive ? static_cast<size_t>(st->small_node) * e : 0;
     const double inv_gs = st->inv_gscale, inv_hs = st->inv_hscale;
     DevNode& N = nodes[nd];
     const bool eligible = N.depth < p.max_depth && N.count >= 2 * p.min_samples_leaf;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (blockIdx.x == 0 && warp == 0) {
-        // Node totals from feature 0 (every feature's bins sum to the same exact integers).
-        long long g = 0, h = 0, c = 0;
-        for (int b = lane; b < kBins; b += 32) {
-            g += G[b];
-            h += H[b];
-            c += C[b];
-        }
-        g = warp_sum(g);
-        h = warp_sum(h);
-        c = warp_sum(c);
-        if (lane == 0) {
-            N.G = g;
-            N.H = h;
-            N.C = c;
-            const double dg = static_cast<double>(g) * inv_gs, dh = static_cast<double>(h) * inv_hs;
-            N.value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
-            if (!eligible) {
-                DevSplit s{};
-                s.gain = -1e300;
-                s.valid = 0;
-                s.feature = s.threshold = -1;
-                s.missing_left = 1;
-                splits[nd] = s;
-            }
-        }
-    }
-    if (!eligible) return;
     __shared__ Cand sbest[kScanWarps];
     __shared__ int last;
     Cand best{-1e300, 0x7fffffff};
     const int f = blockIdx.x * kScanWarps + warp;
-    if (f < p.n_features) {
+    if (f < p.n_features && (eligible || f == 0)) {
+        const size_t fo = static_cast<size_t>(f) * kBins;
         long long Gt, Ht, Ct;
-        best = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
-                            C + static_cast<size_t>(f) * kBins, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
-                            p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
+        best = scan_feature(G + fo, H + fo, C + fo, hs.G + po + fo, hs.H + po + fo, hs.C + po + fo, hs.G + so + fo,
+                            hs.H + so + fo, hs.C + so + fo, derive, eligible, f, p.n_bins, inv_gs, inv_hs, p.l2,
+                            p.min_split_gain, p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
+        if (f == 0 && lane == 0) {
+            // Node totals from feature 0 (every feature's bins sum to the same exact integers).
+            N.G = Gt;
+            N.H = Ht;
+            N.C = Ct;
+            const double dg = static_cast<double>(Gt) * inv_gs, dh = static_cast<double>(Ht) * inv_hs;
+            N.value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
+        }
     }
+    // A node that cannot split still takes part in the ticket protocol: its CTAs carry no
+    // candidate, so the last one records an invalid split, and the launch-wide count that
+    // triggers the leaf choice sees every node.
     if (lane == 0) sbest[warp] = best;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -205,23 +224,35 @@ __global__ void __launch_bounds__(kScanWarps * 32)
             splits[nd] = s;
             sc.ticket[blockIdx.y] = 0;  // ready for the next launch
         }
+        // The last node of the launch to finish picks the next leaf to split.
+        int sel = 0;
+        if (lane == 0 && do_select) {
+            __threadfence();
+            sel = atomicAdd(&sc.ticket[2], 1) == static_cast<int>(gridDim.y) - 1;
+            if (sel) sc.ticket[2] = 0;
+            __threadfence();
+        }
+        sel = __shfl_sync(0xffffffffu, sel, 0);
+        if (sel) select_body(p, nodes, splits, st);
     }
 }
 
-__global__ void select_kernel(GrowParams p, DevNode* __restrict__ nodes, DevSplit* __restrict__ splits,
-                              DevTreeState* __restrict__ st) {
-    if (st->done) return;
-    const int lane = threadIdx.x;
+// grow_tree's leaf choice (cpp/src/tree.cpp:343-383), one warp.  Split records are read
+// past L1 (__ldcg): inside the fused scan they were written by other CTAs of the launch.
+__device__ void select_body(const GrowParams& p, DevNode* __restrict__ nodes, DevSplit* __restrict__ splits,
+                            DevTreeState* __restrict__ st) {
+    const int lane = threadIdx.x & 31;
     const int nn = st->n_nodes;
     double best_gain = p.min_split_gain;
     int best_id = 0x7fffffff;
     for (int k = lane; k < nn; k += 32) {
         const DevNode& N = nodes[k];
         if (!N.is_leaf || N.depth >= p.max_depth || N.count < 2 * p.min_samples_leaf) continue;
-        const DevSplit& s = splits[k];
-        if (!s.valid || !(s.gain >= p.min_split_gain)) continue;
-        if (s.gain > best_gain) {
-            best_gain = s.gain;
+        const int valid = __ldcg(&splits[k].valid);
+        const double gain = __ldcg(&splits[k].gain);
+        if (!valid || !(gain >= p.min_split_gain)) continue;
+        if (gain > best_gain) {
+            best_gain = gain;
             best_id = k;
         }
     }
@@ -240,12 +271,11 @@ __global__ void select_kernel(GrowParams p, DevNode* __restrict__ nodes, DevSpli
         return;
     }
     DevNode& P = nodes[best_id];
-    const DevSplit& s = splits[best_id];
     P.is_leaf = 0;
-    P.feature = s.feature;
-    P.threshold = s.threshold;
-    P.missing_left = s.missing_left;
-    P.gain = s.gain;
+    P.feature = __ldcg(&splits[best_id].feature);
+    P.threshold = __ldcg(&splits[best_id].threshold);
+    P.missing_left = __ldcg(&splits[best_id].missing_left);
+    P.gain = __ldcg(&splits[best_id].gain);
     const int l = nn, r = nn + 1;
     P.left = l;
     P.right = r;
@@ -276,9 +306,12 @@ __global__ void __launch_bounds__(kScanWarps * 32)
     const int f = blockIdx.x * kScanWarps + warp;
     if (f >= n_f) return;
     long long Gt, Ht, Ct;
-    const Cand c = scan_feature(G + static_cast<size_t>(f) * kBins, H + static_cast<size_t>(f) * kBins,
-                                C + static_cast<size_t>(f) * kBins, f, n_bins, inv_gs, inv_hs, lam, gamma,
-                                min_leaf, min_hess, Gt, Ht, Ct);
+    const size_t fo = static_cast<size_t>(f) * kBins;
+    long long* Gm = const_cast<long long*>(G + fo);
+    long long* Hm = const_cast<long long*>(H + fo);
+    int* Cm = const_cast<int*>(C + fo);
+    const Cand c = scan_feature(Gm, Hm, Cm, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false, true, f,
+                                n_bins, inv_gs, inv_hs, lam, gamma, min_leaf, min_hess, Gt, Ht, Ct);
     if (lane == 0) {
         const bool ok = c.key != 0x7fffffff;
         gain[f] = c.gain;
@@ -291,17 +324,11 @@ __global__ void __launch_bounds__(kScanWarps * 32)
 
 int scan_ctas_per_node(int n_f) { return (n_f + kScanWarps - 1) / kScanWarps; }
 
-void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
-                       const DevTreeState* st, int mode, int node, ScanScratch sc, cudaStream_t s) {
+void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits, DevTreeState* st,
+                       int mode, int node, ScanScratch sc, bool do_select, cudaStream_t s) {
     dim3 grid(scan_ctas_per_node(p.n_features), mode == 1 ? 2 : 1);
-    split_scan_kernel<<<grid, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc);
+    split_scan_kernel<<<grid, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc, do_select ? 1 : 0);
     check(cudaGetLastError(), "split_scan launch");
-}
-
-void launch_select(const GrowParams& p, DevNode* nodes, DevSplit* splits, DevTreeState* st,
-                   cudaStream_t s) {
-    select_kernel<<<1, 32, 0, s>>>(p, nodes, splits, st);
-    check(cudaGetLastError(), "select launch");
 }
 
 void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,

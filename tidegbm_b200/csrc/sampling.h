@@ -109,6 +109,54 @@ inline bool shuffle_pairs(int64_t m) {
     return m > 0 && urngrange / static_cast<unsigned long>(m) >= static_cast<unsigned long>(m);
 }
 
+// The draws i in [i, m) of a shuffle whose first `keep` positions are tracked in out
+// (which has room for keep + 1 entries: out[keep] absorbs the draws that land outside
+// the prefix, so the store is branch-free).  A word whose Lemire product has low half
+// >= its range is accepted as is; the first word of a 16-word group that fails that
+// test sends the group to the exact bounded() path.
+inline void shuffle_tail(int64_t i, int64_t m, int64_t keep, Mt32& rng, int32_t* out) {
+    const uint32_t K = static_cast<uint32_t>(keep);
+    while (i < m) {
+        if (rng.pos >= 624) rng.refill();
+        const uint32_t* w = rng.out + rng.pos;
+        const int k = static_cast<int>(std::min<int64_t>(624 - rng.pos, m - i));
+        int l = 0;
+        while (l + 16 <= k) {
+            const uint32_t r0 = static_cast<uint32_t>(i + l + 1);
+            uint32_t bad = 0;
+            for (int q = 0; q < 16; ++q) bad |= static_cast<uint32_t>(w[l + q] * (r0 + q) < r0 + q);
+            if (bad) break;
+            for (int q = 0; q < 16; ++q) {
+                const uint32_t j = static_cast<uint32_t>((static_cast<uint64_t>(w[l + q]) * (r0 + q)) >> 32);
+                out[j < K ? j : K] = static_cast<int32_t>(i + l + q);
+            }
+            l += 16;
+        }
+        for (; l < k; ++l) {
+            const uint32_t r = static_cast<uint32_t>(i + l + 1);
+            const uint64_t p = static_cast<uint64_t>(w[l]) * r;
+            if (static_cast<uint32_t>(p) < r) break;
+            const uint32_t j = static_cast<uint32_t>(p >> 32);
+            out[j < K ? j : K] = static_cast<int32_t>(i + l);
+        }
+        rng.pos += l;
+        i += l;
+        if (l < k) {  // a word that may be rejected: the exact draw (it can consume more words)
+            const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
+            if (j < K) out[j] = static_cast<int32_t>(i);
+            ++i;
+        }
+    }
+}
+
+template <class G>
+inline void shuffle_tail(int64_t i, int64_t m, int64_t keep, G& rng, int32_t* out) {
+    for (; i < m; ++i) {
+        const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
+        if (static_cast<int64_t>(j) < keep) out[j] = static_cast<int32_t>(i);
+    }
+}
+
 // out[p] = index (in [0, m)) of the element std::shuffle(iota(m), rng) puts at p < keep.
 template <class G>
 inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
@@ -121,16 +169,15 @@ inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
         std::copy(v.begin(), v.begin() + keep, out);
         return;
     }
-    std::iota(out, out + keep, 0);
+    std::vector<int32_t> buf(static_cast<size_t>(keep) + 1);
+    std::iota(buf.begin(), buf.end() - 1, 0);
     int64_t i = 1;
     for (; i < keep; ++i) {
         const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
-        std::swap(out[i], out[j]);
+        std::swap(buf[i], buf[j]);
     }
-    for (; i < m; ++i) {
-        const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
-        if (static_cast<int64_t>(j) < keep) out[j] = static_cast<int32_t>(i);
-    }
+    shuffle_tail(std::max<int64_t>(i, 1), m, keep, rng, buf.data());
+    std::copy(buf.begin(), buf.end() - 1, out);
 }
 
 // Number of leading words of w[0..k) (a multiple of 16) whose draws take Lemire's fast

@@ -65,8 +65,6 @@ struct PartJob {
     long long col_n;
     int count;
     int feature, threshold, missing_left;
-    int n_tiles;
-    int n_left;
     int left_only;
     int pad;
 };
@@ -111,30 +109,72 @@ struct GossWork {
 
 void check(cudaError_t e, const char* what);
 
+// Owning device buffer (freed on scope exit).
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    void alloc(size_t k) {
+        release();
+        if (k) check(cudaMalloc(reinterpret_cast<void**>(&p), k * sizeof(T)), "cudaMalloc");
+        n = k;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+};
+
 // binning (kernels_bin.cu)
 void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
                               uint8_t* codes, int stride, cudaStream_t s);
 void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edges, const int* n_edges,
                               uint8_t* codes, int stride, cudaStream_t s);
 
+// device half of Binner::fit (kernels_binfit.cu); X walks use chunks of kFitChunk rows
+constexpr int kFitChunk = 4096;
+void launch_nonnan_counts(const void* X, int x_dtype, int n, int n_f, int* counts, cudaStream_t s);
+void launch_keep_bits(const int32_t* keep, int bin_sample, int n_f, const uint8_t* take_all, uint32_t* bits,
+                      long long words, cudaStream_t s);
+void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const uint32_t* bits,
+                          long long words, const uint8_t* take_all, void* sample, long long cap, int* fill,
+                          cudaStream_t s);
+size_t sample_sort_bytes(int x_dtype, long long total, int n_f);
+void launch_sample_sort(int x_dtype, const void* in, void* out, long long total, int n_f, const int* seg_begin,
+                        const int* seg_end, void* tmp, size_t tmp_bytes, cudaStream_t s);
+void launch_quantile_edges(int x_dtype, const void* sorted, void* uniq, long long cap, const int* cnt, int n_f,
+                           int n_bins, double* edges, int* n_edges, cudaStream_t s);
+
 // histograms + tree state (kernels_hist.cu)
+// const_h (mse): reads gq from launch_quantize; otherwise g, h and goss_flag.
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows, const DevNode* nodes,
-                      const DevTreeState* st, int node, const double* g, const double* h,
+                      const DevTreeState* st, int node, const double* g, const double* h, const long long* gq,
                       const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs, int grid_rows,
                       unsigned long long* rows_counter, bool const_h, cudaStream_t s);
+// gq[r] = (rint(g[r] * goss_factor * st->gscale) << 1) | GOSS-scaled, for the st->n_sample
+// rows of rows[] (the tree's sample); run after launch_scales.
+void launch_quantize(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
+                     const DevTreeState* st, long long* gq, int max_rows, cudaStream_t s);
 void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* rows, int n_rows,
                       const double* g, const double* h, int gshift, int hshift, long long* G, long long* H,
                       int* C, cudaStream_t s);
-void launch_hist_subtract(const DevTreeState* st, HistSlotPtrs hs, cudaStream_t s);
 void launch_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_sample_host, int use_dev_count,
                       cudaStream_t s);
 void launch_iota_rows(int32_t* rows, int n, cudaStream_t s);
 void launch_scales(const int32_t* rows, const double* g, const double* h, const uint8_t* goss_flag,
                    double goss_scale, DevTreeState* st, int max_rows, cudaStream_t s);
-int hist_grid_rows(int n_f, int max_rows);
+// Row chunks per feature group of a histogram launch (const_h: a multiple of the cluster size).
+int hist_grid_rows(int n_f, int max_rows, bool const_h);
 
-// split scan + selection (kernels_split.cu); mode 0 = node `node`, 1 = children of st->parent.
-// ScanScratch: per-CTA candidates (2 x scan_ctas_per_node) and 2 ticket counters that
+// split scan + selection (kernels_split.cu); mode 0 = node `node`, 1 = children of st->parent
+// (the large child's histogram is derived as parent - small child on the way).  With
+// do_select the launch ends with the next leaf choice (nodes, splits, st updated).
+// ScanScratch: per-CTA candidates (2 x scan_ctas_per_node) and 3 ticket counters that
 // must start at zero (the kernel leaves them at zero).
 struct ScanScratch {
     double* gain;
@@ -142,25 +182,25 @@ struct ScanScratch {
     int* ticket;
 };
 int scan_ctas_per_node(int n_f);
-void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits,
-                       const DevTreeState* st, int mode, int node, ScanScratch sc, cudaStream_t s);
-void launch_select(const GrowParams& p, DevNode* nodes, DevSplit* splits, DevTreeState* st, cudaStream_t s);
+void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits, DevTreeState* st,
+                       int mode, int node, ScanScratch sc, bool do_select, cudaStream_t s);
 void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
                       double inv_gscale, double inv_hscale, double lam, double gamma, int min_leaf,
                       double min_hess, double* gain, int* thr, int* ml, cudaStream_t s);
 
-// partition (kernels_part.cu); job_mem: device PartJob
+// partition (kernels_part.cu); tile_counts: device scratch of ceil(rows / kPartTile) ints.
+// Tree mode: the job is the split of st->parent read from the node table.
 void launch_partition(const uint8_t* codes, int stride, const uint8_t* codes_col, long long n_rows_total,
                       int32_t* const* rows, DevNode* nodes, DevTreeState* st, int* tile_counts, int max_tiles,
-                      void* job_mem, cudaStream_t s);
+                      cudaStream_t s);
 // Column-major copy of the row-major codes: col[f * codes_col_pitch(n) + r] = codes[r][f].
 inline long long codes_col_pitch(int n) { return (static_cast<long long>(n) + 15) / 16 * 16; }
 void launch_codes_transpose(const uint8_t* codes, int stride, int n, int n_f, uint8_t* col, cudaStream_t s);
 void launch_partition_rows(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
                            int threshold, int missing_left, int32_t* out, int* n_left_dev, int* tile_counts,
-                           void* job_mem, cudaStream_t s);
+                           cudaStream_t s);
 void launch_compact_flagged(const uint8_t* flag, int n, int32_t* out, int* n_out_dev, int* tile_counts,
-                            void* job_mem, cudaStream_t s);
+                            cudaStream_t s);
 // Same partition with its scratch in a fixed device array of kernels_part.cu (no allocation).
 int partition_noalloc_max_rows();
 void launch_partition_rows_noalloc(const uint8_t* codes, int stride, const int32_t* rows, int n_rows, int feature,
@@ -179,8 +219,7 @@ void launch_loss_finalize(int kind, const double* partials, const int* valid, in
 // GOSS (kernels_goss.cu)
 size_t goss_cub_bytes(int n);
 void launch_goss_select(const double* g, int n, int n_top, int n_other, const int32_t* rest_pos, GossWork& w,
-                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, void* job_mem, DevTreeState* st,
-                        cudaStream_t s);
+                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, DevTreeState* st, cudaStream_t s);
 
 // post-tree sweep (kernels_post.cu)
 void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s);

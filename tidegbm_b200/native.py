@@ -57,6 +57,8 @@ def lib() -> C.CDLL:
         "tgb_tree_export": ([vp, i, vp, vp, vp, vp, vp], i),
         "tgb_edges": ([vp, i, vp], i),
         "tgb_fit_stats": ([vp, vp], i),
+        "tgb_fit_stat": ([vp, cp, vp], i),
+        "tgb_binner_fit_device": ([vp, i, i, i, i, i, C.c_uint, vp, vp, vp], i),
         "tgb_binner_fit": ([vp, i, i, i, i, i, C.c_uint, vp, vp], i),
         "tgb_shuffled_prefix": ([ll, ll, C.c_uint, vp], i),
         "tgb_bin_transform": ([vp, i, i, i, vp, vp, vp, i, vp], i),
@@ -93,7 +95,7 @@ def _ptr(a) -> C.c_void_p | None:
 _INT_KEYS = {"n_estimators", "max_depth", "max_leaves", "min_samples_leaf", "max_bin", "n_time_buckets",
              "random_state", "n_jobs", "iid_mode", "halo", "pair_splits", "horizon", "embargo", "goss",
              "bin_sample", "finer_torb", "causal_bins", "causal_structure", "verbose", "col_major_hist",
-             "cat_min_count", "timing_from", "profile_hist"}
+             "cat_min_count", "timing_from", "timing_to", "profile_hist"}
 _DOUBLE_KEYS = {"learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
                 "colsample_bynode", "goss_top", "goss_other", "torb_min_cover", "max_delta_step", "time_decay",
                 "structure_frac", "entity_subsample"}
@@ -227,7 +229,12 @@ class Booster:
         keys = ["total", "sort", "bin_fit", "upload_transform", "trees", "download", "host_rng", "kernel_launches",
                 "timed_ms", "timed_trees", "timed_launches", "hist_ms", "hist_launches", "hist_rows", "alloc", "h2d",
                 "transpose", "goss_producer"]
-        return dict(zip(keys, o.tolist()))
+        res = dict(zip(keys, o.tolist()))
+        for k in ("bin_counts", "bin_draws", "bin_edges"):
+            v = C.c_double()
+            check(lib().tgb_fit_stat(self._h, k.encode(), C.byref(v)))
+            res[k] = v.value
+        return res
 
     def build_hist_gpu(self, xb: np.ndarray, idx: np.ndarray, g: np.ndarray, h: np.ndarray, n_bins: int) -> np.ndarray:
         """Drop-in for build_hist_gpu (cpp/src/histogram_cuda.cu:81-167): returns the
