@@ -87,7 +87,9 @@ TGB_API int tgb_edges(tgb_booster* b, int f, double* out);
 TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
 /* One value of the last fit's breakdown by name (wall seconds): "total", "bin_fit",
  * "bin_counts", "bin_draws", "bin_edges" (the device binner's stages), "h2d", "alloc",
- * "transpose", "trees".  Unknown names return -1. */
+ * "transpose", "trees", "pre_upload" / "prep" (host set-up before the upload / before
+ * the tree loop), "goss_refits" (1 when the fit was repeated with the full 64-bit GOSS
+ * sort).  Unknown names return -1. */
 TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);
 
 /* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:

@@ -116,6 +116,51 @@ def test_fit_min_samples_leaf_stops_growth(native, oracle):
             oracle.oracle_free(h)
 
 
+def _clustered_gradients(n, rel, seed):
+    """Targets c * (1 + i * rel) with random signs: after the first tree's mean, the |g|
+    values are distinct but packed within rel of each other, so many of them share the
+    top 32 bits the GOSS sort keys on."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, 6)).astype(np.float32)
+    i = rng.permutation(n).astype(np.float64)
+    y = 3.0 * (1.0 + i * rel) * np.where(X[:, 0] < 0.0, -1.0, 1.0)
+    return X, y
+
+
+@pytest.mark.parametrize("rel,refits", [(6e-10, 0), (1e-11, 1)])
+def test_fit_goss_tied_sort_keys(native, oracle, rel, refits):
+    """GOSS order under many near-equal |g|: short runs of tied 32-bit keys are fixed up on
+    the device; a run too long for that repeats the fit with the 64-bit sort."""
+    n = 40000
+    X, y = _clustered_gradients(n, rel, 1)
+    params = dict(n_estimators=4, learning_rate=0.1, max_depth=5, max_leaves=15, iid_mode=1, objective="mse", goss=1,
+                  random_state=2, pair_splits=False)
+    gpu = native.Booster(**params)
+    gpu.fit(X, y)
+    assert gpu.fit_stats()["goss_refits"] == refits
+    ref, h = oracle.oracle_fit(params, X.astype(np.float64), y)
+    try:
+        _compare(gpu, ref)
+    finally:
+        oracle.oracle_free(h)
+
+
+def test_fit_goss_all_gradients_equal(native):
+    """|g| identical on every row (targets +-3 around a zero mean): one run of tied sort
+    keys whose full patterns are all equal needs no reordering (no refit), and the
+    sample is the stable index order, the same on every run."""
+    n = 20000
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((n, 5)).astype(np.float32)
+    y = np.where(np.arange(n) % 2 == 0, 3.0, -3.0)
+    params = dict(n_estimators=2, learning_rate=0.1, max_depth=4, max_leaves=8, iid_mode=1, objective="mse", goss=1,
+                  random_state=0, pair_splits=False)
+    a = native.Booster(**params).fit(X, y)
+    assert a.fit_stats()["goss_refits"] == 0
+    b = native.Booster(**params).fit(X, y)
+    np.testing.assert_array_equal(a.raw_predict(X), b.raw_predict(X))
+
+
 def test_fit_iid_float64_input(native, oracle):
     """iid mode (no TORB), float64 X, max_leaves 15, depth 4."""
     rng = np.random.default_rng(5)

@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -50,6 +51,31 @@ void parallel_for(int n, int n_threads, F&& fn) {
 }
 
 inline bool is_nan(double v) { return !(v == v); }
+
+// Device scratch taken from a caller's arena while it has room, else allocated (and
+// freed with the Scratch).  Pieces are 256-byte aligned.
+class Scratch {
+public:
+    Scratch(void* base, size_t bytes) : base_(static_cast<unsigned char*>(base)), size_(base ? bytes : 0) {}
+    template <class T>
+    T* get(size_t count) {
+        const size_t bytes = (std::max<size_t>(1, count * sizeof(T)) + 255) / 256 * 256;
+        if (used_ + bytes <= size_) {
+            T* p = reinterpret_cast<T*>(base_ + used_);
+            used_ += bytes;
+            return p;
+        }
+        owned_.push_back(std::make_unique<DBuf<unsigned char>>());
+        owned_.back()->alloc(bytes);
+        return reinterpret_cast<T*>(owned_.back()->p);
+    }
+
+private:
+    unsigned char* base_;
+    size_t size_;
+    size_t used_ = 0;
+    std::vector<std::unique_ptr<DBuf<unsigned char>>> owned_;
+};
 
 double wall_now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -171,16 +197,16 @@ bool binner_fits_device(int n, int n_f, int bin_sample) {
 
 int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                       std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
-                      BinFitTimes* tm) {
+                      void* arena, size_t arena_bytes, BinFitTimes* tm) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scratch(arena, arena_bytes);
     const double t0 = wall_now();
     const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
     const size_t nc = static_cast<size_t>(n_chunks) * n_f;
-    DBuf<int> counts;
-    counts.alloc(nc);
-    launch_nonnan_counts(Xd, x_dtype, n, n_f, counts.p, s);
+    int* counts = scratch.get<int>(nc);
+    launch_nonnan_counts(Xd, x_dtype, n, n_f, counts, s);
     std::vector<int> ch(nc);
-    check(cudaMemcpyAsync(ch.data(), counts.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
+    check(cudaMemcpyAsync(ch.data(), counts, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
     check(cudaStreamSynchronize(s), "non-NaN counts");
     const double t1 = wall_now();
     // per-feature totals and the first non-NaN rank of every (chunk, feature)
@@ -212,59 +238,49 @@ int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, 
         });
     }
     const double t2 = wall_now();
-    DBuf<long long> base_d;
-    base_d.alloc(nc);
-    check(cudaMemcpyAsync(base_d.p, base.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, s), "bases upload");
-    DBuf<uint8_t> take_d;
-    take_d.alloc(n_f);
-    check(cudaMemcpyAsync(take_d.p, take_all.data(), n_f, cudaMemcpyHostToDevice, s), "flags upload");
+    long long* base_d = scratch.get<long long>(nc);
+    check(cudaMemcpyAsync(base_d, base.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, s), "bases upload");
+    uint8_t* take_d = scratch.get<uint8_t>(n_f);
+    check(cudaMemcpyAsync(take_d, take_all.data(), n_f, cudaMemcpyHostToDevice, s), "flags upload");
     const long long words = max_sampled > 0 ? (max_sampled + 31) / 32 : 1;
-    DBuf<uint32_t> bits;
-    bits.alloc(static_cast<size_t>(n_f) * words);
-    DBuf<int32_t> keep_d;
+    uint32_t* bits = scratch.get<uint32_t>(static_cast<size_t>(n_f) * words);
     if (max_sampled > 0) {
-        check(cudaMemsetAsync(bits.p, 0, sizeof(uint32_t) * bits.n, s), "bits reset");
-        keep_d.alloc(keep.size());
-        check(cudaMemcpyAsync(keep_d.p, keep.data(), sizeof(int32_t) * keep.size(), cudaMemcpyHostToDevice, s),
+        check(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * static_cast<size_t>(n_f) * words, s), "bits reset");
+        int32_t* keep_d = scratch.get<int32_t>(keep.size());
+        check(cudaMemcpyAsync(keep_d, keep.data(), sizeof(int32_t) * keep.size(), cudaMemcpyHostToDevice, s),
               "kept ranks upload");
-        launch_keep_bits(keep_d.p, bin_sample, n_f, take_d.p, bits.p, words, s);
+        launch_keep_bits(keep_d, bin_sample, n_f, take_d, bits, words, s);
     }
-    DBuf<int> fill;
-    fill.alloc(n_f);
-    check(cudaMemsetAsync(fill.p, 0, sizeof(int) * n_f, s), "fill reset");
+    int* fill = scratch.get<int>(n_f);
+    check(cudaMemsetAsync(fill, 0, sizeof(int) * n_f, s), "fill reset");
     const size_t esz = x_dtype == 0 ? sizeof(float) : sizeof(double);
     const long long total = static_cast<long long>(n_f) * cap;
-    DBuf<unsigned char> smp_a, smp_b;
-    smp_a.alloc(static_cast<size_t>(total) * esz);
-    smp_b.alloc(static_cast<size_t>(total) * esz);
-    launch_sample_gather(Xd, x_dtype, n, n_f, base_d.p, bits.p, words, take_d.p, smp_a.p, cap, fill.p, s);
+    unsigned char* smp_a = scratch.get<unsigned char>(static_cast<size_t>(total) * esz);
+    unsigned char* smp_b = scratch.get<unsigned char>(static_cast<size_t>(total) * esz);
+    launch_sample_gather(Xd, x_dtype, n, n_f, base_d, bits, words, take_d, smp_a, cap, fill, s);
     std::vector<int> seg(2 * static_cast<size_t>(n_f));
     for (int f = 0; f < n_f; ++f) {
         seg[f] = static_cast<int>(f * cap);
         seg[n_f + f] = static_cast<int>(f * cap + kept[f]);
     }
-    DBuf<int> seg_d, kept_d;
-    seg_d.alloc(seg.size());
-    kept_d.alloc(n_f);
-    check(cudaMemcpyAsync(seg_d.p, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice, s), "segs upload");
-    check(cudaMemcpyAsync(kept_d.p, kept.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "kept upload");
-    DBuf<unsigned char> tmp;
+    int* seg_d = scratch.get<int>(seg.size());
+    int* kept_d = scratch.get<int>(n_f);
+    check(cudaMemcpyAsync(seg_d, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice, s), "segs upload");
+    check(cudaMemcpyAsync(kept_d, kept.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "kept upload");
     const size_t tmp_bytes = sample_sort_bytes(x_dtype, total, n_f);
-    tmp.alloc(std::max<size_t>(tmp_bytes, 16));
-    launch_sample_sort(x_dtype, smp_a.p, smp_b.p, total, n_f, seg_d.p, seg_d.p + n_f, tmp.p, tmp_bytes, s);
-    DBuf<double> ed;
-    DBuf<int> ne;
-    ed.alloc(static_cast<size_t>(n_f) * 256);
-    ne.alloc(n_f);
-    check(cudaMemsetAsync(ed.p, 0, sizeof(double) * ed.n, s), "edges reset");
-    launch_quantile_edges(x_dtype, smp_b.p, smp_a.p, cap, kept_d.p, n_f, max_bin - 1, ed.p, ne.p, s);
+    unsigned char* tmp = scratch.get<unsigned char>(std::max<size_t>(tmp_bytes, 16));
+    launch_sample_sort(x_dtype, smp_a, smp_b, total, n_f, seg_d, seg_d + n_f, tmp, tmp_bytes, s);
+    double* ed = scratch.get<double>(static_cast<size_t>(n_f) * 256);
+    int* ne = scratch.get<int>(n_f);
+    check(cudaMemsetAsync(ed, 0, sizeof(double) * static_cast<size_t>(n_f) * 256, s), "edges reset");
+    launch_quantile_edges(x_dtype, smp_b, smp_a, cap, kept_d, n_f, max_bin - 1, ed, ne, s);
     edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
     n_edges.assign(n_f, 0);
     std::vector<int> fill_h(n_f);
-    check(cudaMemcpyAsync(edges.data(), ed.p, sizeof(double) * edges.size(), cudaMemcpyDeviceToHost, s),
+    check(cudaMemcpyAsync(edges.data(), ed, sizeof(double) * edges.size(), cudaMemcpyDeviceToHost, s),
           "edges download");
-    check(cudaMemcpyAsync(n_edges.data(), ne.p, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "edges download");
-    check(cudaMemcpyAsync(fill_h.data(), fill.p, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "fill download");
+    check(cudaMemcpyAsync(n_edges.data(), ne, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "edges download");
+    check(cudaMemcpyAsync(fill_h.data(), fill, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "fill download");
     check(cudaStreamSynchronize(s), "quantile edges");
     for (int f = 0; f < n_f; ++f)
         if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");

@@ -108,7 +108,8 @@ struct DeviceState {
     DBuf<int> tile_counts;
     DBuf<double> scan_gain;
     DBuf<int> scan_key, scan_ticket;
-    DBuf<unsigned long long> keys_in, keys_out;
+    DBuf<unsigned long long> keys_in, keys_out;  // 64-bit slots; the fast GOSS path uses them as 32-bit
+    DBuf<int> goss_overflow;
     DBuf<int32_t> vals_in, vals_out, rest_pos;
     DBuf<unsigned char> cub_tmp;
     DBuf<uint8_t> goss_flag;
@@ -146,6 +147,20 @@ GpuBooster::~GpuBooster() {
 
 void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, int n_f, const int64_t* ts_in,
                      const int64_t* ent_in) {
+    // The GOSS order comes from a 32-bit-key sort plus an exact fix-up of tied runs; a
+    // run too long for the fix-up (many distinct |g| within 2^-21 relative of each other)
+    // is reported by the device, and the fit is then repeated with the full 64-bit sort.
+    const bool overflow = fit_once(X_in, x_dtype, y_in, n, n_f, ts_in, ent_in, false);
+    if (overflow) {
+        const FitStats first = stats;
+        fit_once(X_in, x_dtype, y_in, n, n_f, ts_in, ent_in, true);
+        stats.goss_refits = 1;
+        stats.t_total += first.t_total;
+    }
+}
+
+bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int n, int n_f, const int64_t* ts_in,
+                          const int64_t* ent_in, bool exact_goss) {
     const double t0 = now();
     stats = FitStats();
     const long long launches0 = g_kernel_launches.load();
@@ -204,6 +219,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         }
     }
     stats.t_sort = now() - t0;
+    const double t_pre0 = now();
 
     // GOSS: booster.cpp:554-585 (sample = all rows since subsample = 1).  The draw
     // positions depend only on n and the config, so the sampler's producer starts now and
@@ -293,16 +309,18 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         fill_prefix = init_prefix;
     }
 
+    stats.t_pre_upload = now() - t_pre0;  // GOSS sampler start, TORB buckets and cuts
     // ---- device buffers ----
     double tb = now();
     const int stride = (n_f + 15) / 16 * 16;
     const int max_nodes = 2 * c.max_leaves - 1;
     const size_t slot = static_cast<size_t>(n_f) * kBins;
     D.codes.alloc(static_cast<size_t>(n) * stride);
+    D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n));
     D.y.alloc(n);
     D.pred.alloc(n);
     D.g.alloc(n);
-    D.h.alloc(n);
+    if (c.objective != 0) D.h.alloc(n);  // MSE hessians are implicit (unit)
     if (c.objective == 0) D.gq.alloc(n);
     D.rows0.alloc(n);
     D.rows1.alloc(n);
@@ -342,7 +360,8 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         BinFitTimes bt;
         if (binner_fits_device(n, n_f, c.bin_sample))
             n_bins = binner_fit_device(Xd.p, x_dtype, n, n_f, c.max_bin, c.bin_sample,
-                                       static_cast<uint32_t>(c.random_state), edges, n_edges, n_threads, s, &bt);
+                                       static_cast<uint32_t>(c.random_state), edges, n_edges, n_threads, s,
+                                       D.codes_col.p, D.codes_col.n, &bt);  // scratch: codes_col, filled later
         else
             n_bins = binner_fit(X, x_dtype, n, n_f, c.max_bin, c.bin_sample, static_cast<uint32_t>(c.random_state),
                                 edges, n_edges, n_threads);
@@ -377,11 +396,11 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     }
     // Column-major copy for the partition's reads of one feature over a row list.
     const double ttr = now();
-    D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n));
     launch_codes_transpose(D.codes.p, stride, n, n_f, D.codes_col.p, s);
     check(cudaStreamSynchronize(s), "transpose");
     stats.t_transpose = now() - ttr;
     stats.t_upload = now() - tb - stats.t_binfit;
+    const double t_prep0 = now();
 
     // TORB segments: distinct cuts split the time-sorted rows into segments; CTAs of the
     // post-tree sweep own segment-aligned chunks.
@@ -461,11 +480,15 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         D.vals_out.alloc(n);
         D.goss_flag.alloc(n);
         D.rest_pos.alloc(std::max(1, n_other));
-        const size_t cb = goss_cub_bytes(n);
+        const size_t cb = goss_cub_bytes(n, exact_goss);
         D.cub_tmp.alloc(cb);
+        D.goss_overflow.alloc(1);
+        check(cudaMemsetAsync(D.goss_overflow.p, 0, sizeof(int), s), "overflow reset");
+        launch_goss_iota(D.vals_in.p, n, s);
         sampler->start_workers();
     }
-    GossWork gw{D.keys_in.p, D.keys_out.p, D.vals_in.p, D.vals_out.p, D.cub_tmp.p, D.cub_tmp.n};
+    GossWork gw{D.keys_in.p, D.keys_out.p, D.vals_in.p, D.vals_out.p, D.cub_tmp.p, D.cub_tmp.n,
+                D.goss_overflow.p, exact_goss};
 
     GrowParams gp{n_f, stride, n_bins, c.max_depth, c.max_leaves, c.min_samples_leaf, c.min_child_weight, c.l2,
                   c.min_split_gain};
@@ -476,6 +499,7 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     int32_t* rows[2] = {D.rows0.p, D.rows1.p};
     const int grid_rows = hist_grid_rows(n_f, n, c.objective == 0);
     const double ttree = now();
+    stats.t_prep = ttree - t_prep0;  // TORB segments, rank groups, GOSS buffers, initial predictions
 
     // Measurement hooks: events bracket the timed trees; optional event pairs bracket
     // every histogram launch in that range; a device counter adds up the rows.
@@ -518,10 +542,17 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
             check(cudaEventRecord(ev_end, s), "event record");
             launches_end = g_kernel_launches.load();
         }
-        // gradients (booster.cpp:701)
-        if (c.objective == 0) launch_grad_mse(D.y.p, D.pred.p, n, D.g.p, D.h.p, s);
-        else launch_grad_pairwise(D.y.p, D.pred.p, D.run_start.p, D.run_len.p, order_d, n_runs, n, D.g.p, D.h.p, s);
-        launch_all_scale(D.g.p, D.h.p, n, D.all_scale.p, s);
+        // gradients (booster.cpp:701).  MSE: one pass also reduces the all-row maxima;
+        // its unit hessians are never materialised (h = nullptr below).
+        const bool const_h = c.objective == 0;
+        if (const_h) {
+            launch_grad_mse_fused(D.y.p, D.pred.p, n, D.g.p, D.all_scale.p, s);
+            launch_all_scale_finalize(D.all_scale.p, n, s);
+        } else {
+            launch_grad_pairwise(D.y.p, D.pred.p, D.run_start.p, D.run_len.p, order_d, n_runs, n, D.g.p, D.h.p, s);
+            launch_all_scale(D.g.p, D.h.p, n, D.all_scale.p, s);
+        }
+        const double* h_rows = const_h ? nullptr : D.h.p;
         // sample
         if (use_goss) {
             const double tr = now();
@@ -530,16 +561,18 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
             check(cudaMemcpyAsync(D.rest_pos.p, pos, sizeof(int32_t) * std::max(1, n_other), cudaMemcpyHostToDevice, s),
                   "positions upload");
             sampler->release(t, s);
-            launch_goss_select(D.g.p, n, n_top, n_other, D.rest_pos.p, gw, D.goss_flag.p, D.rows0.p, D.tile_counts.p,
-                               D.st.p, s);
+            launch_goss_select(D.g.p, h_rows, n, n_top, n_other, D.rest_pos.p, gw, D.all_scale.p, goss_scale,
+                               D.goss_flag.p,
+                               D.rows0.p, D.tile_counts.p, D.st.p, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, 0, 1, s);
+            launch_scales(D.st.p, nullptr, s);
         } else {
             launch_iota_rows(D.rows0.p, n, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, n, 0, s);
+            launch_scales(D.st.p, D.all_scale.p, s);
         }
         const uint8_t* flag = use_goss ? D.goss_flag.p : nullptr;
-        launch_scales(D.rows0.p, D.g.p, D.h.p, flag, goss_scale, D.st.p, n, s);
-        if (c.objective == 0) launch_quantize(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, D.gq.p, n, s);
+        if (const_h) launch_quantize(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, D.gq.p, n, s);
         check(cudaMemsetAsync(D.histG.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histH.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histC.p, 0, sizeof(int) * slot * max_nodes, s), "hist reset");
@@ -557,16 +590,16 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
         double* values_t = D.values_all.p + static_cast<size_t>(t) * max_nodes;
         double* prefix_t = D.prefix_all.p + static_cast<size_t>(t) * nbk * max_nodes;
         int* cover_t = D.cover_all.p + static_cast<size_t>(t) * max_nodes;
-        launch_apply_accum(D.codes.p, stride, D.nodes.p, D.st.p, D.g.p, D.h.p, D.chunks.p,
+        launch_apply_accum(D.codes.p, stride, D.nodes.p, D.st.p, D.g.p, h_rows, D.chunks.p,
                            static_cast<int>(chunks.size()), D.all_scale.p, D.nid.p, D.seg_sums.p, n_segments, s);
         launch_finalize_tree(pp, D.st.p, D.seg_sums.p, D.bucket_seg_end.p, D.cuts.p, D.all_scale.p, values_t,
                              cover_t, prefix_t, s);
-        launch_pred_update(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, s);
-        // training loss (booster.cpp:704-706)
-        if (c.objective == 0) {
-            launch_loss_mse(D.y.p, D.pred.p, n, D.loss_part.p, 592, s);
+        // prediction update, then the training loss (booster.cpp:704-706)
+        if (const_h) {
+            launch_pred_update_loss(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, D.y.p, D.loss_part.p, 592, s);
             launch_loss_finalize(0, D.loss_part.p, nullptr, 592, n, D.losses.p + t, s);
         } else {
+            launch_pred_update(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, s);
             launch_loss_pairwise(D.y.p, D.pred.p, D.run_start.p, D.run_len.p, order_d, n_runs, D.loss_part.p,
                                  D.loss_valid.p, s);
             launch_loss_finalize(5, D.loss_part.p, D.loss_valid.p, n_runs, n, D.losses.p + t, s);
@@ -644,6 +677,10 @@ void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, i
     D.trees_flat = 0;
     stats.gpu_launches = static_cast<int>(g_kernel_launches.load() - launches0);
     stats.t_total = now() - t0;
+    int overflow = 0;
+    if (use_goss && !exact_goss)
+        check(cudaMemcpy(&overflow, D.goss_overflow.p, sizeof(int), cudaMemcpyDeviceToHost), "overflow flag");
+    return overflow != 0;
 }
 
 void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double* out) {

@@ -83,6 +83,8 @@ struct FitStats {
     double t_rng = 0;
     double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
     double t_bin_counts = 0, t_bin_draws = 0, t_bin_edges = 0;  // stages of the device binner
+    int goss_refits = 0;  // 1 when the fit was repeated with the 64-bit GOSS sort
+    double t_pre_upload = 0, t_prep = 0;  // host set-up before the upload and before the tree loop
     int gpu_launches = 0;
     // timed range (cfg.timing_from .. last tree), device time from CUDA events
     double timed_ms = 0;
@@ -122,6 +124,10 @@ public:
     void predict_raw(const void* X, int x_dtype, int n, int n_f, double* out);
 
 private:
+    // One fit; exact_goss sorts GOSS keys on all 64 bits.  Returns true when the 32-bit
+    // GOSS sort met a tied run too long to fix up (the result must then be recomputed).
+    bool fit_once(const void* X, int x_dtype, const double* y, int n, int n_f, const int64_t* ts,
+                  const int64_t* entity, bool exact_goss);
     DeviceState* ds_ = nullptr;
 };
 
@@ -136,8 +142,9 @@ struct BinFitTimes {
     double counts = 0, draws = 0, edges = 0;  // wall seconds of the three stages
 };
 bool binner_fits_device(int n, int n_f, int bin_sample);
+// arena / arena_bytes: device memory the binner may use as scratch (nullptr: allocate).
 int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                       std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
-                      BinFitTimes* tm);
+                      void* arena, size_t arena_bytes, BinFitTimes* tm);
 
 }  // namespace tgb

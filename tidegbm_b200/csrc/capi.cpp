@@ -313,7 +313,7 @@ int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_features, int
         std::vector<int> ne;
         nb = tgb::binner_fit_device(X, x_dtype, n, n_features, max_bin, bin_sample, seed, e, ne,
                                     static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), stream,
-                                    nullptr);
+                                    nullptr, 0, nullptr);
         std::copy(e.begin(), e.end(), edges_out);
         std::copy(ne.begin(), ne.end(), n_edges_out);
     });
@@ -334,6 +334,9 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "transpose") *out = s.t_transpose;
         else if (k == "trees") *out = s.t_trees;
         else if (k == "total") *out = s.t_total;
+        else if (k == "goss_refits") *out = s.goss_refits;
+        else if (k == "pre_upload") *out = s.t_pre_upload;
+        else if (k == "prep") *out = s.t_prep;
         else throw tgb::TideError("unknown fit stat: " + k);
     });
 }

@@ -402,38 +402,10 @@ __global__ void tree_init_kernel(DevNode* nodes, DevSplit* splits, DevTreeState*
     st->parent = -1;
     st->small_node = st->large_node = -1;
     st->n_sample = count;
-    st->max_abs_g_bits = 0ull;
-    st->max_h_bits = 0ull;
 }
 
 __global__ void iota_kernel(int32_t* rows, int n) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) rows[k] = k;
-}
-
-__global__ void scales_reduce_kernel(const int32_t* __restrict__ rows, const double* __restrict__ g,
-                                     const double* __restrict__ h, const uint8_t* __restrict__ goss_flag,
-                                     double goss_scale, DevTreeState* st) {
-    const int count = st->n_sample;
-    double mg = 0.0, mh = 0.0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        const int r = rows[k];
-        double gv = fabs(g[r]), hv = fabs(h[r]);
-        if (goss_flag != nullptr && goss_flag[r] == 2) {
-            gv = fabs(g[r] * goss_scale);
-            hv = fabs(h[r] * goss_scale);
-        }
-        mg = fmax(mg, gv);
-        mh = fmax(mh, hv);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
-        mh = fmax(mh, __shfl_xor_sync(0xffffffffu, mh, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        // Non-negative doubles order like their bit patterns.
-        atomicMax(&st->max_abs_g_bits, static_cast<unsigned long long>(__double_as_longlong(mg)));
-        atomicMax(&st->max_h_bits, static_cast<unsigned long long>(__double_as_longlong(mh)));
-    }
 }
 
 // Largest shift with count * max_abs * 2^s < 2^62 (no sum can overflow) and
@@ -448,7 +420,12 @@ __device__ int shift_for(double max_abs, int count) {
     return max(-1000, min(1000, s));
 }
 
-__global__ void scales_finalize_kernel(DevTreeState* st) {
+// all != nullptr: the sample is every row, whose maxima the gradient pass reduced.
+__global__ void scales_finalize_kernel(DevTreeState* st, const AllScale* __restrict__ all) {
+    if (all) {
+        st->max_abs_g_bits = all->maxg_bits;
+        st->max_h_bits = all->maxh_bits;
+    }
     const double mg = __longlong_as_double(static_cast<long long>(st->max_abs_g_bits));
     const double mh = __longlong_as_double(static_cast<long long>(st->max_h_bits));
     st->gshift = shift_for(mg, st->n_sample);
@@ -537,12 +514,8 @@ void launch_iota_rows(int32_t* rows, int n, cudaStream_t s) {
     check(cudaGetLastError(), "iota launch");
 }
 
-void launch_scales(const int32_t* rows, const double* g, const double* h, const uint8_t* goss_flag,
-                   double goss_scale, DevTreeState* st, int max_rows, cudaStream_t s) {
-    const int blocks = std::max(1, std::min(1184, (max_rows + 255) / 256));
-    scales_reduce_kernel<<<blocks, 256, 0, s>>>(rows, g, h, goss_flag, goss_scale, st);
-    check(cudaGetLastError(), "scales launch");
-    scales_finalize_kernel<<<1, 1, 0, s>>>(st);
+void launch_scales(DevTreeState* st, const AllScale* all, cudaStream_t s) {
+    scales_finalize_kernel<<<1, 1, 0, s>>>(st, all);
     check(cudaGetLastError(), "scales_finalize launch");
 }
 

@@ -28,6 +28,24 @@ __global__ void grad_mse_kernel(const double* __restrict__ y, const double* __re
     }
 }
 
+// The MSE gradient fused with the all-row maxima the fit needs from it: g = pred - y
+// (the unit hessian is implicit), max |g| and max h = 1 for the all-row fixed-point scale.
+__global__ void grad_mse_fused_kernel(const double* __restrict__ y, const double* __restrict__ pred, int n,
+                                      double* __restrict__ g, AllScale* __restrict__ sc) {
+    double mg = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double gv = 1.0 * (pred[i] - y[i]);
+        g[i] = gv;
+        mg = fmax(mg, fabs(gv));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+    // Non-negative doubles order like their bit patterns.
+    if ((threadIdx.x & 31) == 0) atomicMax(&sc->maxg_bits, static_cast<unsigned long long>(__double_as_longlong(mg)));
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        atomicMax(&sc->maxh_bits, static_cast<unsigned long long>(__double_as_longlong(1.0)));
+}
+
 __device__ __forceinline__ int row_at(const int* order, int p) { return order ? order[p] : p; }
 
 __global__ void grad_pairwise_kernel(const double* __restrict__ y, const double* __restrict__ pred,
@@ -201,6 +219,13 @@ void launch_grad_mse(const double* y, const double* pred, int n, double* g, doub
     if (n <= 0) return;
     grad_mse_kernel<<<std::min(2368, (n + 255) / 256), 256, 0, s>>>(y, pred, n, g, h);
     check(cudaGetLastError(), "grad_mse launch");
+}
+
+void launch_grad_mse_fused(const double* y, const double* pred, int n, double* g, AllScale* sc, cudaStream_t s) {
+    check(cudaMemsetAsync(sc, 0, 2 * sizeof(unsigned long long), s), "all scale reset");
+    if (n <= 0) return;
+    grad_mse_fused_kernel<<<std::min(2368, (n + 255) / 256), 256, 0, s>>>(y, pred, n, g, sc);
+    check(cudaGetLastError(), "grad_mse_fused launch");
 }
 
 void launch_grad_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len,

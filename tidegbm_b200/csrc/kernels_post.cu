@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kApplyThreads)
     // line at most, so the walk's byte loads hit the same line (L1) after the first
     // touch; g and h are loaded before the walk so their latency overlaps it.
     for (int r = ch.y + threadIdx.x; r < ch.z; r += blockDim.x) {
-        const double gv = g[r], hv = h[r];
+        const double gv = g[r], hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
         const uint8_t* row = codes + static_cast<size_t>(r) * stride;
         int k = 0;
         while (!s_leaf[k]) {
@@ -182,6 +182,37 @@ __global__ void pred_update_kernel(PostParams pp, const int16_t* __restrict__ ni
     }
 }
 
+// pred update fused with the MSE training loss on the updated predictions
+// (booster.cpp:655-664 then 704-706): per-block partial sums of (pred - y)^2.
+__global__ void pred_update_loss_kernel(PostParams pp, const int16_t* __restrict__ nid,
+                                        const double* __restrict__ prefix, const DevTreeState* __restrict__ st,
+                                        double* __restrict__ pred, const double* __restrict__ y,
+                                        double* __restrict__ partials) {
+    const int nn = st->n_nodes;
+    const int n = pp.n;
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = 0;
+        if (!pp.iid_mode) {
+            b = static_cast<int>(static_cast<double>(i) / max(n, 1) * pp.n_buckets);
+            if (b >= pp.n_buckets) b = pp.n_buckets - 1;
+        }
+        const double p = pred[i] + pp.learning_rate * prefix[static_cast<size_t>(b) * nn + nid[i]];
+        pred[i] = p;
+        const double d = p - y[i];
+        acc += 1.0 * d * d;
+    }
+    __shared__ double ws[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += ws[w];
+        partials[blockIdx.x] = t;
+    }
+}
+
 __global__ void fill_pred_kernel(const double* __restrict__ init_prefix, int n, int n_buckets, int iid_mode,
                                  double* __restrict__ pred) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -237,6 +268,17 @@ void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t
         codes, stride, n, tree_feat, tree_left, tree_right, tree_thr, tree_ml, tree_val, tree_off, n_trees, base,
         lr, out);
     check(cudaGetLastError(), "predict_trees launch");
+}
+
+void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
+                             double* pred, const double* y, double* partials, int n_part, cudaStream_t s) {
+    pred_update_loss_kernel<<<n_part, 256, 0, s>>>(pp, nid, prefix, st, pred, y, partials);
+    check(cudaGetLastError(), "pred_update_loss launch");
+}
+
+void launch_all_scale_finalize(AllScale* sc, int n, cudaStream_t s) {
+    all_scale_finalize_kernel<<<1, 1, 0, s>>>(sc, n);
+    check(cudaGetLastError(), "all_scale_finalize launch");
 }
 
 void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s) {

@@ -6,9 +6,13 @@
 // thresholds b = 1 .. n_bins-2 with a non-empty bin b, missing (bin 0) sent left or
 // right, min_samples_leaf on counts and min_child_weight on hessians, and ties broken
 // exactly as the reference's strict '>' does: lowest (feature, threshold,
-// missing_left) wins.  Prefix sums run in exact 64-bit integers (warp-shuffle scan,
-// 8 bins per lane); only the gain is FP64.  This file is compiled with -fmad=false
-// so the gain arithmetic follows the reference's statement order.
+// missing_left) wins.  Prefix sums run in exact 64-bit integers; only the gain is FP64.
+// This file is compiled with -fmad=false so the gain arithmetic follows the
+// reference's statement order.
+//
+// Launch shape: one CTA of 256 threads per (node, feature), thread = bin, so every
+// thread evaluates at most two candidates (missing left / right) and the launch is a
+// few dependent steps deep: the scan is latency-bound, not throughput-bound.
 //
 // select restates the leaf choice of grow_tree (cpp/src/tree.cpp:343-383): among
 // leaves with depth < max_depth and at least 2*min_samples_leaf rows, the largest
@@ -20,7 +24,8 @@ namespace tgb {
 
 namespace {
 
-constexpr int kScanWarps = 2;  // 2 warps per CTA: 64 CTAs per node at 128 features
+constexpr int kScanThreads = kBins;  // thread = bin
+constexpr int kScanWarps = kScanThreads / 32;
 
 struct Cand {
     double gain;
@@ -40,93 +45,7 @@ __device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
     return v;
 }
 
-__device__ __forceinline__ long long warp_sum(long long v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// One warp scans one feature of a histogram; returns the warp's best candidate
-// (identical in every lane) and the node totals.  With Pp / Ps set the histogram is
-// derived first: hist = parent - small sibling (subtract_hist_inplace,
-// cpp/src/histogram.cpp:108-117, exact in fixed point) and stored to Gf / Hf / Cf.
-// scan = false only derives and totals (a node that cannot split).
-__device__ Cand scan_feature(long long* __restrict__ Gf, long long* __restrict__ Hf, int* __restrict__ Cf,
-                             const long long* __restrict__ PGf, const long long* __restrict__ PHf,
-                             const int* __restrict__ PCf, const long long* __restrict__ SGf,
-                             const long long* __restrict__ SHf, const int* __restrict__ SCf, bool derive, bool scan,
-                             int f, int n_bins, double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
-                             double min_hess, long long& Gt, long long& Ht, long long& Ct) {
-    const int lane = threadIdx.x & 31;
-    long long g[8], hh[8];
-    int c[8];
-    if (derive) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int b = lane * 8 + i;
-            g[i] = PGf[b] - SGf[b];
-            hh[i] = PHf[b] - SHf[b];
-            c[i] = PCf[b] - SCf[b];
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i += 2) {
-            const int b = lane * 8 + i;
-            *reinterpret_cast<longlong2*>(Gf + b) = make_longlong2(g[i], g[i + 1]);
-            *reinterpret_cast<longlong2*>(Hf + b) = make_longlong2(hh[i], hh[i + 1]);
-        }
-        *reinterpret_cast<int4*>(Cf + lane * 8) = make_int4(c[0], c[1], c[2], c[3]);
-        *reinterpret_cast<int4*>(Cf + lane * 8 + 4) = make_int4(c[4], c[5], c[6], c[7]);
-    } else {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            g[i] = Gf[lane * 8 + i];
-            hh[i] = Hf[lane * 8 + i];
-            c[i] = Cf[lane * 8 + i];
-        }
-    }
-    long long sg = 0, sh = 0, sc = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        sg += g[i];
-        sh += hh[i];
-        sc += c[i];
-    }
-    const long long ig = warp_incl_scan(sg, lane), ih = warp_incl_scan(sh, lane),
-                    ic = warp_incl_scan(sc, lane);
-    Gt = __shfl_sync(0xffffffffu, ig, 31);
-    Ht = __shfl_sync(0xffffffffu, ih, 31);
-    Ct = __shfl_sync(0xffffffffu, ic, 31);
-    Cand best{-1e300, 0x7fffffff};
-    if (!scan) return best;
-    const long long G0 = __shfl_sync(0xffffffffu, g[0], 0);
-    const long long H0 = __shfl_sync(0xffffffffu, hh[0], 0);
-    const long long C0 = __shfl_sync(0xffffffffu, static_cast<long long>(c[0]), 0);
-    const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
-    const double parent = (dGt * dGt) / (dHt + lam);
-    long long pg = ig - sg, ph = ih - sh, pc = ic - sc;  // exclusive prefix of this lane
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        pg += g[i];
-        ph += hh[i];
-        pc += c[i];
-        const int b = lane * 8 + i;
-        if (b < 1 || b > n_bins - 2 || c[i] == 0) continue;
-        const long long GL = pg - G0, HL = ph - H0, CL = pc - C0;
-#pragma unroll
-        for (int ml = 0; ml <= 1; ++ml) {
-            const long long gL = GL + (ml ? G0 : 0), hL = HL + (ml ? H0 : 0), cL = CL + (ml ? C0 : 0);
-            const long long cR = Ct - cL;
-            if (cL < min_leaf || cR < min_leaf) continue;
-            const double dgL = static_cast<double>(gL) * inv_gs, dhL = static_cast<double>(hL) * inv_hs;
-            const double dgR = static_cast<double>(Gt - gL) * inv_gs,
-                         dhR = static_cast<double>(Ht - hL) * inv_hs;
-            if (dhL < min_hess || dhR < min_hess) continue;
-            const double gain =
-                0.5 * ((dgL * dgL) / (dhL + lam) + (dgR * dgR) / (dhR + lam) - parent) - gamma;
-            const Cand cand{gain, f * 512 + b * 2 + ml};
-            if (better(cand, best)) best = cand;
-        }
-    }
+__device__ __forceinline__ Cand warp_best(Cand best) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         Cand other{__shfl_xor_sync(0xffffffffu, best.gain, o), __shfl_xor_sync(0xffffffffu, best.key, o)};
@@ -135,15 +54,101 @@ __device__ Cand scan_feature(long long* __restrict__ Gf, long long* __restrict__
     return best;
 }
 
+struct ScanShared {
+    long long wg[kScanWarps], wh[kScanWarps], wc[kScanWarps];
+    long long g0, h0, c0;
+    Cand wbest[kScanWarps];
+};
+
+// One CTA scans one feature of a histogram; thread b owns bin b.  Returns the CTA's
+// best candidate in thread 0 and the feature's totals in every thread.  derive: the
+// histogram is first derived as parent - small sibling (subtract_hist_inplace,
+// cpp/src/histogram.cpp:108-117, exact in fixed point) and stored to Gf / Hf / Cf.
+// scan = false only derives and totals (a node that cannot split).
+__device__ Cand scan_feature(long long* __restrict__ Gf, long long* __restrict__ Hf, int* __restrict__ Cf,
+                             const long long* __restrict__ PGf, const long long* __restrict__ PHf,
+                             const int* __restrict__ PCf, const long long* __restrict__ SGf,
+                             const long long* __restrict__ SHf, const int* __restrict__ SCf, bool derive, bool scan,
+                             int f, int n_bins, double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
+                             double min_hess, ScanShared& sm, long long& Gt, long long& Ht, long long& Ct) {
+    const int b = threadIdx.x, lane = b & 31, warp = b >> 5;
+    long long g, hh, c;
+    if (derive) {
+        g = PGf[b] - SGf[b];
+        hh = PHf[b] - SHf[b];
+        c = PCf[b] - SCf[b];
+        Gf[b] = g;
+        Hf[b] = hh;
+        Cf[b] = static_cast<int>(c);
+    } else {
+        g = Gf[b];
+        hh = Hf[b];
+        c = Cf[b];
+    }
+    long long ig = warp_incl_scan(g, lane), ih = warp_incl_scan(hh, lane), ic = warp_incl_scan(c, lane);
+    if (lane == 31) {
+        sm.wg[warp] = ig;
+        sm.wh[warp] = ih;
+        sm.wc[warp] = ic;
+    }
+    if (b == 0) {
+        sm.g0 = g;
+        sm.h0 = hh;
+        sm.c0 = c;
+    }
+    __syncthreads();
+    Gt = Ht = Ct = 0;
+#pragma unroll
+    for (int w = 0; w < kScanWarps; ++w) {
+        if (w < warp) {
+            ig += sm.wg[w];
+            ih += sm.wh[w];
+            ic += sm.wc[w];
+        }
+        Gt += sm.wg[w];
+        Ht += sm.wh[w];
+        Ct += sm.wc[w];
+    }
+    Cand best{-1e300, 0x7fffffff};
+    if (scan && b >= 1 && b <= n_bins - 2 && c != 0) {
+        const long long G0 = sm.g0, H0 = sm.h0, C0 = sm.c0;
+        const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
+        const double parent = (dGt * dGt) / (dHt + lam);
+        const long long GL = ig - G0, HL = ih - H0, CL = ic - C0;  // bins 1..b
+#pragma unroll
+        for (int ml = 0; ml <= 1; ++ml) {
+            const long long gL = GL + (ml ? G0 : 0), hL = HL + (ml ? H0 : 0), cL = CL + (ml ? C0 : 0);
+            const long long cR = Ct - cL;
+            if (cL < min_leaf || cR < min_leaf) continue;
+            const double dgL = static_cast<double>(gL) * inv_gs, dhL = static_cast<double>(hL) * inv_hs;
+            const double dgR = static_cast<double>(Gt - gL) * inv_gs, dhR = static_cast<double>(Ht - hL) * inv_hs;
+            if (dhL < min_hess || dhR < min_hess) continue;
+            const double gain = 0.5 * ((dgL * dgL) / (dhL + lam) + (dgR * dgR) / (dhR + lam) - parent) - gamma;
+            const Cand cand{gain, f * 512 + b * 2 + ml};
+            if (better(cand, best)) best = cand;
+        }
+    }
+    if (!scan) return best;
+    best = warp_best(best);
+    if (lane == 0) sm.wbest[warp] = best;
+    __syncthreads();
+    if (b == 0) {
+#pragma unroll
+        for (int w = 1; w < kScanWarps; ++w)
+            if (better(sm.wbest[w], best)) best = sm.wbest[w];
+    }
+    return best;
+}
+
 __device__ void select_body(const GrowParams& p, DevNode* __restrict__ nodes, DevSplit* __restrict__ splits,
                             DevTreeState* __restrict__ st);
 
-// grid = (ceil(F / kScanWarps), nodes): one warp per (node, feature).  Each CTA reduces
-// its warps' candidates and stores one per CTA; the last CTA of a node to finish
-// (ticket counter, no waiting) reduces the per-CTA candidates, lowest feature on ties.
-// mode 1 (the two children of st->parent): the large child's histogram is derived from
-// the parent's and the small child's on the way (no separate subtraction pass).
-__global__ void __launch_bounds__(kScanWarps * 32)
+// grid = (F, nodes): one CTA per (node, feature).  Each CTA stores its best candidate;
+// the last CTA of a node to finish (ticket counter, no waiting) reduces them, lowest
+// feature on ties.  mode 1 (the two children of st->parent): the large child's
+// histogram is derived from the parent's and the small child's on the way (no separate
+// subtraction pass).  The last node of the launch to finish then picks the next leaf.
+__global__ void __launch_bounds__(kScanThreads)
     split_scan_kernel(GrowParams p, HistSlotPtrs hs, DevNode* __restrict__ nodes,
                       DevSplit* __restrict__ splits, DevTreeState* __restrict__ st, int mode,
                       int node, ScanScratch sc, int do_select) {
@@ -156,26 +161,25 @@ __global__ void __launch_bounds__(kScanWarps * 32)
         derive = nd == st->large_node;
     }
     const size_t e = hs.slot_elems;
-    long long* G = hs.G + nd * e;
-    long long* H = hs.H + nd * e;
-    int* C = hs.C + nd * e;
     const size_t po = derive ? static_cast<size_t>(st->parent) * e : 0;
     const size_t so = derive ? static_cast<size_t>(st->small_node) * e : 0;
     const double inv_gs = st->inv_gscale, inv_hs = st->inv_hscale;
     DevNode& N = nodes[nd];
     const bool eligible = N.depth < p.max_depth && N.count >= 2 * p.min_samples_leaf;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __shared__ Cand sbest[kScanWarps];
+    const int f = blockIdx.x;
+    __shared__ ScanShared sm;
     __shared__ int last;
     Cand best{-1e300, 0x7fffffff};
-    const int f = blockIdx.x * kScanWarps + warp;
-    if (f < p.n_features && (eligible || f == 0)) {
+    // A node that cannot split only needs its totals (feature 0); its other CTAs carry no
+    // candidate but still take part in the ticket protocol below.
+    if (eligible || f == 0) {
         const size_t fo = static_cast<size_t>(f) * kBins;
         long long Gt, Ht, Ct;
-        best = scan_feature(G + fo, H + fo, C + fo, hs.G + po + fo, hs.H + po + fo, hs.C + po + fo, hs.G + so + fo,
-                            hs.H + so + fo, hs.C + so + fo, derive, eligible, f, p.n_bins, inv_gs, inv_hs, p.l2,
-                            p.min_split_gain, p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
-        if (f == 0 && lane == 0) {
+        best = scan_feature(hs.G + nd * e + fo, hs.H + nd * e + fo, hs.C + nd * e + fo, hs.G + po + fo,
+                            hs.H + po + fo, hs.C + po + fo, hs.G + so + fo, hs.H + so + fo, hs.C + so + fo, derive,
+                            eligible, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain, p.min_samples_leaf,
+                            p.min_child_weight, sm, Gt, Ht, Ct);
+        if (f == 0 && threadIdx.x == 0) {
             // Node totals from feature 0 (every feature's bins sum to the same exact integers).
             N.G = Gt;
             N.H = Ht;
@@ -184,57 +188,44 @@ __global__ void __launch_bounds__(kScanWarps * 32)
             N.value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
         }
     }
-    // A node that cannot split still takes part in the ticket protocol: its CTAs carry no
-    // candidate, so the last one records an invalid split, and the launch-wide count that
-    // triggers the leaf choice sees every node.
-    if (lane == 0) sbest[warp] = best;
-    __syncthreads();
     if (threadIdx.x == 0) {
-        Cand b = sbest[0];
-        for (int w = 1; w < kScanWarps; ++w)
-            if (better(sbest[w], b)) b = sbest[w];
         const int slot = blockIdx.y * gridDim.x + blockIdx.x;
-        sc.gain[slot] = b.gain;
-        sc.key[slot] = b.key;
+        sc.gain[slot] = best.gain;
+        sc.key[slot] = best.key;
         __threadfence();
         last = atomicAdd(&sc.ticket[blockIdx.y], 1) == static_cast<int>(gridDim.x) - 1;
     }
     __syncthreads();
-    if (!last) return;
-    if (warp == 0) {
-        __threadfence();
-        Cand b{-1e300, 0x7fffffff};
-        for (int k = lane; k < static_cast<int>(gridDim.x); k += 32) {
-            const int slot = blockIdx.y * gridDim.x + k;
-            const Cand c{static_cast<volatile double*>(sc.gain)[slot], static_cast<volatile int*>(sc.key)[slot]};
-            if (better(c, b)) b = c;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            Cand other{__shfl_xor_sync(0xffffffffu, b.gain, o), __shfl_xor_sync(0xffffffffu, b.key, o)};
-            if (better(other, b)) b = other;
-        }
-        if (lane == 0) {
-            DevSplit s;
-            s.gain = b.gain;
-            s.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
-            s.feature = s.valid ? b.key / 512 : -1;
-            s.threshold = s.valid ? (b.key % 512) / 2 : -1;
-            s.missing_left = s.valid ? (b.key & 1) : 1;
-            splits[nd] = s;
-            sc.ticket[blockIdx.y] = 0;  // ready for the next launch
-        }
-        // The last node of the launch to finish picks the next leaf to split.
-        int sel = 0;
-        if (lane == 0 && do_select) {
-            __threadfence();
-            sel = atomicAdd(&sc.ticket[2], 1) == static_cast<int>(gridDim.y) - 1;
-            if (sel) sc.ticket[2] = 0;
-            __threadfence();
-        }
-        sel = __shfl_sync(0xffffffffu, sel, 0);
-        if (sel) select_body(p, nodes, splits, st);
+    if (!last || threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    __threadfence();
+    Cand b{-1e300, 0x7fffffff};
+    for (int k = lane; k < static_cast<int>(gridDim.x); k += 32) {
+        const int slot = blockIdx.y * gridDim.x + k;
+        const Cand c{static_cast<volatile double*>(sc.gain)[slot], static_cast<volatile int*>(sc.key)[slot]};
+        if (better(c, b)) b = c;
     }
+    b = warp_best(b);
+    if (lane == 0) {
+        DevSplit s;
+        s.gain = b.gain;
+        s.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
+        s.feature = s.valid ? b.key / 512 : -1;
+        s.threshold = s.valid ? (b.key % 512) / 2 : -1;
+        s.missing_left = s.valid ? (b.key & 1) : 1;
+        splits[nd] = s;
+        sc.ticket[blockIdx.y] = 0;  // ready for the next launch
+    }
+    // The last node of the launch to finish picks the next leaf to split.
+    int sel = 0;
+    if (lane == 0 && do_select) {
+        __threadfence();
+        sel = atomicAdd(&sc.ticket[2], 1) == static_cast<int>(gridDim.y) - 1;
+        if (sel) sc.ticket[2] = 0;
+        __threadfence();
+    }
+    sel = __shfl_sync(0xffffffffu, sel, 0);
+    if (sel) select_body(p, nodes, splits, st);
 }
 
 // grow_tree's leaf choice (cpp/src/tree.cpp:343-383), one warp.  Split records are read
@@ -298,21 +289,20 @@ __device__ void select_body(const GrowParams& p, DevNode* __restrict__ nodes, De
     st->n_nodes = nn + 2;
 }
 
-__global__ void __launch_bounds__(kScanWarps * 32)
+__global__ void __launch_bounds__(kScanThreads)
     scan_hist_kernel(const long long* G, const long long* H, const int* C, int n_f, int n_bins,
                      double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
                      double min_hess, double* gain, int* thr, int* ml) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int f = blockIdx.x * kScanWarps + warp;
-    if (f >= n_f) return;
+    const int f = blockIdx.x;
+    __shared__ ScanShared sm;
     long long Gt, Ht, Ct;
     const size_t fo = static_cast<size_t>(f) * kBins;
     long long* Gm = const_cast<long long*>(G + fo);
     long long* Hm = const_cast<long long*>(H + fo);
     int* Cm = const_cast<int*>(C + fo);
     const Cand c = scan_feature(Gm, Hm, Cm, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, false, true, f,
-                                n_bins, inv_gs, inv_hs, lam, gamma, min_leaf, min_hess, Gt, Ht, Ct);
-    if (lane == 0) {
+                                n_bins, inv_gs, inv_hs, lam, gamma, min_leaf, min_hess, sm, Gt, Ht, Ct);
+    if (threadIdx.x == 0) {
         const bool ok = c.key != 0x7fffffff;
         gain[f] = c.gain;
         thr[f] = ok ? (c.key % 512) / 2 : -1;
@@ -322,12 +312,12 @@ __global__ void __launch_bounds__(kScanWarps * 32)
 
 }  // namespace
 
-int scan_ctas_per_node(int n_f) { return (n_f + kScanWarps - 1) / kScanWarps; }
+int scan_ctas_per_node(int n_f) { return n_f; }
 
 void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits, DevTreeState* st,
                        int mode, int node, ScanScratch sc, bool do_select, cudaStream_t s) {
     dim3 grid(scan_ctas_per_node(p.n_features), mode == 1 ? 2 : 1);
-    split_scan_kernel<<<grid, kScanWarps * 32, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc, do_select ? 1 : 0);
+    split_scan_kernel<<<grid, kScanThreads, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc, do_select ? 1 : 0);
     check(cudaGetLastError(), "split_scan launch");
 }
 
@@ -335,7 +325,7 @@ void launch_scan_hist(const long long* G, const long long* H, const int* C, int 
                       double inv_gscale, double inv_hscale, double lam, double gamma, int min_leaf,
                       double min_hess, double* gain, int* thr, int* ml, cudaStream_t s) {
     if (n_f <= 0) return;
-    scan_hist_kernel<<<(n_f + kScanWarps - 1) / kScanWarps, kScanWarps * 32, 0, s>>>(
+    scan_hist_kernel<<<n_f, kScanThreads, 0, s>>>(
         G, H, C, n_f, n_bins, inv_gscale, inv_hscale, lam, gamma, min_leaf, min_hess, gain, thr, ml);
     check(cudaGetLastError(), "scan_hist launch");
 }

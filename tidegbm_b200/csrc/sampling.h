@@ -25,6 +25,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
+#include <immintrin.h>
+#endif
 #include <numeric>
 #include <random>
 #include <vector>
@@ -109,6 +112,40 @@ inline bool shuffle_pairs(int64_t m) {
     return m > 0 && urngrange / static_cast<unsigned long>(m) >= static_cast<unsigned long>(m);
 }
 
+#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
+#define TGB_HAVE_AVX512_TAIL 1
+// Groups of 16 consecutive draws of the tail with AVX-512: the 32x32->64 Lemire products
+// of the 16 words, a stop at the first group holding a word whose low half is below its
+// range (it goes to the exact path), and a masked scatter of out[j] = i for the draws
+// that land in the prefix.  Scatter writes to one address keep the highest lane, i.e.
+// the latest draw, as the sequential loop does.  Returns the number of words consumed.
+__attribute__((target("avx512f"))) inline int tail_groups_avx512(const uint32_t* w, int64_t i, int k, uint32_t K,
+                                                                  int32_t* out) {
+    const __m512i lane = _mm512_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
+    const __m512i vK = _mm512_set1_epi32(static_cast<int>(K));
+    int l = 0;
+    while (l + 16 <= k) {
+        const __m512i W = _mm512_loadu_si512(w + l);
+        const __m512i R = _mm512_add_epi32(_mm512_set1_epi32(static_cast<int>(i + l + 1)), lane);
+        const __m512i pe = _mm512_mul_epu32(W, R);
+        const __m512i po = _mm512_mul_epu32(_mm512_srli_epi64(W, 32), _mm512_srli_epi64(R, 32));
+        const __m512i lo = _mm512_mask_blend_epi32(0xAAAA, pe, _mm512_slli_epi64(po, 32));
+        if (_mm512_cmplt_epu32_mask(lo, R)) break;
+        const __m512i hi = _mm512_mask_blend_epi32(0xAAAA, _mm512_srli_epi64(pe, 32), po);
+        const __mmask16 hit = _mm512_cmplt_epu32_mask(hi, vK);
+        const __m512i I = _mm512_add_epi32(_mm512_set1_epi32(static_cast<int>(i + l)), lane);
+        _mm512_mask_i32scatter_epi32(out, hit, hi, I, 4);
+        l += 16;
+    }
+    return l;
+}
+
+inline bool have_avx512() {
+    static const bool ok = __builtin_cpu_supports("avx512f");
+    return ok;
+}
+#endif
+
 // The draws i in [i, m) of a shuffle whose first `keep` positions are tracked in out
 // (which has room for keep + 1 entries: out[keep] absorbs the draws that land outside
 // the prefix, so the store is branch-free).  A word whose Lemire product has low half
@@ -121,6 +158,9 @@ inline void shuffle_tail(int64_t i, int64_t m, int64_t keep, Mt32& rng, int32_t*
         const uint32_t* w = rng.out + rng.pos;
         const int k = static_cast<int>(std::min<int64_t>(624 - rng.pos, m - i));
         int l = 0;
+#ifdef TGB_HAVE_AVX512_TAIL
+        if (have_avx512()) l = tail_groups_avx512(w, i, k, K, out);
+#endif
         while (l + 16 <= k) {
             const uint32_t r0 = static_cast<uint32_t>(i + l + 1);
             uint32_t bad = 0;

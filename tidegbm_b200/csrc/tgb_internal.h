@@ -99,12 +99,14 @@ struct HistSlotPtrs {
 };
 
 struct GossWork {
-    unsigned long long* keys_in;
-    unsigned long long* keys_out;
+    void* keys_in;   // per row: 32-bit keys (fast path) or 64-bit |g| bit patterns (exact path)
+    void* keys_out;
     int32_t* vals_in;
     int32_t* vals_out;
     void* cub_tmp;
     size_t cub_tmp_bytes;
+    int* overflow;   // device flag: a run of equal 32-bit keys was too long to fix up
+    bool exact;
 };
 
 void check(cudaError_t e, const char* what);
@@ -166,8 +168,9 @@ void launch_hist_rows(const uint8_t* codes, int stride, int n_f, const int32_t* 
 void launch_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_sample_host, int use_dev_count,
                       cudaStream_t s);
 void launch_iota_rows(int32_t* rows, int n, cudaStream_t s);
-void launch_scales(const int32_t* rows, const double* g, const double* h, const uint8_t* goss_flag,
-                   double goss_scale, DevTreeState* st, int max_rows, cudaStream_t s);
+// Per-tree histogram scales from the sample maxima in st (reduced by the GOSS mark), or,
+// when the sample is every row, from the all-row maxima in `all`.
+void launch_scales(DevTreeState* st, const AllScale* all, cudaStream_t s);
 // Row chunks per feature group of a histogram launch (const_h: a multiple of the cluster size).
 int hist_grid_rows(int n_f, int max_rows, bool const_h);
 
@@ -208,6 +211,8 @@ void launch_partition_rows_noalloc(const uint8_t* codes, int stride, const int32
 
 // objectives (kernels_obj.cu)
 void launch_grad_mse(const double* y, const double* pred, int n, double* g, double* h, cudaStream_t s);
+// g = pred - y, sc <- max |g| and max h = 1 (reset first).
+void launch_grad_mse_fused(const double* y, const double* pred, int n, double* g, AllScale* sc, cudaStream_t s);
 void launch_grad_pairwise(const double* y, const double* pred, const int* run_start, const int* run_len,
                           const int* order, int n_runs, int n, double* g, double* h, cudaStream_t s);
 void launch_loss_mse(const double* y, const double* pred, int n, double* partials, int n_part, cudaStream_t s);
@@ -217,12 +222,19 @@ void launch_loss_finalize(int kind, const double* partials, const int* valid, in
                           double* out, cudaStream_t s);
 
 // GOSS (kernels_goss.cu)
-size_t goss_cub_bytes(int n);
-void launch_goss_select(const double* g, int n, int n_top, int n_other, const int32_t* rest_pos, GossWork& w,
-                        uint8_t* goss_flag, int32_t* rows0, int* tile_counts, DevTreeState* st, cudaStream_t s);
+size_t goss_cub_bytes(int n, bool exact);
+void launch_goss_iota(int32_t* vals, int n, cudaStream_t s);  // w.vals_in, once per fit
+// all: the all-row maxima of the tree's gradients (the 32-bit sort keys are relative to max |g|).
+void launch_goss_select(const double* g, const double* h, int n, int n_top, int n_other, const int32_t* rest_pos,
+                        GossWork& w, const AllScale* all, double goss_scale, uint8_t* goss_flag, int32_t* rows0,
+                        int* tile_counts, DevTreeState* st, cudaStream_t s);
 
 // post-tree sweep (kernels_post.cu)
 void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s);
+void launch_all_scale_finalize(AllScale* sc, int n, cudaStream_t s);
+// pred += lr * prefix[bucket][leaf] and per-block sums of (pred - y)^2 into partials[n_part].
+void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
+                             double* pred, const double* y, double* partials, int n_part, cudaStream_t s);
 void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
                         int16_t* nid, unsigned long long* seg_sums, int n_segments, cudaStream_t s);

@@ -230,7 +230,7 @@ class Booster:
                 "timed_ms", "timed_trees", "timed_launches", "hist_ms", "hist_launches", "hist_rows", "alloc", "h2d",
                 "transpose", "goss_producer"]
         res = dict(zip(keys, o.tolist()))
-        for k in ("bin_counts", "bin_draws", "bin_edges"):
+        for k in ("bin_counts", "bin_draws", "bin_edges", "goss_refits", "pre_upload", "prep"):
             v = C.c_double()
             check(lib().tgb_fit_stat(self._h, k.encode(), C.byref(v)))
             res[k] = v.value
