@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <thread>
 
@@ -33,6 +34,35 @@ void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw TideError(std::string("CUDA ") + what + ": " + cudaGetErrorString(e));
     const size_t L = std::strlen(what);
     if (L > 7 && std::strcmp(what + L - 7, " launch") == 0) g_kernel_launches.fetch_add(1);
+}
+
+void* device_alloc(size_t bytes) {
+    static std::mutex mu;
+    static bool configured[64] = {};
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev >= 0 && dev < 64) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!configured[dev]) {
+            cudaMemPool_t pool;
+            check(cudaDeviceGetDefaultMemPool(&pool, dev), "default mem pool");
+            uint64_t keep = ~0ull;  // never hand freed blocks back to the driver
+            check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "mem pool threshold");
+            configured[dev] = true;
+        }
+    }
+    void* p = nullptr;
+    check(cudaMallocAsync(&p, bytes, nullptr), "cudaMallocAsync");
+    check(cudaStreamSynchronize(nullptr), "cudaMallocAsync");  // usable from any stream from here on
+    return p;
+}
+
+void device_free(void* p) {
+    if (!p) return;
+    // Like cudaFree: wait until no queued work can still use the block, then return it
+    // to the pool.
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, nullptr);
 }
 
 void Config::validate() const {

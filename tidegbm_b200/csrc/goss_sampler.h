@@ -27,6 +27,38 @@
 
 namespace tgb {
 
+// Pinned host blocks kept for reuse across fits of the process (cudaMallocHost and
+// cudaFreeHost cost milliseconds each).
+inline std::mutex& pinned_cache_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+inline std::vector<std::pair<size_t, void*>>& pinned_cache() {
+    static std::vector<std::pair<size_t, void*>> cache;
+    return cache;
+}
+inline void* pinned_take(size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lk(pinned_cache_mutex());
+        auto& c = pinned_cache();
+        for (size_t k = 0; k < c.size(); ++k)
+            if (c[k].first == bytes) {
+                void* p = c[k].second;
+                c.erase(c.begin() + static_cast<long>(k));
+                return p;
+            }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) throw std::runtime_error("cudaMallocHost (GOSS positions)");
+    return p;
+}
+inline void pinned_give(size_t bytes, void* p) {
+    std::lock_guard<std::mutex> lk(pinned_cache_mutex());
+    auto& c = pinned_cache();
+    if (c.size() < 64) c.emplace_back(bytes, p);
+    else cudaFreeHost(p);
+}
+
 class GossSampler {
 public:
     GossSampler(uint32_t seed, int64_t m, int64_t keep, int n_trees, int n_slots, int n_workers)
@@ -34,8 +66,7 @@ public:
           snaps_(n_trees), produced_(n_trees, 0), ready_(n_trees, 0), released_(n_trees, 0),
           slot_(S_, nullptr), slot_ev_(S_, nullptr) {
         for (int k = 0; k < S_; ++k) {
-            if (cudaMallocHost(reinterpret_cast<void**>(&slot_[k]), sizeof(int32_t) * keep_) != cudaSuccess)
-                throw std::runtime_error("cudaMallocHost (GOSS positions)");
+            slot_[k] = static_cast<int32_t*>(pinned_take(sizeof(int32_t) * keep_));
             if (cudaEventCreateWithFlags(&slot_ev_[k], cudaEventDisableTiming) != cudaSuccess)
                 throw std::runtime_error("cudaEventCreate (GOSS positions)");
         }
@@ -66,7 +97,7 @@ public:
     ~GossSampler() {
         stop();
         for (int k = 0; k < S_; ++k) {
-            if (slot_[k]) cudaFreeHost(slot_[k]);
+            if (slot_[k]) pinned_give(sizeof(int32_t) * keep_, slot_[k]);
             if (slot_ev_[k]) cudaEventDestroy(slot_ev_[k]);
         }
     }

@@ -214,6 +214,16 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
                            const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st, int node,
                            const long long* __restrict__ gq, double goss_scale, HistSlotPtrs hs,
                            unsigned long long* rows_counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);
+    unsigned int* pHi = pLo + kPlane;
+    unsigned int* pCn = pHi + kPlane;
+    {  // private state first: it overlaps the previous kernel's tail
+        uint4* z = reinterpret_cast<uint4*>(smem_raw);
+        for (int k = threadIdx.x; k < 3 * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
+    }
+    pdl_wait();
+    pdl_trigger();
     if (st->done || (node < 0 && st->small_node < 0)) return;  // uniform over the grid
     const int nd = node >= 0 ? node : st->small_node;
     const DevNode& N = nodes[nd];
@@ -226,11 +236,6 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
     int* C = hs.C + nd * hs.slot_elems;
     const double hscale = st->hscale;
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);
-    unsigned int* pHi = pLo + kPlane;
-    unsigned int* pCn = pHi + kPlane;
-
     // Row chunks: a multiple of kCluster, so whole clusters are active or idle.
     const int need = (count + kMinRowsPerCta - 1) / kMinRowsPerCta;
     const int n_chunks = min(static_cast<int>(gridDim.y), (max(1, need) + kCluster - 1) / kCluster * kCluster);
@@ -239,10 +244,6 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
     const int r0 = min(count, static_cast<int>(blockIdx.y) * chunk);
     const int r1 = min(count, r0 + chunk);
 
-    {
-        uint4* z = reinterpret_cast<uint4*>(smem_raw);
-        for (int k = threadIdx.x; k < 3 * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
-    }
     long long accG[kCells];
     unsigned int accC1[kCells], accC2[kCells];
 #pragma unroll
@@ -474,8 +475,9 @@ void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const*
     dim3 grid((n_f + kFG - 1) / kFG, max(1, grid_rows));
     if (const_h) {
         set_smem(hist_node_const_kernel, kConstSmem);
-        hist_node_const_kernel<<<grid, kHistThreads, kConstSmem, s>>>(codes, stride, n_f, rows[0], rows[1], nodes, st,
-                                                                      node, gq, goss_scale, hs, rows_counter);
+        launch_pdl(hist_node_const_kernel, grid, dim3(kHistThreads), kConstSmem, s, "hist_node launch", codes, stride,
+                   n_f, rows[0], rows[1], nodes, st, node, gq, goss_scale, hs, rows_counter);
+        return;
     } else {
         set_smem(hist_node_kernel<false>, hist_smem(false));
         hist_node_kernel<false><<<grid, kHistThreads, hist_smem(false), s>>>(

@@ -91,6 +91,8 @@ __global__ void __launch_bounds__(kPartThreads)
     part_count_kernel(const uint8_t* __restrict__ codes, int stride, PartJob given, const DevNode* __restrict__ nodes,
                       const DevTreeState* __restrict__ st, int32_t* rows0, int32_t* rows1,
                       int* __restrict__ tile_counts) {
+    pdl_wait();
+    pdl_trigger();
     PartJob j;
     if (!resolve_job(given, nodes, st, rows0, rows1, j)) return;
     __shared__ int red[kPartWarps];
@@ -113,6 +115,8 @@ __global__ void __launch_bounds__(kPartThreads)
     part_scatter_kernel(const uint8_t* __restrict__ codes, int stride, PartJob given, DevNode* __restrict__ nodes,
                         DevTreeState* __restrict__ st, int32_t* rows0, int32_t* rows1,
                         const int* __restrict__ tile_counts) {
+    pdl_wait();
+    pdl_trigger();
     PartJob j;
     if (!resolve_job(given, nodes, st, rows0, rows1, j)) return;
     __shared__ int red[kPartWarps];
@@ -191,10 +195,10 @@ __global__ void __launch_bounds__(kPartThreads)
 void run_partition(const uint8_t* codes, int stride, const PartJob& j, DevNode* nodes, DevTreeState* st,
                    int32_t* rows0, int32_t* rows1, int* tile_counts, int max_tiles, cudaStream_t s) {
     const int grid = max(1, min(max_tiles, 148 * 8));
-    part_count_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, j, nodes, st, rows0, rows1, tile_counts);
-    check(cudaGetLastError(), "part_count launch");
-    part_scatter_kernel<<<grid, kPartThreads, 0, s>>>(codes, stride, j, nodes, st, rows0, rows1, tile_counts);
-    check(cudaGetLastError(), "part_scatter launch");
+    launch_pdl(part_count_kernel, dim3(grid), dim3(kPartThreads), 0, s, "part_count launch", codes, stride, j, nodes,
+               st, rows0, rows1, tile_counts);
+    launch_pdl(part_scatter_kernel, dim3(grid), dim3(kPartThreads), 0, s, "part_scatter launch", codes, stride, j,
+               nodes, st, rows0, rows1, static_cast<const int*>(tile_counts));
 }
 
 }  // namespace

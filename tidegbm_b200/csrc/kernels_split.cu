@@ -152,6 +152,8 @@ __global__ void __launch_bounds__(kScanThreads)
     split_scan_kernel(GrowParams p, HistSlotPtrs hs, DevNode* __restrict__ nodes,
                       DevSplit* __restrict__ splits, DevTreeState* __restrict__ st, int mode,
                       int node, ScanScratch sc, int do_select) {
+    pdl_wait();
+    pdl_trigger();
     if (st->done || (mode == 1 && st->parent < 0)) return;
     int nd = node;
     bool derive = false;
@@ -317,8 +319,8 @@ int scan_ctas_per_node(int n_f) { return n_f; }
 void launch_split_scan(const GrowParams& p, HistSlotPtrs hs, DevNode* nodes, DevSplit* splits, DevTreeState* st,
                        int mode, int node, ScanScratch sc, bool do_select, cudaStream_t s) {
     dim3 grid(scan_ctas_per_node(p.n_features), mode == 1 ? 2 : 1);
-    split_scan_kernel<<<grid, kScanThreads, 0, s>>>(p, hs, nodes, splits, st, mode, node, sc, do_select ? 1 : 0);
-    check(cudaGetLastError(), "split_scan launch");
+    launch_pdl(split_scan_kernel, grid, dim3(kScanThreads), 0, s, "split_scan launch", p, hs, nodes, splits, st, mode,
+               node, sc, do_select ? 1 : 0);
 }
 
 void launch_scan_hist(const long long* G, const long long* H, const int* C, int n_f, int n_bins,

@@ -111,6 +111,40 @@ struct GossWork {
 
 void check(cudaError_t e, const char* what);
 
+#if defined(__CUDACC__)
+// Programmatic dependent launch.  A kernel launched with launch_pdl may start while the
+// previous kernel of its stream is still running: before pdl_wait() it may only touch
+// its own registers and shared memory; pdl_wait() returns once the previous kernel has
+// completed and its writes are visible.  pdl_trigger() lets the next such kernel launch
+// (its own pdl_wait() still waits for this kernel to complete).  Outside a programmatic
+// launch both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const char* what,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    check(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...), what);
+}
+#endif
+
+// Device memory from the current device's stream-ordered pool, which keeps freed blocks
+// for later allocations of the process (repeated fits do not map fresh pages each time).
+// Both calls complete before they return, as cudaMalloc / cudaFree do: the block is usable
+// from any stream, and it is released only once the device is idle.
+void* device_alloc(size_t bytes);
+void device_free(void* p);
+
 // Owning device buffer (freed on scope exit).
 template <class T>
 struct DBuf {
@@ -121,11 +155,11 @@ struct DBuf {
     DBuf& operator=(const DBuf&) = delete;
     void alloc(size_t k) {
         release();
-        if (k) check(cudaMalloc(reinterpret_cast<void**>(&p), k * sizeof(T)), "cudaMalloc");
+        if (k) p = static_cast<T*>(device_alloc(k * sizeof(T)));
         n = k;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) device_free(p);
         p = nullptr;
         n = 0;
     }
