@@ -269,6 +269,19 @@ def plain_gpu_hist(native, X32, edges, n_edges, idx, g, h, n_bins) -> dict | Non
 
 
 # ---------------------------------------------------------------- ours
+def held_out_ic(pred, panel) -> float:
+    """Mean over dates of the Pearson correlation between prediction and target (rows are
+    sorted by date with equal cross-sections)."""
+    d = int(panel.ts.max()) + 1
+    a = pred.reshape(d, -1)
+    b = panel.y.reshape(d, -1)
+    a = a - a.mean(axis=1, keepdims=True)
+    b = b - b.mean(axis=1, keepdims=True)
+    den = np.sqrt((a * a).sum(axis=1) * (b * b).sum(axis=1))
+    ok = den > 0
+    return float(((a * b).sum(axis=1)[ok] / den[ok]).mean())
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -361,6 +374,35 @@ def run_ours(args) -> None:
             "algorithmic_bytes": "rows x (128 code bytes + 16 B f64 g,h) per built node",
             "traffic_note": "DRAM bytes per launch: ncu dram__bytes_read+write of the root launch of the 4M-row case "
                             "per row (profiles/hist_traffic.json) x rows per launch here"}
+    # int8 precision mode on the same workload: device trees/s, histogram GB/s, and the
+    # held-out IC of both modes on a fresh 1M-row panel of the same target function.
+    precision = None
+    if rank == 0:
+        try:
+            bq = native.Booster(device=local, **dict(PARAMS, n_estimators=n_est, timing_from=W, timing_to=W + K,
+                                                     hist_bits=8))
+            bq.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+            sq = bq.fit_stats()
+            bqp = native.Booster(device=local, **dict(PARAMS, n_estimators=W + 2, timing_from=W, timing_to=W + 2,
+                                                      profile_hist=1, hist_bits=8))
+            bqp.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+            sqp = bqp.fit_stats()
+            del bqp
+            q_gbs = sqp["hist_rows"] * (nf + 16) / (sqp["hist_ms"] / 1e3) / 1e9 if sqp["hist_ms"] > 0 else None
+            from tidegbm_b200 import panels
+
+            ho = panels.panel_scale(n_dates=500, seed=2, sample_seed=12)
+            ic_e, ic_q = held_out_ic(b.raw_predict(ho.X), ho), held_out_ic(bq.raw_predict(ho.X), ho)
+            precision = {"mode": "hist_bits=8 (int8 gradients, stochastic rounding, one shared reduction per code)",
+                         "value": 1000.0 / (sq["timed_ms"] / sq["timed_trees"]), "unit": "trees/s",
+                         "ms_per_step": sq["timed_ms"] / sq["timed_trees"], "hist_gbs": q_gbs,
+                         "hist_roofline_frac": (q_gbs / pk["hbm_gbs"]) if q_gbs else None,
+                         "held_out_ic_exact": ic_e, "held_out_ic_int8": ic_q, "ic_change": ic_q - ic_e,
+                         "held_out": "1M rows (500 dates x 2000): the training panel's target function, new rows "
+                                     "(sample seed 12)"}
+            del bq
+        except Exception as e:
+            precision = {"unavailable": f"{type(e).__name__}: {e}"}
     line = {"metric": METRIC, "value": value, "unit": "trees/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 (int64 fixed-point histograms)", "data": "synthetic",
@@ -370,7 +412,7 @@ def run_ours(args) -> None:
             "hist_gbs": hist_gbs, "roofline": roof, "e2e": e2e,
             "gpu_launches": int(st["timed_launches"]),
             "gpu_launches_note": "this library's kernels per K timed trees (+ CUB radix-sort passes inside GOSS)",
-            "clocks": clk.summary()}
+            "clocks": clk.summary(), "precision_int8": precision}
     if rank == 0 and not args.no_baselines:
         try:
             line["cpu_baseline"] = {k: v for k, v in ref_cpu_trees_per_s(1, 3).items() if k != "per_tree_s_sample"}

@@ -46,7 +46,11 @@ TGB_API int tgb_booster_create(int device, tgb_booster** out);
 TGB_API void tgb_booster_free(tgb_booster* b);
 
 /* tide_set_int / tide_set_double (c_api.cpp:234-272), extended to every Config key the
- * GPU path reads (cpp/include/tidegbm/config.hpp:49-113).  Unknown keys return -1. */
+ * GPU path reads (cpp/include/tidegbm/config.hpp:49-113).  Unknown keys return -1.
+ * One int key is this library's own: "hist_bits" = 0 (default: exact 64-bit fixed-point
+ * histograms, results match the reference) or 8 (int8 gradients with stochastic rounding,
+ * one shared reduction per code: a faster, approximate split search; leaf values stay
+ * exact; objective mse only). */
 TGB_API int tgb_set_int(tgb_booster* b, const char* key, long long value);
 TGB_API int tgb_set_double(tgb_booster* b, const char* key, double value);
 /* String keys the reference only sets through pybind (bindings.cpp:78, 115-125):

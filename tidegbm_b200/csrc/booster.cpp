@@ -90,6 +90,8 @@ void Config::validate() const {
     if (causal_bins || causal_structure || structure_frac < 1.0 || entity_subsample < 1.0)
         throw TideError("GPU path: causal_bins / causal_structure / structure_frac / entity_subsample unsupported");
     if (goss_top <= 0.0) throw TideError("GPU path: goss_top must be > 0");
+    if (hist_bits != 0 && hist_bits != 8) throw TideError("hist_bits must be 0 (exact) or 8 (int8 gradients)");
+    if (hist_bits == 8 && objective != 0) throw TideError("hist_bits = 8 needs a constant hessian (objective mse)");
 }
 
 namespace {
@@ -129,6 +131,7 @@ struct DeviceState {
     DBuf<uint8_t> codes, codes_col;
     DBuf<double> y, pred, g, h;
     DBuf<long long> gq;  // per-tree packed fixed-point g (constant-hessian histograms)
+    DBuf<short> gq8;     // per-tree packed int8 g (int8 precision mode)
     DBuf<int32_t> rows0, rows1;
     DBuf<long long> histG, histH;
     DBuf<int> histC;
@@ -351,7 +354,8 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     D.pred.alloc(n);
     D.g.alloc(n);
     if (c.objective != 0) D.h.alloc(n);  // MSE hessians are implicit (unit)
-    if (c.objective == 0) D.gq.alloc(n);
+    if (c.objective == 0 && c.hist_bits == 0) D.gq.alloc(n);
+    if (c.hist_bits == 8) D.gq8.alloc(n);
     D.rows0.alloc(n);
     D.rows1.alloc(n);
     D.histG.alloc(slot * max_nodes);
@@ -499,7 +503,7 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
         }
         check(cudaStreamSynchronize(s), "runs upload");
     } else {
-        D.loss_part.alloc(592);
+        D.loss_part.alloc(2368);
     }
 
     // GOSS device buffers (the sample itself is set up with the sampler, above).
@@ -553,7 +557,9 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     auto hist_launch = [&](int node, const uint8_t* flag, bool in_timed) {
         const bool prof = in_timed && c.profile_hist && hist_ev_used + 2 <= hist_ev.size();
         if (prof) check(cudaEventRecord(hist_ev[hist_ev_used], s), "event record");
-        launch_hist_node(D.codes.p, stride, n_f, rows, D.nodes.p, D.st.p, node, D.g.p, D.h.p, D.gq.p, flag, goss_scale, hs,
+        const void* gq = c.hist_bits == 8 ? static_cast<const void*>(D.gq8.p) : static_cast<const void*>(D.gq.p);
+        launch_hist_node(D.codes.p, stride, n_f, rows, D.nodes.p, D.st.p, node, D.g.p, D.h.p, gq, c.hist_bits == 8,
+                         flag, goss_scale, hs,
                          grid_rows, in_timed ? rows_counter.p : nullptr, c.objective == 0, s);
         if (prof) {
             check(cudaEventRecord(hist_ev[hist_ev_used + 1], s), "event record");
@@ -591,18 +597,28 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
             check(cudaMemcpyAsync(D.rest_pos.p, pos, sizeof(int32_t) * std::max(1, n_other), cudaMemcpyHostToDevice, s),
                   "positions upload");
             sampler->release(t, s);
-            launch_goss_select(D.g.p, h_rows, n, n_top, n_other, D.rest_pos.p, gw, D.all_scale.p, goss_scale,
+            launch_goss_select(D.g.p, h_rows, n, n_top, n_other, D.rest_pos.p, sampler->min_pos(t), gw,
+                               D.all_scale.p, goss_scale,
                                D.goss_flag.p,
                                D.rows0.p, D.tile_counts.p, D.st.p, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, 0, 1, s);
-            launch_scales(D.st.p, nullptr, s);
+            launch_scales(D.st.p, nullptr, c.hist_bits == 8, s);
         } else {
             launch_iota_rows(D.rows0.p, n, s);
             launch_tree_init(D.nodes.p, D.splits.p, D.st.p, n, 0, s);
-            launch_scales(D.st.p, D.all_scale.p, s);
+            launch_scales(D.st.p, D.all_scale.p, c.hist_bits == 8, s);
         }
         const uint8_t* flag = use_goss ? D.goss_flag.p : nullptr;
-        if (const_h) launch_quantize(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, D.gq.p, n, s);
+        if (c.hist_bits == 8) {
+            // per-tree stream of the stochastic rounding (SplitMix64 of seed and tree)
+            uint64_t z = (static_cast<uint64_t>(static_cast<uint32_t>(c.random_state)) << 32) + static_cast<uint64_t>(t);
+            z += 0x9e3779b97f4a7c15ull;
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+            launch_quantize8(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, z ^ (z >> 31), D.gq8.p, n, s);
+        } else if (const_h) {
+            launch_quantize(D.rows0.p, D.g.p, flag, goss_scale, D.st.p, D.gq.p, n, s);
+        }
         check(cudaMemsetAsync(D.histG.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histH.p, 0, sizeof(long long) * slot * max_nodes, s), "hist reset");
         check(cudaMemsetAsync(D.histC.p, 0, sizeof(int) * slot * max_nodes, s), "hist reset");
@@ -626,8 +642,8 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
                              cover_t, prefix_t, s);
         // prediction update, then the training loss (booster.cpp:704-706)
         if (const_h) {
-            launch_pred_update_loss(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, D.y.p, D.loss_part.p, 592, s);
-            launch_loss_finalize(0, D.loss_part.p, nullptr, 592, n, D.losses.p + t, s);
+            launch_pred_update_loss(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, D.y.p, D.loss_part.p, 2368, s);
+            launch_loss_finalize(0, D.loss_part.p, nullptr, 2368, n, D.losses.p + t, s);
         } else {
             launch_pred_update(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, s);
             launch_loss_pairwise(D.y.p, D.pred.p, D.run_start.p, D.run_len.p, order_d, n_runs, D.loss_part.p,

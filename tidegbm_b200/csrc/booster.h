@@ -56,6 +56,10 @@ struct Config {
     bool causal_structure = false;
     double structure_frac = 1.0;
     double entity_subsample = 1.0;
+    // Histogram precision: 0 = exact 64-bit fixed point (results match the reference), 8 =
+    // int8 gradients with stochastic rounding (one shared reduction per code; approximate
+    // split search, exact leaf values).  8 needs a constant hessian (mse).
+    int hist_bits = 0;
     // Measurement hooks (no effect on results): CUDA events around trees
     // [timing_from, timing_to) (timing_to < 0: through the last tree), and per-launch
     // events around every histogram kernel in that range.

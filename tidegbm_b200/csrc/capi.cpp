@@ -117,6 +117,7 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "causal_structure") c.causal_structure = v != 0;
         else if (k == "timing_from") c.timing_from = static_cast<int>(v);
         else if (k == "timing_to") c.timing_to = static_cast<int>(v);
+        else if (k == "hist_bits") c.hist_bits = static_cast<int>(v);
         else if (k == "profile_hist") c.profile_hist = v != 0;
         else if (k == "verbose" || k == "col_major_hist" || k == "cat_min_count") { /* no effect on GPU path */ }
         else throw tgb::TideError("unknown int key");

@@ -63,7 +63,7 @@ class GossSampler {
 public:
     GossSampler(uint32_t seed, int64_t m, int64_t keep, int n_trees, int n_slots, int n_workers)
         : m_(m), keep_(std::max<int64_t>(1, keep)), T_(n_trees), S_(std::max(1, n_slots)),
-          snaps_(n_trees), produced_(n_trees, 0), ready_(n_trees, 0), released_(n_trees, 0),
+          snaps_(n_trees), min_pos_(n_trees, 0), produced_(n_trees, 0), ready_(n_trees, 0), released_(n_trees, 0),
           slot_(S_, nullptr), slot_ev_(S_, nullptr) {
         for (int k = 0; k < S_; ++k) {
             slot_[k] = static_cast<int32_t*>(pinned_take(sizeof(int32_t) * keep_));
@@ -110,6 +110,10 @@ public:
         if (!error_.empty()) throw std::runtime_error(error_);
         return slot_[t % S_];
     }
+
+    // Smallest position of tree t's draw (valid once wait(t) returned): the sampled row of
+    // the remainder with the largest |g|.
+    int32_t min_pos(int t) const { return min_pos_[t]; }
 
     // After the consumer enqueued the copy of tree t's slot on `stream`.
     void release(int t, cudaStream_t stream) {
@@ -165,6 +169,7 @@ private:
             }
             Mt32 rng = snaps_[t];
             shuffled_prefix(m_, keep_, rng, slot_[k]);
+            min_pos_[t] = *std::min_element(slot_[k], slot_[k] + keep_);
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 ready_[t] = 1;
@@ -176,6 +181,7 @@ private:
     int64_t m_, keep_;
     int T_, S_;
     std::vector<Mt32> snaps_;
+    std::vector<int32_t> min_pos_;
     std::vector<char> produced_, ready_, released_;
     std::vector<int32_t*> slot_;
     std::vector<cudaEvent_t> slot_ev_;

@@ -94,30 +94,37 @@ __global__ void goss_iota_kernel(int32_t* __restrict__ vals, int n) {
 }
 
 // Marks the sample and reduces the maxima the histogram scales need over it: |g| and
-// |h| of the top rows, |g * scale| and |h * scale| of the sampled others (the values
-// the tree sees); h == nullptr means unit hessians.
+// |h| of the top rows, |g * scale| and |h * scale| of the sampled others (the values the
+// tree sees).  With unit hessians (h == nullptr) the maxima are known from two rows: the
+// first of the |g| order (the largest |g|) and the sampled other of smallest remainder
+// rank (min_rest, the largest |g| among them); only those two threads read g.
 __global__ void goss_mark_kernel(const int32_t* __restrict__ order, const unsigned int* __restrict__ k32,
                                  const int32_t* __restrict__ fixed, int n, int n_top, int n_other,
-                                 const int32_t* __restrict__ rest_pos, const double* __restrict__ g,
+                                 const int32_t* __restrict__ rest_pos, int min_rest, const double* __restrict__ g,
                                  const double* __restrict__ h, double goss_scale, uint8_t* __restrict__ flag,
                                  DevTreeState* __restrict__ st) {
     const int total = n_top + n_other;
     double mg = 0.0, mh = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
         const bool top = p < n_top;
-        const int pos = top ? p : n_top + rest_pos[p - n_top];
+        const int rp = top ? 0 : rest_pos[p - n_top];
+        const int pos = top ? p : n_top + rp;
         const int r = (k32 != nullptr && in_run(k32, pos, n)) ? fixed[pos] : order[pos];
         flag[r] = top ? 1 : 2;
-        const double hv = h ? h[r] : 1.0;
-        mg = fmax(mg, top ? fabs(g[r]) : fabs(g[r] * goss_scale));
-        mh = fmax(mh, top ? fabs(hv) : fabs(hv * goss_scale));
+        if (h != nullptr) {
+            mg = fmax(mg, top ? fabs(g[r]) : fabs(g[r] * goss_scale));
+            mh = fmax(mh, top ? fabs(h[r]) : fabs(h[r] * goss_scale));
+        } else if (top ? p == 0 : rp == min_rest) {
+            mg = fmax(mg, top ? fabs(g[r]) : fabs(g[r] * goss_scale));
+            mh = fmax(mh, top ? 1.0 : fabs(1.0 * goss_scale));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
         mh = fmax(mh, __shfl_xor_sync(0xffffffffu, mh, o));
     }
-    if ((threadIdx.x & 31) == 0) {
+    if ((threadIdx.x & 31) == 0 && (mg > 0.0 || mh > 0.0)) {
         atomicMax(&st->max_abs_g_bits, static_cast<unsigned long long>(__double_as_longlong(mg)));
         atomicMax(&st->max_h_bits, static_cast<unsigned long long>(__double_as_longlong(mh)));
     }
@@ -148,8 +155,8 @@ void launch_goss_iota(int32_t* vals, int n, cudaStream_t s) {
 }
 
 void launch_goss_select(const double* g, const double* h, int n, int n_top, int n_other, const int32_t* rest_pos,
-                        GossWork& w, const AllScale* all, double goss_scale, uint8_t* goss_flag, int32_t* rows0,
-                        int* tile_counts, DevTreeState* st, cudaStream_t s) {
+                        int min_rest, GossWork& w, const AllScale* all, double goss_scale, uint8_t* goss_flag,
+                        int32_t* rows0, int* tile_counts, DevTreeState* st, cudaStream_t s) {
     const int blocks = std::max(1, std::min(2368, (n + 255) / 256));
     if (w.exact) goss_keys_kernel<true><<<blocks, 256, 0, s>>>(g, n, all, w.keys_in);
     else goss_keys_kernel<false><<<blocks, 256, 0, s>>>(g, n, all, w.keys_in);
@@ -175,7 +182,7 @@ void launch_goss_select(const double* g, const double* h, int n, int n_top, int 
     check(cudaMemsetAsync(goss_flag, 0, static_cast<size_t>(n), s), "goss flag reset");
     check(cudaMemsetAsync(&st->max_abs_g_bits, 0, 2 * sizeof(unsigned long long), s), "sample max reset");
     goss_mark_kernel<<<std::max(1, std::min(2368, (n_top + n_other + 255) / 256)), 256, 0, s>>>(
-        w.vals_out, k32, fixed, n, n_top, n_other, rest_pos, g, h, goss_scale, goss_flag, st);
+        w.vals_out, k32, fixed, n, n_top, n_other, rest_pos, min_rest, g, h, goss_scale, goss_flag, st);
     check(cudaGetLastError(), "goss_mark launch");
     launch_compact_flagged(goss_flag, n, rows0, &st->n_sample, tile_counts, s);
 }

@@ -209,18 +209,31 @@ __device__ __forceinline__ void rotate_words(unsigned int (&w)[8], int k) {
 constexpr int kCluster = 4;
 constexpr size_t kConstSmem = static_cast<size_t>(kPlane) * 4 * 4;  // 3 accumulation planes, then 4 total planes
 
+// kQ8 (the int8 precision mode): gq holds int16 (q << 1) | s per row, q in [-127, 127]
+// the stochastically rounded g * goss_factor * gscale.  Each code then costs ONE 32-bit
+// reduction, (1 << 20) | (q + 128), into the plane of its row class (unscaled / GOSS-
+// scaled; the two planes share banks, so a warp mixing classes stays conflict-free):
+// over kSub8 = 3072 rows the low 20 bits hold sum(q + 128) <= 255 * 3072 and the high 12
+// the row count, exactly.
+constexpr int kSub8 = 3072;
+
+template <bool kQ8>
 __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
     hist_node_const_kernel(const uint8_t* __restrict__ codes, int stride, int n_f, int32_t* rows0, int32_t* rows1,
                            const DevNode* __restrict__ nodes, const DevTreeState* __restrict__ st, int node,
-                           const long long* __restrict__ gq, double goss_scale, HistSlotPtrs hs,
+                           const void* __restrict__ gq_any, double goss_scale, HistSlotPtrs hs,
                            unsigned long long* rows_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);
-    unsigned int* pHi = pLo + kPlane;
+    unsigned int* pLo = reinterpret_cast<unsigned int*>(smem_raw);  // kQ8: class-1 plane
+    unsigned int* pHi = pLo + kPlane;                               // kQ8: class-2 plane
     unsigned int* pCn = pHi + kPlane;
+    constexpr int kPlanes = kQ8 ? 2 : 3;
+    constexpr int kSubRows = kQ8 ? kSub8 : kSub;
+    const long long* __restrict__ gq = static_cast<const long long*>(gq_any);
+    const short* __restrict__ gq8 = static_cast<const short*>(gq_any);
     {  // private state first: it overlaps the previous kernel's tail
         uint4* z = reinterpret_cast<uint4*>(smem_raw);
-        for (int k = threadIdx.x; k < 3 * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
+        for (int k = threadIdx.x; k < kPlanes * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
     }
     pdl_wait();
     pdl_trigger();
@@ -259,17 +272,29 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
     // stride and fg0 are multiples of 16 and 32: the group has 16 or >= 32 bytes in a row
     const bool two_chunks = stride - fg0 >= 32;
     const int q = lane >> 2, sh = (lane & 3) * 8;
-    for (int s0 = r0; s0 < r1; s0 += kSub) {
-        const int s1 = min(r1, s0 + kSub);
+    for (int s0 = r0; s0 < r1; s0 += kSubRows) {
+        const int s1 = min(r1, s0 + kSubRows);
+        // the next row id is loaded one iteration ahead, so each iteration waits for one
+        // memory round trip (its row's g and codes) instead of two
+        int r_next = s0 + warp * 32 + lane < s1 ? rows[s0 + warp * 32 + lane] : -1;
         for (int base = s0 + warp * 32; base < s1; base += kHistWarps * 32) {
-            const int k = base + lane;
-            if (k < s1) {
-                const int r = rows[k];
-                const long long p = gq[r];
-                const long long v = p >> 1;
-                const unsigned int lo = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
-                const unsigned int hi = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
-                const unsigned int inc = (p & 1) ? 0x10000u : 1u;
+            const int r = r_next;
+            const int kn = base + kHistWarps * 32 + lane;
+            r_next = kn < s1 ? rows[kn] : -1;
+            if (r >= 0) {
+                unsigned int lo = 0, hi = 0, inc = 0, word = 0;
+                unsigned int* plane = pLo;
+                if (kQ8) {
+                    const int p8 = gq8[r];
+                    word = (1u << 20) | static_cast<unsigned int>((p8 >> 1) + 128);
+                    plane = (p8 & 1) ? pHi : pLo;
+                } else {
+                    const long long p = gq[r];
+                    const long long v = p >> 1;
+                    lo = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
+                    hi = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
+                    inc = (p & 1) ? 0x10000u : 1u;
+                }
                 const uint4* src = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r) * stride + fg0);
                 const uint4 a = __ldg(src);
                 const uint4 b = two_chunks ? __ldg(src + 1) : make_uint4(0, 0, 0, 0);
@@ -283,9 +308,13 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
                     const int f = (j + lane) & 31;
                     const unsigned int code = (R[j >> 2] >> ((j & 3) * 8)) & 0xffu;
                     const int cell = static_cast<int>(code) * 32 + f;
-                    atomicAdd(&pLo[cell], lo);
-                    atomicAdd(&pHi[cell], hi);
-                    atomicAdd(&pCn[cell], inc);
+                    if (kQ8) {
+                        atomicAdd(&plane[cell], word);
+                    } else {
+                        atomicAdd(&pLo[cell], lo);
+                        atomicAdd(&pHi[cell], hi);
+                        atomicAdd(&pCn[cell], inc);
+                    }
                 }
             }
         }
@@ -293,11 +322,21 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
 #pragma unroll
         for (int c = 0; c < kCells; ++c) {
             const int cell = threadIdx.x + c * kHistThreads;
-            accG[c] += static_cast<long long>(static_cast<int>(pHi[cell])) * (1ll << kLoBits) + pLo[cell];
-            const unsigned int cn = pCn[cell];
-            accC1[c] += cn & 0xffffu;
-            accC2[c] += cn >> 16;
-            pLo[cell] = pHi[cell] = pCn[cell] = 0u;
+            if (kQ8) {
+                const unsigned int w1 = pLo[cell], w2 = pHi[cell];
+                const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
+                accG[c] += static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
+                           128ll * static_cast<long long>(n1 + n2);
+                accC1[c] += n1;
+                accC2[c] += n2;
+                pLo[cell] = pHi[cell] = 0u;
+            } else {
+                accG[c] += static_cast<long long>(static_cast<int>(pHi[cell])) * (1ll << kLoBits) + pLo[cell];
+                const unsigned int cn = pCn[cell];
+                accC1[c] += cn & 0xffffu;
+                accC2[c] += cn >> 16;
+                pLo[cell] = pHi[cell] = pCn[cell] = 0u;
+            }
         }
         __syncthreads();
     }
@@ -339,6 +378,37 @@ __global__ void __cluster_dims__(1, kCluster, 1) __launch_bounds__(kHistThreads)
         atomicAdd(C + o, static_cast<int>(cn));
     }
     cluster.sync();  // no CTA leaves while others read its shared memory
+}
+
+// int8 precision mode: gq8[r] = (q << 1) | (GOSS-scaled ? 1 : 0) for the sampled rows,
+// q = floor(x + u) with x = g[r] * goss_factor * gscale in [-127, 127] (gscale =
+// 127 / max |g * factor| over the sample) and u in [0, 1) from a counter-based hash of
+// (row, tree, seed): stochastic rounding, unbiased (E[q] = x) and reproducible.  The hash
+// is the SplitMix64 output function (Steele, Lea and Flood, OOPSLA 2014).
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void quantize8_kernel(const int32_t* __restrict__ rows, const double* __restrict__ g,
+                                 const uint8_t* __restrict__ goss_flag, double goss_scale,
+                                 const DevTreeState* __restrict__ st, unsigned long long seed,
+                                 short* __restrict__ gq8) {
+    const int count = st->n_sample;
+    const double gscale = st->gscale;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const int r = rows[k];
+        double gv = g[r];
+        const bool sc = goss_flag != nullptr && goss_flag[r] == 2;
+        if (sc) gv *= goss_scale;
+        const double x = gv * gscale;
+        const double u = static_cast<double>(splitmix64(seed ^ (static_cast<unsigned long long>(r) << 20)) >> 11) *
+                         (1.0 / 9007199254740992.0);  // 53 bits -> [0, 1)
+        const int q = max(-127, min(127, static_cast<int>(floor(x + u))));
+        gq8[r] = static_cast<short>((q * 2) | (sc ? 1 : 0));
+    }
 }
 
 // gq[r] = (rint(g[r] * goss_factor * 2^gshift) << 1) | (GOSS-scaled ? 1 : 0) for the rows
@@ -422,19 +492,26 @@ __device__ int shift_for(double max_abs, int count) {
 }
 
 // all != nullptr: the sample is every row, whose maxima the gradient pass reduced.
-__global__ void scales_finalize_kernel(DevTreeState* st, const AllScale* __restrict__ all) {
+// q8: the gradient scale maps max |g * factor| to 127 (int8 precision mode).
+__global__ void scales_finalize_kernel(DevTreeState* st, const AllScale* __restrict__ all, int q8) {
     if (all) {
         st->max_abs_g_bits = all->maxg_bits;
         st->max_h_bits = all->maxh_bits;
     }
     const double mg = __longlong_as_double(static_cast<long long>(st->max_abs_g_bits));
     const double mh = __longlong_as_double(static_cast<long long>(st->max_h_bits));
-    st->gshift = shift_for(mg, st->n_sample);
     st->hshift = shift_for(mh, st->n_sample);
-    st->gscale = ldexp(1.0, st->gshift);
     st->hscale = ldexp(1.0, st->hshift);
-    st->inv_gscale = ldexp(1.0, -st->gshift);
     st->inv_hscale = ldexp(1.0, -st->hshift);
+    if (q8) {
+        st->gshift = 0;
+        st->gscale = mg > 0.0 ? 127.0 / mg : 1.0;
+        st->inv_gscale = 1.0 / st->gscale;
+    } else {
+        st->gshift = shift_for(mg, st->n_sample);
+        st->gscale = ldexp(1.0, st->gshift);
+        st->inv_gscale = ldexp(1.0, -st->gshift);
+    }
 }
 
 constexpr size_t hist_smem(bool const_h) { return static_cast<size_t>(kPlane) * 4 * (const_h ? 4 : 5); }
@@ -452,13 +529,14 @@ int hist_grid_rows(int n_f, int max_rows, bool const_h) {
     const int need = (max_rows + kMinRowsPerCta - 1) / kMinRowsPerCta;
     if (!const_h) return std::max(1, std::min(need, (148 + groups - 1) / groups));
     // Clusters that fit on the device at once, shared among the feature groups.
-    set_smem(hist_node_const_kernel, kConstSmem);
+    set_smem(hist_node_const_kernel<false>, kConstSmem);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(groups, kCluster, 1);
     cfg.blockDim = dim3(kHistThreads, 1, 1);
     cfg.dynamicSmemBytes = kConstSmem;
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, hist_node_const_kernel, &cfg) != cudaSuccess || clusters <= 0) {
+    if (cudaOccupancyMaxActiveClusters(&clusters, hist_node_const_kernel<false>, &cfg) != cudaSuccess ||
+        clusters <= 0) {
         (void)cudaGetLastError();
         clusters = 148 / kCluster;
     }
@@ -469,14 +547,15 @@ int hist_grid_rows(int n_f, int max_rows, bool const_h) {
 
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows,
                       const DevNode* nodes, const DevTreeState* st, int node, const double* g,
-                      const double* h, const long long* gq, const uint8_t* goss_flag, double goss_scale,
+                      const double* h, const void* gq, bool q8, const uint8_t* goss_flag, double goss_scale,
                       HistSlotPtrs hs, int grid_rows, unsigned long long* rows_counter, bool const_h,
                       cudaStream_t s) {
     dim3 grid((n_f + kFG - 1) / kFG, max(1, grid_rows));
     if (const_h) {
-        set_smem(hist_node_const_kernel, kConstSmem);
-        launch_pdl(hist_node_const_kernel, grid, dim3(kHistThreads), kConstSmem, s, "hist_node launch", codes, stride,
-                   n_f, rows[0], rows[1], nodes, st, node, gq, goss_scale, hs, rows_counter);
+        auto kern = q8 ? hist_node_const_kernel<true> : hist_node_const_kernel<false>;
+        set_smem(kern, kConstSmem);
+        launch_pdl(kern, grid, dim3(kHistThreads), kConstSmem, s, "hist_node launch", codes, stride, n_f, rows[0],
+                   rows[1], nodes, st, node, gq, goss_scale, hs, rows_counter);
         return;
     } else {
         set_smem(hist_node_kernel<false>, hist_smem(false));
@@ -484,6 +563,13 @@ void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const*
             codes, stride, n_f, rows[0], rows[1], nodes, st, node, g, h, goss_flag, goss_scale, hs, rows_counter);
     }
     check(cudaGetLastError(), "hist_node launch");
+}
+
+void launch_quantize8(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
+                      const DevTreeState* st, unsigned long long seed, short* gq8, int max_rows, cudaStream_t s) {
+    const int blocks = std::max(1, std::min(1184, (max_rows + 255) / 256));
+    quantize8_kernel<<<blocks, 256, 0, s>>>(rows, g, goss_flag, goss_scale, st, seed, gq8);
+    check(cudaGetLastError(), "quantize8 launch");
 }
 
 void launch_quantize(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
@@ -516,8 +602,8 @@ void launch_iota_rows(int32_t* rows, int n, cudaStream_t s) {
     check(cudaGetLastError(), "iota launch");
 }
 
-void launch_scales(DevTreeState* st, const AllScale* all, cudaStream_t s) {
-    scales_finalize_kernel<<<1, 1, 0, s>>>(st, all);
+void launch_scales(DevTreeState* st, const AllScale* all, bool q8, cudaStream_t s) {
+    scales_finalize_kernel<<<1, 1, 0, s>>>(st, all, q8 ? 1 : 0);
     check(cudaGetLastError(), "scales_finalize launch");
 }
 

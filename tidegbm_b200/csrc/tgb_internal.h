@@ -187,11 +187,16 @@ void launch_quantile_edges(int x_dtype, const void* sorted, void* uniq, long lon
                            int n_bins, double* edges, int* n_edges, cudaStream_t s);
 
 // histograms + tree state (kernels_hist.cu)
-// const_h (mse): reads gq from launch_quantize; otherwise g, h and goss_flag.
+// const_h (mse): reads gq from launch_quantize (int64 per row) or, with q8, from
+// launch_quantize8 (int16 per row); otherwise g, h and goss_flag.
 void launch_hist_node(const uint8_t* codes, int stride, int n_f, int32_t* const* rows, const DevNode* nodes,
-                      const DevTreeState* st, int node, const double* g, const double* h, const long long* gq,
+                      const DevTreeState* st, int node, const double* g, const double* h, const void* gq, bool q8,
                       const uint8_t* goss_flag, double goss_scale, HistSlotPtrs hs, int grid_rows,
                       unsigned long long* rows_counter, bool const_h, cudaStream_t s);
+// int8 precision mode: gq8[r] = (q << 1) | GOSS-scaled, q the stochastically rounded
+// g * factor * st->gscale in [-127, 127]; seed varies per tree.
+void launch_quantize8(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
+                      const DevTreeState* st, unsigned long long seed, short* gq8, int max_rows, cudaStream_t s);
 // gq[r] = (rint(g[r] * goss_factor * st->gscale) << 1) | GOSS-scaled, for the st->n_sample
 // rows of rows[] (the tree's sample); run after launch_scales.
 void launch_quantize(const int32_t* rows, const double* g, const uint8_t* goss_flag, double goss_scale,
@@ -203,8 +208,9 @@ void launch_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, int n_
                       cudaStream_t s);
 void launch_iota_rows(int32_t* rows, int n, cudaStream_t s);
 // Per-tree histogram scales from the sample maxima in st (reduced by the GOSS mark), or,
-// when the sample is every row, from the all-row maxima in `all`.
-void launch_scales(DevTreeState* st, const AllScale* all, cudaStream_t s);
+// when the sample is every row, from the all-row maxima in `all`.  q8: the int8 precision
+// mode's gradient scale (127 / max |g * factor|) instead of a power-of-two shift.
+void launch_scales(DevTreeState* st, const AllScale* all, bool q8, cudaStream_t s);
 // Row chunks per feature group of a histogram launch (const_h: a multiple of the cluster size).
 int hist_grid_rows(int n_f, int max_rows, bool const_h);
 
@@ -258,10 +264,11 @@ void launch_loss_finalize(int kind, const double* partials, const int* valid, in
 // GOSS (kernels_goss.cu)
 size_t goss_cub_bytes(int n, bool exact);
 void launch_goss_iota(int32_t* vals, int n, cudaStream_t s);  // w.vals_in, once per fit
-// all: the all-row maxima of the tree's gradients (the 32-bit sort keys are relative to max |g|).
+// all: the all-row maxima of the tree's gradients (the 32-bit sort keys are relative to max |g|);
+// min_rest: the smallest of rest_pos[0..n_other).
 void launch_goss_select(const double* g, const double* h, int n, int n_top, int n_other, const int32_t* rest_pos,
-                        GossWork& w, const AllScale* all, double goss_scale, uint8_t* goss_flag, int32_t* rows0,
-                        int* tile_counts, DevTreeState* st, cudaStream_t s);
+                        int min_rest, GossWork& w, const AllScale* all, double goss_scale, uint8_t* goss_flag,
+                        int32_t* rows0, int* tile_counts, DevTreeState* st, cudaStream_t s);
 
 // post-tree sweep (kernels_post.cu)
 void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s);

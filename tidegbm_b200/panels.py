@@ -116,9 +116,12 @@ def panel_pairwise(n_dates: int = 2000, n_features: int = 64, seed: int = 1,
     return Panel(X, _demean_by_date(lin, ts), ts, ent, "panel_pairwise")
 
 
-def panel_scale(n_dates: int = 5000, n_entities: int = 2000, n_features: int = 128, seed: int = 2) -> Panel:
+def panel_scale(n_dates: int = 5000, n_entities: int = 2000, n_features: int = 128, seed: int = 2,
+                sample_seed: int | None = None) -> Panel:
     """Scale: N(0,1) columns mixed with log-normal (sigma = 1) columns (every fourth
-    column), 1% NaN; y = 16-sparse linear + 0.1 sin(x_k) + N(0,1), demeaned."""
+    column), 1% NaN; y = 16-sparse linear + 0.1 sin(x_k) + N(0,1), demeaned.  `seed` fixes
+    the target function (support, weights), `sample_seed` (default: seed) the rows, so a
+    held-out panel of the same function takes another sample_seed."""
     rng0 = np.random.default_rng([seed, 10**6])
     n_support = min(16, n_features)
     support = rng0.choice(n_features, n_support, replace=False)
@@ -135,7 +138,7 @@ def panel_scale(n_dates: int = 5000, n_entities: int = 2000, n_features: int = 1
         lo[:] = sig + rng.standard_normal(m)
         Xo[rng.random((m, n_features), dtype=np.float32) < 0.01] = np.nan
 
-    X, lin = _chunked(sizes, n_features, seed, fill)
+    X, lin = _chunked(sizes, n_features, seed if sample_seed is None else sample_seed, fill)
     ts = np.repeat(np.arange(n_dates, dtype=np.int64), sizes)
     ent = np.tile(np.arange(n_entities, dtype=np.int32), n_dates)
     return Panel(X, _demean_by_date(lin, ts), ts, ent, "panel_scale")
