@@ -266,3 +266,70 @@ def ref_predict(handle, X) -> np.ndarray:
 
 def ref_free(handle) -> None:
     ref_lib().ref_free(handle)
+
+
+def ref_import(n_features: int, n_bins: int, n_buckets: int, init_score: float, init_prefix, edges, n_edges,
+               max_bin: int, learning_rate: float, objective, iid_mode: bool, trees) -> int:
+    """A fitted reference Booster holding a model grown elsewhere (trees as TreeArrays,
+    edges F x 256 with n_edges[f] used); returns its handle (free with ref_free)."""
+    L = ref_lib()
+    obj = OBJECTIVES[objective] if isinstance(objective, str) else int(objective)
+    nodes = np.array([t.is_leaf.size for t in trees], np.int32)
+    I = np.ascontiguousarray(np.concatenate([np.stack([t.is_leaf, t.feature, t.threshold, t.left, t.right,
+                                                       t.missing_left, t.n_samples, t.depth], axis=1).ravel()
+                                             for t in trees]).astype(np.int32))
+    Fv = np.ascontiguousarray(np.concatenate([np.stack([t.value, t.gain], axis=1).ravel() for t in trees]))
+    vals = np.ascontiguousarray(np.concatenate([t.values for t in trees]))
+    cov = np.ascontiguousarray(np.concatenate([t.cover for t in trees]).astype(np.int32))
+    pre = np.ascontiguousarray(np.concatenate([np.asarray(t.prefix).ravel() for t in trees]))
+    ip = np.ascontiguousarray(np.asarray(init_prefix, np.float64))
+    E = np.ascontiguousarray(np.asarray(edges, np.float64).reshape(n_features, 256))
+    ne = np.ascontiguousarray(np.asarray(n_edges, np.int32))
+    h = L.ref_create()
+    vp = C.c_void_p
+    L.ref_import_model.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, vp, vp, C.c_int,
+                                   C.c_double, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
+    rc = L.ref_import_model(h, n_features, n_bins, n_buckets, init_score, _ptr(ip), ip.size, _ptr(E), _ptr(ne),
+                            max_bin, learning_rate, obj, int(iid_mode), len(trees), _ptr(nodes), _ptr(I), _ptr(Fv),
+                            _ptr(vals), _ptr(cov), _ptr(pre))
+    if rc != 0:
+        L.ref_free(h)
+        raise ValueError(L.ref_last_error().decode())
+    return h
+
+
+def ref_edges_of(handle, n_features: int) -> tuple[np.ndarray, np.ndarray]:
+    """Edges (F x 256) and their counts of a fitted reference Booster."""
+    L = ref_lib()
+    L.ref_edges.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.ref_edges.restype = C.c_int
+    E = np.zeros((n_features, 256))
+    ne = np.zeros(n_features, np.int32)
+    for f in range(n_features):
+        ne[f] = L.ref_edges(handle, f, None)
+        L.ref_edges(handle, f, E[f].ctypes.data_as(C.c_void_p))
+    return E, ne
+
+
+def ref_save(handle) -> bytes:
+    """The reference's .tgbm blob (Booster::save_binary)."""
+    L = ref_lib()
+    L.ref_save_binary.argtypes = [C.c_void_p, C.c_char_p, C.c_longlong]
+    L.ref_save_binary.restype = C.c_longlong
+    n = L.ref_save_binary(handle, None, 0)
+    if n < 0:
+        raise ValueError(L.ref_last_error().decode())
+    buf = C.create_string_buffer(int(n))
+    L.ref_save_binary(handle, buf, n)
+    return buf.raw[: int(n)]
+
+
+def ref_load(blob: bytes) -> int:
+    """A reference Booster from a .tgbm blob (Booster::load_binary)."""
+    L = ref_lib()
+    L.ref_load_binary.argtypes = [C.c_char_p, C.c_longlong]
+    L.ref_load_binary.restype = C.c_void_p
+    h = L.ref_load_binary(blob, len(blob))
+    if not h:
+        raise ValueError(L.ref_last_error().decode())
+    return h

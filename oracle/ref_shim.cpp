@@ -12,7 +12,9 @@
 //   * build_hist_col (cpp/src/histogram.cpp:44-76);
 //   * best_numeric_missing (cpp/src/histogram.cpp:144-193);
 //   * Objective::grad_hess / loss (cpp/src/objective.cpp:102-329);
-//   * apply_all (cpp/src/tree.cpp:43-55).
+//   * apply_all (cpp/src/tree.cpp:43-55);
+//   * a fitted Booster built from exported arrays, and Booster::save_binary /
+//     load_binary (cpp/src/serialize.cpp:65-255), the .tgbm blob.
 #include "tidegbm/booster.hpp"
 #include "tidegbm/histogram.hpp"
 
@@ -244,6 +246,104 @@ double ref_loss(int kind, const double* y, const double* pred, const long long* 
     Objective o;
     o.kind = objective_from_code(kind);
     return o.loss(y, pred, nullptr, reinterpret_cast<const i64*>(groups), n);
+}
+
+// ---- a fitted model from exported arrays, and the .tgbm blob ------------------
+
+// Fills a reference Booster with a model grown elsewhere (the GPU path's export):
+// config fields the prediction and the .tgbm format read, the numeric binner
+// (edges F x 256, first n_edges[f] used; n_bins_col = n_edges + 2 as Binner::fit sets
+// it, binning.cpp:100), and the trees, concatenated: tree t has tree_nodes[t] nodes,
+// int32 [is_leaf, feature, threshold_bin, left, right, missing_go_left, n_samples,
+// depth] and f64 [value, gain] per node, values / cover per node and n_buckets x
+// n_nodes prefix values.  This is what a TideGBM maintainer's import step does after
+// Booster::fit dispatched to the GPU.
+int ref_import_model(void* hb, int n_features, int n_bins, int n_buckets, double init_score,
+                     const double* init_prefix, int n_prefix, const double* edges, const int* n_edges, int max_bin,
+                     double learning_rate, int objective, int iid_mode, int n_trees, const int* tree_nodes,
+                     const int* inodes, const double* fnodes, const double* values, const int* cover,
+                     const double* prefix) {
+    try {
+        Booster& b = *static_cast<Booster*>(hb);
+        b.cfg.n_estimators = n_trees;
+        b.cfg.learning_rate = learning_rate;
+        b.cfg.max_bin = max_bin;
+        b.cfg.objective = objective_from_code(objective);
+        b.cfg.iid_mode = iid_mode != 0;
+        b.cfg.n_jobs = 1;
+        b.obj.kind = b.cfg.objective;
+        b.n_features = n_features;
+        b.n_bins = n_bins;
+        b.n_time_buckets = n_buckets;
+        b.init_score = init_score;
+        b.init_prefix.assign(init_prefix, init_prefix + n_prefix);
+        b.is_cat.assign(n_features, 0);
+        b.binner.max_bin = max_bin;
+        b.binner.n_features = n_features;
+        b.binner.is_cat.assign(n_features, 0);
+        b.binner.edges.assign(n_features, {});
+        b.binner.cat_values.assign(n_features, {});
+        b.binner.n_bins_col.assign(n_features, 2);
+        for (int f = 0; f < n_features; ++f) {
+            const double* e = edges + static_cast<size_t>(f) * 256;
+            b.binner.edges[f].assign(e, e + n_edges[f]);
+            b.binner.n_bins_col[f] = n_edges[f] + 2;
+        }
+        b.trees.assign(n_trees, Tree());
+        size_t off = 0;
+        for (int t = 0; t < n_trees; ++t) {
+            Tree& tr = b.trees[t];
+            const int nn = tree_nodes[t];
+            tr.n_buckets = n_buckets;
+            tr.nodes.resize(nn);
+            for (int k = 0; k < nn; ++k) {
+                const int* o = inodes + 8 * (off + k);
+                Node& d = tr.nodes[k];
+                d.is_leaf = o[0] != 0;
+                d.feature = o[1];
+                d.threshold_bin = o[2];
+                d.left = o[3];
+                d.right = o[4];
+                d.missing_go_left = o[5];
+                d.n_samples = o[6];
+                d.depth = o[7];
+                d.value = fnodes[2 * (off + k)];
+                d.gain = fnodes[2 * (off + k) + 1];
+            }
+            tr.values.assign(values + off, values + off + nn);
+            tr.cover.assign(cover + off, cover + off + nn);
+            tr.prefix_values.assign(prefix + off * n_buckets, prefix + (off + nn) * n_buckets);
+            off += nn;
+        }
+        b.fitted = true;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// Booster::save_binary (serialize.cpp:65-148): returns the blob size; copies it when
+// out != NULL and cap is large enough.
+long long ref_save_binary(void* hb, char* out, long long cap) {
+    try {
+        const std::string blob = static_cast<Booster*>(hb)->save_binary();
+        if (out && cap >= static_cast<long long>(blob.size())) std::memcpy(out, blob.data(), blob.size());
+        return static_cast<long long>(blob.size());
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// Booster::load_binary (serialize.cpp:150-255) into a new handle (NULL on error).
+void* ref_load_binary(const char* blob, long long n) {
+    try {
+        return new Booster(Booster::load_binary(std::string(blob, static_cast<size_t>(n))));
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
 }
 
 }  // extern "C"

@@ -244,3 +244,40 @@ def test_gpu_rejects_unsupported_options(native):
         native.Booster(pair_splits=False).fit(X, y, timestamps=np.arange(100))
     with pytest.raises(native.TideError, match="colsample"):
         native.Booster(iid_mode=1, pair_splits=False, colsample=0.5).fit(X, y)
+
+
+@pytest.mark.parametrize("objective", ["mse", "pairwise"])
+def test_gpu_model_loads_into_reference_and_tgbm(native, oracle, objective):
+    """The GPU-grown model, read back through the C ABI (tree export, edges, model info),
+    rebuilds a reference Booster whose predict_raw matches the GPU's within 1e-12, also
+    after the reference's .tgbm blob round trip (cpp/src/serialize.cpp:65-255): the import
+    step a TideGBM maintainer adds after dispatching Booster::fit to the GPU."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    from tidegbm_b200 import panels
+
+    p = panels.panel_small(n_dates=80, n_entities=150, n_features=12)
+    params = dict(n_estimators=8, learning_rate=0.1, max_depth=6, horizon=1, objective=objective, goss=0,
+                  random_state=4, pair_splits=False)
+    gpu = native.Booster(**params).fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
+    info = gpu.info()
+    nf = p.X.shape[1]
+    E = np.zeros((nf, 256))
+    ne = np.zeros(nf, np.int32)
+    for f in range(nf):
+        e = gpu.edges(f)
+        E[f, : e.size] = e
+        ne[f] = e.size
+    h = oracle.ref_import(nf, info["n_bins"], info["n_buckets"], info["init_score"], gpu.init_prefix(), E, ne, 255,
+                          0.1, objective, False, gpu.trees())
+    try:
+        X = p.X.astype(np.float64)
+        want = gpu.raw_predict(p.X)
+        np.testing.assert_allclose(oracle.ref_predict(h, X), want, rtol=0, atol=1e-12)
+        h2 = oracle.ref_load(oracle.ref_save(h))
+        try:
+            np.testing.assert_allclose(oracle.ref_predict(h2, X), want, rtol=0, atol=1e-12)
+        finally:
+            oracle.ref_free(h2)
+    finally:
+        oracle.ref_free(h)
