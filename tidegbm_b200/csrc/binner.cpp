@@ -195,49 +195,53 @@ bool binner_fits_device(int n, int n_f, int bin_sample) {
     return static_cast<long long>(n_f) * std::max(1LL, cap) < (1LL << 31) - 1;
 }
 
-int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
-                      std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
-                      void* arena, size_t arena_bytes, BinFitTimes* tm) {
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    Scratch scratch(arena, arena_bytes);
-    const double t0 = wall_now();
+void binner_plan(const std::vector<int>& ch, int n, int n_f, int bin_sample, uint32_t seed, int n_threads,
+                 BinPlan& plan) {
     const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
     const size_t nc = static_cast<size_t>(n_chunks) * n_f;
-    int* counts = scratch.get<int>(nc);
-    launch_nonnan_counts(Xd, x_dtype, n, n_f, counts, s);
-    std::vector<int> ch(nc);
-    check(cudaMemcpyAsync(ch.data(), counts, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
-    check(cudaStreamSynchronize(s), "non-NaN counts");
-    const double t1 = wall_now();
+    plan.n_chunks = n_chunks;
     // per-feature totals and the first non-NaN rank of every (chunk, feature)
-    std::vector<int64_t> m(n_f, 0);
-    std::vector<long long> base(nc);
+    plan.m.assign(n_f, 0);
+    plan.base.assign(nc, 0);
     for (int c = 0; c < n_chunks; ++c)
         for (int f = 0; f < n_f; ++f) {
-            base[static_cast<size_t>(c) * n_f + f] = m[f];
-            m[f] += ch[static_cast<size_t>(c) * n_f + f];
+            plan.base[static_cast<size_t>(c) * n_f + f] = plan.m[f];
+            plan.m[f] += ch[static_cast<size_t>(c) * n_f + f];
         }
-    std::vector<uint8_t> take_all(n_f, 1);
-    std::vector<int> kept(n_f, 0);
-    int64_t max_sampled = 0;
-    long long cap = 1;
+    plan.take_all.assign(n_f, 1);
+    plan.kept.assign(n_f, 0);
+    plan.max_sampled = 0;
+    plan.cap = 1;
     for (int f = 0; f < n_f; ++f) {
-        take_all[f] = (bin_sample > 0 && m[f] > bin_sample) ? 0 : 1;
-        kept[f] = take_all[f] ? static_cast<int>(m[f]) : bin_sample;
-        if (!take_all[f]) max_sampled = std::max(max_sampled, m[f]);
-        cap = std::max<long long>(cap, kept[f]);
+        plan.take_all[f] = (bin_sample > 0 && plan.m[f] > bin_sample) ? 0 : 1;
+        plan.kept[f] = plan.take_all[f] ? static_cast<int>(plan.m[f]) : bin_sample;
+        if (!plan.take_all[f]) plan.max_sampled = std::max(plan.max_sampled, plan.m[f]);
+        plan.cap = std::max<long long>(plan.cap, plan.kept[f]);
     }
     // kept ranks: the exact prefix of std::shuffle(mt19937(seed + f * 2654435761)), binning.cpp:93-97
-    std::vector<int32_t> keep;
-    if (max_sampled > 0) {
-        keep.resize(static_cast<size_t>(n_f) * bin_sample);
+    plan.keep.clear();
+    if (plan.max_sampled > 0) {
+        plan.keep.resize(static_cast<size_t>(n_f) * bin_sample);
         parallel_for(n_f, n_threads, [&](int f) {
-            if (take_all[f]) return;
+            if (plan.take_all[f]) return;
             Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
-            shuffled_prefix(m[f], bin_sample, rng, keep.data() + static_cast<size_t>(f) * bin_sample);
+            shuffled_prefix(plan.m[f], bin_sample, rng, plan.keep.data() + static_cast<size_t>(f) * bin_sample);
         });
     }
-    const double t2 = wall_now();
+}
+
+int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n, int n_f, int max_bin,
+                         int bin_sample, std::vector<double>& edges, std::vector<int>& n_edges, void* stream,
+                         void* arena, size_t arena_bytes) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch scratch(arena, arena_bytes);
+    const size_t nc = static_cast<size_t>(plan.n_chunks) * n_f;
+    const std::vector<long long>& base = plan.base;
+    const std::vector<uint8_t>& take_all = plan.take_all;
+    const std::vector<int>& kept = plan.kept;
+    const std::vector<int32_t>& keep = plan.keep;
+    const int64_t max_sampled = plan.max_sampled;
+    const long long cap = plan.cap;
     long long* base_d = scratch.get<long long>(nc);
     check(cudaMemcpyAsync(base_d, base.data(), sizeof(long long) * nc, cudaMemcpyHostToDevice, s), "bases upload");
     uint8_t* take_d = scratch.get<uint8_t>(n_f);
@@ -284,14 +288,38 @@ int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, 
     check(cudaStreamSynchronize(s), "quantile edges");
     for (int f = 0; f < n_f; ++f)
         if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");
+    int mx = 2;
+    for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + 2);
+    return std::max(mx, max_bin);  // Binner::max_bins, binning.cpp:130-134
+}
+
+int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
+                      std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
+                      void* arena, size_t arena_bytes, BinFitTimes* tm) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const double t0 = wall_now();
+    const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
+    const size_t nc = static_cast<size_t>(n_chunks) * n_f;
+    std::vector<int> ch(nc);
+    {
+        DBuf<int> counts;
+        counts.alloc(nc);
+        launch_nonnan_counts(Xd, x_dtype, n, n_f, counts.p, s);
+        check(cudaMemcpyAsync(ch.data(), counts.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
+        check(cudaStreamSynchronize(s), "non-NaN counts");
+    }
+    const double t1 = wall_now();
+    BinPlan plan;
+    binner_plan(ch, n, n_f, bin_sample, seed, n_threads, plan);
+    const double t2 = wall_now();
+    const int nb = binner_fit_from_plan(plan, Xd, x_dtype, n, n_f, max_bin, bin_sample, edges, n_edges, stream, arena,
+                                        arena_bytes);
     if (tm) {
         tm->counts = t1 - t0;
         tm->draws = t2 - t1;
         tm->edges = wall_now() - t2;
     }
-    int mx = 2;
-    for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + 2);
-    return std::max(mx, max_bin);  // Binner::max_bins, binning.cpp:130-134
+    return nb;
 }
 
 int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,

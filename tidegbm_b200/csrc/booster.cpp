@@ -100,6 +100,23 @@ double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// fn(begin, end, part) over `parts` contiguous ranges of [0, n), one thread each.
+template <typename F>
+void parallel_ranges(int n, int parts, F&& fn) {
+    parts = std::max(1, std::min(parts, n / 65536 + 1));
+    if (parts == 1) {
+        fn(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int k = 0; k < parts; ++k) {
+        const int b = static_cast<int>(static_cast<long long>(n) * k / parts);
+        const int e = static_cast<int>(static_cast<long long>(n) * (k + 1) / parts);
+        th.emplace_back([&fn, b, e, k] { fn(b, e, k); });
+    }
+    for (auto& t : th) t.join();
+}
+
 float ceil_f32(double e) {
     float f = static_cast<float>(e);
     if (static_cast<double>(f) < e) f = std::nextafter(f, INFINITY);
@@ -223,11 +240,16 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     std::vector<double> y_own;
     std::vector<int64_t> ts_own;
     if (!c.iid_mode && n > 1) {
-        bool sorted = true;
-        for (int i = 1; i < n && sorted; ++i) {
-            if (ts_in[i] < ts_in[i - 1]) sorted = false;
-            else if (ts_in[i] == ts_in[i - 1] && ent_in && ent_in[i] < ent_in[i - 1]) sorted = false;
-        }
+        std::atomic<bool> unsorted{false};
+        parallel_ranges(n, n_threads, [&](int b, int e, int) {
+            for (int i = std::max(1, b); i < e && !unsorted.load(std::memory_order_relaxed); ++i) {
+                if (ts_in[i] < ts_in[i - 1] || (ts_in[i] == ts_in[i - 1] && ent_in && ent_in[i] < ent_in[i - 1])) {
+                    unsorted = true;
+                    break;
+                }
+            }
+        });
+        const bool sorted = !unsorted.load();
         if (!sorted) {
             std::vector<int> ord(n);
             std::iota(ord.begin(), ord.end(), 0);
@@ -278,21 +300,36 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     int64_t embargo = c.embargo;
     std::vector<int> cut(1, 0);
     if (!c.iid_mode) {
+        // distinct timestamps in row order (rows are time-sorted), per range then joined
+        std::vector<std::vector<int64_t>> parts(std::max(1, n_threads));
+        parallel_ranges(n, n_threads, [&](int b, int e, int k) {
+            for (int i = b; i < e; ++i)
+                if (i == 0 || ts[i] != ts[i - 1]) parts[k].push_back(ts[i]);
+        });
         std::vector<int64_t> uniq;
         uniq.reserve(1024);
-        for (int i = 0; i < n; ++i)
-            if (i == 0 || ts[i] != ts[i - 1]) uniq.push_back(ts[i]);
+        for (auto& v : parts) uniq.insert(uniq.end(), v.begin(), v.end());
         const int uniq_n = std::max(2, static_cast<int>(uniq.size()));
         int want = c.n_time_buckets;
         if (want <= 0) want = auto_time_buckets(uniq, std::max<int64_t>(c.horizon, 0), uniq_n);
         nbk = c.finer_torb ? std::max(2, std::min(want, uniq_n)) : std::max(2, want);
         embargo += std::max<int64_t>(c.horizon, 0);
         cut.assign(nbk, 0);
+        // first row of each time bucket (time_buckets, booster.cpp:60-72): the bucket of row
+        // i is non-decreasing in i, so each first row is a binary search on the same expression
+        auto bucket_of = [&](int i) {
+            const int b = static_cast<int>(static_cast<double>(i) / std::max(n, 1) * nbk);
+            return b >= nbk ? nbk - 1 : b;
+        };
         std::vector<int> first(nbk, -1);
-        for (int i = 0; i < n; ++i) {
-            int b = static_cast<int>(static_cast<double>(i) / std::max(n, 1) * nbk);
-            if (b >= nbk) b = nbk - 1;
-            if (first[b] < 0) first[b] = i;
+        for (int b = 0; b < nbk; ++b) {
+            int lo = 0, hi = n;  // smallest i with bucket_of(i) >= b
+            while (lo < hi) {
+                const int mid = lo + (hi - lo) / 2;
+                if (bucket_of(mid) >= b) hi = mid;
+                else lo = mid + 1;
+            }
+            if (lo < n && bucket_of(lo) == b) first[b] = lo;
         }
         int run = 0;
         for (int b = 0; b < nbk; ++b) {

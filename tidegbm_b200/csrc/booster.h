@@ -146,6 +146,24 @@ struct BinFitTimes {
     double counts = 0, draws = 0, edges = 0;  // wall seconds of the three stages
 };
 bool binner_fits_device(int n, int n_f, int bin_sample);
+// binner_fit_device's two stages: binner_plan (per-feature totals, rank bases and the
+// kept ranks of the shuffle, from non-NaN counts per 4096-row chunk and feature) and
+// binner_fit_from_plan (the device part on X in device memory).
+struct BinPlan {
+    int n_chunks = 0;
+    std::vector<int64_t> m;
+    std::vector<long long> base;
+    std::vector<uint8_t> take_all;
+    std::vector<int> kept;
+    int64_t max_sampled = 0;
+    long long cap = 1;
+    std::vector<int32_t> keep;
+};
+void binner_plan(const std::vector<int>& counts, int n, int n_f, int bin_sample, uint32_t seed, int n_threads,
+                 BinPlan& plan);
+int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n, int n_f, int max_bin,
+                         int bin_sample, std::vector<double>& edges, std::vector<int>& n_edges, void* stream,
+                         void* arena, size_t arena_bytes);
 // arena / arena_bytes: device memory the binner may use as scratch (nullptr: allocate).
 int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                       std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
