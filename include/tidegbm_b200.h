@@ -105,8 +105,10 @@ TGB_API int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, in
 
 /* Binner::fit on X in device memory (row-major n x n_features of x_dtype, on `stream`):
  * the same edges as tgb_binner_fit, with the non-NaN counts, the value gather, the
- * sample sort and the edge arithmetic as kernels; only the kept ranks of the shuffle are
- * drawn on the host.  edges_out / n_edges_out are host arrays as in tgb_binner_fit.
+ * sample sort, the edge arithmetic and all but the first bin_sample draws of each
+ * feature's shuffle as kernels; those first draws (the ones that swap inside the kept
+ * prefix) are made on the host.  edges_out / n_edges_out are host arrays as in
+ * tgb_binner_fit.
  * Requires n_features * min(bin_sample, n) < 2^31.  Returns max_bins() or -1. */
 TGB_API int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
                                   unsigned seed, double* edges_out, int* n_edges_out, void* stream);
@@ -115,6 +117,11 @@ TGB_API int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_featu
  * computed without materialising the range — the GOSS and bin-sample draw
  * (cpp/src/booster.cpp:572, cpp/src/binning.cpp:95). */
 TGB_API int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out);
+
+/* The same prefix written to device memory out[keep] (on `stream`, synchronised before
+ * returning): the draws that swap inside the prefix run on the host, the rest as one
+ * kernel continuing the generator's stream.  1 <= keep <= m < 2^31. */
+TGB_API int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* out, void* stream);
 
 /* ---- Kernel level: one reference function each, on device memory ---- */
 

@@ -99,3 +99,17 @@ def test_device_binner_wide_features(oracle, native):
     assert nb1 == nb2
     assert np.array_equal(n1, n2)
     assert np.array_equal(e1, e2)
+
+
+@pytest.mark.parametrize("m,keep,seed", [(1, 1, 0), (10, 3, 1), (65536, 100, 4), (65537, 65537, 5),
+                                         (300000, 26214, 6), (1_000_000, 100_000, 7), (3_000_000, 262_144, 8),
+                                         (9_900_000, 262_144, 2654435761 * 5 % 2**32), (2_000_000, 1, 10)])
+def test_device_shuffle_tail_equals_std_shuffle(native, oracle, m, keep, seed):
+    """Head on the host, tail as one kernel: the same prefix as libstdc++'s std::shuffle."""
+    out = torch.full((keep,), -1, dtype=torch.int32, device="cuda")
+    native.check(native.lib().tgb_shuffled_prefix_device(m, keep, seed, C.c_void_p(out.data_ptr()), None))
+    ref = np.zeros(keep, np.int32)
+    L = oracle.oracle_lib()
+    L.orc_shuffle_prefix.argtypes = [C.c_int64, C.c_int64, C.c_uint32, C.c_void_p]
+    L.orc_shuffle_prefix(m, keep, seed, ref.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(out.cpu().numpy(), ref)

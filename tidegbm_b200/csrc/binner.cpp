@@ -15,8 +15,10 @@
 // (kernels_bin.cu) then maps X to codes.
 //
 // binner_fit_device runs the same steps on X already in device memory: the two
-// passes, the sample sort and the edge arithmetic run as kernels (kernels_binfit.cu);
-// the host only turns the non-NaN counts into kept ranks.
+// passes, the sample sort and the edge arithmetic run as kernels (kernels_binfit.cu).
+// The host turns the non-NaN counts into rank bases and makes the first bin_sample
+// draws of each shuffle (the ones that swap inside the prefix); the remaining draws,
+// ~m per feature, run on the device (kernels_shuffle.cu).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -218,14 +220,23 @@ void binner_plan(const std::vector<int>& ch, int n, int n_f, int bin_sample, uin
         if (!plan.take_all[f]) plan.max_sampled = std::max(plan.max_sampled, plan.m[f]);
         plan.cap = std::max<long long>(plan.cap, plan.kept[f]);
     }
-    // kept ranks: the exact prefix of std::shuffle(mt19937(seed + f * 2654435761)), binning.cpp:93-97
+    // kept ranks: the exact prefix of std::shuffle(mt19937(seed + f * 2654435761)), binning.cpp:93-97.
+    // The head of each shuffle runs here; its tail runs on the device (kernels_shuffle.cu).
     plan.keep.clear();
+    plan.tail_from.assign(n_f, 0);
+    plan.mt.clear();
     if (plan.max_sampled > 0) {
         plan.keep.resize(static_cast<size_t>(n_f) * bin_sample);
+        plan.mt.assign(static_cast<size_t>(n_f) * 625, 0u);
         parallel_for(n_f, n_threads, [&](int f) {
             if (plan.take_all[f]) return;
             Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
-            shuffled_prefix(plan.m[f], bin_sample, rng, plan.keep.data() + static_cast<size_t>(f) * bin_sample);
+            const int64_t i = shuffle_head(plan.m[f], bin_sample, rng,
+                                           plan.keep.data() + static_cast<size_t>(f) * bin_sample);
+            plan.tail_from[f] = i;
+            uint32_t* g = plan.mt.data() + static_cast<size_t>(f) * 625;
+            std::copy(rng.st, rng.st + 624, g);
+            g[624] = static_cast<uint32_t>(rng.pos);
         });
     }
 }
@@ -248,11 +259,25 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     check(cudaMemcpyAsync(take_d, take_all.data(), n_f, cudaMemcpyHostToDevice, s), "flags upload");
     const long long words = max_sampled > 0 ? (max_sampled + 31) / 32 : 1;
     uint32_t* bits = scratch.get<uint32_t>(static_cast<size_t>(n_f) * words);
+    int* err_d = scratch.get<int>(1);
+    check(cudaMemsetAsync(err_d, 0, sizeof(int), s), "error flag reset");
     if (max_sampled > 0) {
         check(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * static_cast<size_t>(n_f) * words, s), "bits reset");
         int32_t* keep_d = scratch.get<int32_t>(keep.size());
         check(cudaMemcpyAsync(keep_d, keep.data(), sizeof(int32_t) * keep.size(), cudaMemcpyHostToDevice, s),
               "kept ranks upload");
+        std::vector<long long> span(2 * static_cast<size_t>(n_f));
+        for (int f = 0; f < n_f; ++f) {
+            span[f] = plan.tail_from[f];
+            span[n_f + f] = take_all[f] ? 0 : plan.m[f];
+        }
+        long long* span_d = scratch.get<long long>(span.size());
+        uint32_t* mt_d = scratch.get<uint32_t>(plan.mt.size());
+        check(cudaMemcpyAsync(span_d, span.data(), sizeof(long long) * span.size(), cudaMemcpyHostToDevice, s),
+              "tail spans upload");
+        check(cudaMemcpyAsync(mt_d, plan.mt.data(), sizeof(uint32_t) * plan.mt.size(), cudaMemcpyHostToDevice, s),
+              "generator states upload");
+        launch_shuffle_tail(mt_d, span_d, span_d + n_f, n_f, bin_sample, keep_d, err_d, s);
         launch_keep_bits(keep_d, bin_sample, n_f, take_d, bits, words, s);
     }
     int* fill = scratch.get<int>(n_f);
@@ -281,11 +306,14 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
     n_edges.assign(n_f, 0);
     std::vector<int> fill_h(n_f);
+    int err_h = 0;
     check(cudaMemcpyAsync(edges.data(), ed, sizeof(double) * edges.size(), cudaMemcpyDeviceToHost, s),
           "edges download");
     check(cudaMemcpyAsync(n_edges.data(), ne, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "edges download");
     check(cudaMemcpyAsync(fill_h.data(), fill, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "fill download");
+    check(cudaMemcpyAsync(&err_h, err_d, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag download");
     check(cudaStreamSynchronize(s), "quantile edges");
+    if (err_h) throw TideError("device binner: shuffle tail ran past its refill limit");
     for (int f = 0; f < n_f; ++f)
         if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");
     int mx = 2;

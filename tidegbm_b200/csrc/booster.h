@@ -157,7 +157,12 @@ struct BinPlan {
     std::vector<int> kept;
     int64_t max_sampled = 0;
     long long cap = 1;
+    // [n_f][bin_sample]: the shuffle prefix after its head (sampling.h shuffle_head);
+    // the device finishes draws tail_from[f] .. m[f]-1 from generator state
+    // mt[f*625 .. +625) (624 words and the position).
     std::vector<int32_t> keep;
+    std::vector<long long> tail_from;
+    std::vector<uint32_t> mt;
 };
 void binner_plan(const std::vector<int>& counts, int n, int n_f, int bin_sample, uint32_t seed, int n_threads,
                  BinPlan& plan);

@@ -350,6 +350,37 @@ int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out) {
     });
 }
 
+int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* out, void* stream) {
+    return guard([&] {
+        need(m >= 1 && m < (1ll << 31) && keep >= 1 && keep <= m, "bad sizes");
+        need(out != nullptr, "out is null");
+        cudaStream_t s = as_stream(stream);
+        tgb::Mt32 rng(seed);
+        std::vector<int32_t> head(static_cast<size_t>(keep));
+        const long long from = tgb::shuffle_head(m, keep, rng, head.data());
+        std::vector<uint32_t> mt(625);
+        std::copy(rng.st, rng.st + 624, mt.begin());
+        mt[624] = static_cast<uint32_t>(rng.pos);
+        const long long span[2] = {from, m};
+        tgb::DBuf<unsigned char> dev;
+        dev.alloc(625 * sizeof(uint32_t) + 2 * sizeof(long long) + sizeof(int));
+        long long* span_d = reinterpret_cast<long long*>(dev.p);
+        int* err_d = reinterpret_cast<int*>(dev.p + 2 * sizeof(long long));
+        uint32_t* mt_d = reinterpret_cast<uint32_t*>(dev.p + 2 * sizeof(long long) + sizeof(int));
+        int err = 0;
+        tgb::check(cudaMemcpyAsync(out, head.data(), sizeof(int32_t) * head.size(), cudaMemcpyHostToDevice, s),
+                   "head upload");
+        tgb::check(cudaMemcpyAsync(span_d, span, sizeof(span), cudaMemcpyHostToDevice, s), "span upload");
+        tgb::check(cudaMemcpyAsync(mt_d, mt.data(), sizeof(uint32_t) * 625, cudaMemcpyHostToDevice, s),
+                   "state upload");
+        tgb::check(cudaMemsetAsync(err_d, 0, sizeof(int), s), "error flag reset");
+        tgb::launch_shuffle_tail(mt_d, span_d, span_d + 1, 1, static_cast<int>(keep), out, err_d, s);
+        tgb::check(cudaMemcpyAsync(&err, err_d, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag download");
+        tgb::check(cudaStreamSynchronize(s), "shuffle tail");
+        need(err == 0, "shuffle tail ran past its refill limit");
+    });
+}
+
 int tgb_bin_transform(const void* X, int x_dtype, int n, int n_features, const void* edges, const int* n_edges,
                       unsigned char* codes, int stride, void* stream) {
     return guard([&] {

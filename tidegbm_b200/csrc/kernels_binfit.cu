@@ -10,7 +10,8 @@
 // (quantile_edges sorts).  So:
 //   nonnan_count_kernel     non-NaN count per (chunk of kFitChunk rows, feature)
 //   (host)                  counts -> per-feature totals and per-chunk rank bases;
-//                           kept ranks from the exact shuffle prefix (sampling.h)
+//                           the head of the exact shuffle prefix (sampling.h)
+//   shuffle_tail_kernel     the shuffle's remaining draws (kernels_shuffle.cu)
 //   keep_bits_kernel        kept ranks -> one bit per non-NaN rank and feature
 //   sample_gather_kernel    X once more; each kept value is appended to its feature
 //   CUB segmented sort      every feature's sample ascending

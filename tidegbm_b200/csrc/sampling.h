@@ -197,26 +197,39 @@ inline void shuffle_tail(int64_t i, int64_t m, int64_t keep, G& rng, int32_t* ou
     }
 }
 
-// out[p] = index (in [0, m)) of the element std::shuffle(iota(m), rng) puts at p < keep.
+// The draws of std::shuffle(iota(m), rng) that land inside the prefix: the first
+// `keep` (0 <= keep <= m) of them, i = 1 .. keep-1, swap within the prefix and are
+// made here; out[0..keep) then holds the prefix as it stands before draw i, where i
+// is the return value.  The remaining draws i .. m-1 (the tail) only overwrite prefix
+// slots: out[j] = i for each draw j < keep.  Returns m when no tail is left (the
+// two-draws-per-call path of short ranges runs whole here).
 template <class G>
-inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
-    if (m <= 0) return;  // std::shuffle of an empty range draws nothing
-    keep = std::max<int64_t>(0, std::min(keep, m));
+inline int64_t shuffle_head(int64_t m, int64_t keep, G& rng, int32_t* out) {
+    if (m <= 0) return 0;  // std::shuffle of an empty range draws nothing
     if (shuffle_pairs(m)) {
         std::vector<int32_t> v(static_cast<size_t>(m));
         std::iota(v.begin(), v.end(), 0);
         std::shuffle(v.begin(), v.end(), rng);
         std::copy(v.begin(), v.begin() + keep, out);
-        return;
+        return m;
     }
-    std::vector<int32_t> buf(static_cast<size_t>(keep) + 1);
-    std::iota(buf.begin(), buf.end() - 1, 0);
+    std::iota(out, out + keep, 0);
     int64_t i = 1;
     for (; i < keep; ++i) {
         const uint32_t j = bounded(rng, static_cast<uint32_t>(i + 1));
-        std::swap(buf[i], buf[j]);
+        std::swap(out[i], out[j]);
     }
-    shuffle_tail(std::max<int64_t>(i, 1), m, keep, rng, buf.data());
+    return std::max<int64_t>(i, 1);
+}
+
+// out[p] = index (in [0, m)) of the element std::shuffle(iota(m), rng) puts at p < keep.
+template <class G>
+inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
+    if (m <= 0) return;
+    keep = std::max<int64_t>(0, std::min(keep, m));
+    std::vector<int32_t> buf(static_cast<size_t>(keep) + 1);
+    const int64_t i = shuffle_head(m, keep, rng, buf.data());
+    if (i < m) shuffle_tail(i, m, keep, rng, buf.data());
     std::copy(buf.begin(), buf.end() - 1, out);
 }
 
