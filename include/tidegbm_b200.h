@@ -105,10 +105,8 @@ TGB_API int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, in
 
 /* Binner::fit on X in device memory (row-major n x n_features of x_dtype, on `stream`):
  * the same edges as tgb_binner_fit, with the non-NaN counts, the value gather, the
- * sample sort, the edge arithmetic and all but the first bin_sample draws of each
- * feature's shuffle as kernels; those first draws (the ones that swap inside the kept
- * prefix) are made on the host.  edges_out / n_edges_out are host arrays as in
- * tgb_binner_fit.
+ * sample sort, the edge arithmetic and the shuffle draws of features with at least 2^16
+ * values as kernels.  edges_out / n_edges_out are host arrays as in tgb_binner_fit.
  * Requires n_features * min(bin_sample, n) < 2^31.  Returns max_bins() or -1. */
 TGB_API int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
                                   unsigned seed, double* edges_out, int* n_edges_out, void* stream);
@@ -118,9 +116,17 @@ TGB_API int tgb_binner_fit_device(const void* X, int x_dtype, int n, int n_featu
  * (cpp/src/booster.cpp:572, cpp/src/binning.cpp:95). */
 TGB_API int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out);
 
-/* The same prefix written to device memory out[keep] (on `stream`, synchronised before
- * returning): the draws that swap inside the prefix run on the host, the rest as one
- * kernel continuing the generator's stream.  1 <= keep <= m < 2^31. */
+/* The GOSS draw sequence of Booster::fit (cpp/src/booster.cpp:569-588): one
+ * std::mt19937(seed) makes n_shuffles std::shuffle's of iota(m), each followed by one
+ * draw (grow_tree's seed); out[s*keep ..] receives the first keep of shuffle s.  The
+ * generator is walked without producing positions and each prefix restarts from a
+ * snapshot, as the fit's GOSS pipeline does.  0 <= keep <= m < 2^31. */
+TGB_API int tgb_shuffle_sequence(long long m, long long keep, unsigned seed, int n_shuffles, int* out);
+
+/* tgb_shuffled_prefix's prefix written to device memory out[keep] (on `stream`, synchronised before
+ * returning), drawn on the device: the generator runs as one CTA and the swaps inside the
+ * prefix are resolved in parallel from the recorded draws.  Ranges below 2^16 (libstdc++'s
+ * two-draws path) are drawn on the host and copied.  1 <= keep <= m < 2^31. */
 TGB_API int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* out, void* stream);
 
 /* ---- Kernel level: one reference function each, on device memory ---- */

@@ -372,6 +372,17 @@ void orc_shuffle_prefix(int64_t m, int64_t keep, uint32_t seed, int32_t* out) {
     std::copy(v.begin(), v.begin() + keep, out);
 }
 
+void orc_shuffle_sequence(int64_t m, int64_t keep, uint32_t seed, int n_shuffles, int32_t* out) {
+    std::mt19937 rng(seed);
+    std::vector<int32_t> v(static_cast<size_t>(m));
+    for (int s = 0; s < n_shuffles; ++s) {
+        std::iota(v.begin(), v.end(), 0);
+        std::shuffle(v.begin(), v.end(), rng);  // booster.cpp:572
+        std::copy(v.begin(), v.begin() + keep, out + static_cast<size_t>(s) * keep);
+        (void)rng();                            // booster.cpp:588
+    }
+}
+
 void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t* groups, int n,
                    double* g, double* h) {
     if (kind == 0) {  // objective.cpp:105-118, w = 1, no cost terms

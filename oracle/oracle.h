@@ -52,6 +52,11 @@ orc_split orc_best_numeric(const double* ghc, int n_bins, int f, double lam, dou
  * reference makes in Binner::fit (binning.cpp:93-97) and GOSS (booster.cpp:572). */
 void orc_shuffle_prefix(int64_t m, int64_t keep, uint32_t seed, int32_t* out);
 
+/* The GOSS draw sequence of Booster::fit: one std::mt19937(seed) makes n_shuffles
+ * std::shuffle's of iota(m) (booster.cpp:572), each followed by grow_tree's seed draw
+ * (booster.cpp:588); out[s*keep ..] holds the first keep of shuffle s. */
+void orc_shuffle_sequence(int64_t m, int64_t keep, uint32_t seed, int n_shuffles, int32_t* out);
+
 /* Objective::grad_hess for MSE (objective.cpp:105-118) and RankPairwise
  * (objective.cpp:179-219), unit weights.  kind: 0 = MSE, 5 = RankPairwise. */
 void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t* groups, int n,

@@ -43,6 +43,20 @@ def test_shuffled_prefix_equals_std_shuffle(native, oracle, m, keep, seed):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("m,keep,seed,n_shuffles", [(1000, 100, 1, 3), (65536, 1000, 2, 4), (300000, 30000, 3, 4),
+                                                    (2_000_000, 200_000, 4, 3), (8_000_000, 1_000_000, 5, 2)])
+def test_shuffle_sequence_equals_std_shuffle(native, oracle, m, keep, seed, n_shuffles):
+    """The GOSS draw sequence: the generator walked between trees without positions (the
+    fit's producer) must land exactly where std::shuffle leaves it, tree after tree."""
+    got = np.zeros(n_shuffles * keep, np.int32)
+    native.check(native.lib().tgb_shuffle_sequence(m, keep, seed, n_shuffles, got.ctypes.data_as(C.c_void_p)))
+    ref = np.zeros(n_shuffles * keep, np.int32)
+    L = oracle.oracle_lib()
+    L.orc_shuffle_sequence.argtypes = [C.c_int64, C.c_int64, C.c_uint32, C.c_int, C.c_void_p]
+    L.orc_shuffle_sequence(m, keep, seed, n_shuffles, ref.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(got, ref)
+
+
 @pytest.mark.parametrize("dtype,bin_sample", [(np.float32, 3000), (np.float64, 0), (np.float64, 70000)])
 def test_host_binner_matches_oracle(native, oracle, dtype, bin_sample):
     rng = np.random.default_rng(11)

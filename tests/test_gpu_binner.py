@@ -103,9 +103,12 @@ def test_device_binner_wide_features(oracle, native):
 
 @pytest.mark.parametrize("m,keep,seed", [(1, 1, 0), (10, 3, 1), (65536, 100, 4), (65537, 65537, 5),
                                          (300000, 26214, 6), (1_000_000, 100_000, 7), (3_000_000, 262_144, 8),
-                                         (9_900_000, 262_144, 2654435761 * 5 % 2**32), (2_000_000, 1, 10)])
+                                         (9_900_000, 262_144, 2654435761 * 5 % 2**32), (2_000_000, 1, 10),
+                                         (500_000, 500_000, 11), (700_000, 699_999, 12), (65_536, 2, 13)])
 def test_device_shuffle_tail_equals_std_shuffle(native, oracle, m, keep, seed):
-    """Head on the host, tail as one kernel: the same prefix as libstdc++'s std::shuffle."""
+    """Draws on the device (generator, then the swaps inside the prefix resolved in parallel):
+    the same prefix as libstdc++'s std::shuffle.  keep == m and m near 10M included; ranges
+    below 2^16 take the host's two-draws path."""
     out = torch.full((keep,), -1, dtype=torch.int32, device="cuda")
     native.check(native.lib().tgb_shuffled_prefix_device(m, keep, seed, C.c_void_p(out.data_ptr()), None))
     ref = np.zeros(keep, np.int32)

@@ -15,10 +15,9 @@
 // (kernels_bin.cu) then maps X to codes.
 //
 // binner_fit_device runs the same steps on X already in device memory: the two
-// passes, the sample sort and the edge arithmetic run as kernels (kernels_binfit.cu).
-// The host turns the non-NaN counts into rank bases and makes the first bin_sample
-// draws of each shuffle (the ones that swap inside the prefix); the remaining draws,
-// ~m per feature, run on the device (kernels_shuffle.cu).
+// passes, the sample sort and the edge arithmetic run as kernels (kernels_binfit.cu), and
+// so do the shuffle draws (kernels_shuffle.cu).  The host only turns the non-NaN counts
+// into rank bases, and draws the features with fewer than 2^16 values itself.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -221,24 +220,19 @@ void binner_plan(const std::vector<int>& ch, int n, int n_f, int bin_sample, uin
         plan.cap = std::max<long long>(plan.cap, plan.kept[f]);
     }
     // kept ranks: the exact prefix of std::shuffle(mt19937(seed + f * 2654435761)), binning.cpp:93-97.
-    // The head of each shuffle runs here; its tail runs on the device (kernels_shuffle.cu).
+    // Features with at least 2^16 values are drawn on the device (kernels_shuffle.cu);
+    // libstdc++'s two-draws path for shorter ranges runs here.
+    plan.seed = seed;
+    plan.host_f.clear();
     plan.keep.clear();
-    plan.tail_from.assign(n_f, 0);
-    plan.mt.clear();
-    if (plan.max_sampled > 0) {
-        plan.keep.resize(static_cast<size_t>(n_f) * bin_sample);
-        plan.mt.assign(static_cast<size_t>(n_f) * 625, 0u);
-        parallel_for(n_f, n_threads, [&](int f) {
-            if (plan.take_all[f]) return;
-            Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
-            const int64_t i = shuffle_head(plan.m[f], bin_sample, rng,
-                                           plan.keep.data() + static_cast<size_t>(f) * bin_sample);
-            plan.tail_from[f] = i;
-            uint32_t* g = plan.mt.data() + static_cast<size_t>(f) * 625;
-            std::copy(rng.st, rng.st + 624, g);
-            g[624] = static_cast<uint32_t>(rng.pos);
-        });
-    }
+    for (int f = 0; f < n_f; ++f)
+        if (!plan.take_all[f] && shuffle_pairs(plan.m[f])) plan.host_f.push_back(f);
+    plan.keep.resize(plan.host_f.size() * static_cast<size_t>(bin_sample));
+    parallel_for(static_cast<int>(plan.host_f.size()), n_threads, [&](int k) {
+        const int f = plan.host_f[k];
+        Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
+        shuffled_prefix(plan.m[f], bin_sample, rng, plan.keep.data() + static_cast<size_t>(k) * bin_sample);
+    });
 }
 
 int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n, int n_f, int max_bin,
@@ -250,7 +244,6 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     const std::vector<long long>& base = plan.base;
     const std::vector<uint8_t>& take_all = plan.take_all;
     const std::vector<int>& kept = plan.kept;
-    const std::vector<int32_t>& keep = plan.keep;
     const int64_t max_sampled = plan.max_sampled;
     const long long cap = plan.cap;
     long long* base_d = scratch.get<long long>(nc);
@@ -261,31 +254,39 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     uint32_t* bits = scratch.get<uint32_t>(static_cast<size_t>(n_f) * words);
     int* err_d = scratch.get<int>(1);
     check(cudaMemsetAsync(err_d, 0, sizeof(int), s), "error flag reset");
-    if (max_sampled > 0) {
-        check(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * static_cast<size_t>(n_f) * words, s), "bits reset");
-        int32_t* keep_d = scratch.get<int32_t>(keep.size());
-        check(cudaMemcpyAsync(keep_d, keep.data(), sizeof(int32_t) * keep.size(), cudaMemcpyHostToDevice, s),
-              "kept ranks upload");
-        std::vector<long long> span(2 * static_cast<size_t>(n_f));
-        for (int f = 0; f < n_f; ++f) {
-            span[f] = plan.tail_from[f];
-            span[n_f + f] = take_all[f] ? 0 : plan.m[f];
-        }
-        long long* span_d = scratch.get<long long>(span.size());
-        uint32_t* mt_d = scratch.get<uint32_t>(plan.mt.size());
-        check(cudaMemcpyAsync(span_d, span.data(), sizeof(long long) * span.size(), cudaMemcpyHostToDevice, s),
-              "tail spans upload");
-        check(cudaMemcpyAsync(mt_d, plan.mt.data(), sizeof(uint32_t) * plan.mt.size(), cudaMemcpyHostToDevice, s),
-              "generator states upload");
-        launch_shuffle_tail(mt_d, span_d, span_d + n_f, n_f, bin_sample, keep_d, err_d, s);
-        launch_keep_bits(keep_d, bin_sample, n_f, take_d, bits, words, s);
-    }
-    int* fill = scratch.get<int>(n_f);
-    check(cudaMemsetAsync(fill, 0, sizeof(int) * n_f, s), "fill reset");
     const size_t esz = x_dtype == 0 ? sizeof(float) : sizeof(double);
     const long long total = static_cast<long long>(n_f) * cap;
     unsigned char* smp_a = scratch.get<unsigned char>(static_cast<size_t>(total) * esz);
     unsigned char* smp_b = scratch.get<unsigned char>(static_cast<size_t>(total) * esz);
+    if (max_sampled > 0) {
+        check(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * static_cast<size_t>(n_f) * words, s), "bits reset");
+        // kept ranks: device draws, with the sample buffers (n_f * cap >= n_f * bin_sample
+        // elements of >= 4 bytes, free until the gather) as the draws' scratch
+        const size_t nk = static_cast<size_t>(n_f) * bin_sample;
+        int32_t* keep_d = scratch.get<int32_t>(nk);
+        int32_t* cnt_d = scratch.get<int32_t>(nk + n_f);
+        std::vector<long long> ms(n_f, 0);
+        std::vector<uint32_t> seeds(n_f);
+        for (int f = 0; f < n_f; ++f) {
+            seeds[f] = plan.seed + static_cast<uint32_t>(f) * 2654435761u;
+            if (!take_all[f] && !shuffle_pairs(plan.m[f])) ms[f] = plan.m[f];
+        }
+        long long* ms_d = scratch.get<long long>(n_f);
+        uint32_t* seeds_d = scratch.get<uint32_t>(n_f);
+        check(cudaMemcpyAsync(ms_d, ms.data(), sizeof(long long) * n_f, cudaMemcpyHostToDevice, s), "sizes upload");
+        check(cudaMemcpyAsync(seeds_d, seeds.data(), sizeof(uint32_t) * n_f, cudaMemcpyHostToDevice, s),
+              "seeds upload");
+        launch_shuffle_prefix(seeds_d, ms_d, n_f, bin_sample, keep_d, reinterpret_cast<int32_t*>(smp_a), cnt_d,
+                              reinterpret_cast<int32_t*>(smp_b), err_d, s);
+        for (size_t k = 0; k < plan.host_f.size(); ++k)
+            check(cudaMemcpyAsync(keep_d + static_cast<size_t>(plan.host_f[k]) * bin_sample,
+                                  plan.keep.data() + k * bin_sample, sizeof(int32_t) * bin_sample,
+                                  cudaMemcpyHostToDevice, s),
+                  "kept ranks upload");
+        launch_keep_bits(keep_d, bin_sample, n_f, take_d, bits, words, s);
+    }
+    int* fill = scratch.get<int>(n_f);
+    check(cudaMemsetAsync(fill, 0, sizeof(int) * n_f, s), "fill reset");
     launch_sample_gather(Xd, x_dtype, n, n_f, base_d, bits, words, take_d, smp_a, cap, fill, s);
     std::vector<int> seg(2 * static_cast<size_t>(n_f));
     for (int f = 0; f < n_f; ++f) {
@@ -313,7 +314,7 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     check(cudaMemcpyAsync(fill_h.data(), fill, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "fill download");
     check(cudaMemcpyAsync(&err_h, err_d, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag download");
     check(cudaStreamSynchronize(s), "quantile edges");
-    if (err_h) throw TideError("device binner: shuffle tail ran past its refill limit");
+    if (err_h) throw TideError("device binner: shuffle draws ran past their refill limit");
     for (int f = 0; f < n_f; ++f)
         if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");
     int mx = 2;

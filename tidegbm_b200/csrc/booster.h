@@ -157,12 +157,12 @@ struct BinPlan {
     std::vector<int> kept;
     int64_t max_sampled = 0;
     long long cap = 1;
-    // [n_f][bin_sample]: the shuffle prefix after its head (sampling.h shuffle_head);
-    // the device finishes draws tail_from[f] .. m[f]-1 from generator state
-    // mt[f*625 .. +625) (624 words and the position).
+    uint32_t seed = 0;
+    // sampled features with fewer than 2^16 values (libstdc++'s two-draws shuffle path)
+    // and their kept ranks [host_f.size()][bin_sample], drawn on the host; the other
+    // sampled features are drawn on the device
+    std::vector<int> host_f;
     std::vector<int32_t> keep;
-    std::vector<long long> tail_from;
-    std::vector<uint32_t> mt;
 };
 void binner_plan(const std::vector<int>& counts, int n, int n_f, int bin_sample, uint32_t seed, int n_threads,
                  BinPlan& plan);

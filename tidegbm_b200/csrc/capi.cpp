@@ -350,34 +350,54 @@ int tgb_shuffled_prefix(long long m, long long keep, unsigned seed, int* out) {
     });
 }
 
+int tgb_shuffle_sequence(long long m, long long keep, unsigned seed, int n_shuffles, int* out) {
+    return guard([&] {
+        need(m >= 0 && m < (1ll << 31) && keep >= 0 && keep <= m && n_shuffles >= 0, "bad sizes");
+        tgb::Mt32 rng(seed);
+        for (int s = 0; s < n_shuffles; ++s) {
+            tgb::Mt32 snap = rng;
+            tgb::shuffled_prefix(m, keep, snap, out + static_cast<size_t>(s) * keep);
+            tgb::skip_shuffle(m, rng);
+            (void)rng();
+        }
+    });
+}
+
 int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* out, void* stream) {
     return guard([&] {
         need(m >= 1 && m < (1ll << 31) && keep >= 1 && keep <= m, "bad sizes");
         need(out != nullptr, "out is null");
         cudaStream_t s = as_stream(stream);
-        tgb::Mt32 rng(seed);
-        std::vector<int32_t> head(static_cast<size_t>(keep));
-        const long long from = tgb::shuffle_head(m, keep, rng, head.data());
-        std::vector<uint32_t> mt(625);
-        std::copy(rng.st, rng.st + 624, mt.begin());
-        mt[624] = static_cast<uint32_t>(rng.pos);
-        const long long span[2] = {from, m};
-        tgb::DBuf<unsigned char> dev;
-        dev.alloc(625 * sizeof(uint32_t) + 2 * sizeof(long long) + sizeof(int));
-        long long* span_d = reinterpret_cast<long long*>(dev.p);
-        int* err_d = reinterpret_cast<int*>(dev.p + 2 * sizeof(long long));
-        uint32_t* mt_d = reinterpret_cast<uint32_t*>(dev.p + 2 * sizeof(long long) + sizeof(int));
+        if (tgb::shuffle_pairs(m)) {  // libstdc++'s two-draws path for short ranges: on the host
+            std::vector<int32_t> h(static_cast<size_t>(keep));
+            tgb::Mt32 rng(seed);
+            tgb::shuffled_prefix(m, keep, rng, h.data());
+            tgb::check(cudaMemcpyAsync(out, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s),
+                       "prefix upload");
+            tgb::check(cudaStreamSynchronize(s), "prefix upload");
+            return;
+        }
+        const size_t k = static_cast<size_t>(keep);
+        tgb::DBuf<int32_t> scratch;
+        scratch.alloc(3 * k + 1);  // head [k], items [k], cnt [k + 1]
+        int32_t* head = scratch.p;
+        int32_t* items = head + k;
+        int32_t* cnt = items + k;
+        tgb::DBuf<long long> ms_d;
+        ms_d.alloc(1);
+        tgb::DBuf<uint32_t> misc;
+        misc.alloc(2);  // seed, error flag
+        const long long ms = m;
+        const uint32_t seed_h = seed;
         int err = 0;
-        tgb::check(cudaMemcpyAsync(out, head.data(), sizeof(int32_t) * head.size(), cudaMemcpyHostToDevice, s),
-                   "head upload");
-        tgb::check(cudaMemcpyAsync(span_d, span, sizeof(span), cudaMemcpyHostToDevice, s), "span upload");
-        tgb::check(cudaMemcpyAsync(mt_d, mt.data(), sizeof(uint32_t) * 625, cudaMemcpyHostToDevice, s),
-                   "state upload");
-        tgb::check(cudaMemsetAsync(err_d, 0, sizeof(int), s), "error flag reset");
-        tgb::launch_shuffle_tail(mt_d, span_d, span_d + 1, 1, static_cast<int>(keep), out, err_d, s);
-        tgb::check(cudaMemcpyAsync(&err, err_d, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag download");
-        tgb::check(cudaStreamSynchronize(s), "shuffle tail");
-        need(err == 0, "shuffle tail ran past its refill limit");
+        tgb::check(cudaMemcpyAsync(ms_d.p, &ms, sizeof(ms), cudaMemcpyHostToDevice, s), "size upload");
+        tgb::check(cudaMemcpyAsync(misc.p, &seed_h, sizeof(seed_h), cudaMemcpyHostToDevice, s), "seed upload");
+        tgb::check(cudaMemsetAsync(misc.p + 1, 0, sizeof(uint32_t), s), "error flag reset");
+        tgb::launch_shuffle_prefix(misc.p, ms_d.p, 1, static_cast<int>(keep), out, head, cnt, items,
+                                   reinterpret_cast<int*>(misc.p + 1), s);
+        tgb::check(cudaMemcpyAsync(&err, misc.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag download");
+        tgb::check(cudaStreamSynchronize(s), "shuffle draws");
+        need(err == 0, "shuffle draws ran past their refill limit");
     });
 }
 

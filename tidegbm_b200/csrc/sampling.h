@@ -37,6 +37,14 @@ namespace tgb {
 // One MT19937 block: twist the 624-word state in place, write the 624 tempered
 // outputs.  Compiled for several x86 vector ISAs and picked at load time (the three
 // loops carry no dependence shorter than 227 words, so they vectorise).
+inline uint32_t mt_temper(uint32_t v) {
+    v ^= v >> 11;
+    v ^= (v << 7) & 0x9d2c5680u;
+    v ^= (v << 15) & 0xefc60000u;
+    v ^= v >> 18;
+    return v;
+}
+
 #if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
 __attribute__((target_clones("avx512f", "avx2", "default")))
 #endif
@@ -44,23 +52,20 @@ inline void mt_refill(uint32_t* __restrict__ st, uint32_t* __restrict__ out) {
     constexpr uint32_t UM = 0x80000000u, LM = 0x7fffffffu, A = 0x9908b0dfu;
     for (int k = 0; k < 227; ++k) {
         const uint32_t y = (st[k] & UM) | (st[k + 1] & LM);
-        st[k] = st[k + 397] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+        const uint32_t v = st[k + 397] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+        st[k] = v;
+        out[k] = mt_temper(v);
     }
     for (int k = 227; k < 623; ++k) {
         const uint32_t y = (st[k] & UM) | (st[k + 1] & LM);
-        st[k] = st[k - 227] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+        const uint32_t v = st[k - 227] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
+        st[k] = v;
+        out[k] = mt_temper(v);
     }
     {
         const uint32_t y = (st[623] & UM) | (st[0] & LM);
         st[623] = st[396] ^ (y >> 1) ^ ((0u - (y & 1u)) & A);
-    }
-    for (int k = 0; k < 624; ++k) {
-        uint32_t v = st[k];
-        v ^= v >> 11;
-        v ^= (v << 7) & 0x9d2c5680u;
-        v ^= (v << 15) & 0xefc60000u;
-        v ^= v >> 18;
-        out[k] = v;
+        out[623] = mt_temper(st[623]);
     }
 }
 
@@ -233,30 +238,50 @@ inline void shuffled_prefix(int64_t m, int64_t keep, G& rng, int32_t* out) {
     std::copy(buf.begin(), buf.end() - 1, out);
 }
 
-// Number of leading words of w[0..k) (a multiple of 16) whose draws take Lemire's fast
-// path: word j paired with range r0 + j has (w * r mod 2^32) >= r, so it consumes no
-// extra word.  One wrapping 32-bit multiply and compare per word; vectorised.
-#if defined(__x86_64__) && defined(__GNUC__) && !defined(__clang__) && !defined(__CUDACC__)
-__attribute__((target_clones("avx512f", "avx2", "default")))
-#endif
-inline int clean_prefix(const uint32_t* __restrict__ w, uint32_t r0, int k) {
-    int done = 0;
-    while (done + 16 <= k) {
-        uint32_t flag = 0;
-        for (int l = 0; l < 16; ++l) {
-            const uint32_t r = r0 + static_cast<uint32_t>(done + l);
-            flag |= static_cast<uint32_t>(w[done + l] * r < r);
-        }
-        if (flag) break;
-        done += 16;
+// Index of the first word of w[0..k) whose draw may take more than one word: word l,
+// paired with range r0 + l, whose product w * r has low half (mod 2^32) below r.  k when
+// there is none.  Every other word is accepted by Lemire's method as it stands.
+inline int first_candidate_scalar(const uint32_t* w, uint32_t r0, int k) {
+    for (int l = 0; l < k; ++l) {
+        const uint32_t r = r0 + static_cast<uint32_t>(l);
+        if (w[l] * r < r) return l;
     }
-    return done;
+    return k;
+}
+
+#ifdef TGB_HAVE_AVX512_TAIL
+// The same, 16 words per step: one 32-bit multiply-low and one unsigned compare into a mask.
+__attribute__((target("avx512f"))) inline int first_candidate_avx512(const uint32_t* w, uint32_t r0, int k) {
+    const __m512i lane = _mm512_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15);
+    int l = 0;
+    for (; l + 16 <= k; l += 16) {
+        const __m512i R = _mm512_add_epi32(_mm512_set1_epi32(static_cast<int>(r0 + static_cast<uint32_t>(l))), lane);
+        const __m512i lo = _mm512_mullo_epi32(_mm512_loadu_si512(w + l), R);
+        const __mmask16 c = _mm512_cmplt_epu32_mask(lo, R);
+        if (c) return l + __builtin_ctz(c);
+    }
+    if (l < k) {
+        const __mmask16 valid = static_cast<__mmask16>((1u << (k - l)) - 1u);
+        const __m512i R = _mm512_add_epi32(_mm512_set1_epi32(static_cast<int>(r0 + static_cast<uint32_t>(l))), lane);
+        const __m512i lo = _mm512_mullo_epi32(_mm512_maskz_loadu_epi32(valid, w + l), R);
+        const __mmask16 c = _mm512_mask_cmplt_epu32_mask(valid, lo, R);
+        if (c) return l + __builtin_ctz(c);
+    }
+    return k;
+}
+#endif
+
+inline int first_candidate(const uint32_t* w, uint32_t r0, int k) {
+#ifdef TGB_HAVE_AVX512_TAIL
+    if (have_avx512()) return first_candidate_avx512(w, r0, k);
+#endif
+    return first_candidate_scalar(w, r0, k);
 }
 
 // Advances rng exactly as std::shuffle of m elements does, without producing positions.
 // A draw consumes extra words only when its first product's low half is below the
-// range (probability range / 2^32), so whole groups of 16 consecutive words are tested
-// at once and only a group containing such a word is replayed draw by draw.
+// range (probability range / 2^32): the words before the first such candidate are
+// skipped in one step, and the candidate itself takes the exact draw.
 inline void skip_shuffle(int64_t m, Mt32& rng) {
     if (m <= 0) return;
     if (shuffle_pairs(m)) {
@@ -267,16 +292,13 @@ inline void skip_shuffle(int64_t m, Mt32& rng) {
     int64_t i = 1;  // next draw uses range i + 1
     while (i < m) {
         if (rng.pos >= 624) rng.refill();
-        const int avail = 624 - rng.pos;
-        const int64_t left = m - i;
-        const int k = static_cast<int>(std::min<int64_t>(avail, left));
-        const int done = clean_prefix(rng.out + rng.pos, static_cast<uint32_t>(i + 1), k);
+        const int k = static_cast<int>(std::min<int64_t>(624 - rng.pos, m - i));
+        const int done = first_candidate(rng.out + rng.pos, static_cast<uint32_t>(i + 1), k);
         rng.pos += done;
         i += done;
         if (done == k) continue;  // block exhausted or m reached
-        // Replay up to 16 draws exactly (one of them may consume extra words).
-        const int64_t stop = std::min<int64_t>(m, i + 16);
-        for (; i < stop; ++i) (void)bounded(rng, static_cast<uint32_t>(i + 1));
+        (void)bounded(rng, static_cast<uint32_t>(i + 1));
+        ++i;
     }
 }
 

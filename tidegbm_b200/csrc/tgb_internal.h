@@ -178,12 +178,14 @@ void launch_nonnan_counts(const void* X, int x_dtype, int n, int n_f, int* count
 void launch_keep_bits(const int32_t* keep, int bin_sample, int n_f, const uint8_t* take_all, uint32_t* bits,
                       long long words, cudaStream_t s);
 
-// tail of a std::shuffle prefix (kernels_shuffle.cu): for range r, draws from[r] ..
-// to[r]-1 continuing the MT19937 state mt[r*625 .. +624) at position mt[r*625 + 624];
-// slots[r*keep ..) holds the prefix after the head and receives the tail's writes.
-// *err is set when a range runs past its refill limit.
-void launch_shuffle_tail(const uint32_t* mt, const long long* from, const long long* to, int n_ranges, int keep,
-                         int32_t* slots, int* err, cudaStream_t s);
+// prefixes of std::shuffle(iota(ms[r]), std::mt19937(seeds[r])) (kernels_shuffle.cu):
+// out[r][0..keep) for every range with ms[r] >= max(keep, 2^16) or ms[r] == keep;
+// ranges with ms[r] == 0 are skipped (their rows of out are left to the caller).
+// out and cnt must hold -1 and 0 (launch_shuffle_prefix sets them); head and items are
+// scratch of n_ranges * keep ints, cnt of n_ranges * (keep + 1).  *err is set when a
+// range runs past its refill limit.
+void launch_shuffle_prefix(const uint32_t* seeds, const long long* ms, int n_ranges, int keep, int32_t* out,
+                           int32_t* head, int32_t* cnt, int32_t* items, int* err, cudaStream_t s);
 void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const uint32_t* bits,
                           long long words, const uint8_t* take_all, void* sample, long long cap, int* fill,
                           cudaStream_t s);

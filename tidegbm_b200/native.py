@@ -62,6 +62,7 @@ def lib() -> C.CDLL:
         "tgb_binner_fit": ([vp, i, i, i, i, i, C.c_uint, vp, vp], i),
         "tgb_shuffled_prefix": ([ll, ll, C.c_uint, vp], i),
         "tgb_shuffled_prefix_device": ([ll, ll, C.c_uint, vp, vp], i),
+        "tgb_shuffle_sequence": ([ll, ll, C.c_uint, i, vp], i),
         "tgb_bin_transform": ([vp, i, i, i, vp, vp, vp, i, vp], i),
         "tgb_hist_build": ([vp, i, i, vp, i, vp, vp, i, i, vp, vp, vp, vp], i),
         "tgb_split_scan": ([vp, vp, vp, i, i, i, i, d, d, i, d, vp, vp, vp, vp], i),
