@@ -70,8 +70,14 @@ __device__ __forceinline__ void add64s(unsigned int* lo, unsigned int* hi, int k
     if (up != 0u) atomicAdd(&hi[k], up);
 }
 
+constexpr int kApplyRows = 8;  // rows a thread walks together
+
+// The tree walk reads the column-major codes: at each level the kApplyRows rows of a
+// thread issue their code loads together, and the 32 lanes of a warp hold 32 consecutive
+// rows, so lanes at nodes with the same split feature read one 32-byte sector.  A row
+// costs about one sector share per level instead of its whole 128-byte row.
 __global__ void __launch_bounds__(kApplyThreads)
-    apply_accum_kernel(const uint8_t* __restrict__ codes, int stride, const DevNode* __restrict__ nodes,
+    apply_accum_kernel(const uint8_t* __restrict__ col, long long pitch, const DevNode* __restrict__ nodes,
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
                        const double* __restrict__ h, const int4* __restrict__ chunks,
                        const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
@@ -94,22 +100,43 @@ __global__ void __launch_bounds__(kApplyThreads)
     const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
     const double gs = sc->gscale, hs = sc->hscale;
     __syncthreads();
-    // Each thread walks its rows straight from the row-major codes: a row is one 128-byte
-    // line at most, so the walk's byte loads hit the same line (L1) after the first
-    // touch; g and h are loaded before the walk so their latency overlaps it.
-    for (int r = ch.y + threadIdx.x; r < ch.z; r += blockDim.x) {
-        const double gv = g[r], hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
-        const uint8_t* row = codes + static_cast<size_t>(r) * stride;
-        int k = 0;
-        while (!s_leaf[k]) {
-            const int b = __ldg(row + s_feat[k]);
-            const bool left = b == 0 ? s_ml[k] != 0 : b <= s_thr[k];
-            k = left ? s_left[k] : s_right[k];
+    for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
+        int r[kApplyRows], k[kApplyRows];
+        double gv[kApplyRows], hv[kApplyRows];
+#pragma unroll
+        for (int i = 0; i < kApplyRows; ++i) {
+            r[i] = base + threadIdx.x + i * kApplyThreads;
+            k[i] = 0;
+            const bool ok = r[i] < ch.z;
+            gv[i] = ok ? g[r[i]] : 0.0;  // loaded before the walk so their latency overlaps it
+            hv[i] = ok && h ? h[r[i]] : 1.0;  // h == nullptr: unit hessians
+            if (!ok) r[i] = -1;
         }
-        nid[r] = static_cast<int16_t>(k);
-        add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
-        add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
-        atomicAdd(&aC[k], 1u);
+        for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
+            unsigned int b[kApplyRows];
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < kApplyRows; ++i) {
+                const bool walk = r[i] >= 0 && !s_leaf[k[i]];
+                b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
+                any |= walk;
+            }
+            if (!any) break;
+#pragma unroll
+            for (int i = 0; i < kApplyRows; ++i) {
+                if (r[i] < 0 || s_leaf[k[i]]) continue;
+                const bool left = b[i] == 0u ? s_ml[k[i]] != 0 : b[i] <= s_thr[k[i]];
+                k[i] = left ? s_left[k[i]] : s_right[k[i]];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kApplyRows; ++i) {
+            if (r[i] < 0) continue;
+            nid[r[i]] = static_cast<int16_t>(k[i]);
+            add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
+            add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
+            atomicAdd(&aC[k[i]], 1u);
+        }
     }
     __syncthreads();
     unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
@@ -289,13 +316,13 @@ void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cud
     check(cudaGetLastError(), "all_scale_finalize launch");
 }
 
-void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, const DevTreeState* st,
+void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks,
                         const AllScale* sc, int16_t* nid, unsigned long long* seg_sums, int n_segments,
                         cudaStream_t s) {
     check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
           "seg sums reset");
-    apply_accum_kernel<<<n_chunks, kApplyThreads, 0, s>>>(codes, stride, nodes, st, g, h, chunks, sc, nid,
+    apply_accum_kernel<<<n_chunks, kApplyThreads, 0, s>>>(col, pitch, nodes, st, g, h, chunks, sc, nid,
                                                           seg_sums);
     check(cudaGetLastError(), "apply_accum launch");
 }

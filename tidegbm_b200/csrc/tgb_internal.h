@@ -285,7 +285,8 @@ void launch_all_scale_finalize(AllScale* sc, int n, cudaStream_t s);
 // pred += lr * prefix[bucket][leaf] and per-block sums of (pred - y)^2 into partials[n_part].
 void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
                              double* pred, const double* y, double* partials, int n_part, cudaStream_t s);
-void launch_apply_accum(const uint8_t* codes, int stride, const DevNode* nodes, const DevTreeState* st,
+// col: column-major codes (col[f * pitch + r], launch_codes_transpose)
+void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
                         int16_t* nid, unsigned long long* seg_sums, int n_segments, cudaStream_t s);
 void launch_finalize_tree(const PostParams& pp, const DevTreeState* st, const unsigned long long* seg_sums,
