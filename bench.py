@@ -282,6 +282,19 @@ def held_out_ic(pred, panel) -> float:
     return float(((a * b).sum(axis=1)[ok] / den[ok]).mean())
 
 
+def max_over_ranks(values, device):
+    """Element-wise max over the ranks of a list of floats (one process per GPU), after a
+    barrier; the values unchanged when no process group of several ranks is running."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -327,13 +340,8 @@ def run_ours(args) -> None:
     # timed trees are exactly trees W .. W+K-1 (the bench's K steps)
     assert int(st["timed_trees"]) == K, st
     ms_per_tree = timed_ms / st["timed_trees"]
-    times = torch.tensor([ms_per_tree], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    ms_max = float(times.item())
+    # the slowest rank sets both whole-job numbers
+    ms_max, e2e_wall = max_over_ranks([ms_per_tree, e2e_wall], "cuda")
     value = world * 1000.0 / ms_max
     info = b.info()
     trees = b.trees()
