@@ -342,42 +342,46 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     n_buckets = nbk;
 
     // ---- initial predictions: booster.cpp:399-457 ----
-    init_prefix.assign(nbk, 0.0);
-    if (c.objective == 5) {
-        init_score = 0.0;
-    } else {
-        // One running FP64 sum in row order: the same partial sums the reference
-        // forms separately for every prefix [0, cut_b) and for [0, n).
-        std::vector<int> order_b(nbk);
-        std::iota(order_b.begin(), order_b.end(), 0);
-        double sw = 0, sy = 0;
-        int i = 0;
-        std::vector<double> at_cut(nbk, 0.0);
-        for (int b = 0; b < nbk && !c.iid_mode; ++b) {
-            for (; i < cut[b]; ++i) {
+    // A sequential FP64 pass over y in row order (the reference's summation order); it
+    // runs on the host while the X upload is in flight (below).
+    std::vector<double> fill_prefix;
+    auto initial_predictions = [&] {
+        init_prefix.assign(nbk, 0.0);
+        if (c.objective == 5) {
+            init_score = 0.0;
+        } else {
+            // One running FP64 sum in row order: the same partial sums the reference
+            // forms separately for every prefix [0, cut_b) and for [0, n).
+            std::vector<int> order_b(nbk);
+            std::iota(order_b.begin(), order_b.end(), 0);
+            double sw = 0, sy = 0;
+            int i = 0;
+            std::vector<double> at_cut(nbk, 0.0);
+            for (int b = 0; b < nbk && !c.iid_mode; ++b) {
+                for (; i < cut[b]; ++i) {
+                    sw += 1.0;
+                    sy += 1.0 * y[i];
+                }
+                at_cut[b] = cut[b] > 0 ? (sw > 0 ? sy / sw : 0) : NAN;
+            }
+            for (; i < n; ++i) {
                 sw += 1.0;
                 sy += 1.0 * y[i];
             }
-            at_cut[b] = cut[b] > 0 ? (sw > 0 ? sy / sw : 0) : NAN;
+            init_score = sw > 0 ? sy / sw : 0;
+            if (!c.iid_mode) init_prefix = at_cut;
         }
-        for (; i < n; ++i) {
-            sw += 1.0;
-            sy += 1.0 * y[i];
+        // Device fill values: the prior of each bucket, or init_score for every row in iid
+        // mode (where the reference leaves init_prefix = {0.0}, booster.cpp:400).
+        if (c.iid_mode) {
+            init_prefix.assign(1, 0.0);
+            fill_prefix.assign(1, init_score);
+        } else {
+            for (int b = 0; b < nbk; ++b)
+                if (!std::isfinite(init_prefix[b])) init_prefix[b] = init_score;
+            fill_prefix = init_prefix;
         }
-        init_score = sw > 0 ? sy / sw : 0;
-        if (!c.iid_mode) init_prefix = at_cut;
-    }
-    // Device fill values: the prior of each bucket, or init_score for every row in iid
-    // mode (where the reference leaves init_prefix = {0.0}, booster.cpp:400).
-    std::vector<double> fill_prefix;
-    if (c.iid_mode) {
-        init_prefix.assign(1, 0.0);
-        fill_prefix.assign(1, init_score);
-    } else {
-        for (int b = 0; b < nbk; ++b)
-            if (!std::isfinite(init_prefix[b])) init_prefix[b] = init_score;
-        fill_prefix = init_prefix;
-    }
+    };
 
     stats.t_pre_upload = now() - t_pre0;  // GOSS sampler start, TORB buckets and cuts
     // ---- device buffers ----
@@ -424,6 +428,7 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
         Xd.alloc(static_cast<size_t>(n) * n_f * xsz);
         check(cudaMemcpyAsync(Xd.p, X, static_cast<size_t>(n) * n_f * xsz, cudaMemcpyHostToDevice, s), "X upload");
         check(cudaMemcpyAsync(D.y.p, y, sizeof(double) * n, cudaMemcpyHostToDevice, s), "y upload");
+        initial_predictions();  // host work while the copies run (they only read X and y)
         check(cudaStreamSynchronize(s), "X upload");
         stats.t_h2d = now() - tb - stats.t_alloc;
         // ---- quantile edges: Binner::fit (binning.cpp:34-102) on the uploaded X ----
