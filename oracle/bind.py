@@ -47,6 +47,8 @@ class _OrcConfig(C.Structure):
         ("iid_mode", C.c_int), ("objective", C.c_int), ("random_state", C.c_int),
         ("goss", C.c_int), ("goss_top", C.c_double), ("goss_other", C.c_double),
         ("bin_sample", C.c_int), ("torb_min_cover", C.c_double), ("finer_torb", C.c_int),
+        ("pair_splits", C.c_int), ("pair_trigger", C.c_double), ("pair_top_k", C.c_int),
+        ("max_pair_splits_per_tree", C.c_int), ("pair_l2", C.c_double),
     ]
 
 
@@ -139,14 +141,18 @@ class TreeArrays:
     values: np.ndarray
     cover: np.ndarray
     prefix: np.ndarray
+    split_type: np.ndarray | None = None  # SplitType per node (0 axis, 1 pair), when exported
+    feature2: np.ndarray | None = None    # second feature of pair splits (-1 otherwise)
 
     @classmethod
-    def from_raw(cls, inodes: np.ndarray, fnodes: np.ndarray, values, cover, prefix) -> "TreeArrays":
+    def from_raw(cls, inodes: np.ndarray, fnodes: np.ndarray, values, cover, prefix,
+                 split: np.ndarray | None = None) -> "TreeArrays":
         I = inodes.reshape(-1, 8)
         F = fnodes.reshape(-1, 2)
+        S = None if split is None else split.reshape(-1, 2)
         return cls(I[:, 0].copy(), I[:, 1].copy(), I[:, 2].copy(), I[:, 3].copy(), I[:, 4].copy(),
                    I[:, 5].copy(), I[:, 6].copy(), I[:, 7].copy(), F[:, 0].copy(), F[:, 1].copy(),
-                   values, cover, prefix)
+                   values, cover, prefix, None if S is None else S[:, 0].copy(), None if S is None else S[:, 1].copy())
 
 
 @dataclass
@@ -162,12 +168,13 @@ class FitResult:
 def _cfg_struct(params: dict) -> _OrcConfig:
     c = _OrcConfig()
     oracle_lib().orc_config_default(C.byref(c))
+    c.pair_splits = 0  # the parity convention ref_fit shares: PAIR only when asked for
     for k, v in params.items():
         if k == "objective":
             v = OBJECTIVES[v] if isinstance(v, str) else int(v)
-        if k in ("pair_splits", "halo", "n_jobs"):
+        if k in ("halo", "n_jobs"):
             continue
-        setattr(c, k, v)
+        setattr(c, k, int(v) if k == "pair_splits" else v)
     return c
 
 
@@ -200,7 +207,9 @@ def oracle_fit(params: dict, X, y, ts=None, entity=None) -> tuple[FitResult, int
         cov = np.zeros(nn, np.int32)
         pre = np.zeros(nn * res.n_buckets)
         L.orc_tree_export(h, t, I, Fv, vals, cov, pre)
-        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre))
+        S = np.zeros(2 * nn, np.int32)
+        L.orc_tree_export_split(h, t, S.ctypes.data_as(C.c_void_p))
+        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre, S))
     return res, h
 
 
@@ -252,7 +261,9 @@ def ref_fit(params: dict, X, y, ts=None, entity=None, n_jobs: int = 0):
         cov = np.zeros(nn, np.int32)
         pre = np.zeros(nn * nb)
         L.ref_tree_export(h, t, I, Fv, vals, cov, pre)
-        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre))
+        S = np.zeros(2 * nn, np.int32)
+        L.ref_tree_export_split(h, t, S.ctypes.data_as(C.c_void_p))
+        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre, S))
     return res, h
 
 

@@ -37,6 +37,8 @@ struct OrcNode {
     double gain = 0.0;
     int n_samples = 0;
     int depth = 0;
+    int split_type = 0;  // SplitType (cpp/include/tidegbm/types.hpp:25): 0 axis, 1 pair
+    int feature2 = -1;   // second feature of a pair split
 };
 
 struct OrcTree {
@@ -87,15 +89,32 @@ inline double leaf_value(double G, double H, double l2) { return -G / (H + l2); 
 // cpp/src/histogram.cpp:126-134 with l1 = 0.
 inline double leaf_score(double G, double H, double lam) { return (G * G) / (H + lam); }
 
-// cpp/src/tree.cpp:15-41 for axis splits on uint8 codes.
-int apply_one(const OrcTree& t, const uint8_t* row) {
+// pair_bin (cpp/include/tidegbm/histogram.hpp:81-85): the two codes hashed into one of
+// n_bins bins, in 32-bit unsigned arithmetic.
+inline int pair_bin(int b1, int b2, int n_bins) {
+    return static_cast<int>((static_cast<uint32_t>(b1) * 2654435761u + static_cast<uint32_t>(b2) * 40503u) %
+                            static_cast<uint32_t>(n_bins));
+}
+
+// Direction of one row at a split node: cpp/src/tree.cpp:21-28 (pair: missing if either
+// code is missing, else the hashed bin against the threshold) and :36-39 (axis).
+inline bool goes_left(const OrcNode& d, const uint8_t* row, int n_bins) {
+    if (d.split_type == 1) {
+        const int b1 = row[d.feature], b2 = row[d.feature2];
+        if (b1 == 0 || b2 == 0) return d.missing_go_left != 0;
+        return pair_bin(b1, b2, n_bins) <= d.threshold_bin;
+    }
+    const int b = row[d.feature];
+    return (b == 0) ? d.missing_go_left != 0 : b <= d.threshold_bin;
+}
+
+// cpp/src/tree.cpp:15-41 for axis and pair splits on uint8 codes.
+int apply_one(const OrcTree& t, const uint8_t* row, int n_bins) {
     int nid = 0;
     for (;;) {
         const OrcNode& d = t.nodes[nid];
         if (d.is_leaf) return nid;
-        const int b = row[d.feature];
-        const bool left = (b == 0) ? d.missing_go_left != 0 : b <= d.threshold_bin;
-        nid = left ? d.left : d.right;
+        nid = goes_left(d, row, n_bins) ? d.left : d.right;
     }
 }
 
@@ -142,8 +161,16 @@ int auto_time_buckets(const int64_t* ts, int n, int64_t horizon, int uniq_cap) {
     return std::max(2, std::min(want, std::max(uniq_cap, 2)));
 }
 
-// cpp/src/tree.cpp:283-472, axis splits only (no colsample, groups, HALO, PAIR,
-// regime, interaction constraints, monotone).  Rows are sorted ascending first.
+// A split candidate: orc_split plus the PAIR fields of SplitCand
+// (cpp/include/tidegbm/histogram.hpp:65-74).
+struct Cand {
+    orc_split s{-1e300, -1, -1, 1};
+    int type = 0;
+    int feature2 = -1;
+};
+
+// cpp/src/tree.cpp:283-472, axis and PAIR splits (no colsample, groups, HALO, regime,
+// interaction constraints, monotone, forced pairs).  Rows are sorted ascending first.
 OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const double* h,
                   std::vector<int32_t> sample, int n_f, int n_bins, const orc_config& c) {
     OrcTree tree;
@@ -163,53 +190,94 @@ OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const doubl
     leaf_hist[0].assign(static_cast<size_t>(n_f) * nb_stride * 3, 0.0);
     orc_build_hist(codes, stride, n_f, sample.data(), static_cast<int>(sample.size()), g, h, n_bins,
                    leaf_hist[0].data());
-    std::vector<orc_split> cached(1);
+    std::vector<Cand> cached(1);
     std::vector<char> ok(1, 0);
 
-    auto best_for_leaf = [&](int lid) {
-        // cpp/src/tree.cpp:106-166
-        orc_split best{-1e300, -1, -1, 1};
+    auto best_for_leaf = [&](int lid, int pair_budget) {
+        // cpp/src/tree.cpp:106-166: the best axis split over the features in ascending order
+        std::vector<orc_split> per_f(n_f);
+        for (int f = 0; f < n_f; ++f)
+            per_f[f] = orc_best_numeric(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
+                                        c.min_samples_leaf, c.min_child_weight);
+        Cand best;
         for (int f = 0; f < n_f; ++f) {
-            orc_split s = orc_best_numeric(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
-                                           c.min_samples_leaf, c.min_child_weight);
-            if (s.feature < 0 || s.gain < c.min_split_gain) continue;
-            if (s.gain > best.gain) best = s;
+            if (per_f[f].feature < 0 || per_f[f].gain < c.min_split_gain) continue;
+            if (per_f[f].gain > best.s.gain) best.s = per_f[f];
+        }
+        // cpp/src/tree.cpp:214-281: PAIR when the best axis gain is weak against the leaf's
+        // gradient energy (sum of g^2 in row order, tree.cpp:355-356)
+        const std::vector<int32_t>& ix = leaf_idx[lid];
+        double energy = 0;
+        for (int32_t i : ix) energy += g[i] * g[i];
+        const bool weak = (best.s.gain < c.pair_trigger * std::max(energy * 0.01, 1e-12)) || best.s.gain <= 0;
+        if (c.pair_splits && pair_budget > 0 && n_f >= 2 && weak) {
+            std::vector<int> top(n_f);
+            std::iota(top.begin(), top.end(), 0);
+            std::sort(top.begin(), top.end(), [&](int a, int b) { return per_f[a].gain > per_f[b].gain; });
+            const int k = std::min(c.pair_top_k, n_f);
+            std::vector<double> hz(static_cast<size_t>(n_bins) * 3);
+            for (int a = 0; a < k; ++a)
+                for (int b = a + 1; b < k; ++b) {
+                    const int f1 = top[a], f2 = top[b];
+                    std::fill(hz.begin(), hz.end(), 0.0);
+                    for (int32_t i : ix) {
+                        const uint8_t* row = codes + static_cast<size_t>(i) * stride;
+                        double* B = hz.data() + 3 * static_cast<size_t>(pair_bin(row[f1], row[f2], n_bins));
+                        B[0] += g[i];
+                        B[1] += h[i];
+                        B[2] += 1;
+                    }
+                    Cand cand;
+                    cand.s = orc_best_numeric(hz.data(), n_bins, 0, c.pair_l2, c.min_split_gain, c.min_samples_leaf,
+                                              c.min_child_weight);
+                    cand.s.feature = f1;
+                    cand.type = 1;
+                    cand.feature2 = f2;
+                    if (cand.s.gain > best.s.gain) best = cand;
+                }
         }
         return best;
     };
+    int pair_used = 0;
 
     for (int iter = 0; iter < c.max_leaves - 1; ++iter) {
         int best_leaf = -1;
-        orc_split best{-1e300, -1, -1, 1};
+        Cand bestc;
         double best_score = c.min_split_gain;
         for (int lid = 0; lid < static_cast<int>(tree.nodes.size()); ++lid) {
             if (!tree.nodes[lid].is_leaf) continue;
             if (tree.nodes[lid].depth >= c.max_depth) continue;
             if (static_cast<int>(leaf_idx[lid].size()) < 2 * c.min_samples_leaf) continue;
             if (!ok[lid]) {
-                cached[lid] = best_for_leaf(lid);
+                cached[lid] = best_for_leaf(lid, c.max_pair_splits_per_tree - pair_used);
                 ok[lid] = 1;
             }
-            const orc_split& rec = cached[lid];
-            if (rec.feature >= 0 && rec.gain >= c.min_split_gain && rec.gain > best_score) {
-                best_score = rec.gain;
+            const Cand& rec = cached[lid];
+            if (rec.s.feature >= 0 && rec.s.gain >= c.min_split_gain && rec.s.gain > best_score) {
+                best_score = rec.s.gain;
                 best_leaf = lid;
-                best = rec;
+                bestc = rec;
             }
         }
         if (best_leaf < 0) break;
+        const orc_split& best = bestc.s;
         OrcNode& p = tree.nodes[best_leaf];
         p.is_leaf = 0;
         p.feature = best.feature;
+        p.feature2 = bestc.feature2;
+        p.split_type = bestc.type;
         p.threshold_bin = best.threshold_bin;
         p.missing_go_left = best.missing_go_left;
         p.gain = best.gain;
+        if (bestc.type == 1) {  // tree.cpp:393-396: a pair split re-scores every leaf
+            pair_used += 1;
+            std::fill(ok.begin(), ok.end(), 0);
+        }
         ok[best_leaf] = 0;
         // cpp/src/tree.cpp:68-91 stable partition
         std::vector<int32_t> L, R;
         for (int32_t i : leaf_idx[best_leaf]) {
-            const int b = codes[static_cast<size_t>(i) * stride + best.feature];
-            const bool left = (b == 0) ? best.missing_go_left != 0 : b <= best.threshold_bin;
+            const bool left = goes_left(tree.nodes[best_leaf], codes + static_cast<size_t>(i) * stride, n_bins);
             (left ? L : R).push_back(i);
         }
         OrcNode nl, nr;
@@ -490,13 +558,19 @@ void orc_config_default(orc_config* c) {
     c->bin_sample = 262144;
     c->torb_min_cover = 0.0;
     c->finer_torb = 1;
+    c->pair_splits = 1;
+    c->pair_trigger = 0.25;
+    c->pair_top_k = 6;
+    c->max_pair_splits_per_tree = 3;
+    c->pair_l2 = 2.0;
 }
 
 void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, int n, int n_f,
               const int64_t* ts_in, const int64_t* ent_in) {
     // cpp/src/booster.cpp:231-742 for the supported subset.
     try {
-        const orc_config c = *cfgp;
+        orc_config c = *cfgp;
+        if (n >= 1000000) c.pair_splits = 0;  // booster.cpp:237-240 (no forced pairs here)
         if (!c.iid_mode && c.horizon < 0) throw std::runtime_error("horizon is required in time mode");
         if (!c.iid_mode && !ts_in) throw std::runtime_error("timestamp is required unless iid_mode");
         auto* M = new OrcModel();
@@ -635,7 +709,7 @@ void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, in
             (void)rng();  // booster.cpp:588 seeds grow_tree's own generator
             // booster.cpp:589-600 full-data leaf values from unscaled g, h
             std::vector<int> nid(n);
-            for (int i = 0; i < n; ++i) nid[i] = apply_one(tree, codes.data() + static_cast<size_t>(i) * n_f);
+            for (int i = 0; i < n; ++i) nid[i] = apply_one(tree, codes.data() + static_cast<size_t>(i) * n_f, M->n_bins);
             const int nn = static_cast<int>(tree.nodes.size());
             std::vector<double> Gs(nn, 0), Hs(nn, 0);
             tree.cover.assign(nn, 0);
@@ -723,6 +797,14 @@ void orc_tree_export(void* m, int t, int* inodes, double* fnodes, double* values
     std::memcpy(prefix, tr.prefix.data(), tr.prefix.size() * sizeof(double));
 }
 
+void orc_tree_export_split(void* m, int t, int* out) {
+    const OrcTree& tr = static_cast<OrcModel*>(m)->trees[t];
+    for (size_t k = 0; k < tr.nodes.size(); ++k) {
+        out[2 * k] = tr.nodes[k].split_type;
+        out[2 * k + 1] = tr.nodes[k].feature2;
+    }
+}
+
 void orc_predict_raw(void* mp, const double* X, int n, double* out) {
     // booster.cpp:744-773 with tree_decay = 1 and best_iteration = n_estimators.
     const OrcModel& M = *static_cast<OrcModel*>(mp);
@@ -731,7 +813,7 @@ void orc_predict_raw(void* mp, const double* X, int n, double* out) {
     for (int i = 0; i < n; ++i) {
         double s = M.init_score;
         for (const OrcTree& t : M.trees)
-            s += M.cfg.learning_rate * t.values[apply_one(t, codes.data() + static_cast<size_t>(i) * M.n_f)];
+            s += M.cfg.learning_rate * t.values[apply_one(t, codes.data() + static_cast<size_t>(i) * M.n_f, M.n_bins)];
         out[i] = s;
     }
 }

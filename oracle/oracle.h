@@ -66,7 +66,7 @@ void orc_grad_hess(int kind, const double* y, const double* pred, const int64_t*
 double orc_loss(int kind, const double* y, const double* pred, const int64_t* groups, int n);
 
 /* Fit configuration: the subset of Config (cpp/include/tidegbm/config.hpp:12-76)
- * that the GPU path supports. */
+ * that the oracle restates. */
 typedef struct {
     int n_estimators;
     double learning_rate;
@@ -89,6 +89,12 @@ typedef struct {
     int bin_sample;
     double torb_min_cover;
     int finer_torb;
+    /* PAIR splits (config.hpp:31-35); turned off for n >= 1M as booster.cpp:237-240 does */
+    int pair_splits;
+    double pair_trigger;
+    int pair_top_k;
+    int max_pair_splits_per_tree;
+    double pair_l2;
 } orc_config;
 
 void orc_config_default(orc_config* c);
@@ -112,6 +118,8 @@ int orc_tree_n_nodes(void* model, int t);
  * left, right, missing_go_left, n_samples, depth}; fnodes[2*k] = {value, gain}. */
 void orc_tree_export(void* model, int t, int* inodes, double* fnodes, double* values, int* cover,
                      double* prefix);
+/* Per node {split_type (0 axis, 1 pair; types.hpp:25), feature2} into out[2*k]. */
+void orc_tree_export_split(void* model, int t, int* out);
 /* Booster::predict_raw (booster.cpp:744-811) on f64 X. */
 void orc_predict_raw(void* model, const double* X, int n, double* out);
 

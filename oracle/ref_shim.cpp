@@ -63,6 +63,10 @@ int ref_set(void* hb, const char* key, double v) {
     else if (k == "iid_mode") c.iid_mode = v != 0;
     else if (k == "halo") c.halo = v != 0;
     else if (k == "pair_splits") c.pair_splits = v != 0;
+    else if (k == "pair_trigger") c.pair_trigger = v;
+    else if (k == "pair_top_k") c.pair_top_k = static_cast<int>(v);
+    else if (k == "max_pair_splits_per_tree") c.max_pair_splits_per_tree = static_cast<int>(v);
+    else if (k == "pair_l2") c.pair_l2 = v;
     else if (k == "objective") c.objective = objective_from_code(static_cast<int>(v));
     else if (k == "n_jobs") c.n_jobs = static_cast<int>(v);
     else if (k == "random_state") c.random_state = static_cast<int>(v);
@@ -168,6 +172,15 @@ void ref_tree_export(void* hb, int t, int* inodes, double* fnodes, double* value
         cover[k] = tr.cover[k];
     }
     std::memcpy(prefix, tr.prefix_values.data(), tr.prefix_values.size() * sizeof(double));
+}
+
+// Per node {split_type (SplitType, types.hpp:25), feature2} into out[2*k].
+void ref_tree_export_split(void* hb, int t, int* out) {
+    const Tree& tr = static_cast<Booster*>(hb)->trees[t];
+    for (size_t k = 0; k < tr.nodes.size(); ++k) {
+        out[2 * k] = static_cast<int>(tr.nodes[k].split_type);
+        out[2 * k + 1] = tr.nodes[k].feature2;
+    }
 }
 
 int ref_edges(void* hb, int f, double* out) {

@@ -11,6 +11,8 @@ Each fixture is the reference's output on a small seeded input:
   fit_mse.npz   Booster::fit (cpp/src/booster.cpp:231-742): trees, values, TORB prefixes,
                 evals, predictions (time mode, mse, GOSS on)
   fit_pair.npz  the same for the pairwise objective
+  fit_pairsplit.npz  mse with PAIR splits on (cpp/src/tree.cpp:214-281) over an interaction
+                target, where the axis splits are weak; trees carry split_type and feature2
 The tests check the oracle restatement (CPU) and the CUDA path (GPU) against them.
 """
 from __future__ import annotations
@@ -30,6 +32,8 @@ from tidegbm_b200 import panels  # noqa: E402
 
 FIT_MSE = dict(n_estimators=8, learning_rate=0.1, max_depth=5, max_leaves=15, horizon=2, objective="mse", goss=1,
                random_state=4, bin_sample=3000)
+FIT_PAIRSPLIT = dict(n_estimators=5, learning_rate=0.1, max_depth=5, max_leaves=15, horizon=1, objective="mse",
+                     random_state=3, pair_splits=1)
 FIT_PAIR = dict(n_estimators=6, learning_rate=0.08, max_depth=4, max_leaves=12, horizon=1, objective="pairwise",
                 random_state=2)
 
@@ -41,6 +45,23 @@ def _X(seed, n, nf, nan=0.03):
     X[:, 2] = np.exp(X[:, 2])
     X[rng.random((n, nf)) < nan] = np.nan
     return X
+
+
+class _Panel:
+    def __init__(self, X, y, ts, entity):
+        self.X, self.y, self.ts, self.entity = X, y, ts, entity
+
+
+def interaction_panel(seed=5, n_dates=50, n_entities=100, nf=8):
+    """y = sign(x0 * x1) + noise: no single feature separates it, so PAIR splits trigger."""
+    rng = np.random.default_rng(seed)
+    n = n_dates * n_entities
+    X = rng.standard_normal((n, nf)).astype(np.float32)
+    X[rng.random((n, nf)) < 0.03] = np.nan
+    y = np.sign(np.nan_to_num(X[:, 0]) * np.nan_to_num(X[:, 1])) + 0.3 * rng.standard_normal(n)
+    ts = np.repeat(np.arange(n_dates), n_entities).astype(np.int64)
+    ent = np.tile(np.arange(n_entities), n_dates).astype(np.int64)
+    return _Panel(X, y, ts, ent)
 
 
 def main() -> None:
@@ -93,7 +114,8 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "pairwise.npz"), y=y, pred=pred, groups=groups, g=gp, h=hp, loss=loss)
     # fits
     for name, params, p in (("fit_mse", FIT_MSE, panels.panel_scale(n_dates=40, n_entities=300, n_features=12)),
-                            ("fit_pair", FIT_PAIR, panels.panel_pairwise(n_dates=30, n_features=10))):
+                            ("fit_pair", FIT_PAIR, panels.panel_pairwise(n_dates=30, n_features=10)),
+                            ("fit_pairsplit", FIT_PAIRSPLIT, interaction_panel())):
         Xp = p.X.astype(np.float64)
         res, hnd = bind.ref_fit(params, Xp, p.y, p.ts, p.entity)
         pr = bind.ref_predict(hnd, Xp[:500])
@@ -103,7 +125,7 @@ def main() -> None:
                 "n_buckets": res.n_buckets, "n_trees": len(res.trees)}
         for t, tr in enumerate(res.trees):
             for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
-                        "value", "gain", "values", "cover", "prefix"):
+                        "value", "gain", "values", "cover", "prefix", "split_type", "feature2"):
                 arrs[f"t{t}_{fld}"] = getattr(tr, fld)
         arrs["params"] = np.array(repr(params))
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrs)

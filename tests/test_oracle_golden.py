@@ -77,7 +77,7 @@ def test_pairwise_gradients_match_reference(oracle):
     assert L.orc_loss(5, d["y"], d["pred"], grp.ctypes.data_as(C.c_void_p), m) == float(d["loss"])
 
 
-@pytest.mark.parametrize("name", ["fit_mse", "fit_pair"])
+@pytest.mark.parametrize("name", ["fit_mse", "fit_pair", "fit_pairsplit"])
 def test_fit_matches_reference(oracle, name):
     d = load(f"{name}.npz")
     params = eval(str(d["params"]))  # the fixture's own dict literal
@@ -90,9 +90,50 @@ def test_fit_matches_reference(oracle, name):
         assert np.array_equal(res.evals_train, d["evals"])
         for t, tr in enumerate(res.trees):
             for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
-                        "value", "gain", "values", "cover", "prefix"):
+                        "value", "gain", "values", "cover", "prefix", "split_type", "feature2"):
                 assert np.array_equal(getattr(tr, fld), d[f"t{t}_{fld}"]), (t, fld)
         pr = oracle.oracle_predict(h, d["X"][:500].astype(np.float64))
         assert np.array_equal(pr, d["pred"])
     finally:
         oracle.oracle_free(h)
+
+
+def test_pair_fixture_has_pair_splits():
+    """The PAIR fixture exercises the pair search: its trees hold pair nodes."""
+    d = load("fit_pairsplit.npz")
+    assert sum(int((d[f"t{t}_split_type"] == 1).sum()) for t in range(int(d["n_trees"]))) > 0
+
+
+@pytest.mark.parametrize("extra", [dict(objective="mse"), dict(objective="mse", goss=1, goss_top=0.3, goss_other=0.2),
+                                   dict(objective="mse", iid_mode=1),
+                                   dict(objective="mse", pair_top_k=3, max_pair_splits_per_tree=5, pair_trigger=1.0,
+                                        pair_l2=0.5),
+                                   dict(objective="pairwise")])
+def test_pair_splits_match_reference(oracle, extra):
+    """PAIR splits (cpp/src/tree.cpp:214-281) in the oracle against the reference core built
+    from source, on an interaction target where the axis splits are weak."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    rng = np.random.default_rng(7)
+    n, nf = 8000, 9
+    X = rng.standard_normal((n, nf))
+    X[rng.random((n, nf)) < 0.05] = np.nan
+    y = np.sign(np.nan_to_num(X[:, 2]) * np.nan_to_num(X[:, 5])) + 0.5 * rng.standard_normal(n)
+    ts = np.repeat(np.arange(80), 100).astype(np.int64)
+    params = dict(n_estimators=4, learning_rate=0.1, max_depth=6, max_leaves=20, horizon=1, random_state=1,
+                  pair_splits=1, **extra)
+    ts_arg = None if params.get("iid_mode") else ts
+    r, hr = oracle.ref_fit(params, X, y, ts_arg)
+    o, ho = oracle.oracle_fit(params, X, y, ts_arg)
+    try:
+        assert len(r.trees) == len(o.trees)
+        assert sum(int((t.split_type == 1).sum()) for t in r.trees) > 0
+        for t, (a, b) in enumerate(zip(r.trees, o.trees)):
+            for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
+                        "value", "gain", "values", "cover", "prefix", "split_type", "feature2"):
+                assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        assert np.array_equal(r.evals_train, o.evals_train)
+        assert np.array_equal(oracle.ref_predict(hr, X[:400]), oracle.oracle_predict(ho, X[:400]))
+    finally:
+        oracle.ref_free(hr)
+        oracle.oracle_free(ho)
