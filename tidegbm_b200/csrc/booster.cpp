@@ -352,8 +352,6 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
         } else {
             // One running FP64 sum in row order: the same partial sums the reference
             // forms separately for every prefix [0, cut_b) and for [0, n).
-            std::vector<int> order_b(nbk);
-            std::iota(order_b.begin(), order_b.end(), 0);
             double sw = 0, sy = 0;
             int i = 0;
             std::vector<double> at_cut(nbk, 0.0);
