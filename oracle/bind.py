@@ -49,6 +49,7 @@ class _OrcConfig(C.Structure):
         ("bin_sample", C.c_int), ("torb_min_cover", C.c_double), ("finer_torb", C.c_int),
         ("pair_splits", C.c_int), ("pair_trigger", C.c_double), ("pair_top_k", C.c_int),
         ("max_pair_splits_per_tree", C.c_int), ("pair_l2", C.c_double),
+        ("cat_smooth", C.c_double), ("cat_min_count", C.c_int),
     ]
 
 
@@ -141,8 +142,9 @@ class TreeArrays:
     values: np.ndarray
     cover: np.ndarray
     prefix: np.ndarray
-    split_type: np.ndarray | None = None  # SplitType per node (0 axis, 1 pair), when exported
+    split_type: np.ndarray | None = None  # SplitType per node (0 axis, 1 pair, 2 categorical), when exported
     feature2: np.ndarray | None = None    # second feature of pair splits (-1 otherwise)
+    cat_left: np.ndarray | None = None    # [n_nodes, 4] uint64 left masks of categorical splits
 
     @classmethod
     def from_raw(cls, inodes: np.ndarray, fnodes: np.ndarray, values, cover, prefix,
@@ -182,15 +184,20 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def oracle_fit(params: dict, X, y, ts=None, entity=None) -> tuple[FitResult, int]:
-    """Runs the oracle restatement's Booster::fit; returns (result, handle)."""
+def oracle_fit(params: dict, X, y, ts=None, entity=None, is_cat=None) -> tuple[FitResult, int]:
+    """Runs the oracle restatement's Booster::fit; returns (result, handle).  is_cat marks
+    categorical features (one flag per column)."""
     L = oracle_lib()
     c = _cfg_struct(params)
     X = np.ascontiguousarray(X, dtype=np.float64)
     y = np.ascontiguousarray(y, dtype=np.float64)
     ts = None if ts is None else np.ascontiguousarray(ts, dtype=np.int64)
     ent = None if entity is None else np.ascontiguousarray(entity, dtype=np.int64)
-    h = L.orc_fit(C.byref(c), X, y, X.shape[0], X.shape[1], _ptr(ts), _ptr(ent))
+    cat = None if is_cat is None else np.ascontiguousarray(is_cat, dtype=np.int32)
+    L.orc_fit_cat.restype = C.c_void_p
+    L.orc_fit_cat.argtypes = [C.POINTER(_OrcConfig), _f64, _f64, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                              C.c_void_p]
+    h = L.orc_fit_cat(C.byref(c), X, y, X.shape[0], X.shape[1], _ptr(ts), _ptr(ent), _ptr(cat))
     if not h:
         raise ValueError(L.orc_last_error().decode())
     res = FitResult(n_bins=L.orc_n_bins(h), n_buckets=L.orc_n_buckets(h), init_score=L.orc_init_score(h))
@@ -209,7 +216,10 @@ def oracle_fit(params: dict, X, y, ts=None, entity=None) -> tuple[FitResult, int
         L.orc_tree_export(h, t, I, Fv, vals, cov, pre)
         S = np.zeros(2 * nn, np.int32)
         L.orc_tree_export_split(h, t, S.ctypes.data_as(C.c_void_p))
-        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre, S))
+        tr = TreeArrays.from_raw(I, Fv, vals, cov, pre, S)
+        tr.cat_left = np.zeros((nn, 4), np.uint64)
+        L.orc_tree_export_cat(h, t, tr.cat_left.ctypes.data_as(C.c_void_p))
+        res.trees.append(tr)
     return res, h
 
 
@@ -224,7 +234,7 @@ def oracle_free(handle) -> None:
     oracle_lib().orc_free(handle)
 
 
-def ref_fit(params: dict, X, y, ts=None, entity=None, n_jobs: int = 0):
+def ref_fit(params: dict, X, y, ts=None, entity=None, n_jobs: int = 0, is_cat=None):
     """Runs the reference core's Booster::fit (rank groups = timestamps, as
     src/tidegbm/native.py:134-137 passes them); returns (FitResult, handle)."""
     L = ref_lib()
@@ -242,7 +252,13 @@ def ref_fit(params: dict, X, y, ts=None, entity=None, n_jobs: int = 0):
     ent = None if entity is None else np.ascontiguousarray(entity, dtype=np.int64)
     obj = settings.get("objective", "mse")
     rg = ts if obj in ("pairwise", 5) else None
-    rc = L.ref_fit(h, X, y, X.shape[0], X.shape[1], _ptr(ts), _ptr(rg), _ptr(ent))
+    if is_cat is None:
+        rc = L.ref_fit(h, X, y, X.shape[0], X.shape[1], _ptr(ts), _ptr(rg), _ptr(ent))
+    else:
+        cat = np.ascontiguousarray(is_cat, dtype=np.int32)
+        L.ref_fit_cat.argtypes = [C.c_void_p, _f64, _f64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]
+        rc = L.ref_fit_cat(h, X, y, X.shape[0], X.shape[1], _ptr(ts), _ptr(rg), _ptr(ent), _ptr(cat))
     if rc != 0:
         err = L.ref_last_error().decode()
         L.ref_free(h)
@@ -263,7 +279,10 @@ def ref_fit(params: dict, X, y, ts=None, entity=None, n_jobs: int = 0):
         L.ref_tree_export(h, t, I, Fv, vals, cov, pre)
         S = np.zeros(2 * nn, np.int32)
         L.ref_tree_export_split(h, t, S.ctypes.data_as(C.c_void_p))
-        res.trees.append(TreeArrays.from_raw(I, Fv, vals, cov, pre, S))
+        tr = TreeArrays.from_raw(I, Fv, vals, cov, pre, S)
+        tr.cat_left = np.zeros((nn, 4), np.uint64)
+        L.ref_tree_export_cat(h, t, tr.cat_left.ctypes.data_as(C.c_void_p))
+        res.trees.append(tr)
     return res, h
 
 

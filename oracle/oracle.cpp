@@ -37,8 +37,9 @@ struct OrcNode {
     double gain = 0.0;
     int n_samples = 0;
     int depth = 0;
-    int split_type = 0;  // SplitType (cpp/include/tidegbm/types.hpp:25): 0 axis, 1 pair
+    int split_type = 0;  // SplitType (cpp/include/tidegbm/types.hpp:25): 0 axis, 1 pair, 2 categorical
     int feature2 = -1;   // second feature of a pair split
+    uint64_t cat_left[4] = {0, 0, 0, 0};  // categorical split: codes that go left (bit 0: missing)
 };
 
 struct OrcTree {
@@ -57,6 +58,8 @@ struct OrcModel {
     std::vector<double> init_prefix;
     std::vector<double> edges;  // n_f x 256
     std::vector<int> n_edges;
+    std::vector<int> is_cat;                     // per feature
+    std::vector<std::vector<double>> cat_values;  // vocabulary of each categorical feature
     std::vector<OrcTree> trees;
     std::vector<double> evals;
 };
@@ -83,6 +86,62 @@ std::vector<double> quantile_edges(std::vector<double>& vals, int n_bins) {
     return e;
 }
 
+// The numeric edges of feature f (cpp/src/binning.cpp:86-100): its non-NaN values, the
+// std::shuffle sample when there are more than bin_sample, quantile_edges.
+std::vector<double> numeric_edges(const double* X, int n, int n_f, int f, int max_bin, int bin_sample,
+                                  uint32_t seed) {
+    std::vector<double> vals;
+    vals.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        const double v = X[static_cast<size_t>(i) * n_f + f];
+        if (!is_nan(v)) vals.push_back(v);
+    }
+    if (bin_sample > 0 && static_cast<int>(vals.size()) > bin_sample) {
+        std::mt19937 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
+        std::shuffle(vals.begin(), vals.end(), rng);
+        vals.resize(static_cast<size_t>(bin_sample));
+    }
+    return quantile_edges(vals, max_bin - 1);
+}
+
+// The vocabulary of categorical feature f (cpp/src/binning.cpp:47-84): its distinct
+// non-NaN values seen at least cat_min_count times (else the most frequent one); the
+// max_bin - 1 most frequent when there are more; ascending.
+std::vector<double> cat_vocabulary(const double* X, int n, int n_f, int f, int max_bin, int cat_min_count) {
+    std::vector<double> raw;
+    raw.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        const double v = X[static_cast<size_t>(i) * n_f + f];
+        if (!is_nan(v)) raw.push_back(v);
+    }
+    std::sort(raw.begin(), raw.end());
+    std::vector<std::pair<int, double>> freq;
+    for (size_t i = 0; i < raw.size();) {
+        size_t j = i + 1;
+        while (j < raw.size() && raw[j] == raw[i]) ++j;
+        freq.emplace_back(static_cast<int>(j - i), raw[i]);
+        i = j;
+    }
+    const int min_c = std::max(1, cat_min_count);
+    std::vector<std::pair<int, double>> kept;
+    for (const auto& q : freq)
+        if (q.first >= min_c) kept.push_back(q);
+    if (kept.empty() && !freq.empty())
+        kept.push_back(*std::max_element(freq.begin(), freq.end(),
+                                         [](const auto& a, const auto& b) { return a.first < b.first; }));
+    const int numeric_bins = max_bin - 1;
+    if (static_cast<int>(kept.size()) > numeric_bins) {
+        std::partial_sort(kept.begin(), kept.begin() + numeric_bins, kept.end(),
+                          [](const auto& a, const auto& b) { return a.first > b.first; });
+        kept.resize(numeric_bins);
+    }
+    std::vector<double> uniq;
+    uniq.reserve(kept.size());
+    for (const auto& q : kept) uniq.push_back(q.second);
+    std::sort(uniq.begin(), uniq.end());
+    return uniq;
+}
+
 // cpp/include/tidegbm/tree.hpp:53-67 with l1 = 0 and max_delta_step = 0.
 inline double leaf_value(double G, double H, double l2) { return -G / (H + l2); }
 
@@ -99,6 +158,10 @@ inline int pair_bin(int b1, int b2, int n_bins) {
 // Direction of one row at a split node: cpp/src/tree.cpp:21-28 (pair: missing if either
 // code is missing, else the hashed bin against the threshold) and :36-39 (axis).
 inline bool goes_left(const OrcNode& d, const uint8_t* row, int n_bins) {
+    if (d.split_type == 2) {  // cat_goes_left, cpp/include/tidegbm/tree.hpp:27-30 (codes are < 256)
+        const int b = row[d.feature];
+        return (d.cat_left[b >> 6] >> (b & 63)) & 1ull;
+    }
     if (d.split_type == 1) {
         const int b1 = row[d.feature], b2 = row[d.feature2];
         if (b1 == 0 || b2 == 0) return d.missing_go_left != 0;
@@ -108,7 +171,7 @@ inline bool goes_left(const OrcNode& d, const uint8_t* row, int n_bins) {
     return (b == 0) ? d.missing_go_left != 0 : b <= d.threshold_bin;
 }
 
-// cpp/src/tree.cpp:15-41 for axis and pair splits on uint8 codes.
+// cpp/src/tree.cpp:15-41 for axis, pair and categorical splits on uint8 codes.
 int apply_one(const OrcTree& t, const uint8_t* row, int n_bins) {
     int nid = 0;
     for (;;) {
@@ -161,18 +224,112 @@ int auto_time_buckets(const int64_t* ts, int n, int64_t horizon, int uniq_cap) {
     return std::max(2, std::min(want, std::max(uniq_cap, 2)));
 }
 
-// A split candidate: orc_split plus the PAIR fields of SplitCand
+// Binner::fit (binning.cpp:34-102) into the model: edges of the numeric features, the
+// vocabularies of the categorical ones.  Returns max_bins() (binning.cpp:130-134).
+int model_binner_fit(OrcModel* M, const double* X, int n, int n_f, const orc_config& c) {
+    M->edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
+    M->n_edges.assign(n_f, 0);
+    M->cat_values.assign(n_f, {});
+    int mx = 2;
+    for (int f = 0; f < n_f; ++f) {
+        int nbc;
+        if (M->is_cat[f]) {
+            M->cat_values[f] = cat_vocabulary(X, n, n_f, f, c.max_bin, c.cat_min_count);
+            nbc = static_cast<int>(M->cat_values[f].size()) + 1;
+        } else {
+            const std::vector<double> e =
+                numeric_edges(X, n, n_f, f, c.max_bin, c.bin_sample, static_cast<uint32_t>(c.random_state));
+            M->n_edges[f] = static_cast<int>(e.size());
+            std::copy(e.begin(), e.end(), M->edges.begin() + static_cast<size_t>(f) * 256);
+            nbc = static_cast<int>(e.size()) + 2;
+        }
+        mx = std::max(mx, nbc);
+    }
+    return std::max(mx, c.max_bin);
+}
+
+// Binner::transform (binning.cpp:104-128): numeric code = 1 + upper_bound(edges, v);
+// categorical code = 1 + the value's vocabulary index, 0 when it is not in the vocabulary;
+// NaN -> 0.
+void model_transform(const OrcModel& M, const double* X, int n, uint8_t* codes) {
+    const int n_f = M.n_f;
+    for (int i = 0; i < n; ++i)
+        for (int f = 0; f < n_f; ++f) {
+            const double v = X[static_cast<size_t>(i) * n_f + f];
+            int b = 0;
+            if (!is_nan(v)) {
+                if (M.is_cat[f]) {
+                    const auto& voc = M.cat_values[f];
+                    auto it = std::lower_bound(voc.begin(), voc.end(), v);
+                    if (it != voc.end() && *it == v) b = static_cast<int>(it - voc.begin()) + 1;
+                } else {
+                    const double* e = M.edges.data() + static_cast<size_t>(f) * 256;
+                    b = static_cast<int>(std::upper_bound(e, e + M.n_edges[f], v) - e) + 1;
+                }
+            }
+            codes[static_cast<size_t>(i) * n_f + f] = static_cast<uint8_t>(b);
+        }
+}
+
+// A split candidate: orc_split plus the PAIR and categorical fields of SplitCand
 // (cpp/include/tidegbm/histogram.hpp:65-74).
 struct Cand {
     orc_split s{-1e300, -1, -1, 1};
     int type = 0;
     int feature2 = -1;
+    uint64_t cat_left[4] = {0, 0, 0, 0};
 };
+
+// best_categorical (cpp/src/histogram.cpp:195-244) with l1 = 0: the non-empty bins (the
+// missing bin 0 included) ordered by g / (h + cat_smooth) with std::sort, then the best
+// prefix of that order as the left side.  missing_go_left is the missing bin's side.
+Cand best_categorical(const double* ghc, int n_bins, int f, double lam, double gamma, int min_leaf,
+                      double min_hess, double cat_smooth) {
+    Cand best;
+    const double* B = ghc + static_cast<size_t>(f) * n_bins * 3;
+    std::vector<int> order;
+    order.reserve(n_bins);
+    double totG = 0, totH = 0;
+    int64_t totC = 0;
+    for (int b = 0; b < n_bins; ++b) {
+        totG += B[3 * b];
+        totH += B[3 * b + 1];
+        totC += static_cast<int64_t>(B[3 * b + 2]);
+        if (static_cast<int64_t>(B[3 * b + 2]) > 0) order.push_back(b);
+    }
+    if (order.size() < 2) return best;
+    const double sm = std::max(cat_smooth, 0.0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        return B[3 * a] / (B[3 * a + 1] + sm) < B[3 * b] / (B[3 * b + 1] + sm);
+    });
+    const double parent = leaf_score(totG, totH, lam);
+    double GL = 0, HL = 0;
+    int64_t CL = 0;
+    uint64_t mask[4] = {0, 0, 0, 0};
+    for (size_t i = 0; i + 1 < order.size(); ++i) {
+        const int b = order[i];
+        GL += B[3 * b];
+        HL += B[3 * b + 1];
+        CL += static_cast<int64_t>(B[3 * b + 2]);
+        mask[b >> 6] |= (uint64_t(1) << (b & 63));
+        const double GR = totG - GL, HR = totH - HL;
+        const int64_t CR = totC - CL;
+        if (CL < min_leaf || CR < min_leaf) continue;
+        if (HL < min_hess || HR < min_hess) continue;
+        const double gain = 0.5 * (leaf_score(GL, HL, lam) + leaf_score(GR, HR, lam) - parent) - gamma;
+        if (gain > best.s.gain) {
+            best.s = orc_split{gain, f, -1, (mask[0] & 1ull) ? 1 : 0};
+            best.type = 2;
+            for (int k = 0; k < 4; ++k) best.cat_left[k] = mask[k];
+        }
+    }
+    return best;
+}
 
 // cpp/src/tree.cpp:283-472, axis and PAIR splits (no colsample, groups, HALO, regime,
 // interaction constraints, monotone, forced pairs).  Rows are sorted ascending first.
 OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const double* h,
-                  std::vector<int32_t> sample, int n_f, int n_bins, const orc_config& c) {
+                  std::vector<int32_t> sample, int n_f, int n_bins, const orc_config& c, const std::vector<int>& is_cat) {
     OrcTree tree;
     std::sort(sample.begin(), sample.end());
     const int nb_stride = n_bins;
@@ -194,15 +351,24 @@ OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const doubl
     std::vector<char> ok(1, 0);
 
     auto best_for_leaf = [&](int lid, int pair_budget) {
-        // cpp/src/tree.cpp:106-166: the best axis split over the features in ascending order
+        // cpp/src/tree.cpp:106-166: the best axis or categorical split over the features in
+        // ascending order
+        std::vector<Cand> per_c(n_f);
         std::vector<orc_split> per_f(n_f);
-        for (int f = 0; f < n_f; ++f)
-            per_f[f] = orc_best_numeric(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
-                                        c.min_samples_leaf, c.min_child_weight);
+        for (int f = 0; f < n_f; ++f) {
+            if (is_cat[f]) {
+                per_c[f] = best_categorical(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
+                                            c.min_samples_leaf, c.min_child_weight, c.cat_smooth);
+            } else {
+                per_c[f].s = orc_best_numeric(leaf_hist[lid].data(), n_bins, f, c.l2, c.min_split_gain,
+                                              c.min_samples_leaf, c.min_child_weight);
+            }
+            per_f[f] = per_c[f].s;
+        }
         Cand best;
         for (int f = 0; f < n_f; ++f) {
             if (per_f[f].feature < 0 || per_f[f].gain < c.min_split_gain) continue;
-            if (per_f[f].gain > best.s.gain) best.s = per_f[f];
+            if (per_f[f].gain > best.s.gain) best = per_c[f];
         }
         // cpp/src/tree.cpp:214-281: PAIR when the best axis gain is weak against the leaf's
         // gradient energy (sum of g^2 in row order, tree.cpp:355-356)
@@ -266,6 +432,7 @@ OrcTree grow_tree(const uint8_t* codes, int stride, const double* g, const doubl
         p.feature = best.feature;
         p.feature2 = bestc.feature2;
         p.split_type = bestc.type;
+        for (int k = 0; k < 4; ++k) p.cat_left[k] = bestc.cat_left[k];
         p.threshold_bin = best.threshold_bin;
         p.missing_go_left = best.missing_go_left;
         p.gain = best.gain;
@@ -342,18 +509,7 @@ int orc_binner_fit(const double* X, int n, int n_f, int max_bin, int bin_sample,
     // cpp/src/binning.cpp:34-102, numeric features, mask all ones.
     int mx = 2;
     for (int f = 0; f < n_f; ++f) {
-        std::vector<double> vals;
-        vals.reserve(n);
-        for (int i = 0; i < n; ++i) {
-            const double v = X[static_cast<size_t>(i) * n_f + f];
-            if (!is_nan(v)) vals.push_back(v);
-        }
-        if (bin_sample > 0 && static_cast<int>(vals.size()) > bin_sample) {
-            std::mt19937 rng(seed + static_cast<uint32_t>(f) * 2654435761u);
-            std::shuffle(vals.begin(), vals.end(), rng);
-            vals.resize(static_cast<size_t>(bin_sample));
-        }
-        std::vector<double> e = quantile_edges(vals, max_bin - 1);
+        const std::vector<double> e = numeric_edges(X, n, n_f, f, max_bin, bin_sample, seed);
         n_edges[f] = static_cast<int>(e.size());
         std::memcpy(edges + static_cast<size_t>(f) * 256, e.data(), e.size() * sizeof(double));
         n_bins_col[f] = static_cast<int>(e.size()) + 2;
@@ -563,10 +719,17 @@ void orc_config_default(orc_config* c) {
     c->pair_top_k = 6;
     c->max_pair_splits_per_tree = 3;
     c->pair_l2 = 2.0;
+    c->cat_smooth = 1.0;
+    c->cat_min_count = 5;
 }
 
 void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, int n, int n_f,
               const int64_t* ts_in, const int64_t* ent_in) {
+    return orc_fit_cat(cfgp, X_in, y_in, n, n_f, ts_in, ent_in, nullptr);
+}
+
+void* orc_fit_cat(const orc_config* cfgp, const double* X_in, const double* y_in, int n, int n_f,
+                  const int64_t* ts_in, const int64_t* ent_in, const int* is_cat) {
     // cpp/src/booster.cpp:231-742 for the supported subset.
     try {
         orc_config c = *cfgp;
@@ -576,6 +739,8 @@ void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, in
         auto* M = new OrcModel();
         M->cfg = c;
         M->n_f = n_f;
+        if (is_cat) M->is_cat.assign(is_cat, is_cat + n_f);  // booster.cpp:246-247
+        else M->is_cat.assign(n_f, 0);
         std::vector<double> X(X_in, X_in + static_cast<size_t>(n) * n_f), y(y_in, y_in + n);
         std::vector<int64_t> ts;
         if (ts_in) ts.assign(ts_in, ts_in + n);
@@ -635,14 +800,9 @@ void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, in
             }
         }
         // booster.cpp:378-383 binning
-        M->edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
-        M->n_edges.assign(n_f, 0);
-        std::vector<int> nbc(n_f);
-        M->n_bins = orc_binner_fit(X.data(), n, n_f, c.max_bin, c.bin_sample,
-                                   static_cast<uint32_t>(c.random_state), M->edges.data(),
-                                   M->n_edges.data(), nbc.data());
+        M->n_bins = model_binner_fit(M, X.data(), n, n_f, c);
         std::vector<uint8_t> codes(static_cast<size_t>(n) * n_f);
-        orc_bin_transform(X.data(), n, n_f, M->edges.data(), M->n_edges.data(), codes.data(), n_f);
+        model_transform(*M, X.data(), n, codes.data());
         // booster.cpp:399-457 initial predictions (Objective::init_score,
         // objective.cpp:80-100: mean for MSE, 0 for ranking).
         auto init_of = [&](int m) -> double {
@@ -705,7 +865,7 @@ void* orc_fit(const orc_config* cfgp, const double* X_in, const double* y_in, in
                 gu = gg.data();
                 hu = hg.data();
             }
-            OrcTree tree = grow_tree(codes.data(), n_f, gu, hu, sample, n_f, M->n_bins, c);
+            OrcTree tree = grow_tree(codes.data(), n_f, gu, hu, sample, n_f, M->n_bins, c, M->is_cat);
             (void)rng();  // booster.cpp:588 seeds grow_tree's own generator
             // booster.cpp:589-600 full-data leaf values from unscaled g, h
             std::vector<int> nid(n);
@@ -797,6 +957,12 @@ void orc_tree_export(void* m, int t, int* inodes, double* fnodes, double* values
     std::memcpy(prefix, tr.prefix.data(), tr.prefix.size() * sizeof(double));
 }
 
+void orc_tree_export_cat(void* m, int t, uint64_t* out) {
+    const OrcTree& tr = static_cast<OrcModel*>(m)->trees[t];
+    for (size_t k = 0; k < tr.nodes.size(); ++k)
+        for (int j = 0; j < 4; ++j) out[4 * k + j] = tr.nodes[k].cat_left[j];
+}
+
 void orc_tree_export_split(void* m, int t, int* out) {
     const OrcTree& tr = static_cast<OrcModel*>(m)->trees[t];
     for (size_t k = 0; k < tr.nodes.size(); ++k) {
@@ -809,7 +975,7 @@ void orc_predict_raw(void* mp, const double* X, int n, double* out) {
     // booster.cpp:744-773 with tree_decay = 1 and best_iteration = n_estimators.
     const OrcModel& M = *static_cast<OrcModel*>(mp);
     std::vector<uint8_t> codes(static_cast<size_t>(n) * M.n_f);
-    orc_bin_transform(X, n, M.n_f, M.edges.data(), M.n_edges.data(), codes.data(), M.n_f);
+    model_transform(M, X, n, codes.data());
     for (int i = 0; i < n; ++i) {
         double s = M.init_score;
         for (const OrcTree& t : M.trees)

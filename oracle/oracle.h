@@ -95,6 +95,9 @@ typedef struct {
     int pair_top_k;
     int max_pair_splits_per_tree;
     double pair_l2;
+    /* categorical features (config.hpp:70-72) */
+    double cat_smooth;
+    int cat_min_count;
 } orc_config;
 
 void orc_config_default(orc_config* c);
@@ -104,6 +107,9 @@ void orc_config_default(orc_config* c);
  * may be NULL.  Returns a handle or NULL (orc_last_error()). */
 void* orc_fit(const orc_config* cfg, const double* X, const double* y, int n, int n_f,
               const int64_t* ts, const int64_t* entity);
+/* The same with categorical features: is_cat[f] != 0 marks feature f (NULL: none). */
+void* orc_fit_cat(const orc_config* cfg, const double* X, const double* y, int n, int n_f,
+                  const int64_t* ts, const int64_t* entity, const int* is_cat);
 void orc_free(void* model);
 const char* orc_last_error(void);
 
@@ -118,7 +124,9 @@ int orc_tree_n_nodes(void* model, int t);
  * left, right, missing_go_left, n_samples, depth}; fnodes[2*k] = {value, gain}. */
 void orc_tree_export(void* model, int t, int* inodes, double* fnodes, double* values, int* cover,
                      double* prefix);
-/* Per node {split_type (0 axis, 1 pair; types.hpp:25), feature2} into out[2*k]. */
+/* Per node the 256-bit left mask of a categorical split (Node::cat_left) into out[4*k]. */
+void orc_tree_export_cat(void* model, int t, uint64_t* out);
+/* Per node {split_type (0 axis, 1 pair, 2 categorical; types.hpp:25), feature2} into out[2*k]. */
 void orc_tree_export_split(void* model, int t, int* out);
 /* Booster::predict_raw (booster.cpp:744-811) on f64 X. */
 void orc_predict_raw(void* model, const double* X, int n, double* out);

@@ -67,6 +67,8 @@ int ref_set(void* hb, const char* key, double v) {
     else if (k == "pair_top_k") c.pair_top_k = static_cast<int>(v);
     else if (k == "max_pair_splits_per_tree") c.max_pair_splits_per_tree = static_cast<int>(v);
     else if (k == "pair_l2") c.pair_l2 = v;
+    else if (k == "cat_smooth") c.cat_smooth = v;
+    else if (k == "cat_min_count") c.cat_min_count = static_cast<int>(v);
     else if (k == "objective") c.objective = objective_from_code(static_cast<int>(v));
     else if (k == "n_jobs") c.n_jobs = static_cast<int>(v);
     else if (k == "random_state") c.random_state = static_cast<int>(v);
@@ -92,6 +94,20 @@ int ref_fit(void* hb, const double* X, const double* y, int n, int n_f, const lo
                                        nullptr, nullptr, nullptr,
                                        reinterpret_cast<const i64*>(rank_groups), nullptr, nullptr,
                                        nullptr, 0, reinterpret_cast<const i64*>(entity), nullptr);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// The same with categorical features: is_cat[f] != 0 marks feature f.
+int ref_fit_cat(void* hb, const double* X, const double* y, int n, int n_f, const long long* ts,
+                const long long* rank_groups, const long long* entity, const int* is_cat) {
+    try {
+        static_cast<Booster*>(hb)->fit(X, y, n, n_f, reinterpret_cast<const i64*>(ts), nullptr, is_cat,
+                                       nullptr, nullptr, reinterpret_cast<const i64*>(rank_groups), nullptr,
+                                       nullptr, nullptr, 0, reinterpret_cast<const i64*>(entity), nullptr);
         return 0;
     } catch (const std::exception& e) {
         g_err = e.what();
@@ -172,6 +188,13 @@ void ref_tree_export(void* hb, int t, int* inodes, double* fnodes, double* value
         cover[k] = tr.cover[k];
     }
     std::memcpy(prefix, tr.prefix_values.data(), tr.prefix_values.size() * sizeof(double));
+}
+
+// Per node the 256-bit left mask of a categorical split (Node::cat_left) into out[4*k].
+void ref_tree_export_cat(void* hb, int t, unsigned long long* out) {
+    const Tree& tr = static_cast<Booster*>(hb)->trees[t];
+    for (size_t k = 0; k < tr.nodes.size(); ++k)
+        for (int j = 0; j < 4; ++j) out[4 * k + j] = tr.nodes[k].cat_left[j];
 }
 
 // Per node {split_type (SplitType, types.hpp:25), feature2} into out[2*k].

@@ -13,6 +13,8 @@ Each fixture is the reference's output on a small seeded input:
   fit_pair.npz  the same for the pairwise objective
   fit_pairsplit.npz  mse with PAIR splits on (cpp/src/tree.cpp:214-281) over an interaction
                 target, where the axis splits are weak; trees carry split_type and feature2
+  fit_cat.npz   mse with categorical features (vocabulary binning, binning.cpp:47-84;
+                best_categorical, histogram.cpp:195-244): trees carry the left masks
 The tests check the oracle restatement (CPU) and the CUDA path (GPU) against them.
 """
 from __future__ import annotations
@@ -62,6 +64,29 @@ def interaction_panel(seed=5, n_dates=50, n_entities=100, nf=8):
     ts = np.repeat(np.arange(n_dates), n_entities).astype(np.int64)
     ent = np.tile(np.arange(n_entities), n_dates).astype(np.int64)
     return _Panel(X, y, ts, ent)
+
+
+def categorical_panel(seed=3, n_dates=60, n_entities=100, nf=6):
+    """Categorical columns 0 (12 values), 3 (400 values: the most frequent 254 are kept) and 5
+    (6 common values and rare ones below cat_min_count), with NaNs."""
+    rng = np.random.default_rng(seed)
+    n = n_dates * n_entities
+    X = rng.standard_normal((n, nf))
+    X[:, 0] = rng.integers(0, 12, n)
+    X[:, 3] = rng.integers(0, 400, n)
+    X[:, 5] = np.where(rng.random(n) < 0.02, rng.integers(100, 130, n), rng.integers(0, 6, n))
+    X[rng.random((n, nf)) < 0.03] = np.nan
+    eff = np.array([0.9, -0.4, 0.1, 1.2, -1.0, 0.0, 0.5, 0.3, -0.7, 0.2, 0.0, -0.2])
+    y = eff[np.nan_to_num(X[:, 0], nan=0).astype(int) % 12] + 0.3 * np.nan_to_num(X[:, 1]) + 0.5 * rng.standard_normal(n)
+    ts = np.repeat(np.arange(n_dates), n_entities).astype(np.int64)
+    ent = np.tile(np.arange(n_entities), n_dates).astype(np.int64)
+    p = _Panel(X, y, ts, ent)
+    p.is_cat = np.array([1, 0, 0, 1, 0, 1], np.int32)
+    return p
+
+
+FIT_CAT = dict(n_estimators=5, learning_rate=0.1, max_depth=6, max_leaves=20, horizon=1, objective="mse",
+               random_state=2)
 
 
 def main() -> None:
@@ -115,9 +140,11 @@ def main() -> None:
     # fits
     for name, params, p in (("fit_mse", FIT_MSE, panels.panel_scale(n_dates=40, n_entities=300, n_features=12)),
                             ("fit_pair", FIT_PAIR, panels.panel_pairwise(n_dates=30, n_features=10)),
-                            ("fit_pairsplit", FIT_PAIRSPLIT, interaction_panel())):
+                            ("fit_pairsplit", FIT_PAIRSPLIT, interaction_panel()),
+                            ("fit_cat", FIT_CAT, categorical_panel())):
         Xp = p.X.astype(np.float64)
-        res, hnd = bind.ref_fit(params, Xp, p.y, p.ts, p.entity)
+        is_cat = getattr(p, "is_cat", None)
+        res, hnd = bind.ref_fit(params, Xp, p.y, p.ts, p.entity, is_cat=is_cat)
         pr = bind.ref_predict(hnd, Xp[:500])
         bind.ref_free(hnd)
         arrs = {"X": p.X, "y": p.y, "ts": p.ts, "entity": p.entity, "pred": pr, "init_score": res.init_score,
@@ -127,6 +154,10 @@ def main() -> None:
             for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
                         "value", "gain", "values", "cover", "prefix", "split_type", "feature2"):
                 arrs[f"t{t}_{fld}"] = getattr(tr, fld)
+            if is_cat is not None:
+                arrs[f"t{t}_cat_left"] = tr.cat_left
+        if is_cat is not None:
+            arrs["is_cat"] = is_cat
         arrs["params"] = np.array(repr(params))
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrs)
     print("fixtures written to", HERE)

@@ -77,11 +77,12 @@ def test_pairwise_gradients_match_reference(oracle):
     assert L.orc_loss(5, d["y"], d["pred"], grp.ctypes.data_as(C.c_void_p), m) == float(d["loss"])
 
 
-@pytest.mark.parametrize("name", ["fit_mse", "fit_pair", "fit_pairsplit"])
+@pytest.mark.parametrize("name", ["fit_mse", "fit_pair", "fit_pairsplit", "fit_cat"])
 def test_fit_matches_reference(oracle, name):
     d = load(f"{name}.npz")
     params = eval(str(d["params"]))  # the fixture's own dict literal
-    res, h = oracle.oracle_fit(params, d["X"].astype(np.float64), d["y"], d["ts"], d["entity"])
+    is_cat = d["is_cat"] if "is_cat" in d.files else None
+    res, h = oracle.oracle_fit(params, d["X"].astype(np.float64), d["y"], d["ts"], d["entity"], is_cat=is_cat)
     try:
         assert len(res.trees) == int(d["n_trees"])
         assert res.n_bins == int(d["n_bins"]) and res.n_buckets == int(d["n_buckets"])
@@ -92,6 +93,8 @@ def test_fit_matches_reference(oracle, name):
             for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
                         "value", "gain", "values", "cover", "prefix", "split_type", "feature2"):
                 assert np.array_equal(getattr(tr, fld), d[f"t{t}_{fld}"]), (t, fld)
+            if is_cat is not None:
+                assert np.array_equal(tr.cat_left, d[f"t{t}_cat_left"]), (t, "cat_left")
         pr = oracle.oracle_predict(h, d["X"][:500].astype(np.float64))
         assert np.array_equal(pr, d["pred"])
     finally:
@@ -134,6 +137,61 @@ def test_pair_splits_match_reference(oracle, extra):
                 assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
         assert np.array_equal(r.evals_train, o.evals_train)
         assert np.array_equal(oracle.ref_predict(hr, X[:400]), oracle.oracle_predict(ho, X[:400]))
+    finally:
+        oracle.ref_free(hr)
+        oracle.oracle_free(ho)
+
+
+def test_cat_fixture_has_categorical_splits():
+    d = load("fit_cat.npz")
+    assert sum(int((d[f"t{t}_split_type"] == 2).sum()) for t in range(int(d["n_trees"]))) > 0
+
+
+def _cat_panel(seed, interaction):
+    rng = np.random.default_rng(seed)
+    n, nf = 9000, 7
+    X = rng.standard_normal((n, nf))
+    X[:, 0] = rng.integers(0, 12, n)
+    X[:, 3] = rng.integers(0, 400, n)
+    X[:, 5] = np.where(rng.random(n) < 0.02, rng.integers(100, 130, n), rng.integers(0, 6, n))
+    X[rng.random((n, nf)) < 0.03] = np.nan
+    if interaction:  # weak single features: PAIR candidates compete with categorical gains
+        y = np.sign(np.nan_to_num(X[:, 1]) * np.nan_to_num(X[:, 2])) + 0.4 * rng.standard_normal(n)
+    else:
+        eff = np.array([0.9, -0.4, 0.1, 1.2, -1.0, 0.0, 0.5, 0.3, -0.7, 0.2, 0.0, -0.2])
+        y = eff[np.nan_to_num(X[:, 0], nan=0).astype(int) % 12] + 0.3 * np.nan_to_num(X[:, 1]) + \
+            0.5 * rng.standard_normal(n)
+    ts = np.repeat(np.arange(90), 100).astype(np.int64)
+    return X, y, ts, np.array([1, 0, 0, 1, 0, 1, 0], np.int32)
+
+
+@pytest.mark.parametrize("extra,interaction", [(dict(objective="mse"), False),
+                                               (dict(objective="mse", cat_min_count=50, cat_smooth=5.0), False),
+                                               (dict(objective="mse", goss=1, goss_top=0.3, goss_other=0.2), False),
+                                               (dict(objective="pairwise"), False),
+                                               (dict(objective="mse", iid_mode=1), False),
+                                               (dict(objective="mse", pair_splits=1), True)])
+def test_categorical_splits_match_reference(oracle, extra, interaction):
+    """Categorical features in the oracle (vocabulary binning, binning.cpp:47-84;
+    best_categorical, histogram.cpp:195-244; cat_goes_left, tree.hpp:27-30) against the
+    reference core built from source: trees with their left masks, losses, predictions."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    X, y, ts, is_cat = _cat_panel(3, interaction)
+    params = dict(n_estimators=4, learning_rate=0.1, max_depth=6, max_leaves=20, horizon=1, random_state=2, **extra)
+    ts_arg = None if params.get("iid_mode") else ts
+    r, hr = oracle.ref_fit(params, X, y, ts_arg, is_cat=is_cat)
+    o, ho = oracle.oracle_fit(params, X, y, ts_arg, is_cat=is_cat)
+    try:
+        assert len(r.trees) == len(o.trees) and r.n_bins == o.n_bins
+        kinds = {int(k) for t in r.trees for k in t.split_type[t.is_leaf == 0]}
+        assert 2 in kinds and (not interaction or 1 in kinds), kinds
+        for t, (a, b) in enumerate(zip(r.trees, o.trees)):
+            for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
+                        "value", "gain", "values", "cover", "prefix", "split_type", "feature2", "cat_left"):
+                assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        assert np.array_equal(r.evals_train, o.evals_train)
+        assert np.array_equal(oracle.ref_predict(hr, X[:500]), oracle.oracle_predict(ho, X[:500]))
     finally:
         oracle.ref_free(hr)
         oracle.oracle_free(ho)
