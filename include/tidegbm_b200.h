@@ -129,6 +129,35 @@ TGB_API int tgb_shuffle_sequence(long long m, long long keep, unsigned seed, int
  * two-draws path) are drawn on the host and copied.  1 <= keep <= m < 2^31. */
 TGB_API int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* out, void* stream);
 
+/* ---- Serving loop ----
+ * Fit and predict requests on one device under a device-memory budget.  Requests start
+ * in arrival order, each as soon as a slot is free, its working set
+ * (tgb_working_set_bytes) fits beside the running ones, and no other request on the same
+ * booster runs.  Each runs on its booster's own stream, so concurrent requests overlap on
+ * the device.  The caller keeps the booster and every host buffer of a request untouched
+ * until the request has finished.  Latency counts from submission to completion. */
+typedef struct tgb_server tgb_server;
+TGB_API int tgb_server_create(int device, double budget_bytes, int slots, tgb_server** out);
+/* Waits for every queued and running request, then frees the server (not the boosters). */
+TGB_API void tgb_server_free(tgb_server* s);
+/* Estimated device working set of a fit (kind 0) or predict (kind 1) request of n rows
+ * with this booster's configuration, the admission figure; -1 on bad arguments. */
+TGB_API long long tgb_working_set_bytes(tgb_booster* b, int kind, int n, int n_features, int x_dtype);
+/* Queues tgb_fit(b, ...) / tgb_predict_raw(b, ...); *id_out receives the request id.
+ * Fails at submission when the working set exceeds the whole budget. */
+TGB_API int tgb_server_submit_fit(tgb_server* s, tgb_booster* b, const void* X, int x_dtype, const double* y, int n,
+                                  int n_features, const long long* timestamps, const long long* entity,
+                                  long long* id_out);
+TGB_API int tgb_server_submit_predict(tgb_server* s, tgb_booster* b, const void* X, int x_dtype, int n,
+                                      int n_features, double* out, long long* id_out);
+/* Waits up to timeout_ms (< 0: no limit) for request id; *state: 0 queued, 1 running,
+ * 2 done, 3 failed (the request's message is then in tgb_last_error).  -1 on a bad id. */
+TGB_API int tgb_server_wait(tgb_server* s, long long id, double timeout_ms, int* state);
+/* out[12]: completed, failed, latency p50, p99 (s), fit p50, p99, predict p50, p99, mean
+ * wait for admission (s), peak requests running, peak admitted bytes, seconds from the
+ * first submission to the last completion. */
+TGB_API int tgb_server_stats(tgb_server* s, double* out);
+
 /* ---- Kernel level: one reference function each, on device memory ---- */
 
 /* Binner::transform (cpp/src/binning.cpp:104-128): codes[i*stride + f] = 1 + #{edges <= x},

@@ -14,6 +14,7 @@
 
 #include "booster.h"
 #include "sampling.h"
+#include "serving.h"
 #include "tgb_internal.h"
 
 namespace tgb {
@@ -43,9 +44,34 @@ struct tgb_booster {
     }
 };
 
+struct tgb_server {
+    tgb::Scheduler* sched = nullptr;
+    int device = 0;
+    ~tgb_server() { delete sched; }  // waits for every queued and running request
+};
+
 namespace {
 
 thread_local std::string g_err;
+
+// Device working set of a fit or predict request, the serving loop's admission figure:
+// the buffers of one fit context (X during binning, row-major and column-major codes,
+// per-row f64 state, row lists, GOSS keys, the node histograms) or of one prediction
+// (X, codes, output), plus a fixed allowance for scratch and the CUDA context's share.
+size_t working_set_bytes(const tgb::Config& c, int kind, long long n, long long n_f, int x_dtype) {
+    const long long xsz = x_dtype == 0 ? 4 : 8;
+    const long long stride = (n_f + 15) / 16 * 16;
+    const long long pitch = (n + 15) / 16 * 16;
+    const long long slack = 64ll << 20;
+    if (kind == 1) return static_cast<size_t>(n * n_f * xsz + n * stride + 8 * n + slack);
+    const long long per_row = 8 * 3              // y, pred, g
+                              + (c.objective == 0 ? 8 : 16)  // gq, or h and its scratch
+                              + 8 + 2            // row lists, leaf ids
+                              + 26;              // GOSS keys, values and flags
+    const long long nodes = 2ll * c.max_leaves - 1;
+    const long long hist = n_f * 256 * 20 * nodes;
+    return static_cast<size_t>(n * n_f * xsz + n * stride + n_f * pitch + per_row * n + hist + slack);
+}
 
 template <class F>
 int guard(F&& f) {
@@ -558,6 +584,91 @@ int tgb_build_hist_gpu(tgb_booster* hb, const unsigned short* xb, int n_f, const
                 out[3 * o + 1] = static_cast<double>(H[q]) * ih;
                 out[3 * o + 2] = static_cast<double>(C[q]);
             }
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int tgb_server_create(int device, double budget_bytes, int slots, tgb_server** out) {
+    return guard([&] {
+        need(out != nullptr, "out is NULL");
+        need(budget_bytes >= 1.0 && slots >= 1, "budget and slots must be positive");
+        auto* h = new tgb_server();
+        h->device = device;
+        h->sched = new tgb::Scheduler(static_cast<size_t>(budget_bytes), slots);
+        *out = h;
+    });
+}
+
+void tgb_server_free(tgb_server* s) { delete s; }
+
+long long tgb_working_set_bytes(tgb_booster* b, int kind, int n, int n_features, int x_dtype) {
+    if (!b || n < 0 || n_features < 1 || (kind != 0 && kind != 1)) return -1;
+    return static_cast<long long>(working_set_bytes(b->b->cfg, kind, n, n_features, x_dtype));
+}
+
+int tgb_server_submit_fit(tgb_server* s, tgb_booster* hb, const void* X, int x_dtype, const double* y, int n,
+                          int n_features, const long long* timestamps, const long long* entity, long long* id_out) {
+    return guard([&] {
+        need(s && hb && X && y && id_out, "NULL argument");
+        const size_t bytes = working_set_bytes(hb->b->cfg, 0, n, n_features, x_dtype);
+        tgb::GpuBooster* b = hb->b;
+        const int device = s->device;
+        *id_out = s->sched->submit(
+            tgb::Scheduler::kFit, bytes,
+            [=] {
+                tgb::check(cudaSetDevice(device), "cudaSetDevice");
+                b->fit(X, x_dtype, y, n, n_features, reinterpret_cast<const int64_t*>(timestamps),
+                       reinterpret_cast<const int64_t*>(entity));
+            },
+            reinterpret_cast<uintptr_t>(b));
+    });
+}
+
+int tgb_server_submit_predict(tgb_server* s, tgb_booster* hb, const void* X, int x_dtype, int n, int n_features,
+                              double* out, long long* id_out) {
+    return guard([&] {
+        need(s && hb && X && out && id_out, "NULL argument");
+        const size_t bytes = working_set_bytes(hb->b->cfg, 1, n, n_features, x_dtype);
+        tgb::GpuBooster* b = hb->b;
+        const int device = s->device;
+        *id_out = s->sched->submit(
+            tgb::Scheduler::kPredict, bytes,
+            [=] {
+                tgb::check(cudaSetDevice(device), "cudaSetDevice");
+                b->predict_raw(X, x_dtype, n, n_features, out);
+            },
+            reinterpret_cast<uintptr_t>(b));
+    });
+}
+
+int tgb_server_wait(tgb_server* s, long long id, double timeout_ms, int* state) {
+    return guard([&] {
+        need(s && state, "NULL argument");
+        std::string err;
+        *state = s->sched->wait(id, timeout_ms < 0 ? -1.0 : timeout_ms / 1000.0, &err);
+        if (*state == tgb::Scheduler::kFailed) g_err = err;
+    });
+}
+
+int tgb_server_stats(tgb_server* s, double* o) {
+    return guard([&] {
+        need(s && o, "NULL argument");
+        const tgb::Scheduler::Stats st = s->sched->stats();
+        o[0] = static_cast<double>(st.completed);
+        o[1] = static_cast<double>(st.failed);
+        o[2] = st.p50_s;
+        o[3] = st.p99_s;
+        o[4] = st.p50_fit_s;
+        o[5] = st.p99_fit_s;
+        o[6] = st.p50_predict_s;
+        o[7] = st.p99_predict_s;
+        o[8] = st.mean_wait_s;
+        o[9] = static_cast<double>(st.peak_running);
+        o[10] = static_cast<double>(st.peak_bytes);
+        o[11] = st.busy_s;
     });
 }
 

@@ -63,6 +63,13 @@ def lib() -> C.CDLL:
         "tgb_shuffled_prefix": ([ll, ll, C.c_uint, vp], i),
         "tgb_shuffled_prefix_device": ([ll, ll, C.c_uint, vp, vp], i),
         "tgb_shuffle_sequence": ([ll, ll, C.c_uint, i, vp], i),
+        "tgb_server_create": ([i, d, i, C.POINTER(vp)], i),
+        "tgb_server_free": ([vp], None),
+        "tgb_working_set_bytes": ([vp, i, i, i, i], ll),
+        "tgb_server_submit_fit": ([vp, vp, vp, i, vp, i, i, vp, vp, C.POINTER(ll)], i),
+        "tgb_server_submit_predict": ([vp, vp, vp, i, i, i, vp, C.POINTER(ll)], i),
+        "tgb_server_wait": ([vp, ll, d, C.POINTER(i)], i),
+        "tgb_server_stats": ([vp, vp], i),
         "tgb_bin_transform": ([vp, i, i, i, vp, vp, vp, i, vp], i),
         "tgb_hist_build": ([vp, i, i, vp, i, vp, vp, i, i, vp, vp, vp, vp], i),
         "tgb_split_scan": ([vp, vp, vp, i, i, i, i, d, d, i, d, vp, vp, vp, vp], i),
@@ -250,6 +257,72 @@ class Booster:
         check(lib().tgb_build_hist_gpu(self._h, _ptr(xb), nf, _ptr(idx), idx.size, _ptr(g), _ptr(h), n_bins,
                                        xb.shape[0], _ptr(out)))
         return out.reshape(nf, n_bins, 3)
+
+
+class Server:
+    """The serving loop (tgb_server_*): fit and predict requests on one device, admitted in
+    arrival order by device-memory budget and free slots, running concurrently on their
+    boosters' own streams.  Each request keeps references to its arrays until it is waited
+    for, so the host buffers stay alive while the device uses them."""
+
+    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, device: int = 0, budget_bytes: float = 150e9, slots: int = 4) -> None:
+        h = C.c_void_p()
+        check(lib().tgb_server_create(int(device), float(budget_bytes), int(slots), C.byref(h)))
+        self._h = h
+        self._keep: dict[int, tuple] = {}
+
+    def close(self) -> None:
+        """Waits for every request, then frees the server."""
+        if self._h:
+            lib().tgb_server_free(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self) -> None:
+        if getattr(self, "_h", None) and _lib is not None:
+            self.close()
+
+    def submit_fit(self, booster: "Booster", X, y, timestamps=None, entity=None) -> int:
+        X = np.asarray(X)
+        X = np.ascontiguousarray(X if X.dtype == np.float32 else X.astype(np.float64))
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        ts = None if timestamps is None else np.ascontiguousarray(timestamps, dtype=np.int64)
+        ent = None if entity is None else np.ascontiguousarray(entity, dtype=np.int64)
+        rid = C.c_longlong()
+        check(lib().tgb_server_submit_fit(self._h, booster._h, _ptr(X), 0 if X.dtype == np.float32 else 1, _ptr(y),
+                                          X.shape[0], X.shape[1], _ptr(ts), _ptr(ent), C.byref(rid)))
+        self._keep[rid.value] = (booster, X, y, ts, ent)
+        return rid.value
+
+    def submit_predict(self, booster: "Booster", X) -> tuple[int, np.ndarray]:
+        """Returns (request id, output array filled once the request is done)."""
+        X = np.asarray(X)
+        X = np.ascontiguousarray(X if X.dtype == np.float32 else X.astype(np.float64))
+        out = np.zeros(X.shape[0])
+        rid = C.c_longlong()
+        check(lib().tgb_server_submit_predict(self._h, booster._h, _ptr(X), 0 if X.dtype == np.float32 else 1,
+                                              X.shape[0], X.shape[1], _ptr(out), C.byref(rid)))
+        self._keep[rid.value] = (booster, X, out)
+        return rid.value, out
+
+    def wait(self, rid: int, timeout_ms: float = -1.0) -> int:
+        """Request state; raises TideError with the request's message when it failed."""
+        st = C.c_int()
+        check(lib().tgb_server_wait(self._h, int(rid), float(timeout_ms), C.byref(st)))
+        if st.value in (self.DONE, self.FAILED):
+            self._keep.pop(rid, None)
+        if st.value == self.FAILED:
+            raise TideError(lib().tgb_last_error().decode())
+        return st.value
+
+    def stats(self) -> dict:
+        o = np.zeros(12)
+        check(lib().tgb_server_stats(self._h, _ptr(o)))
+        keys = ("completed", "failed", "p50_s", "p99_s", "p50_fit_s", "p99_fit_s", "p50_predict_s", "p99_predict_s",
+                "mean_wait_s", "peak_running", "peak_bytes", "busy_s")
+        return dict(zip(keys, o.tolist()))
 
 
 def kernel_launches() -> int:
