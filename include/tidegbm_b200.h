@@ -103,6 +103,15 @@ TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);
 TGB_API int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample,
                            unsigned seed, double* edges_out, int* n_edges_out);
 
+/* Binner::fit with categorical features (cpp/src/binning.cpp:34-134): for a feature with
+ * is_cat[f] != 0, edges_out[f] receives its vocabulary (the distinct values seen at least
+ * cat_min_count times, at most max_bin - 1 of them, ascending; code = 1 + index) and
+ * n_edges_out[f] its length; numeric features as in tgb_binner_fit.  Host only.
+ * Returns max_bins() or -1. */
+TGB_API int tgb_binner_fit_cat(const void* X, int x_dtype, int n, int n_features, const int* is_cat, int max_bin,
+                               int cat_min_count, int bin_sample, unsigned seed, double* edges_out,
+                               int* n_edges_out);
+
 /* Binner::fit on X in device memory (row-major n x n_features of x_dtype, on `stream`):
  * the same edges as tgb_binner_fit, with the non-NaN counts, the value gather, the
  * sample sort, the edge arithmetic and the shuffle draws of features with at least 2^16

@@ -518,6 +518,31 @@ int orc_binner_fit(const double* X, int n, int n_f, int max_bin, int bin_sample,
     return std::max(mx, max_bin);  // binning.cpp:130-134
 }
 
+int orc_binner_fit_cat(const double* X, int n, int n_f, const int* is_cat, int max_bin, int cat_min_count,
+                       int bin_sample, uint32_t seed, double* edges, int* n_edges, uint8_t* codes) {
+    // cpp/src/binning.cpp:34-134 with categorical features.
+    OrcModel M;
+    M.n_f = n_f;
+    M.is_cat.assign(is_cat, is_cat + n_f);
+    orc_config c;
+    orc_config_default(&c);
+    c.max_bin = max_bin;
+    c.cat_min_count = cat_min_count;
+    c.bin_sample = bin_sample;
+    c.random_state = static_cast<int>(seed);
+    const int nb = model_binner_fit(&M, X, n, n_f, c);
+    for (int f = 0; f < n_f; ++f) {
+        const std::vector<double> v =
+            is_cat[f] ? M.cat_values[f]
+                      : std::vector<double>(M.edges.begin() + static_cast<size_t>(f) * 256,
+                                            M.edges.begin() + static_cast<size_t>(f) * 256 + M.n_edges[f]);
+        n_edges[f] = static_cast<int>(v.size());
+        std::copy(v.begin(), v.end(), edges + static_cast<size_t>(f) * 256);
+    }
+    if (codes) model_transform(M, X, n, codes);
+    return nb;
+}
+
 void orc_bin_transform(const double* X, int n, int n_f, const double* edges, const int* n_edges,
                        uint8_t* codes, int stride) {
     // cpp/src/binning.cpp:104-128: code = 1 + upper_bound(edges, v); NaN -> 0.

@@ -34,6 +34,13 @@ typedef struct {
 int orc_binner_fit(const double* X, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                    double* edges, int* n_edges, int* n_bins_col);
 
+/* Binner::fit + transform with categorical features (binning.cpp:34-134): edges[f]
+ * (n_f x 256) holds the vocabulary of a categorical feature (is_cat[f] != 0) or the
+ * edges of a numeric one, n_edges[f] its length; codes (row-major n x n_f, may be NULL)
+ * the uint8 codes.  Returns max_bins(). */
+int orc_binner_fit_cat(const double* X, int n, int n_f, const int* is_cat, int max_bin, int cat_min_count,
+                       int bin_sample, uint32_t seed, double* edges, int* n_edges, uint8_t* codes);
+
 /* Binner::transform (binning.cpp:104-128) into row-major uint8 codes with row
  * stride `stride` bytes. */
 void orc_bin_transform(const double* X, int n, int n_f, const double* edges, const int* n_edges,

@@ -239,6 +239,30 @@ int ref_binner(const double* X, int n, int n_f, int max_bin, int bin_sample, uns
     }
 }
 
+// Binner::fit with categorical features (is_cat[f] != 0) and Binner::transform:
+// edges_out[f] holds the vocabulary (cat_values) of a categorical feature, the edges of a
+// numeric one; codes are the u16 bin codes.
+int ref_binner_cat(const double* X, int n, int n_f, const int* is_cat, int max_bin, int cat_min_count,
+                   int bin_sample, unsigned seed, double* edges_out, int* n_edges, int* max_bins,
+                   unsigned short* codes) {
+    try {
+        Binner b;
+        std::vector<u8> mask(n, 1);
+        b.fit(X, n, n_f, is_cat, mask.data(), max_bin, cat_min_count, bin_sample, seed);
+        for (int f = 0; f < n_f; ++f) {
+            const std::vector<f64>& v = is_cat[f] ? b.cat_values[f] : b.edges[f];
+            n_edges[f] = static_cast<int>(v.size());
+            std::memcpy(edges_out + static_cast<size_t>(f) * 256, v.data(), v.size() * sizeof(double));
+        }
+        *max_bins = b.max_bins();
+        if (codes) b.transform(X, n, n_f, codes);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 // build_hist_col; out is interleaved {g, h, c(as f64)} per (feature, bin).
 void ref_build_hist_col(const unsigned short* xcol, int n_rows, int n_f, const int* idx, int n_idx,
                         const double* g, const double* h, int n_bins, int n_jobs, double* out) {

@@ -95,3 +95,46 @@ def test_host_binner_matches_reference_fixture(native):
     assert nb == int(d["max_bins"])
     assert np.array_equal(ne, d["n_edges"])
     assert np.array_equal(e.reshape(nf, 256), d["edges"])
+
+
+def _cat_X(seed, n=20000, nf=6):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, nf))
+    X[:, 0] = rng.integers(0, 12, n)                                    # few categories
+    X[:, 2] = rng.integers(0, 400, n)                                   # more than max_bin - 1: the most frequent kept
+    X[:, 3] = np.where(rng.random(n) < 0.01, rng.integers(100, 160, n), rng.integers(0, 5, n))  # rare ones dropped
+    X[:, 4] = rng.integers(0, 10**7, n)                                 # nearly all values seen once: all rare
+    X[rng.random((n, nf)) < 0.03] = np.nan
+    return X, np.array([1, 0, 1, 1, 1, 0], np.int32)
+
+
+@pytest.mark.parametrize("dtype,max_bin,min_count,bin_sample", [(np.float64, 255, 5, 3000), (np.float32, 255, 5, 0),
+                                                                (np.float64, 64, 2, 5000), (np.float64, 255, 20, 0)])
+def test_host_categorical_binner_matches_oracle(native, oracle, dtype, max_bin, min_count, bin_sample):
+    """tgb_binner_fit_cat's vocabularies and numeric edges against the oracle's
+    Binner::fit with categorical features, bit for bit."""
+    X, is_cat = _cat_X(4)
+    X = X.astype(dtype)
+    n, nf = X.shape
+    e1 = np.zeros(nf * 256)
+    n1 = np.zeros(nf, np.int32)
+    nb1 = native.lib().tgb_binner_fit_cat(np.ascontiguousarray(X).ctypes.data_as(C.c_void_p),
+                                          0 if dtype == np.float32 else 1, n, nf, is_cat.ctypes.data_as(C.c_void_p),
+                                          max_bin, min_count, bin_sample, 7, e1.ctypes.data_as(C.c_void_p),
+                                          n1.ctypes.data_as(C.c_void_p))
+    assert nb1 > 0, native.lib().tgb_last_error()
+    e2 = np.zeros(nf * 256)
+    n2 = np.zeros(nf, np.int32)
+    L = oracle.oracle_lib()
+    L.orc_binner_fit_cat.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    Xd = np.ascontiguousarray(X, dtype=np.float64)
+    nb2 = L.orc_binner_fit_cat(Xd.ctypes.data_as(C.c_void_p), n, nf, is_cat.ctypes.data_as(C.c_void_p), max_bin,
+                               min_count, bin_sample, 7, e2.ctypes.data_as(C.c_void_p), n2.ctypes.data_as(C.c_void_p),
+                               None)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1, e2)
+    assert n1[2] == max_bin - 1  # the vocabulary cut to the most frequent values
+    if min_count >= 5:
+        assert n1[4] == 1  # no value is frequent enough: the most frequent one alone

@@ -195,3 +195,43 @@ def test_categorical_splits_match_reference(oracle, extra, interaction):
     finally:
         oracle.ref_free(hr)
         oracle.oracle_free(ho)
+
+
+@pytest.mark.parametrize("max_bin,min_count", [(255, 5), (64, 2), (255, 30)])
+def test_categorical_binner_matches_reference(oracle, max_bin, min_count):
+    """The oracle's Binner::fit + transform with categorical features against the reference
+    core: vocabularies, numeric edges, max_bins and the codes."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    import ctypes as C
+    rng = np.random.default_rng(9)
+    n, nf = 15000, 5
+    X = rng.standard_normal((n, nf))
+    X[:, 0] = rng.integers(0, 12, n)
+    X[:, 1] = rng.integers(0, 400, n)
+    X[:, 3] = np.where(rng.random(n) < 0.01, rng.integers(100, 160, n), rng.integers(0, 5, n))
+    X[:, 4] = rng.integers(0, 3000, n)
+    X[rng.random((n, nf)) < 0.03] = np.nan
+    is_cat = np.array([1, 1, 0, 1, 1], np.int32)
+    R = oracle.ref_lib()
+    R.ref_binner_cat.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    e1 = np.zeros(nf * 256)
+    n1 = np.zeros(nf, np.int32)
+    mb = np.zeros(1, np.int32)
+    codes = np.zeros((n, nf), np.uint16)
+    assert R.ref_binner_cat(X.ctypes.data_as(C.c_void_p), n, nf, is_cat.ctypes.data_as(C.c_void_p), max_bin,
+                            min_count, 2000, 5, e1.ctypes.data_as(C.c_void_p), n1.ctypes.data_as(C.c_void_p),
+                            mb.ctypes.data_as(C.c_void_p), codes.ctypes.data_as(C.c_void_p)) == 0
+    L = oracle.oracle_lib()
+    L.orc_binner_fit_cat.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    e2 = np.zeros(nf * 256)
+    n2 = np.zeros(nf, np.int32)
+    c2 = np.zeros((n, nf), np.uint8)
+    nb = L.orc_binner_fit_cat(X.ctypes.data_as(C.c_void_p), n, nf, is_cat.ctypes.data_as(C.c_void_p), max_bin,
+                              min_count, 2000, 5, e2.ctypes.data_as(C.c_void_p), n2.ctypes.data_as(C.c_void_p),
+                              c2.ctypes.data_as(C.c_void_p))
+    assert nb == int(mb[0])
+    assert np.array_equal(n1, n2) and np.array_equal(e1, e2)
+    assert np.array_equal(codes.astype(np.uint8), c2) and codes.max() <= 255

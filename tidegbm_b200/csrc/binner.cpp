@@ -351,6 +351,69 @@ int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, 
     return nb;
 }
 
+namespace {
+
+// The vocabulary of one categorical feature (cpp/src/binning.cpp:47-84): the distinct
+// non-NaN values with at least cat_min_count occurrences (none: the most frequent one,
+// the smallest value on ties), cut to the max_bin - 1 most frequent ones when there are
+// more (std::partial_sort, so ties fall as in the reference), ascending.
+template <typename T>
+std::vector<double> cat_vocabulary(const T* X, int n, int n_f, int f, int max_bin, int cat_min_count) {
+    std::vector<double> v;
+    v.reserve(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        const double x = static_cast<double>(X[static_cast<size_t>(i) * n_f + f]);
+        if (!is_nan(x)) v.push_back(x);
+    }
+    std::sort(v.begin(), v.end());
+    std::vector<std::pair<int, double>> runs;  // (occurrences, value), ascending values
+    for (size_t a = 0; a < v.size();) {
+        size_t b = a + 1;
+        while (b < v.size() && v[b] == v[a]) ++b;
+        runs.emplace_back(static_cast<int>(b - a), v[a]);
+        a = b;
+    }
+    const int min_count = std::max(1, cat_min_count);
+    std::vector<std::pair<int, double>> kept;
+    for (const auto& r : runs)
+        if (r.first >= min_count) kept.push_back(r);
+    if (kept.empty() && !runs.empty())
+        kept.push_back(*std::max_element(runs.begin(), runs.end(),
+                                         [](const auto& a, const auto& b) { return a.first < b.first; }));
+    const int cap = max_bin - 1;
+    if (static_cast<int>(kept.size()) > cap) {
+        std::partial_sort(kept.begin(), kept.begin() + cap, kept.end(),
+                          [](const auto& a, const auto& b) { return a.first > b.first; });
+        kept.resize(static_cast<size_t>(cap));
+    }
+    std::vector<double> vocab;
+    vocab.reserve(kept.size());
+    for (const auto& r : kept) vocab.push_back(r.second);
+    std::sort(vocab.begin(), vocab.end());
+    return vocab;
+}
+
+}  // namespace
+
+int binner_fit_cat(const void* X, int x_dtype, int n, int n_f, const int* is_cat, int max_bin, int cat_min_count,
+                   int bin_sample, uint32_t seed, std::vector<double>& edges, std::vector<int>& n_edges,
+                   int n_threads) {
+    binner_fit(X, x_dtype, n, n_f, max_bin, bin_sample, seed, edges, n_edges, n_threads);
+    parallel_for(n_f, n_threads, [&](int f) {
+        if (!is_cat[f]) return;
+        const std::vector<double> vocab =
+            x_dtype == 0 ? cat_vocabulary(static_cast<const float*>(X), n, n_f, f, max_bin, cat_min_count)
+                         : cat_vocabulary(static_cast<const double*>(X), n, n_f, f, max_bin, cat_min_count);
+        double* e = edges.data() + static_cast<size_t>(f) * 256;
+        std::fill(e, e + 256, 0.0);
+        std::copy(vocab.begin(), vocab.end(), e);
+        n_edges[f] = static_cast<int>(vocab.size());
+    });
+    int mx = 2;  // Binner::max_bins (binning.cpp:130-134): vocabulary + missing, or edges + 2
+    for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + (is_cat[f] ? 1 : 2));
+    return std::max(mx, max_bin);
+}
+
 int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                std::vector<double>& edges, std::vector<int>& n_edges, int n_threads) {
     if (x_dtype == 0) return binner_fit_t<float>(X, n, n_f, max_bin, bin_sample, seed, edges, n_edges, n_threads);

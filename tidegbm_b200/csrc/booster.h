@@ -139,6 +139,11 @@ private:
 // sampled values per feature and their quantile edges.  Returns max_bins().
 int binner_fit(const void* X, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                std::vector<double>& edges, std::vector<int>& n_edges, int n_threads);
+// Binner::fit with categorical features (is_cat[f] != 0): edges[f] holds the vocabulary of
+// a categorical feature (binning.cpp:47-84) and n_edges[f] its length.  Returns max_bins().
+int binner_fit_cat(const void* X, int x_dtype, int n, int n_f, const int* is_cat, int max_bin, int cat_min_count,
+                   int bin_sample, uint32_t seed, std::vector<double>& edges, std::vector<int>& n_edges,
+                   int n_threads);
 // The same edges from X in device memory (row-major n x n_f, stream `stream`, a
 // cudaStream_t).  binner_fits_device says whether one feature-major sample buffer of
 // the sizes involved stays under 2^31 values (else use binner_fit).

@@ -309,6 +309,23 @@ int tgb_fit_stats(tgb_booster* hb, double* o) {
     });
 }
 
+int tgb_binner_fit_cat(const void* X, int x_dtype, int n, int n_features, const int* is_cat, int max_bin,
+                       int cat_min_count, int bin_sample, unsigned seed, double* edges_out, int* n_edges_out) {
+    int nb = -1;
+    const int rc = guard([&] {
+        need(X && is_cat && edges_out && n_edges_out, "NULL argument");
+        need(x_dtype == 0 || x_dtype == 1, "x_dtype must be 0 or 1");
+        need(max_bin >= 8 && max_bin <= 256, "max_bin must be in [8, 256]");
+        std::vector<double> e;
+        std::vector<int> ne;
+        nb = tgb::binner_fit_cat(X, x_dtype, n, n_features, is_cat, max_bin, cat_min_count, bin_sample, seed, e, ne,
+                                 static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+        std::copy(e.begin(), e.end(), edges_out);
+        std::copy(ne.begin(), ne.end(), n_edges_out);
+    });
+    return rc == 0 ? nb : -1;
+}
+
 int tgb_binner_fit(const void* X, int x_dtype, int n, int n_features, int max_bin, int bin_sample, unsigned seed,
                    double* edges_out, int* n_edges_out) {
     int nb = -1;

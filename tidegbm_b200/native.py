@@ -60,6 +60,7 @@ def lib() -> C.CDLL:
         "tgb_fit_stat": ([vp, cp, vp], i),
         "tgb_binner_fit_device": ([vp, i, i, i, i, i, C.c_uint, vp, vp, vp], i),
         "tgb_binner_fit": ([vp, i, i, i, i, i, C.c_uint, vp, vp], i),
+        "tgb_binner_fit_cat": ([vp, i, i, i, vp, i, i, i, C.c_uint, vp, vp], i),
         "tgb_shuffled_prefix": ([ll, ll, C.c_uint, vp], i),
         "tgb_shuffled_prefix_device": ([ll, ll, C.c_uint, vp, vp], i),
         "tgb_shuffle_sequence": ([ll, ll, C.c_uint, i, vp], i),
