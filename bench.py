@@ -282,6 +282,89 @@ def held_out_ic(pred, panel) -> float:
     return float(((a * b).sum(axis=1)[ok] / den[ok]).mean())
 
 
+SERVING_FEATURES = (32, 64, 128, 256)
+
+
+def serving_trace(n_requests: int, seed: int = 7, rate: float = 20.0, max_rows: int = 4_000_000) -> list[dict]:
+    """The serving workload's request trace: Poisson arrivals (mean `rate` per second),
+    70% fit / 30% predict; fits of log-uniform 10k..max_rows rows, features uniform in
+    SERVING_FEATURES, 20..200 trees, depth 6..8, mse or pairwise (50/50); predicts of
+    log-uniform 1k..1M rows against a model fitted earlier in the trace."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    reqs: list[dict] = []
+    fits: list[int] = []
+    for k in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        if not fits or rng.random() < 0.7:
+            rows = int(np.exp(rng.uniform(np.log(10_000), np.log(max_rows))))
+            reqs.append(dict(kind="fit", t=t, rows=rows, features=int(rng.choice(SERVING_FEATURES)),
+                             trees=int(rng.integers(20, 201)), depth=int(rng.integers(6, 9)),
+                             objective="mse" if rng.random() < 0.5 else "pairwise",
+                             offset=int(rng.integers(0, max_rows - rows + 1))))
+            fits.append(k)
+        else:
+            model = int(fits[int(rng.integers(0, len(fits)))])
+            rows = int(np.exp(rng.uniform(np.log(1_000), np.log(1_000_000))))
+            f = reqs[model]["features"]
+            reqs.append(dict(kind="predict", t=t, rows=rows, features=f, model=model,
+                             offset=int(rng.integers(0, max_rows - rows + 1))))
+    return reqs
+
+
+def run_serving(native, n_requests: int, local: int, budget_bytes: float = 150e9, slots: int = 8) -> dict:
+    """Serves the trace through native.Server (tgb_server_*): requests submitted at their
+    arrival times, admitted by the device-memory budget, overlapping on the device; p50/p99
+    latency from submission to completion and the aggregate trees/s of the fits.  Request
+    data are row ranges of one panel_small-generator panel per feature count (the
+    generator of the small workload), prepared before the clock starts."""
+    from tidegbm_b200 import panels
+
+    reqs = serving_trace(n_requests)
+    max_rows = max(r["rows"] + r["offset"] for r in reqs)
+    pools = {}
+    for f in sorted({r["features"] for r in reqs}):
+        n_dates = (max_rows + 249) // 250
+        pools[f] = panels.panel_small(n_dates=n_dates, n_entities=250, n_features=f, seed=100 + f)
+    srv = native.Server(device=local, budget_bytes=budget_bytes, slots=slots)
+    boosters: dict[int, object] = {}
+    ids: list[int] = []
+    t0 = time.perf_counter()
+    for k, r in enumerate(reqs):
+        delay = r["t"] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        p = pools[r["features"]]
+        lo, hi = r["offset"], r["offset"] + r["rows"]
+        if r["kind"] == "fit":
+            b = native.Booster(device=local, n_estimators=r["trees"], max_depth=r["depth"], learning_rate=0.08,
+                               horizon=1, objective=r["objective"], pair_splits=False,
+                               hist_bits=8 if r["objective"] == "mse" else 0)
+            boosters[k] = b
+            ids.append(srv.submit_fit(b, p.X[lo:hi], p.y[lo:hi], timestamps=p.ts[lo:hi], entity=p.entity[lo:hi]))
+        else:
+            rid, _ = srv.submit_predict(boosters[r["model"]], p.X[lo:hi])
+            ids.append(rid)
+    failed = []
+    for rid in ids:
+        try:
+            srv.wait(rid)
+        except native.TideError as e:
+            failed.append(str(e)[:120])
+    st = srv.stats()
+    srv.close()
+    fit_trees = sum(r["trees"] for r in reqs if r["kind"] == "fit")
+    return {"requests": n_requests, "fits": sum(r["kind"] == "fit" for r in reqs),
+            "predicts": sum(r["kind"] == "predict" for r in reqs), "budget_bytes": budget_bytes, "slots": slots,
+            "p50_s": st["p50_s"], "p99_s": st["p99_s"], "p50_fit_s": st["p50_fit_s"], "p99_fit_s": st["p99_fit_s"],
+            "p50_predict_s": st["p50_predict_s"], "p99_predict_s": st["p99_predict_s"],
+            "mean_wait_s": st["mean_wait_s"], "peak_running": st["peak_running"], "peak_bytes": st["peak_bytes"],
+            "trees_per_s": fit_trees / st["busy_s"] if st["busy_s"] > 0 else None, "busy_s": st["busy_s"],
+            "failed": failed[:5], "n_failed": len(failed),
+            "trace": "Poisson 20 req/s, 70% fit (10k..4M rows, 32..256 features, 20..200 trees, depth 6..8, "
+                     "mse int8 / pairwise) / 30% predict (1k..1M rows)"}
+
+
 def max_over_ranks(values, device):
     """Element-wise max over the ranks of a list of floats (one process per GPU), after a
     barrier; the values unchanged when no process group of several ranks is running."""
@@ -436,6 +519,11 @@ def run_ours(args) -> None:
             line["plain_gpu"] = plain_gpu_hist(native, p.X, edges, n_edges, idx, g, h, info["n_bins"])
         except Exception as e:
             line["plain_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank == 0 and args.serving > 0:
+        try:
+            line["serving"] = run_serving(native, args.serving, local)
+        except Exception as e:
+            line["serving"] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -453,6 +541,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dates", type=int, default=5000, help="panel dates (x 2000 rows); default 10M rows")
     ap.add_argument("--no-baselines", action="store_true")
+    ap.add_argument("--serving", type=int, default=0, metavar="N",
+                    help="also serve an N-request trace of the serving workload (p50/p99 latency)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
