@@ -365,6 +365,36 @@ def run_serving(native, n_requests: int, local: int, budget_bytes: float = 150e9
                      "mse int8 / pairwise) / 30% predict (1k..1M rows)"}
 
 
+def run_walkforward(native, local: int, n_dates: int = 8000, n_splits: int = 16, slots: int = 8) -> dict:
+    """The batched walk-forward workload: panel_walkforward (n_dates dates, ~425 rows a
+    date, 64 features), n_splits expanding folds with embargo 5 (walkforward.py), horizon 5,
+    pairwise, depth 6, 100 trees per fold; every fold submitted at once to the serving
+    loop, so the folds train concurrently on the device.  Reports the folds' aggregate
+    trees/s from the first submission to the last completion."""
+    from tidegbm_b200 import panels
+    from tidegbm_b200.walkforward import walk_forward_folds
+
+    p = panels.panel_walkforward(n_dates=n_dates)
+    folds = walk_forward_folds(p.ts, n_splits, embargo=5, min_train_fraction=0.1)
+    srv = native.Server(device=local, slots=slots)
+    boosters, ids = [], []
+    for train, _ in folds:
+        hi = int(train.size)  # rows are time-sorted: the training set is the prefix [0, hi)
+        b = native.Booster(device=local, n_estimators=100, max_depth=6, learning_rate=0.08, horizon=5,
+                           objective="pairwise", pair_splits=False)
+        boosters.append(b)
+        ids.append(srv.submit_fit(b, p.X[:hi], p.y[:hi], timestamps=p.ts[:hi], entity=p.entity[:hi]))
+    for rid in ids:
+        srv.wait(rid)
+    st = srv.stats()
+    srv.close()
+    trees = 100 * len(folds)
+    return {"folds": len(folds), "train_rows": [int(tr.size) for tr, _ in folds], "trees": trees,
+            "busy_s": st["busy_s"], "trees_per_s": trees / st["busy_s"] if st["busy_s"] > 0 else None,
+            "p50_fold_s": st["p50_fit_s"], "p99_fold_s": st["p99_fit_s"], "peak_running": st["peak_running"],
+            "mode": "folds as concurrent requests of the serving loop, one stream each"}
+
+
 def max_over_ranks(values, device):
     """Element-wise max over the ranks of a list of floats (one process per GPU), after a
     barrier; the values unchanged when no process group of several ranks is running."""
@@ -519,6 +549,11 @@ def run_ours(args) -> None:
             line["plain_gpu"] = plain_gpu_hist(native, p.X, edges, n_edges, idx, g, h, info["n_bins"])
         except Exception as e:
             line["plain_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank == 0 and args.walkforward:
+        try:
+            line["walkforward"] = run_walkforward(native, local)
+        except Exception as e:
+            line["walkforward"] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0 and args.serving > 0:
         try:
             line["serving"] = run_serving(native, args.serving, local)
@@ -541,6 +576,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dates", type=int, default=5000, help="panel dates (x 2000 rows); default 10M rows")
     ap.add_argument("--no-baselines", action="store_true")
+    ap.add_argument("--walkforward", action="store_true",
+                    help="also train the batched walk-forward workload's folds concurrently")
     ap.add_argument("--serving", type=int, default=0, metavar="N",
                     help="also serve an N-request trace of the serving workload (p50/p99 latency)")
     args = ap.parse_args()
