@@ -81,6 +81,32 @@ def test_host_binner_matches_oracle(native, oracle, dtype, bin_sample):
     assert np.array_equal(e1, e2)
 
 
+@pytest.mark.parametrize("dtype,max_bin,bin_sample", [(np.float64, 255, 0), (np.float64, 64, 500),
+                                                     (np.float32, 255, 500), (np.float32, 8, 0)])
+def test_host_binner_edge_columns_match_oracle(native, oracle, dtype, max_bin, bin_sample):
+    """tgb_binner_fit on edge columns (tests/edge_columns.py): edges bit for bit, signed zeros
+    included (the kept values reach std::sort in their shuffled order, as in the reference)."""
+    from edge_columns import edge_columns
+
+    with np.errstate(over="ignore"):  # float32: the 1e300 values become infinities, 1e-300 signed zeros
+        X = np.ascontiguousarray(edge_columns().astype(dtype))
+    n, nf = X.shape
+    e1 = np.zeros(nf * 256)
+    n1 = np.zeros(nf, np.int32)
+    nb1 = native.lib().tgb_binner_fit(X.ctypes.data_as(C.c_void_p), 0 if dtype == np.float32 else 1, n, nf,
+                                      max_bin, bin_sample, 7, e1.ctypes.data_as(C.c_void_p),
+                                      n1.ctypes.data_as(C.c_void_p))
+    assert nb1 > 0, native.lib().tgb_last_error()
+    e2 = np.zeros(nf * 256)
+    n2 = np.zeros(nf, np.int32)
+    nbc = np.zeros(nf, np.int32)
+    nb2 = oracle.oracle_lib().orc_binner_fit(np.ascontiguousarray(X, dtype=np.float64), n, nf, max_bin, bin_sample,
+                                             7, e2, n2, nbc)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1.view(np.uint64), e2.view(np.uint64))
+
+
 def test_host_binner_matches_reference_fixture(native):
     """tgb_binner_fit (the host part of binning) against the reference's own edges."""
     import os

@@ -235,3 +235,34 @@ def test_categorical_binner_matches_reference(oracle, max_bin, min_count):
     assert nb == int(mb[0])
     assert np.array_equal(n1, n2) and np.array_equal(e1, e2)
     assert np.array_equal(codes.astype(np.uint8), c2) and codes.max() <= 255
+
+
+@pytest.mark.parametrize("max_bin,bin_sample", [(255, 0), (255, 500), (64, 0), (8, 500)])
+def test_binner_edge_columns_match_reference(oracle, max_bin, bin_sample):
+    """Binner::fit + transform on edge columns (tests/edge_columns.py): the oracle's edges
+    bit for bit (NaN edges from infinite ranges included), n_bins_col, max_bins and codes
+    against the reference core."""
+    from edge_columns import edge_columns
+
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    X = edge_columns()
+    n, nf = X.shape
+    e1 = np.zeros(nf * 256)
+    n1 = np.zeros(nf, np.int32)
+    b1 = np.zeros(nf, np.int32)
+    L = oracle.oracle_lib()
+    mb1 = L.orc_binner_fit(X, n, nf, max_bin, bin_sample, 7, e1, n1, b1)
+    c1 = np.zeros(n * nf, np.uint8)
+    L.orc_bin_transform(X, n, nf, e1, n1, c1, nf)
+    e2 = np.zeros(nf * 256)
+    n2 = np.zeros(nf, np.int32)
+    b2 = np.zeros(nf, np.int32)
+    mb2 = C.c_int()
+    c2 = np.zeros((n, nf), np.uint16)
+    assert oracle.ref_lib().ref_binner(X, n, nf, max_bin, bin_sample, 7, e2, n2, b2, C.byref(mb2),
+                                       c2.ctypes.data_as(C.c_void_p)) == 0
+    assert mb1 == mb2.value
+    assert np.array_equal(n1, n2) and np.array_equal(b1, b2)
+    assert np.array_equal(e1.view(np.uint64), e2.view(np.uint64))
+    assert np.array_equal(c1.reshape(n, nf), c2)

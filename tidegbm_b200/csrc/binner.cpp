@@ -123,8 +123,9 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
             for (int f = 0; f < n_f; ++f) cnt[f] += is_nan(at<T>(X, row + f)) ? 0 : 1;
         }
     });
-    // kept positions per feature (sorted), or "all" when no sampling happens
-    std::vector<std::vector<int32_t>> keep(n_f);
+    // kept positions per feature (sorted), or "all" when no sampling happens; slot[f][i] is
+    // the shuffled position of the i-th smallest kept position
+    std::vector<std::vector<int32_t>> keep(n_f), slot(n_f);
     std::vector<char> take_all(n_f, 0);
     std::vector<int64_t> m(n_f, 0);
     for (int c = 0; c < n_chunks; ++c)
@@ -132,9 +133,18 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
     parallel_for(n_f, n_threads, [&](int f) {
         if (bin_sample > 0 && m[f] > bin_sample) {
             Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);  // std::mt19937's stream
-            keep[f].resize(static_cast<size_t>(bin_sample));
-            shuffled_prefix(m[f], bin_sample, rng, keep[f].data());
-            std::sort(keep[f].begin(), keep[f].end());
+            std::vector<int32_t> prefix(static_cast<size_t>(bin_sample));
+            shuffled_prefix(m[f], bin_sample, rng, prefix.data());
+            std::vector<uint64_t> key(prefix.size());  // (position, shuffled slot), positions distinct
+            for (size_t j = 0; j < prefix.size(); ++j)
+                key[j] = (static_cast<uint64_t>(static_cast<uint32_t>(prefix[j])) << 32) | j;
+            std::sort(key.begin(), key.end());
+            keep[f].resize(key.size());
+            slot[f].resize(key.size());
+            for (size_t i = 0; i < key.size(); ++i) {
+                keep[f][i] = static_cast<int32_t>(key[i] >> 32);
+                slot[f][i] = static_cast<int32_t>(static_cast<uint32_t>(key[i]));
+            }
         } else {
             take_all[f] = 1;
         }
@@ -174,6 +184,15 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
                 ++rank[f];
             }
         }
+    });
+    // The reference sorts the kept values in their shuffled order (binning.cpp:93-98).  Equal
+    // values stay where std::sort leaves them, which depends on that order; of equal doubles
+    // only -0.0 and +0.0 differ in their bits, and the sign of a zero edge follows from it.
+    parallel_for(n_f, n_threads, [&](int f) {
+        if (take_all[f]) return;
+        std::vector<double> shuffled(sample[f].size());
+        for (size_t i = 0; i < shuffled.size(); ++i) shuffled[static_cast<size_t>(slot[f][i])] = sample[f][i];
+        sample[f].swap(shuffled);
     });
     edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
     n_edges.assign(n_f, 0);
