@@ -266,3 +266,47 @@ def test_binner_edge_columns_match_reference(oracle, max_bin, bin_sample):
     assert np.array_equal(n1, n2) and np.array_equal(b1, b2)
     assert np.array_equal(e1.view(np.uint64), e2.view(np.uint64))
     assert np.array_equal(c1.reshape(n, nf), c2)
+
+
+_OPTION_CASES = {
+    "embargo3": dict(horizon=1, embargo=3),
+    "horizon5_embargo2": dict(horizon=5, embargo=2),
+    "buckets7": dict(horizon=1, n_time_buckets=7),
+    "finer": dict(horizon=1, finer_torb=1),
+    "finer_buckets100": dict(horizon=1, finer_torb=1, n_time_buckets=100),
+    "min_cover500": dict(horizon=1, torb_min_cover=500.0),
+    "stump": dict(horizon=1, max_leaves=2),
+    "depth1": dict(horizon=1, max_depth=1),
+    "min_split_gain5": dict(horizon=1, min_split_gain=5.0),
+    "min_child_weight50": dict(horizon=1, min_child_weight=50.0),
+    "pairwise_goss_h2": dict(horizon=2, objective="pairwise", goss=1, goss_top=0.3, goss_other=0.3),
+}
+
+
+@pytest.mark.parametrize("name", sorted(_OPTION_CASES))
+def test_fit_options_match_reference(oracle, name):
+    """The oracle's fit against the reference core under the TORB and growth options:
+    causal cuts with embargo and horizon (booster.cpp:60-72), bucket counts, the cover
+    blend (booster.cpp:604-648) and the growth limits; trees, values, prefixes, losses
+    and predictions bit for bit."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    from tidegbm_b200 import panels
+
+    p = panels.panel_small(n_dates=70, n_entities=90, n_features=8, seed=4)
+    params = {**dict(n_estimators=5, learning_rate=0.1, max_depth=5, objective="mse", random_state=2,
+                     pair_splits=False), **_OPTION_CASES[name]}
+    X = p.X.astype(np.float64)
+    r, hr = oracle.ref_fit(params, X, p.y, p.ts, p.entity, n_jobs=1)
+    o, ho = oracle.oracle_fit(params, X, p.y, p.ts, p.entity)
+    try:
+        assert len(r.trees) == len(o.trees) and r.n_buckets == o.n_buckets
+        for t, (a, b) in enumerate(zip(r.trees, o.trees)):
+            for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
+                        "value", "gain", "values", "cover", "prefix"):
+                assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        assert np.array_equal(r.evals_train, o.evals_train)
+        assert np.array_equal(oracle.ref_predict(hr, X[:500]), oracle.oracle_predict(ho, X[:500]))
+    finally:
+        oracle.ref_free(hr)
+        oracle.oracle_free(ho)
