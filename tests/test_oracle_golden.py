@@ -310,3 +310,26 @@ def test_fit_options_match_reference(oracle, name):
     finally:
         oracle.ref_free(hr)
         oracle.oracle_free(ho)
+
+
+@pytest.mark.parametrize("k", range(8))
+def test_small_shapes_match_reference(oracle, k):
+    """The oracle's fit against the reference core on small and ragged shapes
+    (tests/fit_shapes.py): trees, values, prefixes and predictions bit for bit."""
+    from fit_shapes import SHAPES, shape_case
+
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    X, y, ts, ent, params = shape_case(*SHAPES[k])
+    r, hr = oracle.ref_fit(params, X, y, ts, ent, n_jobs=1)
+    o, ho = oracle.oracle_fit(params, X, y, ts, ent)
+    try:
+        assert len(r.trees) == len(o.trees)
+        for t, (a, b) in enumerate(zip(r.trees, o.trees)):
+            for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "value",
+                        "values", "cover", "prefix"):
+                assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        assert np.array_equal(oracle.ref_predict(hr, X), oracle.oracle_predict(ho, X))
+    finally:
+        oracle.ref_free(hr)
+        oracle.oracle_free(ho)
