@@ -333,3 +333,38 @@ def test_small_shapes_match_reference(oracle, k):
     finally:
         oracle.ref_free(hr)
         oracle.oracle_free(ho)
+
+
+def _pairwise_groups(seed):
+    """Dates of 1, 2, 24, 48, 49, 50, 97 and 800 rows (48 is the last size with every pair,
+    objective.cpp:179-219), ties in y (pairs of equal labels are skipped), one date whose
+    labels are all equal, and predictions far enough apart to reach the exp clamp."""
+    rng = np.random.default_rng(seed)
+    sizes = [1, 2, 24, 48, 49, 50, 97, 800, 30]
+    groups = np.concatenate([np.full(m, k, np.int64) for k, m in enumerate(sizes)])
+    n = groups.size
+    y = np.round(rng.standard_normal(n), 1)
+    y[groups == 8] = 0.5
+    pred = rng.standard_normal(n) * np.where(rng.random(n) < 0.05, 40.0, 1.0)
+    return np.ascontiguousarray(y), np.ascontiguousarray(pred), np.ascontiguousarray(groups)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_pairwise_gradient_edges_match_reference(oracle, seed):
+    """RankPairwise grad_hess and loss at the edges of its pair sampling, oracle against
+    the reference core bit for bit."""
+    if not oracle.ref_available():
+        pytest.skip("reference core not built (oracle/_ref)")
+    y, pred, groups = _pairwise_groups(seed)
+    n = y.size
+    g1, h1, g2, h2 = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n)
+    gp = groups.ctypes.data_as(C.c_void_p)
+    oracle.oracle_lib().orc_grad_hess(5, y, pred, gp, n, g1, h1)
+    oracle.ref_lib().ref_grad_hess(5, y, pred, gp, n, g2, h2)
+    assert np.array_equal(g1, g2) and np.array_equal(h1, h2)
+    R = oracle.ref_lib()
+    R.ref_loss.restype = C.c_double
+    R.ref_loss.argtypes = [C.c_int, np.ctypeslib.ndpointer(np.float64, flags="C"),
+                           np.ctypeslib.ndpointer(np.float64, flags="C"), C.c_void_p, C.c_int]
+    L = oracle.oracle_lib()
+    assert L.orc_loss(5, y, pred, gp, n) == R.ref_loss(5, y, pred, gp, n)
