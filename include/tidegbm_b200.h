@@ -30,7 +30,7 @@ extern "C" {
 
 typedef struct tgb_booster tgb_booster;
 
-/* Message of the last failed call on this thread (tide_last_error, c_api.cpp:220). */
+/* Message of the last failed call on this thread (tide_last_error, c_api.cpp:18). */
 TGB_API const char* tgb_last_error(void);
 
 /* Number of kernel launches issued by this library in this process (for audits). */
@@ -38,15 +38,15 @@ TGB_API long long tgb_kernel_launches(void);
 
 /* ---- Booster level: the device="gpu" Booster (cpp/include/tidegbm/booster.hpp:22-72) ---- */
 
-/* tide_create (c_api.cpp:22-30); one booster owns one CUDA stream and its device
+/* tide_create (c_api.cpp:20-28); one booster owns one CUDA stream and its device
  * buffers on `device` — no process-global state (unlike GpuHistState,
  * cpp/src/histogram_cuda.cu:76-79). */
 TGB_API int tgb_booster_create(int device, tgb_booster** out);
-/* tide_free (c_api.cpp:232). */
+/* tide_free (c_api.cpp:30). */
 TGB_API void tgb_booster_free(tgb_booster* b);
 
-/* tide_set_int / tide_set_double (c_api.cpp:234-272), extended to every Config key the
- * GPU path reads (cpp/include/tidegbm/config.hpp:49-113).  Unknown keys return -1.
+/* tide_set_int / tide_set_double (c_api.cpp:32-70), extended to every Config key the
+ * GPU path reads (cpp/include/tidegbm/config.hpp:12-76).  Unknown keys return -1.
  * One int key is this library's own: "hist_bits" = 0 (default: exact 64-bit fixed-point
  * histograms, results match the reference) or 8 (int8 gradients with stochastic rounding,
  * one shared reduction per code: a faster, approximate split search; leaf values stay
@@ -58,7 +58,7 @@ TGB_API int tgb_set_double(tgb_booster* b, const char* key, double value);
 TGB_API int tgb_set_str(tgb_booster* b, const char* key, const char* value);
 
 /* Booster::fit (cpp/src/booster.cpp:231-742) with device=="gpu", the entry
- * tide_fit (c_api.cpp:274-288) reaches.  X: host, row-major; y: host f64 [n];
+ * tide_fit (c_api.cpp:72-86) reaches.  X: host, row-major; y: host f64 [n];
  * timestamps: host int64 [n] (required unless iid_mode; rank groups of the pairwise
  * objective); entity: host int64 [n] or NULL (sort key after the timestamp). */
 TGB_API int tgb_fit(tgb_booster* b, const void* X, int x_dtype, const double* y, int n, int n_features,
@@ -205,13 +205,14 @@ TGB_API int tgb_partition(const unsigned char* codes, int stride, const int* row
  * tgb_partition asks for: a serving process that reserves all device memory at start-up
  * and must not call cudaMalloc later (it can block the device and fail under memory
  * pressure), or a binding that passes only a call's inputs and outputs.  This variant
- * allocates nothing: its scratch is a fixed device array inside the library (about
- * 33 KB, held on every GPU that loads the library until the process exits), so n_rows
- * is limited to 16,777,216 (larger calls return -1 with a message).  The first call on a
- * device looks up that array's device address; make the first call on each device
- * before any stream capture.  All calls on a device share the array: calls whose
- * kernels may overlap on the GPU (other streams or host threads) race and must be
- * serialised by the caller.  Results equal tgb_partition's. */
+ * allocates nothing: its scratch (the per-tile counts of left rows) is a fixed device
+ * array inside the library (32 KB, held on every GPU that loads the library until the
+ * process exits), so n_rows is limited to 16,777,216 (larger calls return -1 with a
+ * message).  Every call looks up that array's device address with the device current;
+ * the first call on a device may load the library's device code, so make it before any
+ * stream capture.  All calls on a device share the array: calls whose kernels may
+ * overlap on the GPU (other streams or host threads) race and must be serialised by the
+ * caller.  Results equal tgb_partition's. */
 TGB_API int tgb_partition_noalloc(const unsigned char* codes, int stride, const int* rows, int n_rows, int feature,
                                   int threshold, int missing_left, int* out, int* n_left_out, void* stream);
 

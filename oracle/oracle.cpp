@@ -717,7 +717,7 @@ double orc_loss(int kind, const double* y, const double* pred, const int64_t* gr
 }
 
 void orc_config_default(orc_config* c) {
-    // Defaults of cpp/include/tidegbm/config.hpp:13-113.
+    // Defaults of cpp/include/tidegbm/config.hpp:13-76.
     c->n_estimators = 100;
     c->learning_rate = 0.1;
     c->max_depth = 6;

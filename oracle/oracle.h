@@ -7,7 +7,7 @@
  *
  * Every function names the reference file:line it restates (paths relative to
  * the reference project root).  Row-major uint8 bin codes are used throughout:
- * codes fit 8 bits because max_bin <= 256 (cpp/include/tidegbm/config.hpp:118)
+ * codes fit 8 bits because max_bin <= 256 (cpp/include/tidegbm/config.hpp:81)
  * and code = 1 + count(edges <= v) <= 255 (cpp/src/binning.cpp:117-118).
  */
 #ifndef TIDEGBM_ORACLE_H

@@ -2,7 +2,7 @@
 (src/tidegbm/cv.py, with src/tidegbm/utils.py), loaded as standalone modules from the
 reference checkout in this container.
 
-    python tests/golden/make_folds.py      # writes tests/golden/folds.npz
+    TIDEGBM_REF=<reference checkout> python tests/golden/make_folds.py   # writes tests/golden/folds.npz
 
 Each case stores its timestamps, parameters and, per fold, the train and test indices.
 """
@@ -16,7 +16,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/src/tidegbm"
+REF = os.path.join(os.environ.get("TIDEGBM_REF", ""), "src", "tidegbm")
 
 CASES = [  # (name, timestamps, n_splits, embargo, purge, min_train_fraction)
     ("walkforward16", np.repeat(np.arange(800, dtype=np.int64), 5), 16, 5, None, 0.3),

@@ -256,3 +256,35 @@ def test_grad_pairwise_matches_oracle(oracle, native):
     scale = np.abs(g0) + np.abs(h0) + 1e-3
     assert np.all(np.abs(g1 - g0) <= 1e-12 * scale)
     assert np.all(np.abs(h1 - h0) <= 1e-12 * scale)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_build_hist_gpu_seam_matches_oracle(oracle, native, seed):
+    """tgb_build_hist_gpu, the literal drop-in for the reference's build_hist_gpu seam
+    (cpp/include/tidegbm/histogram.hpp:57-58): host row-major uint16 codes, host idx/g/h,
+    the interleaved FP64 {g, h, c} Hist out.  Against the oracle's build_hist_col: counts
+    exact, G within 1e-9 of the per-bin sum of |g| (demeaned gradients make bin totals
+    near zero, so the bound is scaled by sum |g|), H within 1e-9 relative.  Called twice,
+    with a different row list the second time, on one booster: the resident code matrix is
+    reused and the result follows the new rows."""
+    _, _, codes, rows, g, h = _hist_case(seed)
+    n, nf = codes.shape
+    n_bins = 256
+    xb = np.ascontiguousarray(codes.astype(np.uint16))
+    b = native.Booster(device=0)
+    L = native.lib()
+    rng = np.random.default_rng(seed + 10)
+    for idx in (rows, np.sort(rng.choice(n, 777, replace=False)).astype(np.int32)):
+        out = np.zeros(nf * n_bins * 3)
+        native.check(L.tgb_build_hist_gpu(b._h, xb.ctypes.data_as(C.c_void_p), nf, idx.ctypes.data_as(C.c_void_p),
+                                          idx.size, g.ctypes.data_as(C.c_void_p), h.ctypes.data_as(C.c_void_p),
+                                          n_bins, n, out.ctypes.data_as(C.c_void_p)))
+        ref = np.zeros(nf * 256 * 3)
+        oracle.oracle_lib().orc_build_hist(np.ascontiguousarray(codes), nf, nf, idx, idx.size, g, h, 256, ref)
+        out, ref = out.reshape(nf, n_bins, 3), ref.reshape(nf, 256, 3)
+        assert np.array_equal(out[:, :, 2], ref[:, :, 2])
+        absg = np.zeros((nf, 256))
+        for f in range(nf):
+            np.add.at(absg[f], codes[idx, f], np.abs(g[idx]))
+        assert np.all(np.abs(out[:, :, 0] - ref[:, :, 0]) <= 1e-9 * absg + 1e-300)
+        assert np.allclose(out[:, :, 1], ref[:, :, 1], rtol=1e-9, atol=0)

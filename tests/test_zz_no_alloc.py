@@ -33,28 +33,40 @@ def _with_workspace(L, codes, stride, rows, n_rows, feat, thr, ml):
 
 def _without_workspace(L, codes, stride, rows, n_rows, feat, thr, ml):
     out = torch.full((max(1, n_rows),), -1, dtype=torch.int32, device="cuda")
-    nl = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nl = torch.full((1,), -7, dtype=torch.int32, device="cuda")
     rc = L.tgb_partition_noalloc(_p(codes), stride, _p(rows), n_rows, feat, thr, ml, _p(out), _p(nl), None)
     assert rc == 0, L.tgb_last_error()
     torch.cuda.synchronize()
     return out.cpu().numpy()[:n_rows], int(nl.item())
 
 
+def _expected(codes_h, rows_h, feat, thr, ml):
+    """The stable partition as numpy states it: left rows in order, then right rows."""
+    b = codes_h[rows_h, feat].astype(int)
+    left = np.where(b == 0, ml == 1, b <= thr)
+    return np.concatenate([rows_h[left], rows_h[~left]]), int(left.sum())
+
+
 def test_partition_noalloc_matches_workspace_version_twice(native):
     L = native.lib()
     rng = np.random.default_rng(123)
-    n, stride = 300_000, 32
+    n, stride = 3_200_000, 32
     codes_h = np.zeros((n, stride), np.uint8)
     codes_h[:, :24] = rng.integers(0, 256, size=(n, 24))
     codes = torch.from_numpy(codes_h).cuda()
-    # Two calls in a row with different sizes and splits: the second must not see the
-    # first call's leftovers in the shared scratch.
-    cases = [(250_001, 5, 120, 1), (70_000, 17, 30, 0)]
+    # Calls in a row with different sizes and splits: each must be unaffected by the
+    # previous call's leftovers in the shared scratch.  3,000,000 rows are 1,465 tiles, more
+    # than the 1,184 CTAs of a launch, so the grid-stride tile loop and the running prefix
+    # over the shared tile counts run too; 0 rows must report no left rows.
+    cases = [(3_000_000, 9, 200, 1), (250_001, 5, 120, 1), (70_000, 17, 30, 0), (0, 3, 10, 1)]
     for n_rows, feat, thr, ml in cases:
-        rows = torch.from_numpy(np.sort(rng.choice(n, n_rows, replace=False)).astype(np.int32)).cuda()
+        rows_h = np.sort(rng.choice(n, n_rows, replace=False)).astype(np.int32)
+        rows = torch.from_numpy(rows_h if n_rows else np.zeros(1, np.int32)).cuda()
         a, na = _with_workspace(L, codes, stride, rows, n_rows, feat, thr, ml)
         b, nb = _without_workspace(L, codes, stride, rows, n_rows, feat, thr, ml)
-        assert na == nb
+        exp, n_left = _expected(codes_h, rows_h, feat, thr, ml)
+        assert na == nb == n_left
+        assert np.array_equal(b, exp)
         assert np.array_equal(a, b)
 
 

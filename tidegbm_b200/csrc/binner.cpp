@@ -57,7 +57,8 @@ inline bool is_nan(double v) { return !(v == v); }
 // freed with the Scratch).  Pieces are 256-byte aligned.
 class Scratch {
 public:
-    Scratch(void* base, size_t bytes) : base_(static_cast<unsigned char*>(base)), size_(base ? bytes : 0) {}
+    Scratch(void* base, size_t bytes, cudaStream_t s)
+        : base_(static_cast<unsigned char*>(base)), size_(base ? bytes : 0), s_(s) {}
     template <class T>
     T* get(size_t count) {
         const size_t bytes = (std::max<size_t>(1, count * sizeof(T)) + 255) / 256 * 256;
@@ -67,7 +68,7 @@ public:
             return p;
         }
         owned_.push_back(std::make_unique<DBuf<unsigned char>>());
-        owned_.back()->alloc(bytes);
+        owned_.back()->alloc(bytes, s_);
         return reinterpret_cast<T*>(owned_.back()->p);
     }
 
@@ -75,6 +76,7 @@ private:
     unsigned char* base_;
     size_t size_;
     size_t used_ = 0;
+    cudaStream_t s_;
     std::vector<std::unique_ptr<DBuf<unsigned char>>> owned_;
 };
 
@@ -258,7 +260,7 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
                          int bin_sample, std::vector<double>& edges, std::vector<int>& n_edges, void* stream,
                          void* arena, size_t arena_bytes) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    Scratch scratch(arena, arena_bytes);
+    Scratch scratch(arena, arena_bytes, s);
     const size_t nc = static_cast<size_t>(plan.n_chunks) * n_f;
     const std::vector<long long>& base = plan.base;
     const std::vector<uint8_t>& take_all = plan.take_all;
@@ -351,7 +353,7 @@ int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, 
     std::vector<int> ch(nc);
     {
         DBuf<int> counts;
-        counts.alloc(nc);
+        counts.alloc(nc, s);
         launch_nonnan_counts(Xd, x_dtype, n, n_f, counts.p, s);
         check(cudaMemcpyAsync(ch.data(), counts.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, s), "counts download");
         check(cudaStreamSynchronize(s), "non-NaN counts");

@@ -36,7 +36,7 @@ void check(cudaError_t e, const char* what) {
     if (L > 7 && std::strcmp(what + L - 7, " launch") == 0) g_kernel_launches.fetch_add(1);
 }
 
-void* device_alloc(size_t bytes) {
+void* device_alloc(size_t bytes, cudaStream_t s) {
     static std::mutex mu;
     static bool configured[64] = {};
     int dev = 0;
@@ -48,25 +48,25 @@ void* device_alloc(size_t bytes) {
             check(cudaDeviceGetDefaultMemPool(&pool, dev), "default mem pool");
             uint64_t keep = ~0ull;  // never hand freed blocks back to the driver
             check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "mem pool threshold");
+            // A block freed on one stream is handed to another stream only once the free has
+            // completed; the pool never makes one booster's stream wait for another's.
+            int no = 0;
+            check(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no), "mem pool reuse");
             configured[dev] = true;
         }
     }
     void* p = nullptr;
-    check(cudaMallocAsync(&p, bytes, nullptr), "cudaMallocAsync");
-    check(cudaStreamSynchronize(nullptr), "cudaMallocAsync");  // usable from any stream from here on
+    check(cudaMallocAsync(&p, bytes, s), "cudaMallocAsync");
     return p;
 }
 
-void device_free(void* p) {
-    if (!p) return;
-    // Like cudaFree: wait until no queued work can still use the block, then return it
-    // to the pool.
-    cudaDeviceSynchronize();
-    cudaFreeAsync(p, nullptr);
+cudaError_t device_free(void* p, cudaStream_t s) {
+    if (!p) return cudaSuccess;
+    return cudaFreeAsync(p, s);
 }
 
 void Config::validate() const {
-    // The reference's own checks (cpp/include/tidegbm/config.hpp:115-134).
+    // The reference's own checks (cpp/include/tidegbm/config.hpp:78-97).
     if (n_estimators < 1) throw TideError("n_estimators must be >= 1");
     if (learning_rate <= 0 || learning_rate > 1.5) throw TideError("learning_rate out of range");
     if (max_bin < 8 || max_bin > 256) throw TideError("max_bin must be in [8, 256]");
@@ -143,7 +143,20 @@ int auto_time_buckets(const std::vector<int64_t>& uniq, int64_t horizon, int uni
 
 }  // namespace
 
+// The booster's stream outlives its buffers: it is declared first, so it is destroyed
+// last, after every buffer's stream-ordered free has been queued on it.
+struct OwnedStream {
+    cudaStream_t s = nullptr;
+    ~OwnedStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+};
+
 struct DeviceState {
+    OwnedStream owned;
     cudaStream_t stream = nullptr;
     DBuf<uint8_t> codes, codes_col;
     DBuf<double> y, pred, g, h;
@@ -179,15 +192,26 @@ struct DeviceState {
     DBuf<int> t_off;
     size_t trees_flat = 0;
 
-    ~DeviceState() {
-        if (stream) cudaStreamDestroy(stream);
+    // Everything a fit allocates; predict's buffers (pcodes, t_*, pout) stay.
+    void release_fit_buffers() {
+        codes.release(); codes_col.release(); y.release(); pred.release(); g.release(); h.release();
+        gq.release(); gq8.release(); rows0.release(); rows1.release(); histG.release(); histH.release();
+        histC.release(); nodes.release(); nodes_all.release(); splits.release(); st.release(); st_all.release();
+        tile_counts.release(); scan_gain.release(); scan_key.release(); scan_ticket.release();
+        keys_in.release(); keys_out.release(); goss_overflow.release(); vals_in.release(); vals_out.release();
+        rest_pos.release(); cub_tmp.release(); goss_flag.release(); nid.release(); seg_sums.release();
+        chunks.release(); bucket_seg_end.release(); cuts.release(); all_scale.release(); init_prefix.release();
+        values_all.release(); prefix_all.release(); losses.release(); loss_part.release(); cover_all.release();
+        loss_valid.release(); run_start.release(); run_len.release(); order.release();
     }
+
 };
 
 GpuBooster::GpuBooster(int dev) : device(dev) {
     check(cudaSetDevice(device), "cudaSetDevice");
     ds_ = new DeviceState();
-    check(cudaStreamCreateWithFlags(&ds_->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&ds_->owned.s, cudaStreamNonBlocking), "cudaStreamCreate");
+    ds_->stream = ds_->owned.s;
 }
 
 GpuBooster::~GpuBooster() {
@@ -387,43 +411,43 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     const int stride = (n_f + 15) / 16 * 16;
     const int max_nodes = 2 * c.max_leaves - 1;
     const size_t slot = static_cast<size_t>(n_f) * kBins;
-    D.codes.alloc(static_cast<size_t>(n) * stride);
-    D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n));
-    D.y.alloc(n);
-    D.pred.alloc(n);
-    D.g.alloc(n);
-    if (c.objective != 0) D.h.alloc(n);  // MSE hessians are implicit (unit)
-    if (c.objective == 0 && c.hist_bits == 0) D.gq.alloc(n);
-    if (c.hist_bits == 8) D.gq8.alloc(n);
-    D.rows0.alloc(n);
-    D.rows1.alloc(n);
-    D.histG.alloc(slot * max_nodes);
-    D.histH.alloc(slot * max_nodes);
-    D.histC.alloc(slot * max_nodes);
-    D.nodes.alloc(kMaxNodes);
-    D.splits.alloc(kMaxNodes);
-    D.st.alloc(1);
+    D.codes.alloc(static_cast<size_t>(n) * stride, s);
+    D.codes_col.alloc(static_cast<size_t>(n_f) * codes_col_pitch(n), s);
+    D.y.alloc(n, s);
+    D.pred.alloc(n, s);
+    D.g.alloc(n, s);
+    if (c.objective != 0) D.h.alloc(n, s);  // MSE hessians are implicit (unit)
+    if (c.objective == 0 && c.hist_bits == 0) D.gq.alloc(n, s);
+    if (c.hist_bits == 8) D.gq8.alloc(n, s);
+    D.rows0.alloc(n, s);
+    D.rows1.alloc(n, s);
+    D.histG.alloc(slot * max_nodes, s);
+    D.histH.alloc(slot * max_nodes, s);
+    D.histC.alloc(slot * max_nodes, s);
+    D.nodes.alloc(kMaxNodes, s);
+    D.splits.alloc(kMaxNodes, s);
+    D.st.alloc(1, s);
     const int max_tiles = (n + kPartTile - 1) / kPartTile;
-    D.tile_counts.alloc(max_tiles + 1);
-    D.scan_gain.alloc(2 * scan_ctas_per_node(n_f));
-    D.scan_key.alloc(2 * scan_ctas_per_node(n_f));
-    D.scan_ticket.alloc(3);
+    D.tile_counts.alloc(max_tiles + 1, s);
+    D.scan_gain.alloc(2 * scan_ctas_per_node(n_f), s);
+    D.scan_key.alloc(2 * scan_ctas_per_node(n_f), s);
+    D.scan_ticket.alloc(3, s);
     check(cudaMemsetAsync(D.scan_ticket.p, 0, 3 * sizeof(int), s), "ticket reset");
-    D.nid.alloc(n);
-    D.all_scale.alloc(1);
-    D.init_prefix.alloc(nbk);
-    D.nodes_all.alloc(static_cast<size_t>(T) * max_nodes);
-    D.st_all.alloc(T);
-    D.values_all.alloc(static_cast<size_t>(T) * max_nodes);
-    D.cover_all.alloc(static_cast<size_t>(T) * max_nodes);
-    D.prefix_all.alloc(static_cast<size_t>(T) * nbk * max_nodes);
-    D.losses.alloc(T);
+    D.nid.alloc(n, s);
+    D.all_scale.alloc(1, s);
+    D.init_prefix.alloc(nbk, s);
+    D.nodes_all.alloc(static_cast<size_t>(T) * max_nodes, s);
+    D.st_all.alloc(T, s);
+    D.values_all.alloc(static_cast<size_t>(T) * max_nodes, s);
+    D.cover_all.alloc(static_cast<size_t>(T) * max_nodes, s);
+    D.prefix_all.alloc(static_cast<size_t>(T) * nbk * max_nodes, s);
+    D.losses.alloc(T, s);
 
     // X upload + transform, then X is released.
     {
         stats.t_alloc = now() - tb;
         DBuf<unsigned char> Xd;
-        Xd.alloc(static_cast<size_t>(n) * n_f * xsz);
+        Xd.alloc(static_cast<size_t>(n) * n_f * xsz, s);
         check(cudaMemcpyAsync(Xd.p, X, static_cast<size_t>(n) * n_f * xsz, cudaMemcpyHostToDevice, s), "X upload");
         check(cudaMemcpyAsync(D.y.p, y, sizeof(double) * n, cudaMemcpyHostToDevice, s), "y upload");
         initial_predictions();  // host work while the copies run (they only read X and y)
@@ -445,14 +469,14 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
         stats.t_bin_draws = bt.draws;
         stats.t_bin_edges = bt.edges;
         DBuf<int> ne;
-        ne.alloc(n_f);
+        ne.alloc(n_f, s);
         check(cudaMemcpyAsync(ne.p, n_edges.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "edges upload");
         if (x_dtype == 0) {
             std::vector<float> ef(static_cast<size_t>(n_f) * 256, INFINITY);
             for (int f = 0; f < n_f; ++f)
                 for (int k = 0; k < n_edges[f]; ++k) ef[static_cast<size_t>(f) * 256 + k] = ceil_f32(edges[static_cast<size_t>(f) * 256 + k]);
             DBuf<float> ed;
-            ed.alloc(ef.size());
+            ed.alloc(ef.size(), s);
             check(cudaMemcpyAsync(ed.p, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, s), "edges upload");
             launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s);
             check(cudaStreamSynchronize(s), "transform");
@@ -461,7 +485,7 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
             for (int f = 0; f < n_f; ++f)
                 for (int k = 0; k < n_edges[f]; ++k) ed_h[static_cast<size_t>(f) * 256 + k] = edges[static_cast<size_t>(f) * 256 + k];
             DBuf<double> ed;
-            ed.alloc(ed_h.size());
+            ed.alloc(ed_h.size(), s);
             check(cudaMemcpyAsync(ed.p, ed_h.data(), sizeof(double) * ed_h.size(), cudaMemcpyHostToDevice, s),
                   "edges upload");
             launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s);
@@ -490,10 +514,10 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     for (int k = 0, lo = 0; k < static_cast<int>(bounds.size()); lo = bounds[k], ++k)
         for (int a = lo; a < bounds[k]; a += kChunk) chunks.push_back(make_int4(k, a, std::min(bounds[k], a + kChunk), 0));
     const int n_segments = static_cast<int>(bounds.size());
-    D.seg_sums.alloc(static_cast<size_t>(n_segments) * kMaxNodes * 3);
-    D.chunks.alloc(chunks.size());
-    D.bucket_seg_end.alloc(nbk);
-    D.cuts.alloc(nbk);
+    D.seg_sums.alloc(static_cast<size_t>(n_segments) * kMaxNodes * 3, s);
+    D.chunks.alloc(chunks.size(), s);
+    D.bucket_seg_end.alloc(nbk, s);
+    D.cuts.alloc(nbk, s);
     check(cudaMemcpyAsync(D.chunks.p, chunks.data(), sizeof(int4) * chunks.size(), cudaMemcpyHostToDevice, s), "chunks");
     check(cudaMemcpyAsync(D.bucket_seg_end.p, seg_end.data(), sizeof(int) * nbk, cudaMemcpyHostToDevice, s), "segs");
     std::vector<int> cuts_h = c.iid_mode ? std::vector<int>(1, 0) : cut;
@@ -530,33 +554,33 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
             i = j;
         }
         n_runs = static_cast<int>(rs.size());
-        D.run_start.alloc(n_runs);
-        D.run_len.alloc(n_runs);
-        D.loss_part.alloc(n_runs);
-        D.loss_valid.alloc(n_runs);
+        D.run_start.alloc(n_runs, s);
+        D.run_len.alloc(n_runs, s);
+        D.loss_part.alloc(n_runs, s);
+        D.loss_valid.alloc(n_runs, s);
         check(cudaMemcpyAsync(D.run_start.p, rs.data(), sizeof(int) * n_runs, cudaMemcpyHostToDevice, s), "runs");
         check(cudaMemcpyAsync(D.run_len.p, rl.data(), sizeof(int) * n_runs, cudaMemcpyHostToDevice, s), "runs");
         if (!sorted) {
-            D.order.alloc(n);
+            D.order.alloc(n, s);
             check(cudaMemcpyAsync(D.order.p, ord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s), "order");
             order_d = D.order.p;
         }
         check(cudaStreamSynchronize(s), "runs upload");
     } else {
-        D.loss_part.alloc(2368);
+        D.loss_part.alloc(2368, s);
     }
 
     // GOSS device buffers (the sample itself is set up with the sampler, above).
     if (use_goss) {
-        D.keys_in.alloc(n);
-        D.keys_out.alloc(n);
-        D.vals_in.alloc(n);
-        D.vals_out.alloc(n);
-        D.goss_flag.alloc(n);
-        D.rest_pos.alloc(std::max(1, n_other));
+        D.keys_in.alloc(n, s);
+        D.keys_out.alloc(n, s);
+        D.vals_in.alloc(n, s);
+        D.vals_out.alloc(n, s);
+        D.goss_flag.alloc(n, s);
+        D.rest_pos.alloc(std::max(1, n_other), s);
         const size_t cb = goss_cub_bytes(n, exact_goss);
-        D.cub_tmp.alloc(cb);
-        D.goss_overflow.alloc(1);
+        D.cub_tmp.alloc(cb, s);
+        D.goss_overflow.alloc(1, s);
         check(cudaMemsetAsync(D.goss_overflow.p, 0, sizeof(int), s), "overflow reset");
         launch_goss_iota(D.vals_in.p, n, s);
         sampler->start_workers();
@@ -586,7 +610,7 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     if (timing) {
         check(cudaEventCreate(&ev_begin), "event");
         check(cudaEventCreate(&ev_end), "event");
-        rows_counter.alloc(1);
+        rows_counter.alloc(1, s);
         check(cudaMemsetAsync(rows_counter.p, 0, sizeof(unsigned long long), s), "counter reset");
         if (c.profile_hist) {
             hist_ev.resize(static_cast<size_t>(2) * (timing_end - c.timing_from) * c.max_leaves);
@@ -715,7 +739,8 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
             stats.hist_launches += 1;
         }
         unsigned long long rc = 0;
-        check(cudaMemcpy(&rc, rows_counter.p, sizeof(rc), cudaMemcpyDeviceToHost), "counter");
+        check(cudaMemcpyAsync(&rc, rows_counter.p, sizeof(rc), cudaMemcpyDeviceToHost, s), "counter");
+        check(cudaStreamSynchronize(s), "counter");
         stats.hist_rows = static_cast<long long>(rc);
         cudaEventDestroy(ev_begin);
         cudaEventDestroy(ev_end);
@@ -734,12 +759,16 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     std::vector<double> vals_h(static_cast<size_t>(T) * max_nodes), pre_h(static_cast<size_t>(T) * nbk * max_nodes);
     std::vector<int> cov_h(static_cast<size_t>(T) * max_nodes);
     evals_train.assign(T, 0.0);
-    check(cudaMemcpy(nodes_h.data(), D.nodes_all.p, sizeof(DevNode) * nodes_h.size(), cudaMemcpyDeviceToHost), "D2H");
-    check(cudaMemcpy(st_h.data(), D.st_all.p, sizeof(DevTreeState) * T, cudaMemcpyDeviceToHost), "D2H");
-    check(cudaMemcpy(vals_h.data(), D.values_all.p, sizeof(double) * vals_h.size(), cudaMemcpyDeviceToHost), "D2H");
-    check(cudaMemcpy(pre_h.data(), D.prefix_all.p, sizeof(double) * pre_h.size(), cudaMemcpyDeviceToHost), "D2H");
-    check(cudaMemcpy(cov_h.data(), D.cover_all.p, sizeof(int) * cov_h.size(), cudaMemcpyDeviceToHost), "D2H");
-    check(cudaMemcpy(evals_train.data(), D.losses.p, sizeof(double) * T, cudaMemcpyDeviceToHost), "D2H");
+    check(cudaMemcpyAsync(nodes_h.data(), D.nodes_all.p, sizeof(DevNode) * nodes_h.size(), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(st_h.data(), D.st_all.p, sizeof(DevTreeState) * T, cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(vals_h.data(), D.values_all.p, sizeof(double) * vals_h.size(), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(pre_h.data(), D.prefix_all.p, sizeof(double) * pre_h.size(), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(cov_h.data(), D.cover_all.p, sizeof(int) * cov_h.size(), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(evals_train.data(), D.losses.p, sizeof(double) * T, cudaMemcpyDeviceToHost, s), "D2H");
+    int overflow = 0;
+    if (use_goss && !exact_goss)
+        check(cudaMemcpyAsync(&overflow, D.goss_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, s), "overflow flag");
+    check(cudaStreamSynchronize(s), "D2H");
     trees.assign(T, HostTree());
     for (int t = 0; t < T; ++t) {
         const int nn = st_h[t].n_nodes;
@@ -762,10 +791,10 @@ bool GpuBooster::fit_once(const void* X_in, int x_dtype, const double* y_in, int
     fitted = true;
     D.trees_flat = 0;
     stats.gpu_launches = static_cast<int>(g_kernel_launches.load() - launches0);
+    // The fit's working buffers go back to the pool (ordered on the stream); a fitted model
+    // keeps only its host-side trees and edges, and predict allocates what it needs.
+    D.release_fit_buffers();
     stats.t_total = now() - t0;
-    int overflow = 0;
-    if (use_goss && !exact_goss)
-        check(cudaMemcpy(&overflow, D.goss_overflow.p, sizeof(int), cudaMemcpyDeviceToHost), "overflow flag");
     return overflow != 0;
 }
 
@@ -796,36 +825,38 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
                 v.push_back(t.values[k]);
             }
         }
-        D.t_feat.alloc(f.size());
-        D.t_left.alloc(l.size());
-        D.t_right.alloc(r.size());
-        D.t_thr.alloc(th.size());
-        D.t_ml.alloc(ml.size());
-        D.t_val.alloc(v.size());
-        D.t_off.alloc(std::max<size_t>(1, off.size()));
-        check(cudaMemcpy(D.t_feat.p, f.data(), 2 * f.size(), cudaMemcpyHostToDevice), "trees");
-        check(cudaMemcpy(D.t_left.p, l.data(), 2 * l.size(), cudaMemcpyHostToDevice), "trees");
-        check(cudaMemcpy(D.t_right.p, r.data(), 2 * r.size(), cudaMemcpyHostToDevice), "trees");
-        check(cudaMemcpy(D.t_thr.p, th.data(), th.size(), cudaMemcpyHostToDevice), "trees");
-        check(cudaMemcpy(D.t_ml.p, ml.data(), ml.size(), cudaMemcpyHostToDevice), "trees");
-        check(cudaMemcpy(D.t_val.p, v.data(), 8 * v.size(), cudaMemcpyHostToDevice), "trees");
-        if (!off.empty()) check(cudaMemcpy(D.t_off.p, off.data(), 4 * off.size(), cudaMemcpyHostToDevice), "trees");
+        D.t_feat.alloc(f.size(), s);
+        D.t_left.alloc(l.size(), s);
+        D.t_right.alloc(r.size(), s);
+        D.t_thr.alloc(th.size(), s);
+        D.t_ml.alloc(ml.size(), s);
+        D.t_val.alloc(v.size(), s);
+        D.t_off.alloc(std::max<size_t>(1, off.size()), s);
+        check(cudaMemcpyAsync(D.t_feat.p, f.data(), 2 * f.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaMemcpyAsync(D.t_left.p, l.data(), 2 * l.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaMemcpyAsync(D.t_right.p, r.data(), 2 * r.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaMemcpyAsync(D.t_thr.p, th.data(), th.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaMemcpyAsync(D.t_ml.p, ml.data(), ml.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaMemcpyAsync(D.t_val.p, v.data(), 8 * v.size(), cudaMemcpyHostToDevice, s), "trees");
+        if (!off.empty())
+            check(cudaMemcpyAsync(D.t_off.p, off.data(), 4 * off.size(), cudaMemcpyHostToDevice, s), "trees");
+        check(cudaStreamSynchronize(s), "trees");
         D.trees_flat = trees.size();
     }
     DBuf<unsigned char> Xd;
-    Xd.alloc(static_cast<size_t>(n) * n_f * xsz);
-    D.pcodes.alloc(static_cast<size_t>(n) * stride);
-    D.pout.alloc(n);
+    Xd.alloc(static_cast<size_t>(n) * n_f * xsz, s);
+    D.pcodes.alloc(static_cast<size_t>(n) * stride, s);
+    D.pout.alloc(n, s);
     check(cudaMemcpyAsync(Xd.p, X, static_cast<size_t>(n) * n_f * xsz, cudaMemcpyHostToDevice, s), "X upload");
     DBuf<int> ne;
-    ne.alloc(n_f);
+    ne.alloc(n_f, s);
     check(cudaMemcpyAsync(ne.p, n_edges.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "edges");
     if (x_dtype == 0) {
         std::vector<float> ef(static_cast<size_t>(n_f) * 256, INFINITY);
         for (int ff = 0; ff < n_f; ++ff)
             for (int k = 0; k < n_edges[ff]; ++k) ef[static_cast<size_t>(ff) * 256 + k] = ceil_f32(edges[static_cast<size_t>(ff) * 256 + k]);
         DBuf<float> ed;
-        ed.alloc(ef.size());
+        ed.alloc(ef.size(), s);
         check(cudaMemcpyAsync(ed.p, ef.data(), 4 * ef.size(), cudaMemcpyHostToDevice, s), "edges");
         launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s);
         check(cudaStreamSynchronize(s), "transform");
@@ -834,7 +865,7 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
         for (int ff = 0; ff < n_f; ++ff)
             for (int k = 0; k < n_edges[ff]; ++k) eh[static_cast<size_t>(ff) * 256 + k] = edges[static_cast<size_t>(ff) * 256 + k];
         DBuf<double> ed;
-        ed.alloc(eh.size());
+        ed.alloc(eh.size(), s);
         check(cudaMemcpyAsync(ed.p, eh.data(), 8 * eh.size(), cudaMemcpyHostToDevice, s), "edges");
         launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s);
         check(cudaStreamSynchronize(s), "transform");

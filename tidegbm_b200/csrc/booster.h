@@ -14,7 +14,7 @@ struct TideError : std::runtime_error {
     explicit TideError(const std::string& m) : std::runtime_error(m) {}
 };
 
-// The Config fields (cpp/include/tidegbm/config.hpp:12-113) the GPU path reads.  Every
+// The Config fields (cpp/include/tidegbm/config.hpp:12-97) the GPU path reads.  Every
 // other option keeps its default; options the GPU path does not implement are
 // rejected by validate() with a TideError instead of falling back to the CPU.
 struct Config {

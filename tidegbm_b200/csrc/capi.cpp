@@ -1,6 +1,6 @@
 // extern "C" boundary (include/tidegbm_b200.h).  Every entry catches all exceptions
 // and reports -1 + a thread-local message, like the reference C API
-// (cpp/src/c_api.cpp:12-18, 21-157).
+// (cpp/src/c_api.cpp:12-18, 20-158).
 #include "tidegbm_b200.h"
 
 #include <algorithm>
@@ -422,14 +422,14 @@ int tgb_shuffled_prefix_device(long long m, long long keep, unsigned seed, int* 
         }
         const size_t k = static_cast<size_t>(keep);
         tgb::DBuf<int32_t> scratch;
-        scratch.alloc(3 * k + 1);  // head [k], items [k], cnt [k + 1]
+        scratch.alloc(3 * k + 1, s);  // head [k], items [k], cnt [k + 1]
         int32_t* head = scratch.p;
         int32_t* items = head + k;
         int32_t* cnt = items + k;
         tgb::DBuf<long long> ms_d;
-        ms_d.alloc(1);
+        ms_d.alloc(1, s);
         tgb::DBuf<uint32_t> misc;
-        misc.alloc(2);  // seed, error flag
+        misc.alloc(2, s);  // seed, error flag
         const long long ms = m;
         const uint32_t seed_h = seed;
         int err = 0;

@@ -19,7 +19,6 @@
 // kernels compact flagged rows (GOSS sample) in index order.
 #include "tgb_internal.h"
 
-#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -249,39 +248,29 @@ void launch_compact_flagged(const uint8_t* flag, int n, int32_t* out, int* n_out
 // process that reserves all device memory when it starts and treats any later
 // cudaMalloc as a fault (cudaMalloc can block on the whole device and can fail under
 // memory pressure), or a binding that only passes the input and output buffers of a
-// call.  For them the partition's scratch (one PartJob and the per-tile left counts)
-// lives in this fixed device array instead.  Every GPU that loads the library keeps
-// the array (about 33 KB) until the process exits.  All calls on a device share it and
-// it keeps whatever the last call left: each call writes the job and every tile count
-// it reads before reading them, so nothing has to start at zero, but two calls whose
-// kernels overlap on the GPU (different streams, or different host threads) race on it.
+// call.  For them the partition's only scratch, the per-tile counts of left rows, lives
+// in this fixed device array instead (the job itself travels as a kernel argument).
+// Every GPU that loads the library keeps the array (32 KB) until the process exits.
+// All calls on a device share it and it keeps whatever the last call left: the count
+// kernel writes every tile count the scatter kernel reads, so nothing has to start at
+// zero, but two calls whose kernels overlap on the GPU (different streams, or
+// different host threads) race on it.
 constexpr int kNoAllocMaxRows = 1 << 24;
 constexpr int kNoAllocTiles = kNoAllocMaxRows / kPartTile;
-constexpr size_t kNoAllocJobBytes = 256;
-constexpr size_t kNoAllocBytes = kNoAllocJobBytes + sizeof(int) * (kNoAllocTiles + 1);
-static_assert(sizeof(PartJob) <= kNoAllocJobBytes, "job does not fit its slot");
+constexpr size_t kNoAllocBytes = sizeof(int) * kNoAllocTiles;
 
 static __device__ __align__(256) unsigned char g_partition_scratch[kNoAllocBytes];
 
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
-void* g_scratch_addr[kNoAllocMaxDevices] = {};
-std::mutex g_scratch_mu;
-
 // Device address of g_partition_scratch on the current device.  Host code only sees a
-// host-side stand-in under that name, so the address is looked up once per device,
-// with the device current, on the first call there.
+// host-side stand-in under that name, so the address is looked up with the device
+// current.  The lookup is repeated on every call (it is cheap once the module is loaded),
+// so it stays right after a cudaDeviceReset; the first call on a device may load the
+// module, which is why that first call must not happen inside a stream capture.
 unsigned char* partition_scratch_address() {
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= kNoAllocMaxDevices) throw std::runtime_error("device index out of range");
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (g_scratch_addr[dev] == nullptr) {
-        void* p = nullptr;
-        check(cudaGetSymbolAddress(&p, g_partition_scratch), "cudaGetSymbolAddress(partition scratch)");
-        g_scratch_addr[dev] = p;
-    }
-    return static_cast<unsigned char*>(g_scratch_addr[dev]);
+    void* p = nullptr;
+    check(cudaGetSymbolAddress(&p, g_partition_scratch), "cudaGetSymbolAddress(partition scratch)");
+    return static_cast<unsigned char*>(p);
 }
 }  // namespace
 
@@ -294,7 +283,7 @@ void launch_partition_rows_noalloc(const uint8_t* codes, int stride, const int32
                                  std::to_string(kNoAllocMaxRows) + "], got " + std::to_string(n_rows));
     unsigned char* base = partition_scratch_address();
     launch_partition_rows(codes, stride, rows, n_rows, feature, threshold, missing_left, out, n_left_dev,
-                          reinterpret_cast<int*>(base + kNoAllocJobBytes), s);
+                          reinterpret_cast<int*>(base), s);
 }
 
 }  // namespace tgb

@@ -140,30 +140,39 @@ inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
 
 // Device memory from the current device's stream-ordered pool, which keeps freed blocks
 // for later allocations of the process (repeated fits do not map fresh pages each time).
-// Both calls complete before they return, as cudaMalloc / cudaFree do: the block is usable
-// from any stream, and it is released only once the device is idle.
-void* device_alloc(size_t bytes);
-void device_free(void* p);
+// Both calls are ordered on `s` and do not wait: the block may be used by work queued on
+// `s` after the allocation (other streams only after synchronising with `s`), and it
+// returns to the pool once the work queued on `s` before the free has completed.  No
+// other stream or host thread waits for either call, so boosters on their own streams
+// (the serving loop) never stall one another through allocation.
+void* device_alloc(size_t bytes, cudaStream_t s);
+cudaError_t device_free(void* p, cudaStream_t s);
 
-// Owning device buffer (freed on scope exit).
+// Owning device buffer, allocated and freed in the order of one stream (freed on scope
+// exit: the block returns to the pool once the stream's earlier work is done).
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;
     DBuf() = default;
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    void alloc(size_t k) {
+    void alloc(size_t k, cudaStream_t stream) {
         release();
-        if (k) p = static_cast<T*>(device_alloc(k * sizeof(T)));
+        s = stream;
+        if (k) p = static_cast<T*>(device_alloc(k * sizeof(T), stream));
         n = k;
     }
     void release() {
-        if (p) device_free(p);
+        T* q = p;
         p = nullptr;
         n = 0;
+        if (q) check(device_free(q, s), "cudaFreeAsync");
     }
-    ~DBuf() { release(); }
+    ~DBuf() {
+        if (p) (void)device_free(p, s);  // no throw from a destructor; release() reports errors
+    }
 };
 
 // binning (kernels_bin.cu)
