@@ -47,10 +47,15 @@ TGB_API void tgb_booster_free(tgb_booster* b);
 
 /* tide_set_int / tide_set_double (c_api.cpp:32-70), extended to every Config key the
  * GPU path reads (cpp/include/tidegbm/config.hpp:12-76).  Unknown keys return -1.
- * One int key is this library's own: "hist_bits" = 0 (default: exact 64-bit fixed-point
- * histograms, results match the reference) or 8 (int8 gradients with stochastic rounding,
- * one shared reduction per code: a faster, approximate split search; leaf values stay
- * exact; objective mse only). */
+ * Int keys of this library's own: "hist_bits" = 0 (default: exact 64-bit fixed-point
+ * histograms, results match the reference), 16 or 8 (gradients and hessians
+ * stochastically rounded to int16 / int8 per tree, summed exactly in 32-bit words: fewer
+ * shared reductions per code, an approximate split search; leaf values stay exact);
+ * "grow" = 1 (default: batched waves, many leaves per launch) or 0 (one split per
+ * launch sequence; hist_bits 0, or 8 with objective mse); "graph" = 1 (default: a tree's
+ * waves run as one CUDA graph with a device-side loop) or 0 (enqueued by the host);
+ * "hist_tune" = 1 (default: the histogram's launch shape is tuned on the first tree and
+ * kept for the process) or 0. */
 TGB_API int tgb_set_int(tgb_booster* b, const char* key, long long value);
 TGB_API int tgb_set_double(tgb_booster* b, const char* key, double value);
 /* String keys the reference only sets through pybind (bindings.cpp:78, 115-125):
@@ -63,6 +68,16 @@ TGB_API int tgb_set_str(tgb_booster* b, const char* key, const char* value);
  * objective); entity: host int64 [n] or NULL (sort key after the timestamp). */
 TGB_API int tgb_fit(tgb_booster* b, const void* X, int x_dtype, const double* y, int n, int n_features,
             const long long* timestamps, const long long* entity);
+
+/* Several Booster::fit calls at once (the folds of a walk-forward split, or any set of
+ * fits of one feature count on one device): booster k is fitted on (X[k], y[k], n[k],
+ * timestamps[k], entity[k]) exactly as tgb_fit would fit it, while the trees of all of
+ * them grow in the same batched launches (the boosters' "grow" key must be 1, their
+ * "hist_bits" and objective alike, n_estimators equal; at most 64 boosters).  Each
+ * result equals the booster's own tgb_fit.  timestamps / entity may be NULL as in tgb_fit. */
+TGB_API int tgb_fit_batch(tgb_booster* const* boosters, int n_boosters, const void* const* X, int x_dtype,
+                          const double* const* y, const int* n, int n_features, const long long* const* timestamps,
+                          const long long* const* entity);
 
 /* Booster::predict_raw (cpp/src/booster.cpp:805-811): init_score + lr * sum of tree
  * values, computed on the device.  X host, out host f64 [n]. */
@@ -93,7 +108,10 @@ TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
  * "bin_counts", "bin_draws", "bin_edges" (the device binner's stages), "h2d", "alloc",
  * "transpose", "trees", "pre_upload" / "prep" (host set-up before the upload / before
  * the tree loop), "goss_refits" (1 when the fit was repeated with the full 64-bit GOSS
- * sort).  Unknown names return -1. */
+ * sort), "timed_selects" (wave selects run in the timed range: with batched growth a tree
+ * runs 3 + 5 x (selects - 1) kernels in its waves), "graph_used" (1 when the waves ran as
+ * a CUDA graph), "hist_cluster" / "hist_units" (the tuned launch shape of the histogram:
+ * CTAs per cluster, work units per cluster).  Unknown names return -1. */
 TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);
 
 /* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:
@@ -185,6 +203,19 @@ TGB_API int tgb_bin_transform(const void* X, int x_dtype, int n, int n_features,
 TGB_API int tgb_hist_build(const unsigned char* codes, int stride, int n_features, const int* rows, int n_rows,
                    const double* g, const double* h, int gshift, int hshift, long long* G, long long* H,
                    int* C, void* stream);
+
+/* The histogram of tgb_hist_build through the fit's own per-tree payload and histogram
+ * kernels: hist_bits 0 (exact 64-bit fixed point) or 16 / 8 (g, and h unless h is NULL,
+ * stochastically rounded to int16 / int8 with the fit's scale: the largest |g| of the rows
+ * maps to the largest code; `seed` drives the rounding).  h == NULL: unit hessians.
+ * G, H: device int64 [n_features][256], C int32, zeroed by the caller; scales_out[2]
+ * (host) receives the factors that turn G and H back into gradient units (G * scales_out[0]
+ * is the bin's sum of g).  For measuring the quantisation error of the precision modes.
+ * rows: device int32, every value < the rows of codes / g / h. */
+TGB_API int tgb_hist_build_quantized(const unsigned char* codes, int stride, int n_features, const int* rows,
+                                     int n_rows, const double* g, const double* h, int hist_bits,
+                                     unsigned long long seed, long long* G, long long* H, int* C, double* scales_out,
+                                     void* stream);
 
 /* best_numeric_missing (cpp/src/histogram.cpp:144-193, l1 = 0, no monotone) for every
  * feature of one fixed-point histogram: gain[f], thr[f] (-1 = none), ml[f]. */

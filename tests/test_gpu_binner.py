@@ -116,3 +116,56 @@ def test_device_shuffle_tail_equals_std_shuffle(native, oracle, m, keep, seed):
     L.orc_shuffle_prefix.argtypes = [C.c_int64, C.c_int64, C.c_uint32, C.c_void_p]
     L.orc_shuffle_prefix(m, keep, seed, ref.ctypes.data_as(C.c_void_p))
     assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def _ceil_f32(e):
+    f = e.astype(np.float32)
+    with np.errstate(invalid="ignore"):
+        lower = f.astype(np.float64) < e
+    f[lower] = np.nextafter(f[lower], np.float32(np.inf))
+    return f
+
+
+@pytest.mark.parametrize("dtype,max_bin,bin_sample,n", [(np.float64, 255, 0, 6000), (np.float64, 64, 500, 6000),
+                                                        (np.float32, 255, 500, 6000), (np.float32, 8, 0, 6000),
+                                                        (np.float64, 255, 20000, 90000),
+                                                        (np.float32, 64, 30000, 90000)])
+def test_device_binner_edge_columns_match_oracle(oracle, native, dtype, max_bin, bin_sample, n):
+    """The device binner and transform on edge columns (tests/edge_columns.py): all
+    missing, constant, 254 / 255 distinct, infinities, signed zeros, extreme magnitudes,
+    heavy ties, and +inf with interpolated edges (NaN edges in the reference).  Edges bit
+    for bit (the sign of a zero edge and NaN edges included: features whose edges depend on
+    std::sort's order of equal values are recomputed in the reference's order), then codes
+    bit for bit (the transform runs upper_bound's own bisection, so NaN edges bin as in the
+    reference).  90,000 rows take the device shuffle path."""
+    from edge_columns import edge_columns
+
+    with np.errstate(over="ignore"):
+        X = np.ascontiguousarray(edge_columns(n=n).astype(dtype))
+    nrow, nf = X.shape
+    nb1, e1, n1 = _device_edges(native, X, max_bin, bin_sample, 7)
+    nb2, e2, n2 = _oracle_edges(oracle, X, max_bin, bin_sample, 7)
+    assert nb1 == nb2
+    assert np.array_equal(n1, n2)
+    assert np.array_equal(e1.view(np.uint64), e2.view(np.uint64))
+    # codes through the device transform against the oracle's transform
+    L = oracle.oracle_lib()
+    Xd = np.ascontiguousarray(X, dtype=np.float64)
+    ref = np.zeros(nrow * nf, np.uint8)
+    L.orc_bin_transform(Xd, nrow, nf, np.ascontiguousarray(e2.reshape(-1)), n2, ref, nf)
+    stride = (nf + 15) // 16 * 16
+    if dtype == np.float32:
+        E = np.full((nf, 256), np.inf, dtype=np.float32)
+        for f in range(nf):
+            E[f, : n1[f]] = _ceil_f32(e1[f, : n1[f]])
+    else:
+        E = np.full((nf, 256), np.inf)
+        for f in range(nf):
+            E[f, : n1[f]] = e1[f, : n1[f]]
+    Xt, Et, nt = torch.from_numpy(X).cuda(), torch.from_numpy(E).cuda(), torch.from_numpy(n1).cuda()
+    codes = torch.full((nrow, stride), 77, dtype=torch.uint8, device="cuda")
+    native.check(native.lib().tgb_bin_transform(C.c_void_p(Xt.data_ptr()), 0 if dtype == np.float32 else 1, nrow, nf,
+                                                C.c_void_p(Et.data_ptr()), C.c_void_p(nt.data_ptr()),
+                                                C.c_void_p(codes.data_ptr()), stride, None))
+    torch.cuda.synchronize()
+    assert np.array_equal(codes.cpu().numpy()[:, :nf], ref.reshape(nrow, nf))

@@ -288,3 +288,33 @@ def test_build_hist_gpu_seam_matches_oracle(oracle, native, seed):
             np.add.at(absg[f], codes[idx, f], np.abs(g[idx]))
         assert np.all(np.abs(out[:, :, 0] - ref[:, :, 0]) <= 1e-9 * absg + 1e-300)
         assert np.allclose(out[:, :, 1], ref[:, :, 1], rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("bits,bound", [(0, 1e-9), (16, 1e-3), (8, 3e-2)])
+@pytest.mark.parametrize("var_h", [False, True])
+def test_quantized_histogram_error_vs_fp64(oracle, native, bits, bound, var_h):
+    """tgb_hist_build_quantized (the fit's payload and wave histogram kernels) against the
+    oracle's FP64 build_hist_col: counts exact; max over bins of |G - G_fp64| / sum |g|
+    within the mode's bound (exact: 1e-9; int16: 1e-3; int8: 3e-2), and H likewise against
+    sum h.  Stochastic rounding keeps the error unbiased, so it shrinks like sqrt(rows)."""
+    padded, stride, codes, rows, g, h = _hist_case(3, n=60000, nf=45, n_rows=40000)
+    n, nf = codes.shape
+    G = torch.zeros((nf, 256), dtype=torch.int64, device="cuda")
+    H = torch.zeros_like(G)
+    Cn = torch.zeros((nf, 256), dtype=torch.int32, device="cuda")
+    ct, rt = torch.from_numpy(padded).cuda(), torch.from_numpy(rows).cuda()
+    gt, ht = torch.from_numpy(g).cuda(), torch.from_numpy(h).cuda()
+    sc = np.zeros(2)
+    native.check(native.lib().tgb_hist_build_quantized(dptr(ct), stride, nf, dptr(rt), rows.size, dptr(gt),
+                                                       dptr(ht) if var_h else None, bits, 12345, dptr(G), dptr(H),
+                                                       dptr(Cn), sc.ctypes.data_as(C.c_void_p), None))
+    torch.cuda.synchronize()
+    hh = h if var_h else np.ones(n)
+    ref = np.zeros(nf * 256 * 3)
+    oracle.oracle_lib().orc_build_hist(np.ascontiguousarray(codes), nf, nf, rows, rows.size, g, hh, 256, ref)
+    ref = ref.reshape(nf, 256, 3)
+    assert np.array_equal(Cn.cpu().numpy(), ref[:, :, 2].astype(np.int32))
+    Gd = G.cpu().numpy() * sc[0]
+    Hd = H.cpu().numpy() * sc[1]
+    assert np.max(np.abs(Gd - ref[:, :, 0])) <= bound * np.abs(g[rows]).sum()
+    assert np.max(np.abs(Hd - ref[:, :, 1])) <= bound * np.abs(hh[rows]).sum()

@@ -21,7 +21,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtidegbm_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NO_FMA = {"kernels_split.cu", "kernels_obj.cu", "kernels_post.cu", "kernels_binfit.cu"}
+NO_FMA = {"kernels_split.cu", "kernels_obj.cu", "kernels_post.cu", "kernels_binfit.cu", "kernels_wave_scan.cu"}
 
 
 def _cuda_home() -> str:
@@ -39,7 +39,7 @@ def _sources() -> list[str]:
 def _compile(src: str, nvcc: str, cuda_inc: str) -> str:
     path = os.path.join(CSRC, src)
     obj = os.path.join(BUILD, src + ".o")
-    deps = [path] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".h")] + [
+    deps = [path] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))] + [
         os.path.join(INCLUDE, "tidegbm_b200.h")]
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj

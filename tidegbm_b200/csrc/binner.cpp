@@ -110,9 +110,11 @@ std::vector<double> quantile_edges(std::vector<double>& vals, int n_bins) {
     return e;
 }
 
+// fids: the reference feature index of each column of X (its generator seed), nullptr for
+// columns 0 .. n_f - 1.
 template <typename T>
 int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
-                 std::vector<double>& edges, std::vector<int>& n_edges, int n_threads) {
+                 std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, const int* fids = nullptr) {
     const int n_chunks = std::max(1, std::min(n_threads * 4, (n + 65535) / 65536));
     std::vector<int64_t> bounds(n_chunks + 1);
     for (int c = 0; c <= n_chunks; ++c) bounds[c] = static_cast<int64_t>(n) * c / n_chunks;
@@ -134,7 +136,7 @@ int binner_fit_t(const void* X, int n, int n_f, int max_bin, int bin_sample, uin
         for (int f = 0; f < n_f; ++f) m[f] += counts[static_cast<size_t>(c) * n_f + f];
     parallel_for(n_f, n_threads, [&](int f) {
         if (bin_sample > 0 && m[f] > bin_sample) {
-            Mt32 rng(seed + static_cast<uint32_t>(f) * 2654435761u);  // std::mt19937's stream
+            Mt32 rng(seed + static_cast<uint32_t>(fids ? fids[f] : f) * 2654435761u);  // std::mt19937's stream
             std::vector<int32_t> prefix(static_cast<size_t>(bin_sample));
             shuffled_prefix(m[f], bin_sample, rng, prefix.data());
             std::vector<uint64_t> key(prefix.size());  // (position, shuffled slot), positions distinct
@@ -258,7 +260,7 @@ void binner_plan(const std::vector<int>& ch, int n, int n_f, int bin_sample, uin
 
 int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n, int n_f, int max_bin,
                          int bin_sample, std::vector<double>& edges, std::vector<int>& n_edges, void* stream,
-                         void* arena, size_t arena_bytes) {
+                         void* arena, size_t arena_bytes, std::vector<int>* flagged) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch scratch(arena, arena_bytes, s);
     const size_t nc = static_cast<size_t>(plan.n_chunks) * n_f;
@@ -324,10 +326,12 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     double* ed = scratch.get<double>(static_cast<size_t>(n_f) * 256);
     int* ne = scratch.get<int>(n_f);
     check(cudaMemsetAsync(ed, 0, sizeof(double) * static_cast<size_t>(n_f) * 256, s), "edges reset");
-    launch_quantile_edges(x_dtype, smp_b, smp_a, cap, kept_d, n_f, max_bin - 1, ed, ne, s);
+    int* flags_d = scratch.get<int>(n_f);
+    launch_quantile_edges(x_dtype, smp_b, smp_a, cap, kept_d, n_f, max_bin - 1, ed, ne, flags_d, s);
     edges.assign(static_cast<size_t>(n_f) * 256, 0.0);
     n_edges.assign(n_f, 0);
-    std::vector<int> fill_h(n_f);
+    std::vector<int> fill_h(n_f), flags_h(n_f, 0);
+    check(cudaMemcpyAsync(flags_h.data(), flags_d, sizeof(int) * n_f, cudaMemcpyDeviceToHost, s), "flags download");
     int err_h = 0;
     check(cudaMemcpyAsync(edges.data(), ed, sizeof(double) * edges.size(), cudaMemcpyDeviceToHost, s),
           "edges download");
@@ -338,14 +342,58 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
     if (err_h) throw TideError("device binner: shuffle draws ran past their refill limit");
     for (int f = 0; f < n_f; ++f)
         if (fill_h[f] != kept[f]) throw TideError("device binner: sample size mismatch");
+    if (flagged) {
+        flagged->clear();
+        for (int f = 0; f < n_f; ++f)
+            if (flags_h[f]) flagged->push_back(f);
+    }
     int mx = 2;
     for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + 2);
     return std::max(mx, max_bin);  // Binner::max_bins, binning.cpp:130-134
 }
 
+// Edges of the listed features recomputed on the host from their columns, in the
+// reference's order (the kept sample in its shuffled order, std::sort, std::unique):
+// the features whose edges depend on how std::sort places equal values.  X_host: the
+// row-major X on the host, or nullptr to copy the columns from Xd.
+void binner_refit_features(const std::vector<int>& fids, const void* X_host, const void* Xd, int x_dtype, int n,
+                           int n_f, int max_bin, int bin_sample, uint32_t seed, std::vector<double>& edges,
+                           std::vector<int>& n_edges, int n_threads, cudaStream_t s) {
+    if (fids.empty()) return;
+    const int k = static_cast<int>(fids.size());
+    const size_t xsz = x_dtype == 0 ? 4 : 8;
+    std::vector<unsigned char> cols(static_cast<size_t>(n) * k * xsz);
+    if (X_host) {
+        parallel_for(k, n_threads, [&](int j) {
+            const unsigned char* src = static_cast<const unsigned char*>(X_host) + static_cast<size_t>(fids[j]) * xsz;
+            for (int i = 0; i < n; ++i)
+                std::memcpy(cols.data() + (static_cast<size_t>(i) * k + j) * xsz, src + static_cast<size_t>(i) * n_f * xsz,
+                            xsz);
+        });
+    } else {
+        for (int j = 0; j < k; ++j)
+            check(cudaMemcpy2DAsync(cols.data() + j * xsz, k * xsz,
+                                    static_cast<const unsigned char*>(Xd) + static_cast<size_t>(fids[j]) * xsz,
+                                    static_cast<size_t>(n_f) * xsz, xsz, n, cudaMemcpyDeviceToHost, s),
+                  "column download");
+        check(cudaStreamSynchronize(s), "column download");
+    }
+    std::vector<double> e;
+    std::vector<int> ne;
+    if (x_dtype == 0) binner_fit_t<float>(cols.data(), n, k, max_bin, bin_sample, seed, e, ne, n_threads, fids.data());
+    else binner_fit_t<double>(cols.data(), n, k, max_bin, bin_sample, seed, e, ne, n_threads, fids.data());
+    for (int j = 0; j < k; ++j) {
+        const int f = fids[j];
+        std::fill(edges.begin() + static_cast<size_t>(f) * 256, edges.begin() + static_cast<size_t>(f + 1) * 256, 0.0);
+        std::copy(e.begin() + static_cast<size_t>(j) * 256, e.begin() + static_cast<size_t>(j) * 256 + ne[j],
+                  edges.begin() + static_cast<size_t>(f) * 256);
+        n_edges[f] = ne[j];
+    }
+}
+
 int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                       std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
-                      void* arena, size_t arena_bytes, BinFitTimes* tm) {
+                      void* arena, size_t arena_bytes, BinFitTimes* tm, const void* X_host) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const double t0 = wall_now();
     const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
@@ -362,9 +410,18 @@ int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, 
     BinPlan plan;
     binner_plan(ch, n, n_f, bin_sample, seed, n_threads, plan);
     const double t2 = wall_now();
-    const int nb = binner_fit_from_plan(plan, Xd, x_dtype, n, n_f, max_bin, bin_sample, edges, n_edges, stream, arena,
-                                        arena_bytes);
+    std::vector<int> flagged;
+    int nb = binner_fit_from_plan(plan, Xd, x_dtype, n, n_f, max_bin, bin_sample, edges, n_edges, stream, arena,
+                                  arena_bytes, &flagged);
+    if (!flagged.empty()) {
+        binner_refit_features(flagged, X_host, Xd, x_dtype, n, n_f, max_bin, bin_sample, seed, edges, n_edges,
+                              n_threads, s);
+        int mx = 2;
+        for (int f = 0; f < n_f; ++f) mx = std::max(mx, n_edges[f] + 2);
+        nb = std::max(mx, max_bin);  // Binner::max_bins, binning.cpp:130-134
+    }
     if (tm) {
+        tm->refit_features = static_cast<int>(flagged.size());
         tm->counts = t1 - t0;
         tm->draws = t2 - t1;
         tm->edges = wall_now() - t2;

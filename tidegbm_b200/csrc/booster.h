@@ -56,10 +56,19 @@ struct Config {
     bool causal_structure = false;
     double structure_frac = 1.0;
     double entity_subsample = 1.0;
-    // Histogram precision: 0 = exact 64-bit fixed point (results match the reference), 8 =
-    // int8 gradients with stochastic rounding (one shared reduction per code; approximate
-    // split search, exact leaf values).  8 needs a constant hessian (mse).
+    // Histogram precision: 0 = exact 64-bit fixed point (results match the reference); 16 / 8
+    // = gradients (and hessians) stochastically rounded to int16 / int8 per tree and summed
+    // exactly in 32-bit shared words (fewer shared reductions per code; approximate split
+    // search, exact leaf values).  With grow = 0 only 8 with a constant hessian (mse).
     int hist_bits = 0;
+    // Tree growth: 1 = batched waves (many leaves, and many fits, per launch; wave.h),
+    // 0 = one split per iteration.  Both grow the reference's tree.  graph: the waves of a
+    // tree run as one CUDA graph with a device-side loop (1) or are enqueued by the host (0).
+    int grow = 1;
+    int graph = 1;
+    // Batched growth: tune the histogram's launch shape on the first tree (1), or use the
+    // default (0); the choice is kept per shape of the work for the process.
+    int hist_tune = 1;
     // Measurement hooks (no effect on results): CUDA events around trees
     // [timing_from, timing_to) (timing_to < 0: through the last tree), and per-launch
     // events around every histogram kernel in that range.
@@ -97,9 +106,23 @@ struct FitStats {
     double hist_ms = 0;       // sum of histogram-kernel durations in the timed range
     int hist_launches = 0;
     long long hist_rows = 0;  // rows histogrammed in the timed range
+    long long timed_selects = 0;  // wave selects run in the timed range (batched growth)
+    int graph_used = 0;           // the waves ran as a CUDA graph with a device-side loop
+    int hist_cluster = 0, hist_units = 0;  // the histogram's launch shape (autotuned)
 };
 
 struct DeviceState;  // device buffers of one fit
+struct FitRun;
+
+// One fit's inputs (the arguments of GpuBooster::fit).
+struct FitInput {
+    const void* X;
+    int x_dtype;
+    const double* y;
+    int n, n_f;
+    const int64_t* ts;
+    const int64_t* entity;
+};
 
 class GpuBooster {
 public:
@@ -126,8 +149,13 @@ public:
     void fit(const void* X, int x_dtype, const double* y, int n, int n_f, const int64_t* ts,
              const int64_t* entity);
     void predict_raw(const void* X, int x_dtype, int n, int n_f, double* out);
+    // Fits every booster on its input in lockstep on one device: each tree of all of them
+    // grows in the same wave launches (batched growth; boosters[0]'s stream and timing
+    // hooks).  Each result equals the booster's own fit.
+    static void fit_batch(const std::vector<GpuBooster*>& boosters, const std::vector<FitInput>& inputs);
 
 private:
+    friend struct FitRun;
     // One fit; exact_goss sorts GOSS keys on all 64 bits.  Returns true when the 32-bit
     // GOSS sort met a tied run too long to fix up (the result must then be recomputed).
     bool fit_once(const void* X, int x_dtype, const double* y, int n, int n_f, const int64_t* ts,
@@ -149,6 +177,7 @@ int binner_fit_cat(const void* X, int x_dtype, int n, int n_f, const int* is_cat
 // the sizes involved stays under 2^31 values (else use binner_fit).
 struct BinFitTimes {
     double counts = 0, draws = 0, edges = 0;  // wall seconds of the three stages
+    int refit_features = 0;  // features whose edges were recomputed on the host
 };
 bool binner_fits_device(int n, int n_f, int bin_sample);
 // binner_fit_device's two stages: binner_plan (per-feature totals, rank bases and the
@@ -171,12 +200,15 @@ struct BinPlan {
 };
 void binner_plan(const std::vector<int>& counts, int n, int n_f, int bin_sample, uint32_t seed, int n_threads,
                  BinPlan& plan);
+// flagged (optional): features whose edges depend on how std::sort orders equal values
+// (both zero signs, or infinities with interpolated edges), to be recomputed on the host.
 int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n, int n_f, int max_bin,
                          int bin_sample, std::vector<double>& edges, std::vector<int>& n_edges, void* stream,
-                         void* arena, size_t arena_bytes);
+                         void* arena, size_t arena_bytes, std::vector<int>* flagged = nullptr);
 // arena / arena_bytes: device memory the binner may use as scratch (nullptr: allocate).
+// X_host (optional): the same X on the host, read when features are recomputed there.
 int binner_fit_device(const void* Xd, int x_dtype, int n, int n_f, int max_bin, int bin_sample, uint32_t seed,
                       std::vector<double>& edges, std::vector<int>& n_edges, int n_threads, void* stream,
-                      void* arena, size_t arena_bytes, BinFitTimes* tm);
+                      void* arena, size_t arena_bytes, BinFitTimes* tm, const void* X_host = nullptr);
 
 }  // namespace tgb

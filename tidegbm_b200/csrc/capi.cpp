@@ -16,6 +16,7 @@
 #include "sampling.h"
 #include "serving.h"
 #include "tgb_internal.h"
+#include "wave.h"
 
 namespace tgb {
 extern std::atomic<long long> g_kernel_launches;
@@ -145,6 +146,9 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "timing_to") c.timing_to = static_cast<int>(v);
         else if (k == "hist_bits") c.hist_bits = static_cast<int>(v);
         else if (k == "profile_hist") c.profile_hist = v != 0;
+        else if (k == "grow") c.grow = static_cast<int>(v);
+        else if (k == "graph") c.graph = static_cast<int>(v);
+        else if (k == "hist_tune") c.hist_tune = static_cast<int>(v);
         else if (k == "verbose" || k == "col_major_hist" || k == "cat_min_count") { /* no effect on GPU path */ }
         else throw tgb::TideError("unknown int key");
     });
@@ -201,6 +205,25 @@ int tgb_fit(tgb_booster* hb, const void* X, int x_dtype, const double* y, int n,
         need(hb && X && y, "NULL argument");
         hb->b->fit(X, x_dtype, y, n, n_features, reinterpret_cast<const int64_t*>(timestamps),
                    reinterpret_cast<const int64_t*>(entity));
+    });
+}
+
+int tgb_fit_batch(tgb_booster* const* boosters, int n_boosters, const void* const* X, int x_dtype,
+                  const double* const* y, const int* n, int n_features, const long long* const* timestamps,
+                  const long long* const* entity) {
+    return guard([&] {
+        need(boosters && X && y && n && n_boosters >= 1, "NULL argument");
+        std::vector<tgb::GpuBooster*> bs;
+        std::vector<tgb::FitInput> in;
+        for (int k = 0; k < n_boosters; ++k) {
+            need(boosters[k] && X[k] && y[k], "NULL argument");
+            for (int q = 0; q < k; ++q) need(boosters[q] != boosters[k], "a booster appears twice");
+            bs.push_back(boosters[k]->b);
+            in.push_back(tgb::FitInput{X[k], x_dtype, y[k], n[k], n_features,
+                                       timestamps ? reinterpret_cast<const int64_t*>(timestamps[k]) : nullptr,
+                                       entity ? reinterpret_cast<const int64_t*>(entity[k]) : nullptr});
+        }
+        tgb::GpuBooster::fit_batch(bs, in);
     });
 }
 
@@ -379,6 +402,10 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "trees") *out = s.t_trees;
         else if (k == "total") *out = s.t_total;
         else if (k == "goss_refits") *out = s.goss_refits;
+        else if (k == "timed_selects") *out = static_cast<double>(s.timed_selects);
+        else if (k == "graph_used") *out = s.graph_used;
+        else if (k == "hist_cluster") *out = s.hist_cluster;
+        else if (k == "hist_units") *out = s.hist_units;
         else if (k == "pre_upload") *out = s.t_pre_upload;
         else if (k == "prep") *out = s.t_prep;
         else throw tgb::TideError("unknown fit stat: " + k);
@@ -514,6 +541,73 @@ int tgb_grad_pairwise(const double* y, const double* pred, const int* run_start,
                       int n_runs, int n, double* g, double* h, void* stream) {
     return guard([&] {
         tgb::launch_grad_pairwise(y, pred, run_start, run_len, order, n_runs, n, g, h, as_stream(stream));
+    });
+}
+
+int tgb_hist_build_quantized(const unsigned char* codes, int stride, int n_features, const int* rows, int n_rows,
+                             const double* g, const double* h, int hist_bits, unsigned long long seed, long long* G,
+                             long long* H, int* C, double* scales_out, void* stream) {
+    return guard([&] {
+        need(codes && rows && g && G && H && C && scales_out, "NULL argument");
+        need(stride >= n_features && stride % 16 == 0 && n_features > 0, "bad stride");
+        need(hist_bits == 0 || hist_bits == 8 || hist_bits == 16, "hist_bits must be 0, 8 or 16");
+        need(n_rows >= 0, "n_rows < 0");
+        cudaStream_t s = as_stream(stream);
+        const bool const_h = h == nullptr;
+        const int mode = tgb::hist_mode(hist_bits, const_h);
+        // one root job over the caller's rows, through the fit's own quantise and wave
+        // histogram kernels (a context whose sample is `rows`)
+        tgb::DBuf<tgb::DevTreeState> st;
+        tgb::DBuf<tgb::WaveCtl> ctl;
+        tgb::DBuf<tgb::WaveCtx> wc;
+        tgb::DBuf<unsigned char> gq, hq;
+        int n_max = 0;
+        {
+            std::vector<int> rh(static_cast<size_t>(n_rows));
+            if (n_rows > 0)
+                tgb::check(cudaMemcpyAsync(rh.data(), rows, sizeof(int) * n_rows, cudaMemcpyDeviceToHost, s), "rows");
+            tgb::check(cudaStreamSynchronize(s), "rows");
+            for (int r : rh) n_max = std::max(n_max, r + 1);
+        }
+        st.alloc(1, s);
+        ctl.alloc(1, s);
+        wc.alloc(1, s);
+        gq.alloc(static_cast<size_t>(std::max(1, n_max)) * 8, s);
+        if (mode == tgb::kHistExactVar) hq.alloc(static_cast<size_t>(std::max(1, n_max)) * 8, s);
+        tgb::DevTreeState sh{};
+        sh.n_sample = n_rows;
+        tgb::check(cudaMemsetAsync(ctl.p, 0, sizeof(tgb::WaveCtl), s), "control reset");
+        tgb::check(cudaMemcpyAsync(st.p, &sh, sizeof(sh), cudaMemcpyHostToDevice, s), "state upload");
+        const int one = 1;
+        tgb::check(cudaMemcpyAsync(&ctl.p->active, &one, sizeof(int), cudaMemcpyHostToDevice, s), "control");
+        // sample maxima of |g| and h (the per-tree scales)
+        tgb::DBuf<tgb::AllScale> all;
+        all.alloc(1, s);
+        tgb::check(cudaMemsetAsync(all.p, 0, sizeof(tgb::AllScale), s), "scale reset");
+        tgb::launch_rows_max(rows, n_rows, g, h, all.p, s);
+        tgb::launch_wave_scales(st.p, all.p, mode, s);
+        tgb::launch_wave_quantize(mode, rows, g, h, nullptr, 1.0, st.p, seed, gq.p, hq.p, std::max(1, n_rows), s);
+        tgb::WaveCtx w{};
+        w.codes = codes;
+        w.rows0 = const_cast<int32_t*>(rows);
+        w.gq = gq.p;
+        w.hq = hq.p;
+        w.st = st.p;
+        w.ctl = ctl.p;
+        w.G = G;
+        w.H = H;
+        w.C = C;
+        w.gp.n_features = n_features;
+        w.gp.stride = stride;
+        w.goss_scale = 1.0;
+        tgb::check(cudaMemcpyAsync(wc.p, &w, sizeof(w), cudaMemcpyHostToDevice, s), "context upload");
+        tgb::HistTune tune;
+        tune.clusters = tgb::wave_hist_clusters(tune.cluster);
+        tgb::launch_wave_hist(mode, wc.p, 1, 0, tune, nullptr, s);
+        tgb::check(cudaMemcpyAsync(&sh, st.p, sizeof(sh), cudaMemcpyDeviceToHost, s), "state download");
+        tgb::check(cudaStreamSynchronize(s), "quantised histogram");
+        scales_out[0] = sh.inv_gscale;
+        scales_out[1] = sh.inv_hscale;
     });
 }
 

@@ -1,10 +1,11 @@
 // Quantile-bin transform: X (row-major f32 or f64) -> uint8 codes, row-major
 // [n][stride].  Restates Binner::transform (cpp/src/binning.cpp:104-128):
-// code = 1 + #{edges <= v}, NaN -> 0 (kMissingBin, cpp/include/tidegbm/types.hpp:20).
+// code = 1 + upper_bound(edges, v), NaN -> 0 (kMissingBin, cpp/include/tidegbm/types.hpp:20).
 //
 // For f32 input the edges arrive as ceil_f32(edge) (the smallest float >= the f64
-// edge): for a float v, v >= e  <=>  v >= ceil_f32(e), so the float compare gives
-// the reference's f64 upper_bound exactly.  f64 input compares against f64 edges.
+// edge): for a float v, v < e  <=>  v < ceil_f32(e) (a NaN edge stays NaN), so the float
+// compare gives the reference's f64 upper_bound exactly.  f64 input compares against f64
+// edges.
 //
 // Launch shape: one CTA = 8 warps x a group of 32 features; lane = feature, so a
 // warp reads one row's 32 consecutive values (coalesced) and writes 32 code bytes.
@@ -49,11 +50,20 @@ __global__ void __launch_bounds__(kBinWarps * 32)
         const T v = X[static_cast<size_t>(r) * n_f + f0 + lane];
         int code = 0;
         if (!(v != v)) {
-            int pos = 0;
-#pragma unroll
-            for (int step = 128; step >= 1; step >>= 1)
-                if (e[pos + step - 1] <= v) pos += step;
-            code = min(pos, ne) + 1;
+            // std::upper_bound's own bisection (libstdc++ __upper_bound): the same probes
+            // and the same answer as the reference, also when NaN edges break the order
+            int first = 0, len = ne;
+            while (len > 0) {
+                const int half = len >> 1;
+                const int mid = first + half;
+                if (v < e[mid]) {
+                    len = half;
+                } else {
+                    first = mid + 1;
+                    len = len - half - 1;
+                }
+            }
+            code = first + 1;
         }
         codes[static_cast<size_t>(r) * stride + f0 + lane] = static_cast<uint8_t>(code);
     }

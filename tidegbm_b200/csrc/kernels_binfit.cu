@@ -111,14 +111,26 @@ template <typename T>
 __global__ void __launch_bounds__(kEdgeThreads)
     quantile_edges_kernel(const T* __restrict__ sorted, T* __restrict__ uniq, long long cap,
                           const int* __restrict__ cnt, int n_bins, double* __restrict__ edges,
-                          int* __restrict__ n_edges) {
+                          int* __restrict__ n_edges, int* __restrict__ flags) {
     using BlockScan = cub::BlockScan<int, kEdgeThreads>;
     __shared__ typename BlockScan::TempStorage scan_tmp;
     __shared__ double e[256];
+    __shared__ int both_zeros;
     const int f = blockIdx.x;
     const T* v = sorted + f * cap;
     T* u = uniq + f * cap;
     const int m = cnt[f];
+    // Features whose edges depend on the order std::sort leaves equal values in (the
+    // reference sorts the sample in its shuffled order): a sample holding both -0.0 and
+    // +0.0 (which one std::unique keeps decides the sign of a zero edge), and a sample
+    // holding an infinity when edges are interpolated (inf * 0 makes NaN edges, whose
+    // place after std::sort depends on the algorithm).  flags[f] = 1 sends the feature
+    // back to the host, which recomputes it in the reference's order.
+    if (threadIdx.x == 0) both_zeros = 0;
+    __syncthreads();
+    for (int i = 1 + threadIdx.x; i < m; i += kEdgeThreads)
+        if (v[i] == T(0) && v[i - 1] == T(0) && signbit(v[i]) != signbit(v[i - 1])) both_zeros = 1;
+    __syncthreads();
     // std::sort + std::unique (binning.cpp:15-16): keep the first of every run of equal values
     int n_u = 0;
     for (int i0 = 0; i0 < m; i0 += kEdgeThreads) {
@@ -136,6 +148,10 @@ __global__ void __launch_bounds__(kEdgeThreads)
         __syncthreads();
     }
     double* ef = edges + static_cast<size_t>(f) * 256;
+    if (threadIdx.x == 0) {
+        const bool inf = n_u > n_bins && (isinf(static_cast<double>(u[0])) || isinf(static_cast<double>(u[n_u - 1])));
+        flags[f] = (both_zeros || inf) ? 1 : 0;
+    }
     if (n_u == 0) {  // no values: edges {0.0} (binning.cpp:17)
         if (threadIdx.x == 0) {
             ef[0] = 0.0;
@@ -251,16 +267,16 @@ void launch_sample_sort(int x_dtype, const void* in, void* out, long long total,
 }
 
 void launch_quantile_edges(int x_dtype, const void* sorted, void* uniq, long long cap, const int* cnt, int n_f,
-                           int n_bins, double* edges, int* n_edges, cudaStream_t s) {
+                           int n_bins, double* edges, int* n_edges, int* flags, cudaStream_t s) {
     if (n_f <= 0) return;
     if (x_dtype == 0)
         quantile_edges_kernel<float><<<n_f, kEdgeThreads, 0, s>>>(static_cast<const float*>(sorted),
                                                                   static_cast<float*>(uniq), cap, cnt, n_bins,
-                                                                  edges, n_edges);
+                                                                  edges, n_edges, flags);
     else
         quantile_edges_kernel<double><<<n_f, kEdgeThreads, 0, s>>>(static_cast<const double*>(sorted),
                                                                    static_cast<double*>(uniq), cap, cnt, n_bins,
-                                                                   edges, n_edges);
+                                                                   edges, n_edges, flags);
     check(cudaGetLastError(), "quantile_edges launch");
 }
 

@@ -1,0 +1,350 @@
+// Wave scan and select (wave.h describes the scheme).  Compiled with -fmad=false: the
+// gain arithmetic follows the reference's statement order (scan_common.cuh).
+//
+// scan: one CTA of 256 threads (thread = bin) per (child, feature), grid-stride over the
+// children of all planned leaves of all contexts (or over the roots).  The larger child's
+// histogram is derived as parent - smaller child on the way (subtract_hist_inplace,
+// cpp/src/histogram.cpp:108-117, exact in fixed point).  The last CTA of a child to
+// finish (ticket counter, nothing waits) reduces the per-feature candidates, lowest
+// feature on ties (best_for_leaf, cpp/src/tree.cpp:120-166).
+//
+// select: one warp per context.  It commits expanded best leaves in the reference's
+// best-first order (grow_tree, cpp/src/tree.cpp:343-383) and plans the next wave's
+// expansions; the last context to finish sets the launch-loop condition.
+#include "scan_common.cuh"
+#include "wave.h"
+
+namespace tgb {
+
+namespace {
+
+using namespace scan;
+
+constexpr int kRootCand = 2 * kMaxNodes;  // candidate / ticket index of the root
+
+__device__ __forceinline__ void children_prefix(const WaveCtx* ctxs, int n_ctx, int src, int* s_pref) {
+    if (static_cast<int>(threadIdx.x) < n_ctx) {
+        const WaveCtl* ctl = ctxs[threadIdx.x].ctl;
+        s_pref[threadIdx.x] = src == 0 ? (ctl->active ? 1 : 0) : 2 * ctl->n_exp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = 0; c < n_ctx; ++c) {
+            const int v = s_pref[c];
+            s_pref[c] = acc;
+            acc += v;
+        }
+        s_pref[n_ctx] = acc;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ int s_pref[kMaxWaveCtx + 1];
+    __shared__ ScanShared sm;
+    __shared__ int last;
+    children_prefix(ctxs, n_ctx, src, s_pref);
+    const int total = s_pref[n_ctx];
+    const int f = blockIdx.x;
+    for (int j = blockIdx.y; j < total; j += gridDim.y) {
+        int c = 0;
+        while (c + 1 < n_ctx && s_pref[c + 1] <= j) ++c;
+        const WaveCtx& X = ctxs[c];
+        const GrowParams& p = X.gp;
+        if (f >= p.n_features) continue;  // uniform over the CTA
+        const size_t e = static_cast<size_t>(p.n_features) * kBins;
+        DevNode* N;
+        DevSplit* out;
+        int ci, slot, pslot = 0, sslot = 0;
+        bool derive = false;
+        if (src == 0) {
+            N = X.nodes;
+            out = X.splits;
+            ci = kRootCand;
+            slot = 0;
+        } else {
+            const int k = j - s_pref[c];
+            const int L = X.ctl->exp_leaf[k >> 1];
+            const int side = k & 1;
+            ci = 2 * L + side;
+            N = X.spec + ci;
+            out = X.spec_split + ci;
+            slot = N->slot;
+            const DevNode& A = X.spec[2 * L];
+            const DevNode& B = X.spec[2 * L + 1];
+            const int small = A.count <= B.count ? 0 : 1;  // cpp/src/tree.cpp:423
+            derive = side != small;
+            pslot = X.nodes[L].slot;
+            sslot = X.spec[2 * L + small].slot;
+        }
+        const bool eligible = N->depth < p.max_depth && N->count >= 2 * p.min_samples_leaf;
+        const double inv_gs = X.st->inv_gscale, inv_hs = X.st->inv_hscale;
+        Cand best{-1e300, 0x7fffffff};
+        if (eligible || f == 0) {
+            const size_t fo = static_cast<size_t>(f) * kBins;
+            const size_t so = static_cast<size_t>(slot) * e + fo, po = static_cast<size_t>(pslot) * e + fo,
+                         qo = static_cast<size_t>(sslot) * e + fo;
+            long long Gt, Ht, Ct;
+            best = scan_feature(X.G + so, X.H + so, X.C + so, X.G + po, X.H + po, X.C + po, X.G + qo, X.H + qo,
+                                X.C + qo, derive, eligible, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
+                                p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
+            if (f == 0 && threadIdx.x == 0) {
+                // node totals from feature 0 (every feature's bins sum to the same integers)
+                N->G = Gt;
+                N->H = Ht;
+                N->C = Ct;
+                const double dg = static_cast<double>(Gt) * inv_gs, dh = static_cast<double>(Ht) * inv_hs;
+                N->value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
+            }
+        }
+        if (threadIdx.x == 0) {
+            const size_t cs = static_cast<size_t>(ci) * p.n_features + f;
+            X.cand_gain[cs] = best.gain;
+            X.cand_key[cs] = best.key;
+            __threadfence();
+            last = atomicAdd(&X.tickets[ci], 1) == p.n_features - 1;
+        }
+        __syncthreads();
+        if (last && threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            __threadfence();
+            Cand b{-1e300, 0x7fffffff};
+            for (int k = lane; k < p.n_features; k += 32) {
+                const size_t cs = static_cast<size_t>(ci) * p.n_features + k;
+                const Cand cd{static_cast<volatile double*>(X.cand_gain)[cs], static_cast<volatile int*>(X.cand_key)[cs]};
+                if (better(cd, b)) b = cd;
+            }
+            b = warp_best(b);
+            if (lane == 0) {
+                DevSplit sp;
+                sp.gain = b.gain;
+                sp.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
+                sp.feature = sp.valid ? b.key / 512 : -1;
+                sp.threshold = sp.valid ? (b.key % 512) / 2 : -1;
+                sp.missing_left = sp.valid ? (b.key & 1) : 1;
+                *out = sp;
+                X.tickets[ci] = 0;  // ready for the next launch
+            }
+        }
+        __syncthreads();  // shared state reuse
+    }
+}
+
+// A leaf the reference's selection may pick: depth and size limits, a valid split of gain
+// above min_split_gain (tree.cpp:343-383; the strict '>' against min_split_gain).
+__device__ __forceinline__ bool candidate(const GrowParams& p, const DevNode& N, const DevSplit& S) {
+    return N.is_leaf && N.depth < p.max_depth && N.count >= 2 * p.min_samples_leaf && S.valid &&
+           S.gain > p.min_split_gain;
+}
+
+// better leaf: larger gain, lower id on ties
+__device__ __forceinline__ bool better_leaf(double ga, int ia, double gb, int ib) {
+    return ga > gb || (ga == gb && ia < ib);
+}
+
+__global__ void __launch_bounds__(32)
+    wave_select_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int* gsync, unsigned* host_flag,
+                       cudaGraphConditionalHandle cond, int use_cond) {
+    pdl_wait();
+    pdl_trigger();
+    const WaveCtx& X = ctxs[blockIdx.x];
+    const GrowParams& p = X.gp;
+    WaveCtl* ctl = X.ctl;
+    DevTreeState* st = X.st;
+    DevNode* nodes = X.nodes;
+    DevSplit* splits = X.splits;
+    const int lane = threadIdx.x;
+    __shared__ double s_gain[kMaxLeavesCap + 1];
+    __shared__ int s_id[kMaxLeavesCap + 1];
+    int active = 0;
+    if (ctl->active) {
+        const int budget = p.max_leaves - 1;
+        // every select commits at least one split or ends the tree, so a tree takes at most
+        // max_leaves of them; past that bound the tree is ended with the error flag set
+        const bool runaway = ctl->waves > p.max_leaves + 1;
+        if (lane == 0) ctl->waves += 1;
+        int nn = st->n_nodes;
+        int done_splits = ctl->splits_done;
+        bool finished = false;
+        while (true) {
+            if (done_splits >= budget || runaway) {
+                finished = true;
+                break;
+            }
+            double bg = 0.0;
+            int bi = 0x7fffffff;
+            for (int k = lane; k < nn; k += 32) {
+                const DevSplit S = splits[k];
+                if (!candidate(p, nodes[k], S)) continue;
+                if (bi == 0x7fffffff || better_leaf(S.gain, k, bg, bi)) {
+                    bg = S.gain;
+                    bi = k;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double og = __shfl_xor_sync(0xffffffffu, bg, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (oi != 0x7fffffff && (bi == 0x7fffffff || better_leaf(og, oi, bg, bi))) {
+                    bg = og;
+                    bi = oi;
+                }
+            }
+            if (bi == 0x7fffffff) {
+                finished = true;
+                break;
+            }
+            if (!ctl->expanded[bi]) break;
+            // commit: the split of bi, children ids nn, nn + 1 (grow_tree's numbering)
+            if (lane == 0) {
+                DevNode& P = nodes[bi];
+                const DevSplit S = splits[bi];
+                P.is_leaf = 0;
+                P.feature = S.feature;
+                P.threshold = S.threshold;
+                P.missing_left = S.missing_left;
+                P.gain = S.gain;
+                P.left = nn;
+                P.right = nn + 1;
+                nodes[nn] = X.spec[2 * bi];
+                nodes[nn + 1] = X.spec[2 * bi + 1];
+                splits[nn] = X.spec_split[2 * bi];
+                splits[nn + 1] = X.spec_split[2 * bi + 1];
+                ctl->expanded[nn] = 0;
+                ctl->expanded[nn + 1] = 0;
+            }
+            __syncwarp();
+            __threadfence_block();
+            nn += 2;
+            done_splits += 1;
+        }
+        int n_exp = 0;
+        if (!finished) {
+            // candidates of the new state, best first
+            int nc = 0;
+            for (int k0 = 0; k0 < nn; k0 += 32) {
+                const int k = k0 + lane;
+                bool is_c = false;
+                double gk = 0.0;
+                if (k < nn) {
+                    const DevSplit S = splits[k];
+                    is_c = candidate(p, nodes[k], S);
+                    gk = S.gain;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, is_c);
+                if (is_c) {
+                    const int pos = nc + __popc(m & ((1u << lane) - 1u));
+                    if (pos < kMaxLeavesCap) {
+                        s_gain[pos] = gk;
+                        s_id[pos] = k;
+                    }
+                }
+                nc += __popc(m);
+            }
+            nc = min(nc, kMaxLeavesCap);
+            __syncwarp();
+            const int B = budget - done_splits;
+            // expansions: unexpanded candidates ranked below B; in candidate (node id) order
+            int base_tiles = 0;
+            const int slot_first = 1 + 2 * ctl->exp_counter;
+            for (int i0 = 0; i0 < nc; i0 += 32) {
+                const int i = i0 + lane;
+                bool take = false;
+                if (i < nc) {
+                    int rank = 0;
+                    for (int q = 0; q < nc; ++q)
+                        if (q != i && better_leaf(s_gain[q], s_id[q], s_gain[i], s_id[i])) ++rank;
+                    take = rank < B && !ctl->expanded[s_id[i]];
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, take);
+                int tiles = 0;
+                int e = n_exp + __popc(m & ((1u << lane) - 1u));
+                if (take) {
+                    const int L = s_id[i];
+                    const DevNode& N = nodes[L];
+                    tiles = (N.count + kPartTile - 1) / kPartTile;
+                    ctl->exp_leaf[e] = L;
+                    ctl->expanded[L] = 1;
+                    for (int sd = 0; sd < 2; ++sd) {
+                        DevNode ch{};
+                        ch.start = N.start;
+                        ch.count = 0;
+                        ch.buf = 1 - N.buf;
+                        ch.depth = N.depth + 1;
+                        ch.is_leaf = 1;
+                        ch.feature = -1;
+                        ch.threshold = -1;
+                        ch.missing_left = 1;
+                        ch.left = ch.right = -1;
+                        ch.parent = L;
+                        ch.slot = slot_first + 2 * e + sd;
+                        X.spec[2 * L + sd] = ch;
+                    }
+                }
+                // tile prefix in expansion order
+                int incl = tiles;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (take) ctl->exp_tile0[e] = base_tiles + incl - tiles;
+                base_tiles += __shfl_sync(0xffffffffu, incl, 31);
+                n_exp += __popc(m);
+            }
+            if (lane == 0) {
+                ctl->exp_tile0[n_exp] = base_tiles;
+                ctl->tiles_total = base_tiles;
+                ctl->slot0 = slot_first;
+                ctl->exp_counter += n_exp;
+                if (slot_first + 2 * n_exp > X.n_slots || base_tiles > X.max_tiles) ctl->error = 1;
+            }
+            active = n_exp > 0 && slot_first + 2 * n_exp <= X.n_slots && base_tiles <= X.max_tiles;
+        }
+        if (lane == 0) {
+            if (runaway) ctl->error = 1;
+            st->n_nodes = nn;
+            ctl->splits_done = done_splits;
+            ctl->n_exp = active ? n_exp : 0;
+            if (!active) {
+                ctl->tiles_total = 0;
+                ctl->active = 0;
+                st->done = 1;
+            }
+        }
+    }
+    // launch-loop condition: any context still growing (the last context to finish sets it)
+    if (lane == 0) {
+        if (active) atomicOr(&gsync[0], 1);
+        __threadfence();
+        const int t = atomicAdd(&gsync[1], 1);
+        if (t == n_ctx - 1) {
+            __threadfence();
+            const unsigned v = static_cast<unsigned>(atomicExch(&gsync[0], 0));
+            gsync[1] = 0;
+            gsync[2] += 1;  // selects run (for the count of launched kernels)
+            if (host_flag != nullptr) {
+                *reinterpret_cast<volatile unsigned*>(host_flag) = v;
+                __threadfence_system();
+            }
+            if (use_cond) cudaGraphSetConditional(cond, v);
+        }
+    }
+}
+
+}  // namespace
+
+void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, cudaStream_t s) {
+    launch_pdl(wave_scan_kernel, dim3(max_f, ys), dim3(kScanThreads), 0, s, "wave_scan launch", ctxs, n_ctx, src);
+}
+
+void launch_wave_select(const WaveCtx* ctxs, int n_ctx, int* gsync, unsigned* host_flag, unsigned long long cond,
+                        int use_cond, cudaStream_t s) {
+    launch_pdl(wave_select_kernel, dim3(n_ctx), dim3(32), 0, s, "wave_select launch", ctxs, n_ctx, gsync, host_flag,
+               static_cast<cudaGraphConditionalHandle>(cond), use_cond);
+}
+
+}  // namespace tgb

@@ -24,7 +24,7 @@ constexpr int kPartTile = 2048;  // rows per partition tile
 struct DevNode {
     int32_t start, count, buf, depth;
     int32_t is_leaf, feature, threshold, missing_left;
-    int32_t left, right, parent, pad0;
+    int32_t left, right, parent, slot;  // slot: histogram slot (wave engine)
     double gain;        // split gain (internal nodes)
     double value;       // leaf value from the node's sample sums (Node::value)
     long long G, H, C;  // fixed-point sample sums
@@ -201,8 +201,10 @@ void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long
 size_t sample_sort_bytes(int x_dtype, long long total, int n_f);
 void launch_sample_sort(int x_dtype, const void* in, void* out, long long total, int n_f, const int* seg_begin,
                         const int* seg_end, void* tmp, size_t tmp_bytes, cudaStream_t s);
+// flags[f] = 1: the feature's edges depend on std::sort's order of equal values (both zero
+// signs in the sample, or infinities with interpolated edges); the host recomputes them.
 void launch_quantile_edges(int x_dtype, const void* sorted, void* uniq, long long cap, const int* cnt, int n_f,
-                           int n_bins, double* edges, int* n_edges, cudaStream_t s);
+                           int n_bins, double* edges, int* n_edges, int* flags, cudaStream_t s);
 
 // histograms + tree state (kernels_hist.cu)
 // const_h (mse): reads gq from launch_quantize (int64 per row) or, with q8, from

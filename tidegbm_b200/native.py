@@ -49,6 +49,8 @@ def lib() -> C.CDLL:
         "tgb_set_double": ([vp, cp, d], i),
         "tgb_set_str": ([vp, cp, cp], i),
         "tgb_fit": ([vp, vp, i, vp, i, i, vp, vp], i),
+        "tgb_fit_batch": ([vp, i, vp, i, vp, vp, i, vp, vp], i),
+        "tgb_hist_build_quantized": ([vp, i, i, vp, i, vp, vp, i, C.c_ulonglong, vp, vp, vp, vp, vp], i),
         "tgb_predict_raw": ([vp, vp, i, i, i, vp], i),
         "tgb_model_info": ([vp, vp, vp, vp, vp], i),
         "tgb_init_prefix": ([vp, vp], i),
@@ -105,7 +107,7 @@ def _ptr(a) -> C.c_void_p | None:
 _INT_KEYS = {"n_estimators", "max_depth", "max_leaves", "min_samples_leaf", "max_bin", "n_time_buckets",
              "random_state", "n_jobs", "iid_mode", "halo", "pair_splits", "horizon", "embargo", "goss",
              "bin_sample", "finer_torb", "causal_bins", "causal_structure", "verbose", "col_major_hist",
-             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits"}
+             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune"}
 _DOUBLE_KEYS = {"learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
                 "colsample_bynode", "goss_top", "goss_other", "torb_min_cover", "max_delta_step", "time_decay",
                 "structure_frac", "entity_subsample"}
@@ -179,6 +181,28 @@ class Booster:
         check(lib().tgb_fit(self._h, _ptr(X), dt, _ptr(y), X.shape[0], X.shape[1], _ptr(ts), _ptr(ent)))
         return self
 
+    @staticmethod
+    def fit_batch(boosters, Xs, ys, timestamps=None, entities=None) -> None:
+        """Fits boosters[k] on (Xs[k], ys[k], timestamps[k], entities[k]) in lockstep
+        (tgb_fit_batch): every tree of all of them grows in the same batched launches, and
+        each result equals that booster's own fit.  All X share one dtype and feature count."""
+        k = len(boosters)
+        if not (k == len(Xs) == len(ys)) or k == 0:
+            raise TideError("fit_batch: one X and y per booster")
+        Xs = [np.ascontiguousarray(X, dtype=np.float32 if np.asarray(X).dtype == np.float32 else np.float64)
+              for X in Xs]
+        dt = 0 if Xs[0].dtype == np.float32 else 1
+        if any((X.dtype == np.float32) != (dt == 0) or X.shape[1] != Xs[0].shape[1] for X in Xs):
+            raise TideError("fit_batch: X of one dtype and feature count")
+        ys = [np.ascontiguousarray(y, dtype=np.float64) for y in ys]
+        tss = None if timestamps is None else [np.ascontiguousarray(t, dtype=np.int64) for t in timestamps]
+        ens = None if entities is None else [np.ascontiguousarray(e, dtype=np.int64) for e in entities]
+        arr = lambda seq: (C.c_void_p * k)(*[a.ctypes.data for a in seq])
+        hs = (C.c_void_p * k)(*[b._h.value for b in boosters])
+        ns = (C.c_int * k)(*[X.shape[0] for X in Xs])
+        check(lib().tgb_fit_batch(hs, k, arr(Xs), dt, arr(ys), ns, Xs[0].shape[1],
+                                  arr(tss) if tss is not None else None, arr(ens) if ens is not None else None))
+
     def raw_predict(self, X) -> np.ndarray:
         X = np.asarray(X)
         if X.dtype != np.float32:
@@ -240,7 +264,8 @@ class Booster:
                 "timed_ms", "timed_trees", "timed_launches", "hist_ms", "hist_launches", "hist_rows", "alloc", "h2d",
                 "transpose", "goss_producer"]
         res = dict(zip(keys, o.tolist()))
-        for k in ("bin_counts", "bin_draws", "bin_edges", "goss_refits", "pre_upload", "prep"):
+        for k in ("bin_counts", "bin_draws", "bin_edges", "goss_refits", "pre_upload", "prep", "timed_selects",
+                  "graph_used", "hist_cluster", "hist_units"):
             v = C.c_double()
             check(lib().tgb_fit_stat(self._h, k.encode(), C.byref(v)))
             res[k] = v.value
