@@ -193,9 +193,13 @@ struct DeviceState {
     DBuf<double> cand_gain;
     DBuf<int> cand_key, tickets;
     DBuf<WaveCtx> wctx;
+    DBuf<uint8_t> is_cat;                 // categorical flags per feature (fit and predict)
+    DBuf<unsigned long long> cand_cat;    // scan candidates' left masks
     // predict
     DBuf<uint8_t> pcodes;
     DBuf<int16_t> t_feat, t_left, t_right;
+    DBuf<uint8_t> t_type;
+    DBuf<unsigned long long> t_cat;
     DBuf<uint8_t> t_thr, t_ml;
     DBuf<double> t_val, pout;
     DBuf<int> t_off;
@@ -213,7 +217,7 @@ struct DeviceState {
         values_all.release(); prefix_all.release(); losses.release(); loss_part.release(); cover_all.release();
         loss_valid.release(); run_start.release(); run_len.release(); order.release();
         gqw.release(); hqw.release(); spec.release(); spec_split.release(); ctl.release(); cand_gain.release();
-        cand_key.release(); tickets.release(); wctx.release();
+        cand_key.release(); tickets.release(); wctx.release(); cand_cat.release();
     }
 
 };
@@ -243,7 +247,7 @@ struct FitRun {
     bool exact_goss;
     int n = 0, n_f = 0, stride = 0, T = 0, max_nodes = 0, nbk = 1;
     int n_threads = 1;
-    bool use_goss = false, const_h = true;
+    bool use_goss = false, const_h = true, any_cat = false;
     int n_top = 0, n_other = 0;
     double goss_scale = 1.0;
     std::unique_ptr<GossSampler> sampler;
@@ -305,6 +309,11 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
     const size_t xsz = x_dtype == 0 ? 4 : 8;
     n_threads = c.n_jobs > 0 ? c.n_jobs : std::max(1u, std::thread::hardware_concurrency());
     const_h = c.objective == 0;
+    if (!B.is_cat.empty() && static_cast<int>(B.is_cat.size()) != n_f)
+        throw TideError("categorical flags: one per feature");
+    if (B.is_cat.empty()) B.is_cat.assign(n_f, 0);
+    any_cat = std::any_of(B.is_cat.begin(), B.is_cat.end(), [](int v) { return v != 0; });
+    if (any_cat && c.grow == 0) throw TideError("categorical features need grow = 1 (batched waves)");
     mode = hist_mode(c.hist_bits, const_h);
 
     // ---- (ts, entity) order: booster.cpp:264-309 ----
@@ -489,6 +498,7 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
         D.cand_gain.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * n_f, s);
         D.cand_key.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * n_f, s);
         D.tickets.alloc(2 * kMaxNodes + 1, s);
+        if (any_cat) D.cand_cat.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * n_f * 4, s);
         check(cudaMemsetAsync(D.tickets.p, 0, sizeof(int) * (2 * kMaxNodes + 1), s), "ticket reset");
         check(cudaMemsetAsync(D.ctl.p, 0, sizeof(WaveCtl), s), "wave control reset");
     } else {
@@ -520,7 +530,12 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
         // ---- quantile edges: Binner::fit (binning.cpp:34-102) on the uploaded X ----
         const double tbf = now();
         BinFitTimes bt;
-        if (binner_fits_device(n, n_f, c.bin_sample))
+        if (any_cat) {
+            // vocabularies of the categorical features (binning.cpp:47-84) on the host, the
+            // numeric features' edges with them (the host binner, bit-identical)
+            B.n_bins = binner_fit_cat(X, x_dtype, n, n_f, B.is_cat.data(), c.max_bin, c.cat_min_count, c.bin_sample,
+                                      static_cast<uint32_t>(c.random_state), B.edges, B.n_edges, n_threads);
+        } else if (binner_fits_device(n, n_f, c.bin_sample))
             B.n_bins = binner_fit_device(Xd.p, x_dtype, n, n_f, c.max_bin, c.bin_sample,
                                          static_cast<uint32_t>(c.random_state), B.edges, B.n_edges, n_threads, s,
                                          D.codes_col.p, D.codes_col.n, &bt, X);  // scratch: codes_col, filled later
@@ -535,6 +550,16 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
         DBuf<int> ne;
         ne.alloc(n_f, s);
         check(cudaMemcpyAsync(ne.p, B.n_edges.data(), sizeof(int) * n_f, cudaMemcpyHostToDevice, s), "edges upload");
+        if (any_cat) {
+            // on the booster's own stream: the flags stay with the model for its predicts
+            std::vector<uint8_t> ic(n_f);
+            for (int f = 0; f < n_f; ++f) ic[f] = B.is_cat[f] ? 1 : 0;
+            D.is_cat.alloc(n_f, D.stream);
+            check(cudaMemcpyAsync(D.is_cat.p, ic.data(), n_f, cudaMemcpyHostToDevice, D.stream), "categorical flags");
+            check(cudaStreamSynchronize(D.stream), "categorical flags");
+        } else {
+            D.is_cat.release();
+        }
         if (x_dtype == 0) {
             std::vector<float> ef(static_cast<size_t>(n_f) * 256, INFINITY);
             for (int f = 0; f < n_f; ++f)
@@ -543,7 +568,8 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
             DBuf<float> ed;
             ed.alloc(ef.size(), s);
             check(cudaMemcpyAsync(ed.p, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, s), "edges upload");
-            launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s);
+            launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s,
+                                     D.is_cat.p);
             check(cudaStreamSynchronize(s), "transform");
         } else {
             std::vector<double> ed_h(static_cast<size_t>(n_f) * 256, INFINITY);
@@ -554,7 +580,8 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
             ed.alloc(ed_h.size(), s);
             check(cudaMemcpyAsync(ed.p, ed_h.data(), sizeof(double) * ed_h.size(), cudaMemcpyHostToDevice, s),
                   "edges upload");
-            launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s);
+            launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.codes.p, stride, s,
+                                     D.is_cat.p);
             check(cudaStreamSynchronize(s), "transform");
         }
     }
@@ -695,6 +722,9 @@ WaveCtx FitRun::wave_ctx() const {
     w.goss_scale = use_goss ? goss_scale : 1.0;
     w.n_slots = n_slots;
     w.max_tiles = max_tiles;
+    w.is_cat = D.is_cat.p;
+    w.cand_cat = D.cand_cat.p;
+    w.cat_smooth = c.cat_smooth;
     return w;
 }
 
@@ -848,7 +878,11 @@ bool FitRun::finish() {
         for (int k = 0; k < nn; ++k) {
             const DevNode& d = nodes_h[static_cast<size_t>(t) * max_nodes + k];
             tr.nodes[k] = HostNode{d.is_leaf, d.feature, d.threshold, d.left, d.right, d.missing_left,
-                                   d.count, d.depth, d.value, d.is_leaf ? 0.0 : d.gain};
+                                   d.count, d.depth, d.value, d.is_leaf ? 0.0 : d.gain, 0, {0, 0, 0, 0}};
+            if (!d.is_leaf && d.type == 2) {
+                tr.nodes[k].type = 2;
+                for (int q = 0; q < 4; ++q) tr.nodes[k].cat[q] = d.cat[q];
+            }
         }
         tr.values.assign(vals_h.begin() + static_cast<size_t>(t) * max_nodes,
                          vals_h.begin() + static_cast<size_t>(t) * max_nodes + nn);
@@ -1280,7 +1314,8 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
     // Flattened trees (booster.cpp:744-773 uses tree.values, not the TORB prefixes).
     if (D.trees_flat != trees.size()) {
         std::vector<int16_t> f, l, r;
-        std::vector<uint8_t> th, ml;
+        std::vector<uint8_t> th, ml, ty;
+        std::vector<unsigned long long> cm;
         std::vector<double> v;
         std::vector<int> off;
         for (const auto& t : trees) {
@@ -1292,8 +1327,16 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
                 r.push_back(static_cast<int16_t>(d.right));
                 th.push_back(static_cast<uint8_t>(d.threshold < 0 ? 0 : d.threshold));
                 ml.push_back(static_cast<uint8_t>(d.missing_left));
+                ty.push_back(static_cast<uint8_t>(d.is_leaf ? 0 : d.type));
+                for (int q = 0; q < 4; ++q) cm.push_back(d.cat[q]);
                 v.push_back(t.values[k]);
             }
+        }
+        D.t_type.alloc(std::max<size_t>(1, ty.size()), s);
+        D.t_cat.alloc(std::max<size_t>(4, cm.size()), s);
+        if (!ty.empty()) {
+            check(cudaMemcpyAsync(D.t_type.p, ty.data(), ty.size(), cudaMemcpyHostToDevice, s), "trees");
+            check(cudaMemcpyAsync(D.t_cat.p, cm.data(), 8 * cm.size(), cudaMemcpyHostToDevice, s), "trees");
         }
         D.t_feat.alloc(f.size(), s);
         D.t_left.alloc(l.size(), s);
@@ -1328,7 +1371,8 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
         DBuf<float> ed;
         ed.alloc(ef.size(), s);
         check(cudaMemcpyAsync(ed.p, ef.data(), 4 * ef.size(), cudaMemcpyHostToDevice, s), "edges");
-        launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s);
+        launch_bin_transform_f32(reinterpret_cast<const float*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s,
+                                 D.is_cat.p);
         check(cudaStreamSynchronize(s), "transform");
     } else {
         std::vector<double> eh(static_cast<size_t>(n_f) * 256, INFINITY);
@@ -1337,11 +1381,12 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
         DBuf<double> ed;
         ed.alloc(eh.size(), s);
         check(cudaMemcpyAsync(ed.p, eh.data(), 8 * eh.size(), cudaMemcpyHostToDevice, s), "edges");
-        launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s);
+        launch_bin_transform_f64(reinterpret_cast<const double*>(Xd.p), n, n_f, ed.p, ne.p, D.pcodes.p, stride, s,
+                                 D.is_cat.p);
         check(cudaStreamSynchronize(s), "transform");
     }
     launch_predict_trees(D.pcodes.p, stride, n, D.t_feat.p, D.t_left.p, D.t_right.p, D.t_thr.p, D.t_ml.p, D.t_val.p,
-                         D.t_off.p, static_cast<int>(trees.size()), init_score, cfg.learning_rate, D.pout.p, s);
+                         D.t_off.p, static_cast<int>(trees.size()), init_score, cfg.learning_rate, D.t_type.p, D.t_cat.p, D.pout.p, s);
     check(cudaMemcpyAsync(out, D.pout.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "predict D2H");
     check(cudaStreamSynchronize(s), "predict");
 }

@@ -38,6 +38,8 @@ struct Config {
     double goss_other = 0.1;
     int bin_sample = 262144;
     double torb_min_cover = 0.0;
+    double cat_smooth = 1.0;  // config.hpp:70
+    int cat_min_count = 5;    // config.hpp:72
     bool finer_torb = true;
     int n_jobs = 0;
     std::string device = "gpu";
@@ -82,6 +84,8 @@ struct Config {
 struct HostNode {
     int is_leaf, feature, threshold, left, right, missing_left, n_samples, depth;
     double value, gain;
+    int type;                    // 0 axis, 2 categorical (SplitType, cpp/include/tidegbm/types.hpp:25)
+    unsigned long long cat[4];   // categorical: the codes that go left
 };
 
 struct HostTree {
@@ -145,6 +149,9 @@ public:
     std::vector<HostTree> trees;
     std::vector<double> evals_train;
     FitStats stats;
+    // categorical flag per feature for the next fit (Booster::fit's is_cat,
+    // cpp/src/booster.cpp:246-247); empty: every feature numeric
+    std::vector<int> is_cat;
 
     void fit(const void* X, int x_dtype, const double* y, int n, int n_f, const int64_t* ts,
              const int64_t* entity);

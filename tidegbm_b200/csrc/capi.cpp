@@ -149,7 +149,8 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "grow") c.grow = static_cast<int>(v);
         else if (k == "graph") c.graph = static_cast<int>(v);
         else if (k == "hist_tune") c.hist_tune = static_cast<int>(v);
-        else if (k == "verbose" || k == "col_major_hist" || k == "cat_min_count") { /* no effect on GPU path */ }
+        else if (k == "cat_min_count") c.cat_min_count = static_cast<int>(v);
+        else if (k == "verbose" || k == "col_major_hist") { /* no effect on GPU path */ }
         else throw tgb::TideError("unknown int key");
     });
 }
@@ -170,6 +171,7 @@ int tgb_set_double(tgb_booster* hb, const char* key, double v) {
         else if (k == "goss_top") c.goss_top = v;
         else if (k == "goss_other") c.goss_other = v;
         else if (k == "torb_min_cover") c.torb_min_cover = v;
+        else if (k == "cat_smooth") c.cat_smooth = v;
         else if (k == "max_delta_step") c.max_delta_step = v;
         else if (k == "time_decay") c.time_decay = v;
         else if (k == "structure_frac") c.structure_frac = v;
@@ -265,6 +267,28 @@ int tgb_tree_n_nodes(tgb_booster* hb, int t) {
         return -1;
     }
     return static_cast<int>(hb->b->trees[t].nodes.size());
+}
+
+int tgb_tree_export_split(tgb_booster* hb, int t, int* types, unsigned long long* cat_left) {
+    return guard([&] {
+        need(hb != nullptr, "NULL booster");
+        need(t >= 0 && t < static_cast<int>(hb->b->trees.size()), "tree index out of range");
+        const tgb::HostTree& tr = hb->b->trees[t];
+        for (size_t k = 0; k < tr.nodes.size(); ++k) {
+            if (types) types[k] = tr.nodes[k].is_leaf ? 0 : tr.nodes[k].type;
+            if (cat_left)
+                for (int q = 0; q < 4; ++q) cat_left[4 * k + q] = tr.nodes[k].cat[q];
+        }
+    });
+}
+
+int tgb_set_categorical(tgb_booster* hb, const int* is_cat, int n_features) {
+    return guard([&] {
+        need(hb != nullptr, "NULL booster");
+        need(n_features >= 0, "n_features < 0");
+        if (is_cat == nullptr || n_features == 0) hb->b->is_cat.clear();
+        else hb->b->is_cat.assign(is_cat, is_cat + n_features);
+    });
 }
 
 int tgb_tree_export(tgb_booster* hb, int t, int* inodes, double* fnodes, double* values, int* cover, double* prefix) {

@@ -1,6 +1,7 @@
 // Quantile-bin transform: X (row-major f32 or f64) -> uint8 codes, row-major
 // [n][stride].  Restates Binner::transform (cpp/src/binning.cpp:104-128):
-// code = 1 + upper_bound(edges, v), NaN -> 0 (kMissingBin, cpp/include/tidegbm/types.hpp:20).
+// code = 1 + upper_bound(edges, v), NaN -> 0 (kMissingBin, cpp/include/tidegbm/types.hpp:20);
+// a categorical feature's code is 1 + the value's vocabulary index (0 when absent).
 //
 // For f32 input the edges arrive as ceil_f32(edge) (the smallest float >= the f64
 // edge): for a float v, v < e  <=>  v < ceil_f32(e) (a NaN edge stays NaN), so the float
@@ -26,7 +27,7 @@ template <typename T>
 __global__ void __launch_bounds__(kBinWarps * 32)
     bin_transform_kernel(const T* __restrict__ X, int n, int n_f, const T* __restrict__ edges,
                          const int* __restrict__ n_edges, uint8_t* __restrict__ codes, int stride,
-                         int rows_per_cta) {
+                         int rows_per_cta, const uint8_t* __restrict__ is_cat) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* se = reinterpret_cast<T*>(smem_raw);
     __shared__ int sne[32];
@@ -44,12 +45,28 @@ __global__ void __launch_bounds__(kBinWarps * 32)
     if (lane >= nf_here) return;
     const T* e = se + lane * kEdgeStride;
     const int ne = sne[lane];
+    const bool cat = is_cat != nullptr && is_cat[f0 + lane] != 0;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
     for (int r = r0 + warp; r < r1; r += kBinWarps) {
         const T v = X[static_cast<size_t>(r) * n_f + f0 + lane];
         int code = 0;
-        if (!(v != v)) {
+        if (cat && !(v != v)) {
+            // categorical (binning.cpp:112-117): 1 + the value's index in the sorted
+            // vocabulary (std::lower_bound's bisection), 0 when it is not in it
+            int first = 0, len = ne;
+            while (len > 0) {
+                const int half = len >> 1;
+                const int mid = first + half;
+                if (e[mid] < v) {
+                    first = mid + 1;
+                    len = len - half - 1;
+                } else {
+                    len = half;
+                }
+            }
+            code = (first < ne && e[first] == v) ? first + 1 : 0;
+        } else if (!(v != v)) {
             // std::upper_bound's own bisection (libstdc++ __upper_bound): the same probes
             // and the same answer as the reference, also when NaN edges break the order
             int first = 0, len = ne;
@@ -117,7 +134,7 @@ __global__ void __launch_bounds__(256)
 
 template <typename T>
 void launch_bin(const T* X, int n, int n_f, const T* edges, const int* n_edges, uint8_t* codes,
-                int stride, cudaStream_t s) {
+                int stride, cudaStream_t s, const uint8_t* is_cat) {
     if (n <= 0 || n_f <= 0) return;
     const int rows_per_cta = 512;
     dim3 grid((n + rows_per_cta - 1) / rows_per_cta, (n_f + 31) / 32);
@@ -125,7 +142,7 @@ void launch_bin(const T* X, int n, int n_f, const T* edges, const int* n_edges, 
     auto kern = bin_transform_kernel<T>;
     check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
           "bin smem attr");
-    kern<<<grid, kBinWarps * 32, smem, s>>>(X, n, n_f, edges, n_edges, codes, stride, rows_per_cta);
+    kern<<<grid, kBinWarps * 32, smem, s>>>(X, n, n_f, edges, n_edges, codes, stride, rows_per_cta, is_cat);
     check(cudaGetLastError(), "bin_transform launch");
     if (stride > n_f) {
         zero_pad_kernel<<<1184, 256, 0, s>>>(codes, n, n_f, stride);
@@ -143,13 +160,13 @@ void launch_codes_transpose(const uint8_t* codes, int stride, int n, int n_f, ui
 }
 
 void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
-                              uint8_t* codes, int stride, cudaStream_t s) {
-    launch_bin<float>(X, n, n_f, edges, n_edges, codes, stride, s);
+                              uint8_t* codes, int stride, cudaStream_t s, const uint8_t* is_cat) {
+    launch_bin<float>(X, n, n_f, edges, n_edges, codes, stride, s, is_cat);
 }
 
 void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edges, const int* n_edges,
-                              uint8_t* codes, int stride, cudaStream_t s) {
-    launch_bin<double>(X, n, n_f, edges, n_edges, codes, stride, s);
+                              uint8_t* codes, int stride, cudaStream_t s, const uint8_t* is_cat) {
+    launch_bin<double>(X, n, n_f, edges, n_edges, codes, stride, s, is_cat);
 }
 
 }  // namespace tgb

@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(kApplyThreads)
                        const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
                        unsigned long long* __restrict__ seg_sums) {
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
-    __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes];
+    __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes], s_type[kMaxNodes];
+    __shared__ unsigned long long s_cat[kMaxNodes][4];  // left masks of categorical nodes
     // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
     __shared__ unsigned int aGl[kMaxNodes], aGh[kMaxNodes], aHl[kMaxNodes], aHh[kMaxNodes], aC[kMaxNodes];
     const int nn = st->n_nodes;
@@ -94,6 +95,8 @@ __global__ void __launch_bounds__(kApplyThreads)
         s_right[k] = static_cast<int16_t>(N.right);
         s_thr[k] = static_cast<uint8_t>(N.threshold < 0 ? 0 : N.threshold);
         s_ml[k] = static_cast<uint8_t>(N.missing_left);
+        s_type[k] = static_cast<uint8_t>(N.is_leaf ? 0 : N.type);
+        for (int q = 0; q < 4; ++q) s_cat[k][q] = N.type == 2 ? N.cat[q] : 0ull;
         s_leaf[k] = static_cast<uint8_t>(N.is_leaf);
         aGl[k] = aGh[k] = aHl[k] = aHh[k] = aC[k] = 0u;
     }
@@ -125,7 +128,7 @@ __global__ void __launch_bounds__(kApplyThreads)
 #pragma unroll
             for (int i = 0; i < kApplyRows; ++i) {
                 if (r[i] < 0 || s_leaf[k[i]]) continue;
-                const bool left = b[i] == 0u ? s_ml[k[i]] != 0 : b[i] <= s_thr[k[i]];
+                const bool left = goes_left(s_type[k[i]], s_cat[k[i]], s_thr[k[i]], s_ml[k[i]], b[i]);
                 k[i] = left ? s_left[k[i]] : s_right[k[i]];
             }
         }
@@ -259,6 +262,7 @@ __global__ void predict_trees_kernel(const uint8_t* __restrict__ codes, int stri
                                      const int16_t* __restrict__ right, const uint8_t* __restrict__ thr,
                                      const uint8_t* __restrict__ ml, const double* __restrict__ val,
                                      const int* __restrict__ off, int n_trees, double base, double lr,
+                                     const uint8_t* __restrict__ type, const unsigned long long* __restrict__ cat,
                                      double* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint8_t* row = codes + static_cast<size_t>(i) * stride;
@@ -268,7 +272,8 @@ __global__ void predict_trees_kernel(const uint8_t* __restrict__ codes, int stri
             int k = 0;
             while (feat[o + k] >= 0) {
                 const int b = row[feat[o + k]];
-                const bool go_left = b == 0 ? ml[o + k] != 0 : b <= thr[o + k];
+                const bool go_left = goes_left(type[o + k], cat + 4 * static_cast<size_t>(o + k), thr[o + k],
+                                               ml[o + k], static_cast<unsigned>(b));
                 k = go_left ? left[o + k] : right[o + k];
             }
             s += lr * val[o + k];
@@ -289,11 +294,12 @@ void launch_fill_pred(const double* init_prefix, int n, int n_buckets, int iid_m
 void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t* tree_feat,
                           const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
                           const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
-                          double base, double lr, double* out, cudaStream_t s) {
+                          double base, double lr, const uint8_t* tree_type, const unsigned long long* tree_cat,
+                          double* out, cudaStream_t s) {
     if (n <= 0) return;
     predict_trees_kernel<<<std::max(1, std::min(4736, (n + 127) / 128)), 128, 0, s>>>(
         codes, stride, n, tree_feat, tree_left, tree_right, tree_thr, tree_ml, tree_val, tree_off, n_trees, base,
-        lr, out);
+        lr, tree_type, tree_cat, out);
     check(cudaGetLastError(), "predict_trees launch");
 }
 

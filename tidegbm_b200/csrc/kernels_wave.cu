@@ -487,8 +487,12 @@ __device__ __forceinline__ TileRef find_tile(const WaveCtx* ctxs, const int* s_p
     return r;
 }
 
-__device__ __forceinline__ void load_tile(const WaveCtx& X, const int32_t* in, int feature, int threshold, int ml,
-                                          int base, int end, int32_t (&row)[kPartPer], bool (&left)[kPartPer]) {
+__device__ __forceinline__ void load_tile(const WaveCtx& X, const int32_t* in, const DevSplit& S, int base, int end,
+                                          int32_t (&row)[kPartPer], bool (&left)[kPartPer]) {
+    const int feature = S.feature, threshold = S.threshold, ml = S.missing_left, type = S.type;
+    unsigned long long cat[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cat[k] = S.cat[k];
 #pragma unroll
     for (int i = 0; i < kPartPer; ++i) {
         const int k = base + i * kPartThreads + threadIdx.x;
@@ -500,7 +504,7 @@ __device__ __forceinline__ void load_tile(const WaveCtx& X, const int32_t* in, i
     for (int i = 0; i < kPartPer; ++i) b[i] = row[i] >= 0 ? col[row[i]] : 0u;
 #pragma unroll
     for (int i = 0; i < kPartPer; ++i)
-        left[i] = row[i] >= 0 && (b[i] == 0u ? ml != 0 : static_cast<int>(b[i]) <= threshold);
+        left[i] = row[i] >= 0 && goes_left(type, cat, threshold, ml, b[i]);
 }
 
 __device__ __forceinline__ void load_tile_prefix(const WaveCtx* ctxs, int n_ctx, int* s_pref) {
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(kPartThreads)
         const int base = tr.k * kPartTile, end = min(base + kPartTile, N.count);
         int32_t row[kPartPer];
         bool left[kPartPer];
-        load_tile(X, in, S.feature, S.threshold, S.missing_left, base, end, row, left);
+        load_tile(X, in, S, base, end, row, left);
         int cnt = 0;
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) cnt += left[i] ? 1 : 0;
@@ -605,7 +609,7 @@ __global__ void __launch_bounds__(kPartThreads)
         const int base = tr.k * kPartTile, end = min(base + kPartTile, N.count);
         int32_t row[kPartPer];
         bool left[kPartPer];
-        load_tile(X, in, S.feature, S.threshold, S.missing_left, base, end, row, left);
+        load_tile(X, in, S, base, end, row, left);
         unsigned bal[kPartPer];
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) {

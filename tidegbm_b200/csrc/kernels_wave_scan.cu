@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* 
     pdl_trigger();
     __shared__ int s_pref[kMaxWaveCtx + 1];
     __shared__ ScanShared sm;
+    __shared__ CatShared csm;
     __shared__ int last;
     children_prefix(ctxs, n_ctx, src, s_pref);
     const int total = s_pref[n_ctx];
@@ -82,6 +83,7 @@ __global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* 
         }
         const bool eligible = N->depth < p.max_depth && N->count >= 2 * p.min_samples_leaf;
         const double inv_gs = X.st->inv_gscale, inv_hs = X.st->inv_hscale;
+        const bool cat = X.is_cat != nullptr && X.is_cat[f] != 0;
         Cand best{-1e300, 0x7fffffff};
         if (eligible || f == 0) {
             const size_t fo = static_cast<size_t>(f) * kBins;
@@ -89,8 +91,15 @@ __global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* 
                          qo = static_cast<size_t>(sslot) * e + fo;
             long long Gt, Ht, Ct;
             best = scan_feature(X.G + so, X.H + so, X.C + so, X.G + po, X.H + po, X.C + po, X.G + qo, X.H + qo,
-                                X.C + qo, derive, eligible, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
-                                p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
+                                X.C + qo, derive, eligible && !cat, f, p.n_bins, inv_gs, inv_hs, p.l2,
+                                p.min_split_gain, p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
+            if (cat && eligible) {
+                // best_categorical over the stored (possibly just derived) histogram
+                __syncthreads();
+                best = scan_categorical(X.G + so, X.H + so, X.C + so, f, inv_gs, inv_hs, p.l2, p.min_split_gain,
+                                        p.min_samples_leaf, p.min_child_weight, X.cat_smooth, Gt, Ht, Ct, csm,
+                                        X.cand_cat + (static_cast<size_t>(ci) * p.n_features + f) * 4);
+            }
             if (f == 0 && threadIdx.x == 0) {
                 // node totals from feature 0 (every feature's bins sum to the same integers)
                 N->G = Gt;
@@ -119,12 +128,22 @@ __global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* 
             }
             b = warp_best(b);
             if (lane == 0) {
-                DevSplit sp;
+                DevSplit sp{};
                 sp.gain = b.gain;
                 sp.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
                 sp.feature = sp.valid ? b.key / 512 : -1;
                 sp.threshold = sp.valid ? (b.key % 512) / 2 : -1;
                 sp.missing_left = sp.valid ? (b.key & 1) : 1;
+                sp.type = 0;
+                if (sp.valid && X.is_cat != nullptr && X.is_cat[sp.feature]) {
+                    // categorical: the winning feature's left mask; missing follows bin 0's side
+                    const unsigned long long* m =
+                        X.cand_cat + (static_cast<size_t>(ci) * p.n_features + sp.feature) * 4;
+                    sp.type = 2;
+                    sp.threshold = -1;
+                    for (int k = 0; k < 4; ++k) sp.cat[k] = reinterpret_cast<const volatile unsigned long long*>(m)[k];
+                    sp.missing_left = static_cast<int>(sp.cat[0] & 1ull);
+                }
                 *out = sp;
                 X.tickets[ci] = 0;  // ready for the next launch
             }
@@ -207,6 +226,8 @@ __global__ void __launch_bounds__(32)
                 P.threshold = S.threshold;
                 P.missing_left = S.missing_left;
                 P.gain = S.gain;
+                P.type = S.type;
+                for (int k = 0; k < 4; ++k) P.cat[k] = S.cat[k];
                 P.left = nn;
                 P.right = nn + 1;
                 nodes[nn] = X.spec[2 * bi];

@@ -126,6 +126,227 @@ __device__ __forceinline__ Cand scan_feature(long long* __restrict__ Gf, long lo
     return best;
 }
 
+// ---- categorical features ---------------------------------------------------------------
+//
+// std::sort of libstdc++ (introsort: median-of-three quicksort down to runs of 16, heap
+// sort past 2 * floor(log2 n) levels, then insertion sort), restated step for step so
+// that elements the comparator ties end in the order the reference's std::sort leaves
+// them (best_categorical sorts bins by a ratio that ties for bins of equal sums).  One
+// thread, at most 256 elements in shared memory; less(a, b) compares two elements.
+template <typename Less>
+__device__ void libstdcxx_sort(short* v, int n, Less less) {
+    struct Sorter {
+        short* v;
+        Less less;
+        __device__ void swap(int a, int b) {
+            const short t = v[a];
+            v[a] = v[b];
+            v[b] = t;
+        }
+        __device__ void push_heap(int first, int hole, int top, short value) {
+            int parent = (hole - 1) / 2;
+            while (hole > top && less(v[first + parent], value)) {
+                v[first + hole] = v[first + parent];
+                hole = parent;
+                parent = (hole - 1) / 2;
+            }
+            v[first + hole] = value;
+        }
+        __device__ void adjust_heap(int first, int hole, int len, short value) {
+            const int top = hole;
+            int second = hole;
+            while (second < (len - 1) / 2) {
+                second = 2 * (second + 1);
+                if (less(v[first + second], v[first + second - 1])) --second;
+                v[first + hole] = v[first + second];
+                hole = second;
+            }
+            if ((len & 1) == 0 && second == (len - 2) / 2) {
+                second = 2 * (second + 1);
+                v[first + hole] = v[first + second - 1];
+                hole = second - 1;
+            }
+            push_heap(first, hole, top, value);
+        }
+        __device__ void make_heap(int first, int last) {
+            const int len = last - first;
+            if (len < 2) return;
+            for (int parent = (len - 2) / 2;; --parent) {
+                adjust_heap(first, parent, len, v[first + parent]);
+                if (parent == 0) return;
+            }
+        }
+        __device__ void pop_heap(int first, int last, int result) {
+            const short value = v[result];
+            v[result] = v[first];
+            adjust_heap(first, 0, last - first, value);
+        }
+        __device__ void heap_sort(int first, int last) {  // __partial_sort(first, last, last)
+            make_heap(first, last);
+            while (last - first > 1) {
+                --last;
+                pop_heap(first, last, last);
+            }
+        }
+        __device__ void move_median_to_first(int result, int a, int b, int c) {
+            if (less(v[a], v[b])) {
+                if (less(v[b], v[c])) swap(result, b);
+                else if (less(v[a], v[c])) swap(result, c);
+                else swap(result, a);
+            } else if (less(v[a], v[c])) {
+                swap(result, a);
+            } else if (less(v[b], v[c])) {
+                swap(result, c);
+            } else {
+                swap(result, b);
+            }
+        }
+        __device__ int unguarded_partition(int first, int last, int pivot) {
+            while (true) {
+                while (less(v[first], v[pivot])) ++first;
+                --last;
+                while (less(v[pivot], v[last])) --last;
+                if (!(first < last)) return first;
+                swap(first, last);
+                ++first;
+            }
+        }
+        __device__ void introsort_loop(int first, int last, int depth) {
+            // recursion on the right part, as libstdc++ does; depth <= 2 * log2(256)
+            while (last - first > 16) {
+                if (depth == 0) {
+                    heap_sort(first, last);
+                    return;
+                }
+                --depth;
+                const int mid = first + (last - first) / 2;
+                move_median_to_first(first, first + 1, mid, last - 1);
+                const int cut = unguarded_partition(first + 1, last, first);
+                introsort_loop(cut, last, depth);
+                last = cut;
+            }
+        }
+        __device__ void unguarded_linear_insert(int last) {
+            const short val = v[last];
+            int next = last - 1;
+            while (less(val, v[next])) {
+                v[last] = v[next];
+                last = next;
+                --next;
+            }
+            v[last] = val;
+        }
+        __device__ void insertion_sort(int first, int last) {
+            if (first == last) return;
+            for (int i = first + 1; i != last; ++i) {
+                if (less(v[i], v[first])) {
+                    const short val = v[i];
+                    for (int k = i; k > first; --k) v[k] = v[k - 1];
+                    v[first] = val;
+                } else {
+                    unguarded_linear_insert(i);
+                }
+            }
+        }
+    };
+    if (n < 2) return;
+    Sorter s{v, less};
+    int lg = 31 - __clz(n);
+    s.introsort_loop(0, n, 2 * lg);
+    if (n > 16) {
+        s.insertion_sort(0, 16);
+        for (int i = 16; i < n; ++i) s.unguarded_linear_insert(i);
+    } else {
+        s.insertion_sort(0, n);
+    }
+}
+
+struct CatShared {
+    double key[kBins];   // ranking ratio of each bin
+    short order[kBins];  // non-empty bins, then sorted
+    int nnz;
+    int wcnt[kScanWarps];
+    long long pg[kScanWarps], ph[kScanWarps], pc[kScanWarps];
+    Cand wbest[kScanWarps];
+    unsigned long long mask[4];
+};
+
+// best_categorical (cpp/src/histogram.cpp:195-244, l1 = 0) for one feature of a stored
+// fixed-point histogram (thread b owns bin b): the non-empty bins (the missing bin 0
+// included) ranked by g / (h + cat_smooth) with std::sort's own order, the best prefix
+// of that ranking as the left side (strict '>' over the prefixes: the first best wins).
+// Gt / Ht / Ct: the node's totals.  Returns the candidate (key f * 512) and the left mask.
+static __device__ __noinline__ Cand scan_categorical(const long long* __restrict__ Gf, const long long* __restrict__ Hf,
+                                              const int* __restrict__ Cf, int f, double inv_gs, double inv_hs,
+                                              double lam, double gamma, int min_leaf, double min_hess,
+                                              double cat_smooth, long long Gt, long long Ht, long long Ct,
+                                              CatShared& cs, unsigned long long* mask_out) {
+    const int b = threadIdx.x, lane = b & 31, warp = b >> 5;
+    const double sm = fmax(cat_smooth, 0.0);
+    const long long g = Gf[b], hh = Hf[b];
+    const int c = Cf[b];
+    const bool ne = c > 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, ne);
+    if (lane == 0) cs.wcnt[warp] = __popc(bal);
+    if (b < 4) cs.mask[b] = 0ull;
+    cs.key[b] = (static_cast<double>(g) * inv_gs) / (static_cast<double>(hh) * inv_hs + sm);
+    __syncthreads();
+    int before = 0, nnz = 0;
+#pragma unroll
+    for (int w = 0; w < kScanWarps; ++w) {
+        if (w < warp) before += cs.wcnt[w];
+        nnz += cs.wcnt[w];
+    }
+    if (ne) cs.order[before + __popc(bal & ((1u << lane) - 1u))] = static_cast<short>(b);
+    __syncthreads();
+    Cand best{-1e300, 0x7fffffff};
+    if (nnz < 2) return best;
+    if (b == 0) libstdcxx_sort(cs.order, nnz, [&](short x, short y) { return cs.key[x] < cs.key[y]; });
+    __syncthreads();
+    // prefix sums over the ranking, exact
+    const int o = b < nnz ? cs.order[b] : 0;
+    long long pg = b < nnz ? Gf[o] : 0, ph = b < nnz ? Hf[o] : 0, pc = b < nnz ? Cf[o] : 0;
+    pg = warp_incl_scan(pg, lane);
+    ph = warp_incl_scan(ph, lane);
+    pc = warp_incl_scan(pc, lane);
+    if (lane == 31) {
+        cs.pg[warp] = pg;
+        cs.ph[warp] = ph;
+        cs.pc[warp] = pc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < kScanWarps; ++w)
+        if (w < warp) {
+            pg += cs.pg[w];
+            ph += cs.ph[w];
+            pc += cs.pc[w];
+        }
+    if (b + 1 < nnz) {
+        const long long CL = pc, CR = Ct - pc;
+        const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
+        const double parent = (dGt * dGt) / (dHt + lam);
+        const double GL = static_cast<double>(pg) * inv_gs, HL = static_cast<double>(ph) * inv_hs;
+        const double GR = static_cast<double>(Gt - pg) * inv_gs, HR = static_cast<double>(Ht - ph) * inv_hs;
+        if (!(CL < min_leaf || CR < min_leaf) && !(HL < min_hess || HR < min_hess)) {
+            const double gain = 0.5 * ((GL * GL) / (HL + lam) + (GR * GR) / (HR + lam) - parent) - gamma;
+            best = Cand{gain, b};  // key: the prefix position for now (first best wins)
+        }
+    }
+    best = warp_best(best);
+    if (lane == 0) cs.wbest[warp] = best;
+    __syncthreads();
+    best = cs.wbest[0];
+#pragma unroll
+    for (int w = 1; w < kScanWarps; ++w)
+        if (better(cs.wbest[w], best)) best = cs.wbest[w];
+    if (best.key == 0x7fffffff) return best;
+    if (b <= best.key) atomicOr(&cs.mask[o >> 6], 1ull << (o & 63));
+    __syncthreads();
+    if (b < 4) mask_out[b] = cs.mask[b];
+    return Cand{best.gain, f * 512};
+}
+
 
 }  // namespace scan
 }  // namespace tgb

@@ -28,13 +28,28 @@ struct DevNode {
     double gain;        // split gain (internal nodes)
     double value;       // leaf value from the node's sample sums (Node::value)
     long long G, H, C;  // fixed-point sample sums
-    long long pad1;
+    int32_t type;       // split type (SplitType, cpp/include/tidegbm/types.hpp:25): 0 axis, 2 categorical
+    int32_t pad1;
+    unsigned long long cat[4];  // categorical split: the codes that go left (bit b: code b)
 };
 
 struct DevSplit {
     double gain;
     int feature, threshold, missing_left, valid;
+    int type, pad;
+    unsigned long long cat[4];
 };
+
+// Routing of a code at a split node (cpp/include/tidegbm/tree.hpp:27-30, tree.cpp:15-41):
+// categorical nodes test the code's bit of the left mask, axis nodes send missing (code 0)
+// by the learned direction and codes up to the threshold left.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+inline bool goes_left(int type, const unsigned long long* cat, int threshold, int missing_left, unsigned code) {
+    if (type == 2) return (cat[code >> 6] >> (code & 63)) & 1ull;
+    return code == 0u ? missing_left != 0 : static_cast<int>(code) <= threshold;
+}
 
 struct DevTreeState {
     int n_nodes;
@@ -176,10 +191,12 @@ struct DBuf {
 };
 
 // binning (kernels_bin.cu)
+// is_cat: device flags per feature (nullptr: every feature numeric); a categorical feature's
+// "edges" are its sorted vocabulary.
 void launch_bin_transform_f32(const float* X, int n, int n_f, const float* edges, const int* n_edges,
-                              uint8_t* codes, int stride, cudaStream_t s);
+                              uint8_t* codes, int stride, cudaStream_t s, const uint8_t* is_cat = nullptr);
 void launch_bin_transform_f64(const double* X, int n, int n_f, const double* edges, const int* n_edges,
-                              uint8_t* codes, int stride, cudaStream_t s);
+                              uint8_t* codes, int stride, cudaStream_t s, const uint8_t* is_cat = nullptr);
 
 // device half of Binner::fit (kernels_binfit.cu); X walks use chunks of kFitChunk rows
 constexpr int kFitChunk = 4096;
@@ -310,6 +327,7 @@ void launch_fill_pred(const double* init_prefix, int n, int n_buckets, int iid_m
 void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t* tree_feat,
                           const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
                           const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
-                          double base, double lr, double* out, cudaStream_t s);
+                          double base, double lr, const uint8_t* tree_type, const unsigned long long* tree_cat,
+                          double* out, cudaStream_t s);
 
 }  // namespace tgb

@@ -96,6 +96,11 @@ struct WaveCtx {
     double goss_scale;
     int n_slots;
     int max_tiles;
+    // categorical features (nullptr: none): flags per feature, the left masks of the scan
+    // candidates [(2 * kMaxNodes + 1)][F][4], and the ranking's smoothing (cat_smooth)
+    const uint8_t* is_cat;
+    unsigned long long* cand_cat;
+    double cat_smooth;
 };
 
 // Per-tree set-up of one context: root node (all sampled rows, slot 0), control reset.

@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         "tgb_set_str": ([vp, cp, cp], i),
         "tgb_fit": ([vp, vp, i, vp, i, i, vp, vp], i),
         "tgb_fit_batch": ([vp, i, vp, i, vp, vp, i, vp, vp], i),
+        "tgb_tree_export_split": ([vp, i, vp, vp], i),
+        "tgb_set_categorical": ([vp, vp, i], i),
         "tgb_hist_build_quantized": ([vp, i, i, vp, i, vp, vp, i, C.c_ulonglong, vp, vp, vp, vp, vp], i),
         "tgb_predict_raw": ([vp, vp, i, i, i, vp], i),
         "tgb_model_info": ([vp, vp, vp, vp, vp], i),
@@ -108,7 +110,7 @@ _INT_KEYS = {"n_estimators", "max_depth", "max_leaves", "min_samples_leaf", "max
              "random_state", "n_jobs", "iid_mode", "halo", "pair_splits", "horizon", "embargo", "goss",
              "bin_sample", "finer_torb", "causal_bins", "causal_structure", "verbose", "col_major_hist",
              "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune"}
-_DOUBLE_KEYS = {"learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
+_DOUBLE_KEYS = {"cat_smooth", "learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
                 "colsample_bynode", "goss_top", "goss_other", "torb_min_cover", "max_delta_step", "time_decay",
                 "structure_frac", "entity_subsample"}
 _STR_KEYS = {"objective", "device"}
@@ -130,6 +132,8 @@ class Tree:
     values: np.ndarray
     cover: np.ndarray
     prefix: np.ndarray
+    split_type: np.ndarray | None = None  # 0 axis, 2 categorical
+    cat_left: np.ndarray | None = None    # [n_nodes, 4] uint64 left masks of categorical splits
 
 
 class Booster:
@@ -165,9 +169,12 @@ class Booster:
                 raise TideError(f"unknown config key: {k}")
             self.params[k] = v
 
-    def fit(self, X, y, timestamps=None, entity=None, **kw) -> "Booster":
+    def fit(self, X, y, timestamps=None, entity=None, is_cat=None, **kw) -> "Booster":
+        """is_cat: one flag per feature marking the categorical ones (Booster::fit's is_cat)."""
         if kw:
             self.set_config(**kw)
+        ic = None if is_cat is None else np.ascontiguousarray(is_cat, dtype=np.int32)
+        check(lib().tgb_set_categorical(self._h, _ptr(ic), 0 if ic is None else ic.size))
         X = np.asarray(X)
         if X.ndim != 2:
             raise TideError("X must be 2d")
@@ -246,7 +253,11 @@ class Booster:
             check(lib().tgb_tree_export(self._h, t, _ptr(I), _ptr(F), _ptr(vals), _ptr(cov), _ptr(pre)))
             I = I.reshape(-1, 8)
             F = F.reshape(-1, 2)
-            res.append(Tree(*(I[:, k].copy() for k in range(8)), F[:, 0].copy(), F[:, 1].copy(), vals, cov, pre))
+            ty = np.zeros(nn, np.int32)
+            cm = np.zeros((nn, 4), np.uint64)
+            check(lib().tgb_tree_export_split(self._h, t, _ptr(ty), _ptr(cm)))
+            res.append(Tree(*(I[:, k].copy() for k in range(8)), F[:, 0].copy(), F[:, 1].copy(), vals, cov, pre,
+                            ty, cm))
         return res
 
     def edges(self, f: int) -> np.ndarray:
