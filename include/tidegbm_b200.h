@@ -93,10 +93,12 @@ TGB_API int tgb_tree_n_nodes(tgb_booster* b, int tree);
  * depth}; fnodes[2k] = {value, gain}; values/cover per node; prefix n_buckets x n_nodes. */
 TGB_API int tgb_tree_export(tgb_booster* b, int tree, int* inodes, double* fnodes, double* values, int* cover,
                     double* prefix);
-/* Split type of every node (0 axis, 2 categorical; SplitType, cpp/include/tidegbm/types.hpp:25)
- * and, per node, the 256-bit left mask of a categorical split (cat_left[4k .. 4k+3], bit b:
- * code b goes left; Node::cat_left, cpp/include/tidegbm/tree.hpp:24).  Either may be NULL. */
-TGB_API int tgb_tree_export_split(tgb_booster* b, int tree, int* types, unsigned long long* cat_left);
+/* Split type of every node (0 axis, 1 pair, 2 categorical; SplitType,
+ * cpp/include/tidegbm/types.hpp:25), the second feature of pair splits (-1 otherwise;
+ * Node::feature2) and, per node, the 256-bit left mask of a categorical split
+ * (cat_left[4k .. 4k+3], bit b: code b goes left; Node::cat_left,
+ * cpp/include/tidegbm/tree.hpp:24).  Any output may be NULL. */
+TGB_API int tgb_tree_export_split(tgb_booster* b, int tree, int* types, int* feature2, unsigned long long* cat_left);
 
 /* Categorical features of the next fit (Booster::fit's is_cat, cpp/src/booster.cpp:246-247):
  * is_cat[f] != 0 marks feature f; NULL or n_features 0: every feature numeric.  Their codes

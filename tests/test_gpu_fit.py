@@ -196,10 +196,18 @@ def test_fit_int8_precision_mode(native):
     assert len(a.trees()) == 40 and all(t.is_leaf.sum() >= 2 for t in a.trees())
 
 
-def test_fit_int8_rejects_pairwise(native):
+def test_fit_int8_pairwise_needs_batched_growth(native):
+    """int8 histograms with per-row hessians exist on the batched path only: the one-split
+    loop (grow = 0) rejects them, the default (grow = 1) fits."""
+    X, y, ts = np.random.default_rng(1).standard_normal((2000, 3)).astype(np.float32), np.zeros(2000), \
+        np.repeat(np.arange(20), 100)
+    y[:] = X[:, 0]
     with pytest.raises(native.TideError, match="hist_bits"):
-        native.Booster(iid_mode=1, pair_splits=False, objective="pairwise", hist_bits=8).fit(
-            np.zeros((100, 3), np.float32), np.zeros(100), timestamps=np.arange(100))
+        native.Booster(iid_mode=1, pair_splits=False, objective="pairwise", hist_bits=8, grow=0).fit(X, y,
+                                                                                                     timestamps=ts)
+    b = native.Booster(iid_mode=1, pair_splits=False, objective="pairwise", hist_bits=8, n_estimators=3)
+    b.fit(X, y, timestamps=ts)
+    assert len(b.trees()) == 3
 
 
 def test_fit_iid_float64_input(native, oracle):
@@ -237,7 +245,9 @@ def test_gpu_rejects_unsupported_options(native):
     X = np.zeros((100, 3), np.float32)
     y = np.zeros(100)
     with pytest.raises(native.TideError, match="pair_splits"):
-        native.Booster(iid_mode=1, pair_splits=True).fit(X, y)
+        native.Booster(iid_mode=1, pair_splits=True, grow=0).fit(X, y)  # PAIR needs the batched path
+    with pytest.raises(native.TideError, match="pair_splits"):
+        native.Booster(iid_mode=1, pair_splits=True, hist_bits=8).fit(X, y)  # and exact histograms
     with pytest.raises(native.TideError, match="objective"):
         native.Booster(iid_mode=1, objective="huber")
     with pytest.raises(native.TideError, match="horizon"):

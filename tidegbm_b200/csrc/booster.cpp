@@ -195,9 +195,12 @@ struct DeviceState {
     DBuf<WaveCtx> wctx;
     DBuf<uint8_t> is_cat;                 // categorical flags per feature (fit and predict)
     DBuf<unsigned long long> cand_cat;    // scan candidates' left masks
+    DBuf<DevSplit> splits_pair, spec_split_pair, pair_cand;  // PAIR search (wave.h)
+    DBuf<unsigned long long> energy;
+    DBuf<int> pair_tickets;
     // predict
     DBuf<uint8_t> pcodes;
-    DBuf<int16_t> t_feat, t_left, t_right;
+    DBuf<int16_t> t_feat, t_left, t_right, t_feat2;
     DBuf<uint8_t> t_type;
     DBuf<unsigned long long> t_cat;
     DBuf<uint8_t> t_thr, t_ml;
@@ -217,7 +220,8 @@ struct DeviceState {
         values_all.release(); prefix_all.release(); losses.release(); loss_part.release(); cover_all.release();
         loss_valid.release(); run_start.release(); run_len.release(); order.release();
         gqw.release(); hqw.release(); spec.release(); spec_split.release(); ctl.release(); cand_gain.release();
-        cand_key.release(); tickets.release(); wctx.release(); cand_cat.release();
+        cand_key.release(); tickets.release(); wctx.release(); cand_cat.release(); splits_pair.release();
+        spec_split_pair.release(); pair_cand.release(); energy.release(); pair_tickets.release();
     }
 
 };
@@ -297,7 +301,10 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
         c.pair_splits = false;
     }
     c.validate();
-    if (c.pair_splits) throw TideError("GPU path: pair_splits is not supported; pass pair_splits=False");
+    if (c.pair_splits && (c.grow == 0 || c.hist_bits != 0))
+        throw TideError("GPU path: pair_splits needs grow = 1 and hist_bits = 0 (or pass pair_splits=False)");
+    if (c.pair_splits && (c.pair_top_k > 6 || n_f_in > 1024))
+        throw TideError("GPU path: pair_splits needs pair_top_k <= 6 and at most 1024 features");
     if (c.halo) throw TideError("GPU path: halo is not supported");
     if (n <= 0 || n_f <= 0) throw TideError("empty input");
     if (x_dtype != 0 && x_dtype != 1) throw TideError("x_dtype must be 0 (float32) or 1 (float64)");
@@ -499,6 +506,14 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
         D.cand_key.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * n_f, s);
         D.tickets.alloc(2 * kMaxNodes + 1, s);
         if (any_cat) D.cand_cat.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * n_f * 4, s);
+        if (c.pair_splits) {
+            D.splits_pair.alloc(kMaxNodes, s);
+            D.spec_split_pair.alloc(2 * kMaxNodes, s);
+            D.energy.alloc(2 * kMaxNodes + 1, s);
+            D.pair_cand.alloc(static_cast<size_t>(2 * kMaxNodes + 1) * kMaxPairs, s);
+            D.pair_tickets.alloc(2 * kMaxNodes + 1, s);
+            check(cudaMemsetAsync(D.pair_tickets.p, 0, sizeof(int) * (2 * kMaxNodes + 1), s), "pair ticket reset");
+        }
         check(cudaMemsetAsync(D.tickets.p, 0, sizeof(int) * (2 * kMaxNodes + 1), s), "ticket reset");
         check(cudaMemsetAsync(D.ctl.p, 0, sizeof(WaveCtl), s), "wave control reset");
     } else {
@@ -725,6 +740,18 @@ WaveCtx FitRun::wave_ctx() const {
     w.is_cat = D.is_cat.p;
     w.cand_cat = D.cand_cat.p;
     w.cat_smooth = c.cat_smooth;
+    w.pair_on = c.pair_splits ? 1 : 0;
+    w.pair_top_k = c.pair_top_k;
+    w.max_pair = c.max_pair_splits_per_tree;
+    w.pair_trigger = c.pair_trigger;
+    w.pair_l2 = c.pair_l2;
+    w.g = D.g.p;
+    w.goss_flag = use_goss ? D.goss_flag.p : nullptr;
+    w.splits_pair = D.splits_pair.p;
+    w.spec_split_pair = D.spec_split_pair.p;
+    w.energy = D.energy.p;
+    w.pair_cand = D.pair_cand.p;
+    w.pair_tickets = D.pair_tickets.p;
     return w;
 }
 
@@ -776,6 +803,8 @@ void FitRun::tree_begin(int t) {
     const size_t slot = static_cast<size_t>(n_f) * kBins;
     if (wave) {
         launch_wave_quantize(mode, D.rows0.p, D.g.p, h_rows, flag, goss_scale, D.st.p, seed, D.gqw.p, D.hqw.p, n, s);
+        if (c.pair_splits)
+            check(cudaMemsetAsync(D.energy.p + 2 * kMaxNodes, 0, sizeof(unsigned long long), s), "energy reset");
         // the root's slot; the children's slots are cleared by the partition of their wave
         check(cudaMemsetAsync(D.histG.p, 0, sizeof(long long) * slot, s), "hist reset");
         check(cudaMemsetAsync(D.histH.p, 0, sizeof(long long) * slot, s), "hist reset");
@@ -825,7 +854,7 @@ void FitRun::tree_end(int t) {
     double* prefix_t = D.prefix_all.p + static_cast<size_t>(t) * nbk * max_nodes;
     int* cover_t = D.cover_all.p + static_cast<size_t>(t) * max_nodes;
     launch_apply_accum(D.codes_col.p, codes_col_pitch(n), D.nodes.p, D.st.p, D.g.p, h_rows, D.chunks.p,
-                       static_cast<int>(chunks.size()), D.all_scale.p, D.nid.p, D.seg_sums.p, n_segments, s);
+                       static_cast<int>(chunks.size()), D.all_scale.p, D.nid.p, D.seg_sums.p, n_segments, B.n_bins, s);
     launch_finalize_tree(pp, D.st.p, D.seg_sums.p, D.bucket_seg_end.p, D.cuts.p, D.all_scale.p, values_t, cover_t,
                          prefix_t, s);
     if (const_h) {
@@ -879,9 +908,14 @@ bool FitRun::finish() {
             const DevNode& d = nodes_h[static_cast<size_t>(t) * max_nodes + k];
             tr.nodes[k] = HostNode{d.is_leaf, d.feature, d.threshold, d.left, d.right, d.missing_left,
                                    d.count, d.depth, d.value, d.is_leaf ? 0.0 : d.gain, 0, {0, 0, 0, 0}};
+            tr.nodes[k].feature2 = -1;
             if (!d.is_leaf && d.type == 2) {
                 tr.nodes[k].type = 2;
                 for (int q = 0; q < 4; ++q) tr.nodes[k].cat[q] = d.cat[q];
+            }
+            if (!d.is_leaf && d.type == 1) {
+                tr.nodes[k].type = 1;
+                tr.nodes[k].feature2 = d.feature2;
             }
         }
         tr.values.assign(vals_h.begin() + static_cast<size_t>(t) * max_nodes,
@@ -924,6 +958,7 @@ public:
             max_leaves_ = std::max(max_leaves_, r->c.max_leaves);
             leaves += r->c.max_leaves;
             rows_ += r->n;
+            pair_ = pair_ || r->c.pair_splits;
             if (r->mode != runs_[0]->mode) throw TideError("wave: all contexts of a launch share one histogram mode");
         }
         if (leaves > kMaxWaveJobs) throw TideError("wave: too many leaves over the contexts of one launch");
@@ -1063,6 +1098,7 @@ public:
         };
         hist(0);
         launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, s_);
+        if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 0, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, dflag_, 0ull, 0, s_);
         // waves, enqueued ahead; the flag written by wave w's select is read once wave w
         // has completed (its event), two waves behind the host
@@ -1082,6 +1118,7 @@ public:
             launch_wave_partition(ctx_.p, n_ctx_, part_grid_, s_);
             hist(1);
             launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, s_);
+            if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 1, s_);
             launch_wave_select(ctx_.p, n_ctx_, gsync_.p, dflag_, 0ull, 0, s_);
             check(cudaEventRecord(ev_[w], s_), "event record");
         }
@@ -1107,6 +1144,7 @@ private:
               "graph capture");
         launch_wave_hist(mode_, ctx_.p, n_ctx_, 0, tune_, rows_counter_, s_);
         launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, s_);
+        if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 0, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, nullptr, handle, 1, s_);
         cudaStreamCaptureStatus cs;
         const cudaGraphNode_t* deps = nullptr;
@@ -1130,18 +1168,19 @@ private:
         launch_wave_partition(ctx_.p, n_ctx_, part_grid_, s_);
         launch_wave_hist(mode_, ctx_.p, n_ctx_, 1, tune_, rows_counter_, s_);
         launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, s_);
+        if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 1, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, nullptr, handle, 1, s_);
         cudaGraph_t body_out = nullptr;
         check(cudaStreamEndCapture(s_, &body_out), "body capture end");
         check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
         // launches counted per grow (the graph's kernels are this library's)
-        g_kernel_launches.fetch_sub(8);
+        g_kernel_launches.fetch_sub(pair_ ? 12 : 8);
     }
 
     std::vector<FitRun*> runs_;
     cudaStream_t s_;
     unsigned long long* rows_counter_;
-    bool use_graph_, autotune_, ready_ = false;
+    bool use_graph_, autotune_, ready_ = false, pair_ = false;
     HistTune tune_;
     int n_ctx_ = 0, max_f_ = 0, max_leaves_ = 0, mode_ = 0, part_grid_ = 0, scan_ys_ = 0;
     long long rows_ = 0;
@@ -1313,7 +1352,7 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
     const size_t xsz = x_dtype == 0 ? 4 : 8;
     // Flattened trees (booster.cpp:744-773 uses tree.values, not the TORB prefixes).
     if (D.trees_flat != trees.size()) {
-        std::vector<int16_t> f, l, r;
+        std::vector<int16_t> f, l, r, f2;
         std::vector<uint8_t> th, ml, ty;
         std::vector<unsigned long long> cm;
         std::vector<double> v;
@@ -1328,10 +1367,13 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
                 th.push_back(static_cast<uint8_t>(d.threshold < 0 ? 0 : d.threshold));
                 ml.push_back(static_cast<uint8_t>(d.missing_left));
                 ty.push_back(static_cast<uint8_t>(d.is_leaf ? 0 : d.type));
+                f2.push_back(static_cast<int16_t>(!d.is_leaf && d.type == 1 ? d.feature2 : 0));
                 for (int q = 0; q < 4; ++q) cm.push_back(d.cat[q]);
                 v.push_back(t.values[k]);
             }
         }
+        D.t_feat2.alloc(std::max<size_t>(1, f2.size()), s);
+        if (!f2.empty()) check(cudaMemcpyAsync(D.t_feat2.p, f2.data(), 2 * f2.size(), cudaMemcpyHostToDevice, s), "trees");
         D.t_type.alloc(std::max<size_t>(1, ty.size()), s);
         D.t_cat.alloc(std::max<size_t>(4, cm.size()), s);
         if (!ty.empty()) {
@@ -1386,7 +1428,8 @@ void GpuBooster::predict_raw(const void* X, int x_dtype, int n, int n_f, double*
         check(cudaStreamSynchronize(s), "transform");
     }
     launch_predict_trees(D.pcodes.p, stride, n, D.t_feat.p, D.t_left.p, D.t_right.p, D.t_thr.p, D.t_ml.p, D.t_val.p,
-                         D.t_off.p, static_cast<int>(trees.size()), init_score, cfg.learning_rate, D.t_type.p, D.t_cat.p, D.pout.p, s);
+                         D.t_off.p, static_cast<int>(trees.size()), init_score, cfg.learning_rate, D.t_type.p, D.t_cat.p, D.t_feat2.p,
+                         n_bins, D.pout.p, s);
     check(cudaMemcpyAsync(out, D.pout.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "predict D2H");
     check(cudaStreamSynchronize(s), "predict");
 }

@@ -44,9 +44,13 @@ struct Config {
     int n_jobs = 0;
     std::string device = "gpu";
     // Options that exist in the reference but are not implemented on the GPU path.
-    // pair_splits defaults to true as in the reference (config.hpp:31); the fit
-    // rejects it unless n >= 1M, where the reference itself turns it off.
+    // pair_splits defaults to true as in the reference (config.hpp:31), off at n >= 1M as
+    // the reference turns it off there; PAIR needs batched growth and exact histograms.
     bool pair_splits = true;
+    double pair_trigger = 0.25;      // config.hpp:32-35
+    int pair_top_k = 6;
+    int max_pair_splits_per_tree = 3;
+    double pair_l2 = 2.0;
     bool halo = false;
     double subsample = 1.0;
     double colsample = 1.0;
@@ -84,8 +88,9 @@ struct Config {
 struct HostNode {
     int is_leaf, feature, threshold, left, right, missing_left, n_samples, depth;
     double value, gain;
-    int type;                    // 0 axis, 2 categorical (SplitType, cpp/include/tidegbm/types.hpp:25)
+    int type;                    // 0 axis, 1 pair, 2 categorical (SplitType, cpp/include/tidegbm/types.hpp:25)
     unsigned long long cat[4];   // categorical: the codes that go left
+    int feature2;                // pair: the second feature
 };
 
 struct HostTree {

@@ -150,6 +150,8 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "graph") c.graph = static_cast<int>(v);
         else if (k == "hist_tune") c.hist_tune = static_cast<int>(v);
         else if (k == "cat_min_count") c.cat_min_count = static_cast<int>(v);
+        else if (k == "pair_top_k") c.pair_top_k = static_cast<int>(v);
+        else if (k == "max_pair_splits_per_tree") c.max_pair_splits_per_tree = static_cast<int>(v);
         else if (k == "verbose" || k == "col_major_hist") { /* no effect on GPU path */ }
         else throw tgb::TideError("unknown int key");
     });
@@ -172,6 +174,8 @@ int tgb_set_double(tgb_booster* hb, const char* key, double v) {
         else if (k == "goss_other") c.goss_other = v;
         else if (k == "torb_min_cover") c.torb_min_cover = v;
         else if (k == "cat_smooth") c.cat_smooth = v;
+        else if (k == "pair_trigger") c.pair_trigger = v;
+        else if (k == "pair_l2") c.pair_l2 = v;
         else if (k == "max_delta_step") c.max_delta_step = v;
         else if (k == "time_decay") c.time_decay = v;
         else if (k == "structure_frac") c.structure_frac = v;
@@ -269,13 +273,14 @@ int tgb_tree_n_nodes(tgb_booster* hb, int t) {
     return static_cast<int>(hb->b->trees[t].nodes.size());
 }
 
-int tgb_tree_export_split(tgb_booster* hb, int t, int* types, unsigned long long* cat_left) {
+int tgb_tree_export_split(tgb_booster* hb, int t, int* types, int* feature2, unsigned long long* cat_left) {
     return guard([&] {
         need(hb != nullptr, "NULL booster");
         need(t >= 0 && t < static_cast<int>(hb->b->trees.size()), "tree index out of range");
         const tgb::HostTree& tr = hb->b->trees[t];
         for (size_t k = 0; k < tr.nodes.size(); ++k) {
             if (types) types[k] = tr.nodes[k].is_leaf ? 0 : tr.nodes[k].type;
+            if (feature2) feature2[k] = tr.nodes[k].is_leaf ? -1 : tr.nodes[k].feature2;
             if (cat_left)
                 for (int q = 0; q < 4; ++q) cat_left[4 * k + q] = tr.nodes[k].cat[q];
         }

@@ -81,9 +81,10 @@ __global__ void __launch_bounds__(kApplyThreads)
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
                        const double* __restrict__ h, const int4* __restrict__ chunks,
                        const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
-                       unsigned long long* __restrict__ seg_sums) {
+                       unsigned long long* __restrict__ seg_sums, int n_bins) {
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
     __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes], s_type[kMaxNodes];
+    __shared__ int16_t s_feat2[kMaxNodes];
     __shared__ unsigned long long s_cat[kMaxNodes][4];  // left masks of categorical nodes
     // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
     __shared__ unsigned int aGl[kMaxNodes], aGh[kMaxNodes], aHl[kMaxNodes], aHh[kMaxNodes], aC[kMaxNodes];
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(kApplyThreads)
         s_thr[k] = static_cast<uint8_t>(N.threshold < 0 ? 0 : N.threshold);
         s_ml[k] = static_cast<uint8_t>(N.missing_left);
         s_type[k] = static_cast<uint8_t>(N.is_leaf ? 0 : N.type);
+        s_feat2[k] = static_cast<int16_t>(!N.is_leaf && N.type == 1 ? N.feature2 : 0);
         for (int q = 0; q < 4; ++q) s_cat[k][q] = N.type == 2 ? N.cat[q] : 0ull;
         s_leaf[k] = static_cast<uint8_t>(N.is_leaf);
         aGl[k] = aGh[k] = aHl[k] = aHh[k] = aC[k] = 0u;
@@ -116,19 +118,21 @@ __global__ void __launch_bounds__(kApplyThreads)
             if (!ok) r[i] = -1;
         }
         for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
-            unsigned int b[kApplyRows];
+            unsigned int b[kApplyRows], b2[kApplyRows];
             bool any = false;
 #pragma unroll
             for (int i = 0; i < kApplyRows; ++i) {
                 const bool walk = r[i] >= 0 && !s_leaf[k[i]];
                 b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
+                b2[i] = walk && s_type[k[i]] == 1 ? __ldg(col + static_cast<long long>(s_feat2[k[i]]) * pitch + r[i])
+                                                  : 0u;
                 any |= walk;
             }
             if (!any) break;
 #pragma unroll
             for (int i = 0; i < kApplyRows; ++i) {
                 if (r[i] < 0 || s_leaf[k[i]]) continue;
-                const bool left = goes_left(s_type[k[i]], s_cat[k[i]], s_thr[k[i]], s_ml[k[i]], b[i]);
+                const bool left = goes_left(s_type[k[i]], s_cat[k[i]], s_thr[k[i]], s_ml[k[i]], b[i], b2[i], n_bins);
                 k[i] = left ? s_left[k[i]] : s_right[k[i]];
             }
         }
@@ -263,7 +267,7 @@ __global__ void predict_trees_kernel(const uint8_t* __restrict__ codes, int stri
                                      const uint8_t* __restrict__ ml, const double* __restrict__ val,
                                      const int* __restrict__ off, int n_trees, double base, double lr,
                                      const uint8_t* __restrict__ type, const unsigned long long* __restrict__ cat,
-                                     double* __restrict__ out) {
+                                     const int16_t* __restrict__ feat2, int n_bins, double* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint8_t* row = codes + static_cast<size_t>(i) * stride;
         double s = base;
@@ -272,8 +276,9 @@ __global__ void predict_trees_kernel(const uint8_t* __restrict__ codes, int stri
             int k = 0;
             while (feat[o + k] >= 0) {
                 const int b = row[feat[o + k]];
+                const int b2 = type[o + k] == 1 ? row[feat2[o + k]] : 0;
                 const bool go_left = goes_left(type[o + k], cat + 4 * static_cast<size_t>(o + k), thr[o + k],
-                                               ml[o + k], static_cast<unsigned>(b));
+                                               ml[o + k], static_cast<unsigned>(b), static_cast<unsigned>(b2), n_bins);
                 k = go_left ? left[o + k] : right[o + k];
             }
             s += lr * val[o + k];
@@ -295,11 +300,11 @@ void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t
                           const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
                           const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
                           double base, double lr, const uint8_t* tree_type, const unsigned long long* tree_cat,
-                          double* out, cudaStream_t s) {
+                          const int16_t* tree_feat2, int n_bins, double* out, cudaStream_t s) {
     if (n <= 0) return;
     predict_trees_kernel<<<std::max(1, std::min(4736, (n + 127) / 128)), 128, 0, s>>>(
         codes, stride, n, tree_feat, tree_left, tree_right, tree_thr, tree_ml, tree_val, tree_off, n_trees, base,
-        lr, tree_type, tree_cat, out);
+        lr, tree_type, tree_cat, tree_feat2, n_bins, out);
     check(cudaGetLastError(), "predict_trees launch");
 }
 
@@ -325,11 +330,11 @@ void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cud
 void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks,
                         const AllScale* sc, int16_t* nid, unsigned long long* seg_sums, int n_segments,
-                        cudaStream_t s) {
+                        int n_bins, cudaStream_t s) {
     check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
           "seg sums reset");
     apply_accum_kernel<<<n_chunks, kApplyThreads, 0, s>>>(col, pitch, nodes, st, g, h, chunks, sc, nid,
-                                                          seg_sums);
+                                                          seg_sums, n_bins);
     check(cudaGetLastError(), "apply_accum launch");
 }
 

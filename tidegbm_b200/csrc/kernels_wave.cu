@@ -123,8 +123,174 @@ __device__ __forceinline__ JobRows job_rows(const WaveCtx& X, int src, int e) {
     return r;
 }
 
+// The rows [r0, r1) of one unit (one group of 32 features), lane = row: a warp takes 32
+// rows, lane l loads its row's 32 code bytes with two 16-byte loads and rotates them by l
+// bytes, so step j touches feature (j + l) & 31 (conflict-free banks); every code costs
+// the mode's fire-and-forget 32-bit reductions, folded into 64-bit registers every
+// sub-chunk.  Ends with the CTA's totals in the 5 planes (G lo, G hi, H lo, H hi, count).
+// A separate (not inlined) function: the hot loop keeps only its own state in registers.
+// Row counts of the constant-hessian modes travel packed (unscaled | GOSS-scaled << 16);
+// a CTA's share of a unit has fewer than 2^16 rows.
 template <int kMode>
-__global__ void __launch_bounds__(kThreads)
+__device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const int32_t* __restrict__ rows, int r0,
+                                             int r1, const uint8_t* __restrict__ codes, int stride, int fg0,
+                                             const void* __restrict__ gqp, const void* __restrict__ hqp,
+                                             unsigned long long hq1, unsigned long long hq2) {
+    using T = ModeTraits<kMode>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = lane >> 2, sh = (lane & 3) * 8;
+    const bool two_chunks = stride - fg0 >= 32;
+    long long accG[kCells];
+    long long accH[T::var ? kCells : 1];
+    unsigned int accC[kCells];
+#pragma unroll
+    for (int cc = 0; cc < kCells; ++cc) {
+        accG[cc] = 0;
+        if constexpr (T::var) accH[cc] = 0;
+        accC[cc] = 0u;
+    }
+    for (int s0 = r0; s0 < r1; s0 += T::sub) {
+        const int s1 = min(r1, s0 + T::sub);
+        int r_next = s0 + warp * 32 + lane < s1 ? rows[s0 + warp * 32 + lane] : -1;
+        for (int base = s0 + warp * 32; base < s1; base += kWarps * 32) {
+            const int r = r_next;
+            const int kn = base + kWarps * 32 + lane;
+            r_next = kn < s1 ? rows[kn] : -1;
+            if (r < 0) continue;
+            // payload words of this row (mode dependent)
+            unsigned int a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+            unsigned int* plane = P;
+            if constexpr (kMode == kHistExactConst) {
+                const long long p = static_cast<const long long*>(gqp)[r];
+                const long long v = p >> 1;
+                a0 = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
+                a1 = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
+                a2 = (p & 1) ? 0x10000u : 1u;
+            } else if constexpr (kMode == kHistExactVar) {
+                const long long gv = static_cast<const long long*>(gqp)[r];
+                const long long hv = static_cast<const long long*>(hqp)[r];
+                a0 = static_cast<unsigned int>(gv) & ((1u << kLoBits) - 1u);
+                a1 = static_cast<unsigned int>(static_cast<int>(gv >> kLoBits));
+                a2 = static_cast<unsigned int>(hv) & ((1u << kLoBits) - 1u);
+                a3 = static_cast<unsigned int>(static_cast<int>(hv >> kLoBits));
+            } else if constexpr (kMode == kHistQ16Const) {
+                const int p = static_cast<const int*>(gqp)[r];
+                a0 = static_cast<unsigned int>(p >> 1);
+                a1 = (p & 1) ? 0x10000u : 1u;
+            } else if constexpr (kMode == kHistQ16Var) {
+                const unsigned int p = static_cast<const unsigned int*>(gqp)[r];
+                a0 = static_cast<unsigned int>(static_cast<int>(p) >> 16);
+                a1 = p & 0xffffu;
+            } else if constexpr (kMode == kHistQ8Const) {
+                const int p = static_cast<const short*>(gqp)[r];
+                a0 = (1u << 20) | static_cast<unsigned int>((p >> 1) + 128);
+                plane = (p & 1) ? P + kPlane : P;
+            } else {  // kHistQ8Var
+                const unsigned int p = static_cast<const unsigned short*>(gqp)[r];
+                a0 = (1u << 20) | (p & 0xffu);
+                a1 = p >> 8;
+            }
+            const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r) * stride + fg0);
+            const uint4 ca = __ldg(src4);
+            const uint4 cb = two_chunks ? __ldg(src4 + 1) : make_uint4(0, 0, 0, 0);
+            unsigned int wd[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+            rotate_words(wd, q);
+            unsigned int Rw[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) Rw[t] = __funnelshift_r(wd[t], wd[(t + 1) & 7], sh);
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+                const int f = (jj + lane) & 31;
+                const unsigned int code = (Rw[jj >> 2] >> ((jj & 3) * 8)) & 0xffu;
+                const int cell = static_cast<int>(code) * 32 + f;
+                if constexpr (kMode == kHistExactConst) {
+                    atomicAdd(&P[cell], a0);
+                    atomicAdd(&P[kPlane + cell], a1);
+                    atomicAdd(&P[2 * kPlane + cell], a2);
+                } else if constexpr (kMode == kHistExactVar) {
+                    atomicAdd(&P[cell], a0);
+                    atomicAdd(&P[kPlane + cell], a1);
+                    atomicAdd(&P[2 * kPlane + cell], a2);
+                    atomicAdd(&P[3 * kPlane + cell], a3);
+                    atomicAdd(&P[4 * kPlane + cell], 1u);
+                } else if constexpr (kMode == kHistQ16Const) {
+                    atomicAdd(&P[cell], a0);
+                    atomicAdd(&P[kPlane + cell], a1);
+                } else if constexpr (kMode == kHistQ16Var) {
+                    atomicAdd(&P[cell], a0);
+                    atomicAdd(&P[kPlane + cell], a1);
+                    atomicAdd(&P[2 * kPlane + cell], 1u);
+                } else if constexpr (kMode == kHistQ8Const) {
+                    atomicAdd(&plane[cell], a0);
+                } else {
+                    atomicAdd(&P[cell], a0);
+                    atomicAdd(&P[kPlane + cell], a1);
+                }
+            }
+        }
+        __syncthreads();
+        // fold the sub-chunk into 64-bit registers and clear the planes
+#pragma unroll
+        for (int cc = 0; cc < kCells; ++cc) {
+            const int cell = threadIdx.x + cc * kThreads;
+            if constexpr (kMode == kHistExactConst) {
+                accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
+                accC[cc] += P[2 * kPlane + cell];
+            } else if constexpr (kMode == kHistExactVar) {
+                accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
+                accH[cc] +=
+                    static_cast<long long>(static_cast<int>(P[3 * kPlane + cell])) * (1ll << kLoBits) + P[2 * kPlane + cell];
+                accC[cc] += P[4 * kPlane + cell];
+            } else if constexpr (kMode == kHistQ16Const) {
+                accG[cc] += static_cast<int>(P[cell]);
+                accC[cc] += P[kPlane + cell];
+            } else if constexpr (kMode == kHistQ16Var) {
+                accG[cc] += static_cast<int>(P[cell]);
+                accH[cc] += P[kPlane + cell];
+                accC[cc] += P[2 * kPlane + cell];
+            } else if constexpr (kMode == kHistQ8Const) {
+                const unsigned int w1 = P[cell], w2 = P[kPlane + cell];
+                const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
+                accG[cc] += static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
+                            128ll * static_cast<long long>(n1 + n2);
+                accC[cc] += n1 | (n2 << 16);
+            } else {
+                const unsigned int w1 = P[cell];
+                const unsigned int n1 = w1 >> 20;
+                accG[cc] += static_cast<long long>(w1 & 0xfffffu) - 128ll * static_cast<long long>(n1);
+                accH[cc] += P[kPlane + cell];
+                accC[cc] += n1;
+            }
+#pragma unroll
+            for (int pl = 0; pl < T::planes; ++pl) P[pl * kPlane + cell] = 0u;
+        }
+        __syncthreads();
+    }
+    // totals -> 5 planes
+#pragma unroll
+    for (int cc = 0; cc < kCells; ++cc) {
+        const int cell = threadIdx.x + cc * kThreads;
+        unsigned long long Hs;
+        unsigned int Cn;
+        if constexpr (T::var) {
+            Hs = static_cast<unsigned long long>(accH[cc]);
+            Cn = accC[cc];
+        } else {
+            const unsigned int c1 = accC[cc] & 0xffffu, c2 = accC[cc] >> 16;
+            Hs = static_cast<unsigned long long>(c1) * hq1 + static_cast<unsigned long long>(c2) * hq2;
+            Cn = c1 + c2;
+        }
+        const unsigned long long Gs = static_cast<unsigned long long>(accG[cc]);
+        P[cell] = static_cast<unsigned int>(Gs);
+        P[kPlane + cell] = static_cast<unsigned int>(Gs >> 32);
+        P[2 * kPlane + cell] = static_cast<unsigned int>(Hs);
+        P[3 * kPlane + cell] = static_cast<unsigned int>(Hs >> 32);
+        P[4 * kPlane + cell] = Cn;
+    }
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kThreads, 1)
     wave_hist_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src, unsigned long long* rows_counter,
                      int unit_target) {
     using T = ModeTraits<kMode>;
@@ -184,7 +350,9 @@ __global__ void __launch_bounds__(kThreads)
         const unsigned long long target =
             static_cast<unsigned long long>(max(1, unit_target)) * static_cast<unsigned long long>(max(1, n_cl0));
         const unsigned long long u = (tot + target - 1) / target;
-        unit_rows_b = static_cast<int>(min(max(static_cast<unsigned long long>(kMinUnitRows), u), 1ull << 30));
+        // a CTA's share of a unit stays below 2^16 rows: its row counts pack into 16-bit fields
+        const unsigned long long cap = 65535ull * cg::this_cluster().dim_blocks().y;
+        unit_rows_b = static_cast<int>(min(max(static_cast<unsigned long long>(kMinUnitRows), u), cap));
     }
     // units of each job: exclusive prefix over the jobs, a contiguous run per thread
     {
@@ -230,9 +398,6 @@ __global__ void __launch_bounds__(kThreads)
     const int cl = static_cast<int>(blockIdx.y) / csize;
     const int n_cl = static_cast<int>(gridDim.y) / csize;
     const unsigned int rank = cluster.block_rank();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = lane >> 2, sh = (lane & 3) * 8;
-
     for (int u = cl; u < n_units; u += n_cl) {
         // unit -> job (binary search over the unit starts), feature group, row chunk
         int lo = 0, hi = n_jobs - 1;
@@ -244,7 +409,7 @@ __global__ void __launch_bounds__(kThreads)
         const int j = lo;
         const int c = s_job[j] >> 16, e = s_job[j] & 0xffff;
         const WaveCtx& X = ctxs[c];
-        const int n_f = X.gp.n_features, stride = X.gp.stride;
+        const int n_f = X.gp.n_features;
         const int nfg = (n_f + kFG - 1) / kFG;
         const int k = u - s_ustart[j];
         const int fg = k % nfg, chunk = k / nfg;
@@ -257,168 +422,15 @@ __global__ void __launch_bounds__(kThreads)
         const int r0 = min(c1, c0 + static_cast<int>(rank) * qrows), r1 = min(c1, r0 + qrows);
         if (rows_counter != nullptr && rank == 0 && k == 0 && threadIdx.x == 0)
             atomicAdd(rows_counter, static_cast<unsigned long long>(R));
-        const int fg0 = fg * kFG;
-        const int nf_here = min(kFG, n_f - fg0);
-        const bool two_chunks = stride - fg0 >= 32;
-        const int32_t* __restrict__ rows = jr.rows;
-        const uint8_t* __restrict__ codes = X.codes;
-        const void* __restrict__ gqp = X.gq;
-        const void* __restrict__ hqp = X.hq;
-
-        long long accG[kCells], accH[kCells];
-        unsigned int accC1[kCells], accC2[kCells];
-#pragma unroll
-        for (int cc = 0; cc < kCells; ++cc) {
-            accG[cc] = accH[cc] = 0;
-            accC1[cc] = accC2[cc] = 0u;
-        }
-        for (int s0 = r0; s0 < r1; s0 += T::sub) {
-            const int s1 = min(r1, s0 + T::sub);
-            int r_next = s0 + warp * 32 + lane < s1 ? rows[s0 + warp * 32 + lane] : -1;
-            for (int base = s0 + warp * 32; base < s1; base += kWarps * 32) {
-                const int r = r_next;
-                const int kn = base + kWarps * 32 + lane;
-                r_next = kn < s1 ? rows[kn] : -1;
-                if (r < 0) continue;
-                // payload words of this row (mode dependent)
-                unsigned int a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-                unsigned int* plane = P;
-                if constexpr (kMode == kHistExactConst) {
-                    const long long p = static_cast<const long long*>(gqp)[r];
-                    const long long v = p >> 1;
-                    a0 = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
-                    a1 = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
-                    a2 = (p & 1) ? 0x10000u : 1u;
-                } else if constexpr (kMode == kHistExactVar) {
-                    const long long gv = static_cast<const long long*>(gqp)[r];
-                    const long long hv = static_cast<const long long*>(hqp)[r];
-                    a0 = static_cast<unsigned int>(gv) & ((1u << kLoBits) - 1u);
-                    a1 = static_cast<unsigned int>(static_cast<int>(gv >> kLoBits));
-                    a2 = static_cast<unsigned int>(hv) & ((1u << kLoBits) - 1u);
-                    a3 = static_cast<unsigned int>(static_cast<int>(hv >> kLoBits));
-                } else if constexpr (kMode == kHistQ16Const) {
-                    const int p = static_cast<const int*>(gqp)[r];
-                    a0 = static_cast<unsigned int>(p >> 1);
-                    a1 = (p & 1) ? 0x10000u : 1u;
-                } else if constexpr (kMode == kHistQ16Var) {
-                    const unsigned int p = static_cast<const unsigned int*>(gqp)[r];
-                    a0 = static_cast<unsigned int>(static_cast<int>(p) >> 16);
-                    a1 = p & 0xffffu;
-                } else if constexpr (kMode == kHistQ8Const) {
-                    const int p = static_cast<const short*>(gqp)[r];
-                    a0 = (1u << 20) | static_cast<unsigned int>((p >> 1) + 128);
-                    plane = (p & 1) ? P + kPlane : P;
-                } else {  // kHistQ8Var
-                    const unsigned int p = static_cast<const unsigned short*>(gqp)[r];
-                    a0 = (1u << 20) | (p & 0xffu);
-                    a1 = p >> 8;
-                }
-                const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r) * stride + fg0);
-                const uint4 ca = __ldg(src4);
-                const uint4 cb = two_chunks ? __ldg(src4 + 1) : make_uint4(0, 0, 0, 0);
-                unsigned int wd[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
-                rotate_words(wd, q);
-                unsigned int Rw[8];
-#pragma unroll
-                for (int t = 0; t < 8; ++t) Rw[t] = __funnelshift_r(wd[t], wd[(t + 1) & 7], sh);
-#pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const int f = (jj + lane) & 31;
-                    const unsigned int code = (Rw[jj >> 2] >> ((jj & 3) * 8)) & 0xffu;
-                    const int cell = static_cast<int>(code) * 32 + f;
-                    if constexpr (kMode == kHistExactConst) {
-                        atomicAdd(&P[cell], a0);
-                        atomicAdd(&P[kPlane + cell], a1);
-                        atomicAdd(&P[2 * kPlane + cell], a2);
-                    } else if constexpr (kMode == kHistExactVar) {
-                        atomicAdd(&P[cell], a0);
-                        atomicAdd(&P[kPlane + cell], a1);
-                        atomicAdd(&P[2 * kPlane + cell], a2);
-                        atomicAdd(&P[3 * kPlane + cell], a3);
-                        atomicAdd(&P[4 * kPlane + cell], 1u);
-                    } else if constexpr (kMode == kHistQ16Const) {
-                        atomicAdd(&P[cell], a0);
-                        atomicAdd(&P[kPlane + cell], a1);
-                    } else if constexpr (kMode == kHistQ16Var) {
-                        atomicAdd(&P[cell], a0);
-                        atomicAdd(&P[kPlane + cell], a1);
-                        atomicAdd(&P[2 * kPlane + cell], 1u);
-                    } else if constexpr (kMode == kHistQ8Const) {
-                        atomicAdd(&plane[cell], a0);
-                    } else {
-                        atomicAdd(&P[cell], a0);
-                        atomicAdd(&P[kPlane + cell], a1);
-                    }
-                }
-            }
-            __syncthreads();
-            // fold the sub-chunk into 64-bit registers and clear the planes
-#pragma unroll
-            for (int cc = 0; cc < kCells; ++cc) {
-                const int cell = threadIdx.x + cc * kThreads;
-                if constexpr (kMode == kHistExactConst) {
-                    accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
-                    const unsigned int cn = P[2 * kPlane + cell];
-                    accC1[cc] += cn & 0xffffu;
-                    accC2[cc] += cn >> 16;
-                } else if constexpr (kMode == kHistExactVar) {
-                    accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
-                    accH[cc] +=
-                        static_cast<long long>(static_cast<int>(P[3 * kPlane + cell])) * (1ll << kLoBits) + P[2 * kPlane + cell];
-                    accC1[cc] += P[4 * kPlane + cell];
-                } else if constexpr (kMode == kHistQ16Const) {
-                    accG[cc] += static_cast<int>(P[cell]);
-                    const unsigned int cn = P[kPlane + cell];
-                    accC1[cc] += cn & 0xffffu;
-                    accC2[cc] += cn >> 16;
-                } else if constexpr (kMode == kHistQ16Var) {
-                    accG[cc] += static_cast<int>(P[cell]);
-                    accH[cc] += P[kPlane + cell];
-                    accC1[cc] += P[2 * kPlane + cell];
-                } else if constexpr (kMode == kHistQ8Const) {
-                    const unsigned int w1 = P[cell], w2 = P[kPlane + cell];
-                    const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
-                    accG[cc] += static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
-                                128ll * static_cast<long long>(n1 + n2);
-                    accC1[cc] += n1;
-                    accC2[cc] += n2;
-                } else {
-                    const unsigned int w1 = P[cell];
-                    const unsigned int n1 = w1 >> 20;
-                    accG[cc] += static_cast<long long>(w1 & 0xfffffu) - 128ll * static_cast<long long>(n1);
-                    accH[cc] += P[kPlane + cell];
-                    accC1[cc] += n1;
-                }
-#pragma unroll
-                for (int pl = 0; pl < T::planes; ++pl) P[pl * kPlane + cell] = 0u;
-            }
-            __syncthreads();
-        }
-        // this CTA's totals -> 5 planes of its shared memory
         const double hscale = X.st->hscale;
-        const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale));
-        const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * hscale));
-#pragma unroll
-        for (int cc = 0; cc < kCells; ++cc) {
-            const int cell = threadIdx.x + cc * kThreads;
-            unsigned long long Hs;
-            unsigned int Cn;
-            if constexpr (T::var) {
-                Hs = static_cast<unsigned long long>(accH[cc]);
-                Cn = accC1[cc];
-            } else {
-                Hs = static_cast<unsigned long long>(accC1[cc]) * hq1 + static_cast<unsigned long long>(accC2[cc]) * hq2;
-                Cn = accC1[cc] + accC2[cc];
-            }
-            const unsigned long long Gs = static_cast<unsigned long long>(accG[cc]);
-            P[cell] = static_cast<unsigned int>(Gs);
-            P[kPlane + cell] = static_cast<unsigned int>(Gs >> 32);
-            P[2 * kPlane + cell] = static_cast<unsigned int>(Hs);
-            P[3 * kPlane + cell] = static_cast<unsigned int>(Hs >> 32);
-            P[4 * kPlane + cell] = Cn;
-        }
+        // this CTA's rows of the unit -> its totals in the 5 planes of its shared memory
+        accumulate_unit<kMode>(P, jr.rows, r0, r1, X.codes, X.gp.stride, fg * kFG, X.gq, X.hq,
+                               static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale)),
+                               static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * hscale)));
         cluster.sync();
         const int share = kPlane / csize;
+        const int fg0 = fg * kFG;
+        const int nf_here = min(kFG, n_f - fg0);
         const size_t slot_off = static_cast<size_t>(jr.slot) * static_cast<size_t>(n_f) * kBins;
         for (int cell = rank * share + threadIdx.x; cell < static_cast<int>(rank + 1) * share; cell += kThreads) {
             unsigned long long g = 0, hsum = 0;
@@ -498,13 +510,17 @@ __device__ __forceinline__ void load_tile(const WaveCtx& X, const int32_t* in, c
         const int k = base + i * kPartThreads + threadIdx.x;
         row[i] = k < end ? in[k] : -1;
     }
-    unsigned int b[kPartPer];
+    unsigned int b[kPartPer], b2[kPartPer];
     const uint8_t* col = X.codes_col + static_cast<size_t>(feature) * X.col_pitch;
+    const uint8_t* col2 = type == 1 ? X.codes_col + static_cast<size_t>(S.feature2) * X.col_pitch : col;
 #pragma unroll
-    for (int i = 0; i < kPartPer; ++i) b[i] = row[i] >= 0 ? col[row[i]] : 0u;
+    for (int i = 0; i < kPartPer; ++i) {
+        b[i] = row[i] >= 0 ? col[row[i]] : 0u;
+        b2[i] = row[i] >= 0 && type == 1 ? col2[row[i]] : 0u;
+    }
 #pragma unroll
     for (int i = 0; i < kPartPer; ++i)
-        left[i] = row[i] >= 0 && goes_left(type, cat, threshold, ml, b[i]);
+        left[i] = row[i] >= 0 && goes_left(type, cat, threshold, ml, b[i], b2[i], X.gp.n_bins);
 }
 
 __device__ __forceinline__ void load_tile_prefix(const WaveCtx* ctxs, int n_ctx, int* s_pref) {
@@ -672,6 +688,7 @@ __global__ void wave_tree_init_kernel(DevNode* nodes, DevSplit* splits, DevTreeS
         ctl->slot0 = 1;
         ctl->error = 0;
         ctl->waves = 0;
+        ctl->pair_used = 0;
     }
     ctl->expanded[0] = 0;
 }

@@ -21,6 +21,7 @@ namespace {
 using namespace scan;
 
 constexpr int kRootCand = 2 * kMaxNodes;  // candidate / ticket index of the root
+constexpr int kMaxPairFeatures = 1024;    // features the PAIR ranking sorts (host-checked)
 
 __device__ __forceinline__ void children_prefix(const WaveCtx* ctxs, int n_ctx, int src, int* s_pref) {
     if (static_cast<int>(threadIdx.x) < n_ctx) {
@@ -187,6 +188,12 @@ __global__ void __launch_bounds__(32)
         if (lane == 0) ctl->waves += 1;
         int nn = st->n_nodes;
         int done_splits = ctl->splits_done;
+        int pair_used = ctl->pair_used;
+        // the split a leaf takes: with the PAIR candidates while the tree's pair budget lasts
+        // (tree.cpp:214-218, re-scored after every pair split, tree.cpp:393-396)
+        auto split_of = [&](int k) -> DevSplit {
+            return (X.pair_on && pair_used < X.max_pair) ? X.splits_pair[k] : splits[k];
+        };
         bool finished = false;
         while (true) {
             if (done_splits >= budget || runaway) {
@@ -196,7 +203,7 @@ __global__ void __launch_bounds__(32)
             double bg = 0.0;
             int bi = 0x7fffffff;
             for (int k = lane; k < nn; k += 32) {
-                const DevSplit S = splits[k];
+                const DevSplit S = split_of(k);
                 if (!candidate(p, nodes[k], S)) continue;
                 if (bi == 0x7fffffff || better_leaf(S.gain, k, bg, bi)) {
                     bg = S.gain;
@@ -218,15 +225,16 @@ __global__ void __launch_bounds__(32)
             }
             if (!ctl->expanded[bi]) break;
             // commit: the split of bi, children ids nn, nn + 1 (grow_tree's numbering)
+            const DevSplit S = split_of(bi);
             if (lane == 0) {
                 DevNode& P = nodes[bi];
-                const DevSplit S = splits[bi];
                 P.is_leaf = 0;
                 P.feature = S.feature;
                 P.threshold = S.threshold;
                 P.missing_left = S.missing_left;
                 P.gain = S.gain;
                 P.type = S.type;
+                P.feature2 = S.type == 1 ? S.feature2 : -1;
                 for (int k = 0; k < 4; ++k) P.cat[k] = S.cat[k];
                 P.left = nn;
                 P.right = nn + 1;
@@ -234,6 +242,10 @@ __global__ void __launch_bounds__(32)
                 nodes[nn + 1] = X.spec[2 * bi + 1];
                 splits[nn] = X.spec_split[2 * bi];
                 splits[nn + 1] = X.spec_split[2 * bi + 1];
+                if (X.pair_on) {
+                    X.splits_pair[nn] = X.spec_split_pair[2 * bi];
+                    X.splits_pair[nn + 1] = X.spec_split_pair[2 * bi + 1];
+                }
                 ctl->expanded[nn] = 0;
                 ctl->expanded[nn + 1] = 0;
             }
@@ -241,6 +253,7 @@ __global__ void __launch_bounds__(32)
             __threadfence_block();
             nn += 2;
             done_splits += 1;
+            if (S.type == 1) pair_used += 1;
         }
         int n_exp = 0;
         if (!finished) {
@@ -251,7 +264,7 @@ __global__ void __launch_bounds__(32)
                 bool is_c = false;
                 double gk = 0.0;
                 if (k < nn) {
-                    const DevSplit S = splits[k];
+                    const DevSplit S = split_of(k);
                     is_c = candidate(p, nodes[k], S);
                     gk = S.gain;
                 }
@@ -302,7 +315,9 @@ __global__ void __launch_bounds__(32)
                         ch.left = ch.right = -1;
                         ch.parent = L;
                         ch.slot = slot_first + 2 * e + sd;
+                        ch.feature2 = -1;
                         X.spec[2 * L + sd] = ch;
+                        if (X.pair_on) X.energy[2 * L + sd] = 0ull;
                     }
                 }
                 // tile prefix in expansion order
@@ -329,6 +344,7 @@ __global__ void __launch_bounds__(32)
             if (runaway) ctl->error = 1;
             st->n_nodes = nn;
             ctl->splits_done = done_splits;
+            ctl->pair_used = pair_used;
             ctl->n_exp = active ? n_exp : 0;
             if (!active) {
                 ctl->tiles_total = 0;
@@ -356,7 +372,215 @@ __global__ void __launch_bounds__(32)
     }
 }
 
+
+// ---- PAIR stage (tree.cpp:214-281) --------------------------------------------------------
+//
+// energy: the rows' sum of g^2 (g as the tree sees it: GOSS-scaled for sampled others), one
+// fixed-point sum per candidate index (exact integer adds: the same total in any order).
+// pair: one CTA per (child, pair of its top features) when the child's best axis gain is
+// weak against that energy: the histogram of pair_bin(code1, code2) over the child's rows
+// (exact fixed-point sums of the same per-row values the main histogram adds), scanned as
+// one numeric feature with pair_l2; the child's last pair CTA to finish merges the pairs'
+// best splits with the axis split (strict '>' in pair order) into the with-pairs split.
+
+struct ChildRef {
+    int ci;
+    const DevNode* N;
+    const int32_t* rows;
+    DevSplit* axis;
+    DevSplit* with_pairs;
+};
+
+__device__ __forceinline__ ChildRef child_ref(const WaveCtx& X, int src, int k) {
+    ChildRef r;
+    if (src == 0) {
+        r.ci = kRootCand;
+        r.N = X.nodes;
+        r.axis = X.splits;
+        r.with_pairs = X.splits_pair;
+    } else {
+        const int L = X.ctl->exp_leaf[k >> 1];
+        r.ci = 2 * L + (k & 1);
+        r.N = X.spec + r.ci;
+        r.axis = X.spec_split + r.ci;
+        r.with_pairs = X.spec_split_pair + r.ci;
+    }
+    r.rows = (r.N->buf ? X.rows1 : X.rows0) + r.N->start;
+    return r;
+}
+
+__device__ __forceinline__ int energy_shift(const DevTreeState* st) {
+    const double mg = __longlong_as_double(static_cast<long long>(st->max_abs_g_bits));
+    const double e2 = mg * mg;
+    if (!(e2 > 0.0) || st->n_sample <= 0) return 0;
+    int clog = 0;
+    while ((1ll << clog) < static_cast<long long>(st->n_sample)) ++clog;
+    return max(-1000, min(1000, 61 - (ilogb(e2) + 1) - clog));
+}
+
+constexpr int kEnergyRows = 8192;
+
+__global__ void __launch_bounds__(256) wave_energy_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ int s_pref[kMaxWaveCtx + 1];
+    __shared__ unsigned long long s_red[8];
+    children_prefix(ctxs, n_ctx, src, s_pref);
+    const int total = s_pref[n_ctx];
+    for (int j = blockIdx.y; j < total; j += gridDim.y) {
+        int c = 0;
+        while (c + 1 < n_ctx && s_pref[c + 1] <= j) ++c;
+        const WaveCtx& X = ctxs[c];
+        if (!X.pair_on) continue;
+        const ChildRef cr = child_ref(X, src, j - s_pref[c]);
+        const GrowParams& p = X.gp;
+        if (cr.N->depth >= p.max_depth || cr.N->count < 2 * p.min_samples_leaf) continue;
+        const double scale = ldexp(1.0, energy_shift(X.st));
+        const int count = cr.N->count;
+        for (int r0 = blockIdx.x * kEnergyRows; r0 < count; r0 += gridDim.x * kEnergyRows) {
+            unsigned long long acc = 0;
+            const int r1 = min(count, r0 + kEnergyRows);
+            for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const int r = cr.rows[i];
+                double gv = X.g[r];
+                if (X.goss_flag != nullptr && X.goss_flag[r] == 2) gv *= X.goss_scale;
+                acc += static_cast<unsigned long long>(__double2ll_rn(gv * gv * scale));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long t = 0;
+                for (int w = 0; w < 8; ++w) t += s_red[w];
+                atomicAdd(&X.energy[cr.ci], t);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) wave_pair_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ int s_pref[kMaxWaveCtx + 1];
+    __shared__ ScanShared sm;
+    __shared__ unsigned long long sG[kBins], sH[kBins];
+    __shared__ int sC[kBins];
+    __shared__ short s_top[kMaxPairFeatures];
+    __shared__ int last;
+    children_prefix(ctxs, n_ctx, src, s_pref);
+    const int total = s_pref[n_ctx];
+    const int pi = blockIdx.x;
+    for (int j = blockIdx.y; j < total; j += gridDim.y) {
+        int c = 0;
+        while (c + 1 < n_ctx && s_pref[c + 1] <= j) ++c;
+        const WaveCtx& X = ctxs[c];
+        if (!X.pair_on) continue;
+        const ChildRef cr = child_ref(X, src, j - s_pref[c]);
+        const GrowParams& p = X.gp;
+        const int n_f = p.n_features;
+        const bool eligible = cr.N->depth < p.max_depth && cr.N->count >= 2 * p.min_samples_leaf;
+        const DevSplit axis = *cr.axis;
+        const double axis_gain = axis.valid ? axis.gain : -1e300;
+        const double energy = static_cast<double>(X.energy[cr.ci]) * ldexp(1.0, -energy_shift(X.st));
+        const bool weak = eligible && n_f >= 2 &&
+                          ((axis_gain < X.pair_trigger * fmax(energy * 0.01, 1e-12)) || axis_gain <= 0);
+        const int k = min(X.pair_top_k, n_f);
+        const int n_pairs = weak ? k * (k - 1) / 2 : 0;
+        if (n_pairs == 0) {
+            if (pi == 0 && threadIdx.x == 0) *cr.with_pairs = axis;  // no pair search for this child
+            continue;
+        }
+        if (pi >= n_pairs) continue;
+        // top-k features by their best gain, std::sort's order (tree.cpp:223-225)
+        if (threadIdx.x == 0) {
+            for (int f = 0; f < n_f; ++f) s_top[f] = static_cast<short>(f);
+            const double* gains = X.cand_gain + static_cast<size_t>(cr.ci) * n_f;
+            libstdcxx_sort(s_top, n_f, [&](short a, short b) { return gains[a] > gains[b]; });
+        }
+        for (int q = threadIdx.x; q < kBins; q += blockDim.x) {
+            sG[q] = sH[q] = 0ull;
+            sC[q] = 0;
+        }
+        __syncthreads();
+        int a = 0, rem = pi;
+        while (rem >= k - 1 - a) {
+            rem -= k - 1 - a;
+            ++a;
+        }
+        const int f1 = s_top[a], f2 = s_top[a + 1 + rem];
+        const uint8_t* c1 = X.codes_col + static_cast<size_t>(f1) * X.col_pitch;
+        const uint8_t* c2 = X.codes_col + static_cast<size_t>(f2) * X.col_pitch;
+        const bool var = X.hq != nullptr;
+        const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.st->hscale));
+        const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * X.st->hscale));
+        const int count = cr.N->count;
+        for (int i = threadIdx.x; i < count; i += blockDim.x) {
+            const int r = cr.rows[i];
+            const unsigned z = pair_bin(c1[r], c2[r], p.n_bins);
+            unsigned long long gv, hv;
+            if (var) {
+                gv = static_cast<unsigned long long>(static_cast<const long long*>(X.gq)[r]);
+                hv = static_cast<unsigned long long>(static_cast<const long long*>(X.hq)[r]);
+            } else {
+                const long long pk = static_cast<const long long*>(X.gq)[r];
+                gv = static_cast<unsigned long long>(pk >> 1);
+                hv = (pk & 1) ? hq2 : hq1;
+            }
+            atomicAdd(&sG[z], gv);
+            atomicAdd(&sH[z], hv);
+            atomicAdd(&sC[z], 1);
+        }
+        __syncthreads();
+        long long Gt, Ht, Ct;
+        const Cand cd = scan_feature(reinterpret_cast<long long*>(sG), reinterpret_cast<long long*>(sH), sC, nullptr,
+                                     nullptr, nullptr, nullptr, nullptr, nullptr, false, true, 0, p.n_bins,
+                                     X.st->inv_gscale, X.st->inv_hscale, X.pair_l2, p.min_split_gain,
+                                     p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
+        if (threadIdx.x == 0) {
+            DevSplit ps{};
+            ps.gain = cd.gain;
+            ps.valid = cd.key != 0x7fffffff;  // found; min_split_gain is applied at the merge
+            ps.feature = f1;
+            ps.feature2 = f2;
+            ps.type = 1;
+            ps.threshold = ps.valid ? (cd.key % 512) / 2 : -1;
+            ps.missing_left = ps.valid ? (cd.key & 1) : 1;
+            X.pair_cand[static_cast<size_t>(cr.ci) * kMaxPairs + pi] = ps;
+            __threadfence();
+            last = atomicAdd(&X.pair_tickets[cr.ci], 1) == n_pairs - 1;
+        }
+        __syncthreads();
+        if (last && threadIdx.x == 0) {
+            __threadfence();
+            DevSplit best = axis;
+            double bg = axis_gain;
+            for (int q = 0; q < n_pairs; ++q) {
+                DevSplit pc;
+                const volatile int* src_w =
+                    reinterpret_cast<const volatile int*>(X.pair_cand + static_cast<size_t>(cr.ci) * kMaxPairs + q);
+                int* dst_w = reinterpret_cast<int*>(&pc);
+                for (int w = 0; w < static_cast<int>(sizeof(DevSplit) / 4); ++w) dst_w[w] = src_w[w];
+                if (pc.valid && pc.gain > bg) {
+                    bg = pc.gain;
+                    best = pc;
+                    best.valid = pc.gain >= p.min_split_gain;
+                }
+            }
+            *cr.with_pairs = best;
+            X.pair_tickets[cr.ci] = 0;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void launch_wave_pair(const WaveCtx* ctxs, int n_ctx, int src, cudaStream_t s) {
+    launch_pdl(wave_energy_kernel, dim3(16, 32), dim3(256), 0, s, "wave_energy launch", ctxs, n_ctx, src);
+    launch_pdl(wave_pair_kernel, dim3(kMaxPairs, 32), dim3(kScanThreads), 0, s, "wave_pair launch", ctxs, n_ctx, src);
+}
 
 void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, cudaStream_t s) {
     launch_pdl(wave_scan_kernel, dim3(max_f, ys), dim3(kScanThreads), 0, s, "wave_scan launch", ctxs, n_ctx, src);

@@ -28,26 +28,42 @@ struct DevNode {
     double gain;        // split gain (internal nodes)
     double value;       // leaf value from the node's sample sums (Node::value)
     long long G, H, C;  // fixed-point sample sums
-    int32_t type;       // split type (SplitType, cpp/include/tidegbm/types.hpp:25): 0 axis, 2 categorical
-    int32_t pad1;
+    int32_t type;       // split type (SplitType, cpp/include/tidegbm/types.hpp:25): 0 axis, 1 pair, 2 categorical
+    int32_t feature2;   // pair split: the second feature
     unsigned long long cat[4];  // categorical split: the codes that go left (bit b: code b)
 };
 
 struct DevSplit {
     double gain;
     int feature, threshold, missing_left, valid;
-    int type, pad;
+    int type, feature2;
     unsigned long long cat[4];
 };
 
-// Routing of a code at a split node (cpp/include/tidegbm/tree.hpp:27-30, tree.cpp:15-41):
-// categorical nodes test the code's bit of the left mask, axis nodes send missing (code 0)
-// by the learned direction and codes up to the threshold left.
 #if defined(__CUDACC__)
-__host__ __device__
+#define TGB_HD __host__ __device__
+#else
+#define TGB_HD
 #endif
-inline bool goes_left(int type, const unsigned long long* cat, int threshold, int missing_left, unsigned code) {
+
+// pair_bin (cpp/include/tidegbm/histogram.hpp:81-85): two codes hashed into one of n_bins
+// bins in 32-bit unsigned arithmetic.
+TGB_HD inline unsigned pair_bin(unsigned b1, unsigned b2, int n_bins) {
+    return (b1 * 2654435761u + b2 * 40503u) % static_cast<unsigned>(n_bins);
+}
+
+// Routing of a row at a split node (cpp/include/tidegbm/tree.hpp:27-30, tree.cpp:15-41):
+// categorical nodes test the code's bit of the left mask; pair nodes send a row missing
+// either code by the learned direction, else compare the hashed pair bin; axis nodes send
+// missing (code 0) by the learned direction and codes up to the threshold left.  code2:
+// the row's code of the second feature (pair nodes only).
+TGB_HD inline bool goes_left(int type, const unsigned long long* cat, int threshold, int missing_left, unsigned code,
+                             unsigned code2 = 0u, int n_bins = 1) {
     if (type == 2) return (cat[code >> 6] >> (code & 63)) & 1ull;
+    if (type == 1) {
+        if (code == 0u || code2 == 0u) return missing_left != 0;
+        return static_cast<int>(pair_bin(code, code2, n_bins)) <= threshold;
+    }
     return code == 0u ? missing_left != 0 : static_cast<int>(code) <= threshold;
 }
 
@@ -316,7 +332,7 @@ void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const dou
 // col: column-major codes (col[f * pitch + r], launch_codes_transpose)
 void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
-                        int16_t* nid, unsigned long long* seg_sums, int n_segments, cudaStream_t s);
+                        int16_t* nid, unsigned long long* seg_sums, int n_segments, int n_bins, cudaStream_t s);
 void launch_finalize_tree(const PostParams& pp, const DevTreeState* st, const unsigned long long* seg_sums,
                           const int* bucket_seg_end, const int* cuts, const AllScale* sc, double* values,
                           int* cover, double* prefix, cudaStream_t s);
@@ -328,6 +344,6 @@ void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t
                           const int16_t* tree_left, const int16_t* tree_right, const uint8_t* tree_thr,
                           const uint8_t* tree_ml, const double* tree_val, const int* tree_off, int n_trees,
                           double base, double lr, const uint8_t* tree_type, const unsigned long long* tree_cat,
-                          double* out, cudaStream_t s);
+                          const int16_t* tree_feat2, int n_bins, double* out, cudaStream_t s);
 
 }  // namespace tgb

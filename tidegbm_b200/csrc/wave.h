@@ -65,6 +65,8 @@ struct WaveCtl {
     int slot0;        // first histogram slot of the planned expansions
     int error;        // a slot, buffer or wave-count bound was hit (never expected)
     int waves;        // selects run for this tree (bounded: a tree needs at most max_leaves)
+    int pair_used;    // PAIR splits committed in this tree
+    int pad[3];
     int exp_leaf[kMaxLeavesCap];
     int exp_tile0[kMaxLeavesCap + 1];
     int expanded[kMaxNodes];
@@ -101,7 +103,27 @@ struct WaveCtx {
     const uint8_t* is_cat;
     unsigned long long* cand_cat;
     double cat_smooth;
+    // PAIR splits (tree.cpp:214-281; pair_on 0: off).  A leaf whose best axis gain is weak
+    // against its gradient energy also tries the pairs of its top-k features through the
+    // histogram of the hashed code pair; splits_pair / spec_split_pair hold the best split
+    // with those pairs (the split a leaf takes while the tree's pair budget lasts), splits /
+    // spec_split the one without.  energy: per candidate index, fixed point (2^-energy_shift
+    // of the rows' sum of g^2); pair_cand: per candidate index and pair, the pair's best.
+    int pair_on;
+    int pair_top_k;
+    int max_pair;
+    int pad_pair;
+    double pair_trigger;
+    double pair_l2;
+    const double* g;           // the rows' gradients (the tree's g before GOSS scaling)
+    const uint8_t* goss_flag;  // GOSS classes (nullptr: no GOSS); class 2 rows are scaled
+    DevSplit* splits_pair;
+    DevSplit* spec_split_pair;
+    unsigned long long* energy;  // [2 * kMaxNodes + 1]
+    DevSplit* pair_cand;         // [(2 * kMaxNodes + 1)][kMaxPairs]
+    int* pair_tickets;           // [2 * kMaxNodes + 1], zero between launches
 };
+constexpr int kMaxPairs = 15;  // pairs of the top pair_top_k <= 6 features
 
 // Per-tree set-up of one context: root node (all sampled rows, slot 0), control reset.
 // use_dev_count: the sample size is st->n_sample (GOSS), else n_sample_host.
@@ -134,6 +156,10 @@ void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys
 void launch_wave_select(const WaveCtx* ctxs, int n_ctx, int* gsync, unsigned* host_flag,
                         unsigned long long cond, int use_cond, cudaStream_t s);
 void launch_wave_partition(const WaveCtx* ctxs, int n_ctx, int grid, cudaStream_t s);
+// PAIR stage after a scan (contexts with pair_on): the children's (or roots') gradient
+// energy, then for the weak ones the pair histograms and their best splits, merged into
+// spec_split_pair (roots: splits_pair[0]).
+void launch_wave_pair(const WaveCtx* ctxs, int n_ctx, int src, cudaStream_t s);
 // sc->maxg_bits / maxh_bits <- max |g[rows]| and max h[rows] (h == nullptr: 1); sc zeroed.
 void launch_rows_max(const int32_t* rows, int n_rows, const double* g, const double* h, AllScale* sc,
                      cudaStream_t s);

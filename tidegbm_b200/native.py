@@ -50,7 +50,7 @@ def lib() -> C.CDLL:
         "tgb_set_str": ([vp, cp, cp], i),
         "tgb_fit": ([vp, vp, i, vp, i, i, vp, vp], i),
         "tgb_fit_batch": ([vp, i, vp, i, vp, vp, i, vp, vp], i),
-        "tgb_tree_export_split": ([vp, i, vp, vp], i),
+        "tgb_tree_export_split": ([vp, i, vp, vp, vp], i),
         "tgb_set_categorical": ([vp, vp, i], i),
         "tgb_hist_build_quantized": ([vp, i, i, vp, i, vp, vp, i, C.c_ulonglong, vp, vp, vp, vp, vp], i),
         "tgb_predict_raw": ([vp, vp, i, i, i, vp], i),
@@ -109,8 +109,9 @@ def _ptr(a) -> C.c_void_p | None:
 _INT_KEYS = {"n_estimators", "max_depth", "max_leaves", "min_samples_leaf", "max_bin", "n_time_buckets",
              "random_state", "n_jobs", "iid_mode", "halo", "pair_splits", "horizon", "embargo", "goss",
              "bin_sample", "finer_torb", "causal_bins", "causal_structure", "verbose", "col_major_hist",
-             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune"}
-_DOUBLE_KEYS = {"cat_smooth", "learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
+             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune",
+             "pair_top_k", "max_pair_splits_per_tree"}
+_DOUBLE_KEYS = {"cat_smooth", "pair_trigger", "pair_l2", "learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
                 "colsample_bynode", "goss_top", "goss_other", "torb_min_cover", "max_delta_step", "time_decay",
                 "structure_frac", "entity_subsample"}
 _STR_KEYS = {"objective", "device"}
@@ -134,6 +135,7 @@ class Tree:
     prefix: np.ndarray
     split_type: np.ndarray | None = None  # 0 axis, 2 categorical
     cat_left: np.ndarray | None = None    # [n_nodes, 4] uint64 left masks of categorical splits
+    feature2: np.ndarray | None = None    # second feature of pair splits (-1 otherwise)
 
 
 class Booster:
@@ -254,10 +256,11 @@ class Booster:
             I = I.reshape(-1, 8)
             F = F.reshape(-1, 2)
             ty = np.zeros(nn, np.int32)
+            f2 = np.zeros(nn, np.int32)
             cm = np.zeros((nn, 4), np.uint64)
-            check(lib().tgb_tree_export_split(self._h, t, _ptr(ty), _ptr(cm)))
+            check(lib().tgb_tree_export_split(self._h, t, _ptr(ty), _ptr(f2), _ptr(cm)))
             res.append(Tree(*(I[:, k].copy() for k in range(8)), F[:, 0].copy(), F[:, 1].copy(), vals, cov, pre,
-                            ty, cm))
+                            ty, cm, f2))
         return res
 
     def edges(self, f: int) -> np.ndarray:
