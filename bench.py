@@ -788,7 +788,11 @@ def main() -> None:
     ap.add_argument("--quick", action="store_true", help="headline line only (no side workloads)")
     ap.add_argument("--serving", type=int, default=40, metavar="N",
                     help="serve an N-request trace of the serving workload (p50/p99 latency); 0: skip")
+    ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
+                    help="0: host-driven waves, every kernel its own launch (for per-kernel launch lists)")
     args = ap.parse_args()
+    if args.graph == 0:
+        PARAMS["graph"] = 0
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -965,7 +965,6 @@ public:
         mode_ = runs_[0]->mode;
         tune_.cluster = 4;
         tune_.clusters = wave_hist_clusters(4);
-        tune_.units = 2;
         ctx_.alloc(n_ctx_, s_);
         std::vector<WaveCtx> h(n_ctx_);
         for (int k = 0; k < n_ctx_; ++k) h[k] = runs_[k]->wave_ctx();
@@ -1009,26 +1008,23 @@ public:
         HistTune best = tune_;
         float best_ms = 1e30f;
         for (int cl : {1, 2, 4}) {
-            for (int un : {1, 2, 4}) {
-                HistTune t;
-                t.cluster = cl;
-                t.clusters = wave_hist_clusters(cl);
-                t.units = un;
-                float ms_min = 1e30f;
-                for (int rep = 0; rep < 3; ++rep) {
-                    zero_roots();
-                    check(cudaEventRecord(a, s_), "event record");
-                    launch_wave_hist(mode_, ctx_.p, n_ctx_, 0, t, nullptr, s_);
-                    check(cudaEventRecord(b, s_), "event record");
-                    check(cudaEventSynchronize(b), "tune event");
-                    float ms = 0.f;
-                    check(cudaEventElapsedTime(&ms, a, b), "tune time");
-                    if (rep > 0) ms_min = std::min(ms_min, ms);
-                }
-                if (ms_min < best_ms) {
-                    best_ms = ms_min;
-                    best = t;
-                }
+            HistTune t;
+            t.cluster = cl;
+            t.clusters = wave_hist_clusters(cl);
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                zero_roots();
+                check(cudaEventRecord(a, s_), "event record");
+                launch_wave_hist(mode_, ctx_.p, n_ctx_, 0, t, nullptr, s_);
+                check(cudaEventRecord(b, s_), "event record");
+                check(cudaEventSynchronize(b), "tune event");
+                float ms = 0.f;
+                check(cudaEventElapsedTime(&ms, a, b), "tune time");
+                if (rep > 0) ms_min = std::min(ms_min, ms);
+            }
+            if (ms_min < best_ms) {
+                best_ms = ms_min;
+                best = t;
             }
         }
         cudaEventDestroy(a);
@@ -1256,7 +1252,7 @@ void fit_runs(std::vector<FitRun*>& runs, cudaStream_t s) {
     if (drv) {
         r0.st.graph_used = drv->graph_used() ? 1 : 0;
         r0.st.hist_cluster = drv->tune().cluster;
-        r0.st.hist_units = drv->tune().units;
+        r0.st.hist_clusters = drv->tune().clusters;
     }
     check(cudaStreamSynchronize(s), "tree loop");
     for (auto* r : runs) r->st.t_trees = now() - ttree;

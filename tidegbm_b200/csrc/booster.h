@@ -117,7 +117,7 @@ struct FitStats {
     long long hist_rows = 0;  // rows histogrammed in the timed range
     long long timed_selects = 0;  // wave selects run in the timed range (batched growth)
     int graph_used = 0;           // the waves ran as a CUDA graph with a device-side loop
-    int hist_cluster = 0, hist_units = 0;  // the histogram's launch shape (autotuned)
+    int hist_cluster = 0, hist_clusters = 0;  // the histogram's launch shape (autotuned)
 };
 
 struct DeviceState;  // device buffers of one fit

@@ -434,7 +434,7 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "timed_selects") *out = static_cast<double>(s.timed_selects);
         else if (k == "graph_used") *out = s.graph_used;
         else if (k == "hist_cluster") *out = s.hist_cluster;
-        else if (k == "hist_units") *out = s.hist_units;
+        else if (k == "hist_clusters") *out = s.hist_clusters;
         else if (k == "pre_upload") *out = s.t_pre_upload;
         else if (k == "prep") *out = s.t_prep;
         else throw tgb::TideError("unknown fit stat: " + k);

@@ -4,17 +4,18 @@
 // Histogram (build_hist_col, cpp/src/histogram.cpp:44-76, for the smaller child of every
 // planned leaf; subtract_hist_inplace's larger child is derived in the scan).  One
 // persistent launch of clusters of 1, 2 or 4 CTAs (the autotuned privatisation depth:
-// how many CTA-private histograms a flush merges).  The work is cut into units (context,
-// leaf, group of 32 features, chunk of rows), about `units` per cluster; a cluster takes
-// units in turn and its CTAs split the unit's rows.  Inside a CTA the accumulation is the lane-per-row scheme:
+// how many CTA-private histograms a flush merges).  The work (rows x groups of 32
+// features, summed over the jobs) is cut into one contiguous range per cluster, walked as
+// pieces (job, feature group, rows) whose rows the cluster's CTAs split.  Inside a CTA the
+// accumulation is the lane-per-row scheme:
 // a warp takes 32 rows, lane l loads its row's 32 code bytes of the group with two
 // 16-byte loads and rotates them by l bytes in registers, so step j of the 32-step loop
 // touches feature (j + l) & 31: 32 lanes, 32 features, 32 banks of the [bin][feature]
 // layout, conflict-free whatever the codes.  Every code costs fire-and-forget 32-bit
 // shared reductions only (their count depends on the payload mode, below), exact over a
-// sub-chunk of rows, folded into per-thread 64-bit registers after every sub-chunk.  At
-// the end of a unit the cluster adds its partial histograms through distributed shared
-// memory and each CTA flushes its share of the cells with 64-bit global atomics.
+// sub-chunk of rows, folded into 64-bit totals after every sub-chunk.  At the end of a
+// piece the cluster adds its CTAs' totals through distributed shared memory and each CTA
+// writes its share of the cells out (coalesced: consecutive bins of a feature).
 //
 // Payload modes (HistMode, per row):
 //   exact const  int64 (v << 1 | goss):  v split into a 19-bit low and a signed high
@@ -44,12 +45,8 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kFG = 32;
 constexpr int kPlane = kFG * kBins;  // 32-bit words per plane (8192)
 constexpr int kCells = kPlane / kThreads;  // cells a thread folds (8)
-constexpr int kTotPlanes = 5;  // totals: G lo, G hi, H lo, H hi, count
 constexpr size_t kPlaneBytes = static_cast<size_t>(kPlane) * 4;
-constexpr size_t kJobBytes = static_cast<size_t>(kMaxWaveJobs) * 4 * 3 + 4 * 8;
-constexpr size_t kWaveSmem = kPlaneBytes * kTotPlanes + kJobBytes;
 constexpr int kLoBits = 19;
-constexpr int kMinUnitRows = 4096;
 
 template <int kMode>
 struct ModeTraits;
@@ -123,30 +120,186 @@ __device__ __forceinline__ JobRows job_rows(const WaveCtx& X, int src, int e) {
     return r;
 }
 
-// The rows [r0, r1) of one unit (one group of 32 features), lane = row: a warp takes 32
-// rows, lane l loads its row's 32 code bytes with two 16-byte loads and rotates them by l
-// bytes, so step j touches feature (j + l) & 31 (conflict-free banks); every code costs
-// the mode's fire-and-forget 32-bit reductions, folded into 64-bit registers every
-// sub-chunk.  Ends with the CTA's totals in the 5 planes (G lo, G hi, H lo, H hi, count).
-// A separate (not inlined) function: the hot loop keeps only its own state in registers.
-// Row counts of the constant-hessian modes travel packed (unscaled | GOSS-scaled << 16);
-// a CTA's share of a unit has fewer than 2^16 rows.
+// A CTA's totals in a padded [feature][bin] layout, index f * kTotPitch + b: the fold
+// writes one bin of a warp's 32 features and the flush reads 32 consecutive bins of one
+// feature, and with a pitch of 257 words both touch 32 distinct banks; the flush's global
+// writes are then consecutive bins of a feature (whole sectors).
+constexpr int kTotPitch = kBins + 1;
+constexpr int kTot = kFG * kTotPitch;  // 8224 cells
+// Rows of one CTA's share of a piece: the constant-hessian modes pack their two row counts
+// (unscaled, GOSS-scaled) into 16-bit halves.
+constexpr int kMaxShareRows = 65535;
+
+// Dynamic shared memory of one instantiation.  Constant-hessian modes: the working planes,
+// then the totals (G as 64-bit words, packed counts), folded every sub-chunk.  Per-row
+// hessian modes: 64-bit register accumulators, their totals (G, H as 64-bit words, counts)
+// written over the working planes at the end of a piece.  Then the work prefix of the jobs.
 template <int kMode>
-__device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const int32_t* __restrict__ rows, int r0,
-                                             int r1, const uint8_t* __restrict__ codes, int stride, int fg0,
-                                             const void* __restrict__ gqp, const void* __restrict__ hqp,
-                                             unsigned long long hq1, unsigned long long hq2) {
+struct SmemLayout {
+    using T = ModeTraits<kMode>;
+    static constexpr size_t work = static_cast<size_t>(T::planes) * kPlaneBytes;
+    static constexpr size_t tot_bytes = static_cast<size_t>(kTot) * (T::var ? 20 : 12);
+    static constexpr size_t tot_off = T::var ? 0 : work;
+    static constexpr size_t region = T::var ? (work > tot_bytes ? work : tot_bytes) : work + tot_bytes;
+    static constexpr size_t plan_off = (region + 15) / 16 * 16;
+    static constexpr size_t bytes = plan_off + sizeof(unsigned long long) * (kMaxWaveJobs + 1);
+    static_assert(bytes + 2048 <= 232448, "wave histogram shared memory above the 227 KB opt-in");
+    static_assert(region % 16 == 0 && tot_off % 16 == 0, "16-byte zeroing");
+};
+
+template <int kMode>
+struct ConstPayload;
+template <>
+struct ConstPayload<kHistExactConst> {
+    using type = long long;
+};
+template <>
+struct ConstPayload<kHistQ16Const> {
+    using type = int;
+};
+template <>
+struct ConstPayload<kHistQ8Const> {
+    using type = short;
+};
+
+// One row of a constant-hessian mode: its 32 codes (two 16-byte words, rotated by the
+// lane so that step j touches feature (j + lane) & 31) into the working planes.
+template <int kMode>
+__device__ __forceinline__ void add_row_const(unsigned int* __restrict__ P, typename ConstPayload<kMode>::type p,
+                                              const uint4 ca, const uint4 cb, int lane, int q, int sh) {
+    unsigned int a0, a1 = 0u, a2 = 0u;
+    unsigned int* plane = P;
+    if constexpr (kMode == kHistExactConst) {
+        const long long v = p >> 1;
+        a0 = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
+        a1 = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
+        a2 = (p & 1) ? 0x10000u : 1u;
+    } else if constexpr (kMode == kHistQ16Const) {
+        a0 = static_cast<unsigned int>(p >> 1);
+        a1 = (p & 1) ? 0x10000u : 1u;
+    } else {
+        const int pv = p;
+        a0 = (1u << 20) | static_cast<unsigned int>((pv >> 1) + 128);
+        plane = (pv & 1) ? P + kPlane : P;
+    }
+    unsigned int wd[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+    rotate_words(wd, q);
+    unsigned int Rw[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) Rw[t] = __funnelshift_r(wd[t], wd[(t + 1) & 7], sh);
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) {
+        const int f = (jj + lane) & 31;
+        const unsigned int code = (Rw[jj >> 2] >> ((jj & 3) * 8)) & 0xffu;
+        const int cell = static_cast<int>(code) * 32 + f;
+        if constexpr (kMode == kHistExactConst) {
+            atomicAdd(&P[cell], a0);
+            atomicAdd(&P[kPlane + cell], a1);
+            atomicAdd(&P[2 * kPlane + cell], a2);
+        } else if constexpr (kMode == kHistQ16Const) {
+            atomicAdd(&P[cell], a0);
+            atomicAdd(&P[kPlane + cell], a1);
+        } else {
+            atomicAdd(&plane[cell], a0);
+        }
+    }
+}
+
+// The rows [r0, r1) of a CTA's share of one piece (one group of 32 features), constant-
+// hessian modes, lane = row: every code costs the mode's fire-and-forget 32-bit shared
+// reductions, exact over a sub-chunk of rows and folded into the shared 64-bit totals after
+// it.  Software-pipelined: a warp's next row index is loaded two steps ahead and its codes
+// and payload one step ahead, so their latency overlaps the current step's reductions.  A
+// separate (not inlined) function: the loop keeps only its own state in registers.
+template <int kMode>
+__device__ __noinline__ void accumulate_const(unsigned int* __restrict__ P, unsigned long long* __restrict__ Gt,
+                                              unsigned int* __restrict__ Ct, const int32_t* __restrict__ rows, int r0,
+                                              int r1, const uint8_t* __restrict__ codes, int stride, int fg0,
+                                              const void* __restrict__ gqp) {
+    using T = ModeTraits<kMode>;
+    using PT = typename ConstPayload<kMode>::type;
+    const PT* __restrict__ pay = static_cast<const PT*>(gqp);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = lane >> 2, sh = (lane & 3) * 8;
+    const bool two_chunks = stride - fg0 >= 32;
+    constexpr int kStep = kWarps * 32;
+    for (int s0 = r0; s0 < r1; s0 += T::sub) {
+        const int s1 = min(r1, s0 + T::sub);
+        const int k0 = s0 + warp * 32 + lane;
+        int r_cur = k0 < s1 ? rows[k0] : -1;
+        int r_nxt = k0 + kStep < s1 ? rows[k0 + kStep] : -1;
+        uint4 ca = make_uint4(0, 0, 0, 0), cb = make_uint4(0, 0, 0, 0);
+        PT p = 0;
+        if (r_cur >= 0) {
+            const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r_cur) * stride + fg0);
+            ca = __ldg(src4);
+            if (two_chunks) cb = __ldg(src4 + 1);
+            p = pay[r_cur];
+        }
+        for (int base = s0 + warp * 32; base < s1; base += kStep) {
+            const int r = r_cur;
+            const uint4 xa = ca, xb = cb;
+            const PT xp = p;
+            r_cur = r_nxt;
+            const int kn = base + 2 * kStep + lane;
+            r_nxt = kn < s1 ? rows[kn] : -1;
+            if (r_cur >= 0) {
+                const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r_cur) * stride + fg0);
+                ca = __ldg(src4);
+                cb = two_chunks ? __ldg(src4 + 1) : make_uint4(0, 0, 0, 0);
+                p = pay[r_cur];
+            }
+            if (r >= 0) add_row_const<kMode>(P, xp, xa, xb, lane, q, sh);
+        }
+        __syncthreads();
+        // fold the sub-chunk into the totals and clear the working planes
+#pragma unroll
+        for (int cc = 0; cc < kCells; ++cc) {
+            const int cell = threadIdx.x + cc * kThreads;
+            const int ti = (cell & 31) * kTotPitch + (cell >> 5);
+            long long dg;
+            unsigned int dc;
+            if constexpr (kMode == kHistExactConst) {
+                dg = static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
+                dc = P[2 * kPlane + cell];
+            } else if constexpr (kMode == kHistQ16Const) {
+                dg = static_cast<int>(P[cell]);
+                dc = P[kPlane + cell];
+            } else {
+                const unsigned int w1 = P[cell], w2 = P[kPlane + cell];
+                const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
+                dg = static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
+                     128ll * static_cast<long long>(n1 + n2);
+                dc = n1 | (n2 << 16);
+            }
+            Gt[ti] += static_cast<unsigned long long>(dg);
+            Ct[ti] += dc;
+#pragma unroll
+            for (int pl = 0; pl < T::planes; ++pl) P[pl * kPlane + cell] = 0u;
+        }
+        __syncthreads();
+    }
+}
+
+// The rows [r0, r1) of a CTA's share of one piece, per-row hessian modes: the same lane-
+// per-row reductions, folded into per-thread 64-bit registers every sub-chunk; the totals
+// are written over the (then clear) working planes at the end.
+template <int kMode>
+__device__ __noinline__ void accumulate_var(unsigned int* __restrict__ P, unsigned long long* __restrict__ Gt,
+                                            unsigned long long* __restrict__ Ht, unsigned int* __restrict__ Ct,
+                                            const int32_t* __restrict__ rows, int r0, int r1,
+                                            const uint8_t* __restrict__ codes, int stride, int fg0,
+                                            const void* __restrict__ gqp, const void* __restrict__ hqp) {
     using T = ModeTraits<kMode>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q = lane >> 2, sh = (lane & 3) * 8;
     const bool two_chunks = stride - fg0 >= 32;
-    long long accG[kCells];
-    long long accH[T::var ? kCells : 1];
+    long long accG[kCells], accH[kCells];
     unsigned int accC[kCells];
 #pragma unroll
     for (int cc = 0; cc < kCells; ++cc) {
         accG[cc] = 0;
-        if constexpr (T::var) accH[cc] = 0;
+        accH[cc] = 0;
         accC[cc] = 0u;
     }
     for (int s0 = r0; s0 < r1; s0 += T::sub) {
@@ -157,34 +310,18 @@ __device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const
             const int kn = base + kWarps * 32 + lane;
             r_next = kn < s1 ? rows[kn] : -1;
             if (r < 0) continue;
-            // payload words of this row (mode dependent)
             unsigned int a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-            unsigned int* plane = P;
-            if constexpr (kMode == kHistExactConst) {
-                const long long p = static_cast<const long long*>(gqp)[r];
-                const long long v = p >> 1;
-                a0 = static_cast<unsigned int>(v) & ((1u << kLoBits) - 1u);
-                a1 = static_cast<unsigned int>(static_cast<int>(v >> kLoBits));
-                a2 = (p & 1) ? 0x10000u : 1u;
-            } else if constexpr (kMode == kHistExactVar) {
+            if constexpr (kMode == kHistExactVar) {
                 const long long gv = static_cast<const long long*>(gqp)[r];
                 const long long hv = static_cast<const long long*>(hqp)[r];
                 a0 = static_cast<unsigned int>(gv) & ((1u << kLoBits) - 1u);
                 a1 = static_cast<unsigned int>(static_cast<int>(gv >> kLoBits));
                 a2 = static_cast<unsigned int>(hv) & ((1u << kLoBits) - 1u);
                 a3 = static_cast<unsigned int>(static_cast<int>(hv >> kLoBits));
-            } else if constexpr (kMode == kHistQ16Const) {
-                const int p = static_cast<const int*>(gqp)[r];
-                a0 = static_cast<unsigned int>(p >> 1);
-                a1 = (p & 1) ? 0x10000u : 1u;
             } else if constexpr (kMode == kHistQ16Var) {
                 const unsigned int p = static_cast<const unsigned int*>(gqp)[r];
                 a0 = static_cast<unsigned int>(static_cast<int>(p) >> 16);
                 a1 = p & 0xffffu;
-            } else if constexpr (kMode == kHistQ8Const) {
-                const int p = static_cast<const short*>(gqp)[r];
-                a0 = (1u << 20) | static_cast<unsigned int>((p >> 1) + 128);
-                plane = (p & 1) ? P + kPlane : P;
             } else {  // kHistQ8Var
                 const unsigned int p = static_cast<const unsigned short*>(gqp)[r];
                 a0 = (1u << 20) | (p & 0xffu);
@@ -203,25 +340,16 @@ __device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const
                 const int f = (jj + lane) & 31;
                 const unsigned int code = (Rw[jj >> 2] >> ((jj & 3) * 8)) & 0xffu;
                 const int cell = static_cast<int>(code) * 32 + f;
-                if constexpr (kMode == kHistExactConst) {
-                    atomicAdd(&P[cell], a0);
-                    atomicAdd(&P[kPlane + cell], a1);
-                    atomicAdd(&P[2 * kPlane + cell], a2);
-                } else if constexpr (kMode == kHistExactVar) {
+                if constexpr (kMode == kHistExactVar) {
                     atomicAdd(&P[cell], a0);
                     atomicAdd(&P[kPlane + cell], a1);
                     atomicAdd(&P[2 * kPlane + cell], a2);
                     atomicAdd(&P[3 * kPlane + cell], a3);
                     atomicAdd(&P[4 * kPlane + cell], 1u);
-                } else if constexpr (kMode == kHistQ16Const) {
-                    atomicAdd(&P[cell], a0);
-                    atomicAdd(&P[kPlane + cell], a1);
                 } else if constexpr (kMode == kHistQ16Var) {
                     atomicAdd(&P[cell], a0);
                     atomicAdd(&P[kPlane + cell], a1);
                     atomicAdd(&P[2 * kPlane + cell], 1u);
-                } else if constexpr (kMode == kHistQ8Const) {
-                    atomicAdd(&plane[cell], a0);
                 } else {
                     atomicAdd(&P[cell], a0);
                     atomicAdd(&P[kPlane + cell], a1);
@@ -233,27 +361,15 @@ __device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const
 #pragma unroll
         for (int cc = 0; cc < kCells; ++cc) {
             const int cell = threadIdx.x + cc * kThreads;
-            if constexpr (kMode == kHistExactConst) {
-                accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
-                accC[cc] += P[2 * kPlane + cell];
-            } else if constexpr (kMode == kHistExactVar) {
+            if constexpr (kMode == kHistExactVar) {
                 accG[cc] += static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
                 accH[cc] +=
                     static_cast<long long>(static_cast<int>(P[3 * kPlane + cell])) * (1ll << kLoBits) + P[2 * kPlane + cell];
                 accC[cc] += P[4 * kPlane + cell];
-            } else if constexpr (kMode == kHistQ16Const) {
-                accG[cc] += static_cast<int>(P[cell]);
-                accC[cc] += P[kPlane + cell];
             } else if constexpr (kMode == kHistQ16Var) {
                 accG[cc] += static_cast<int>(P[cell]);
                 accH[cc] += P[kPlane + cell];
                 accC[cc] += P[2 * kPlane + cell];
-            } else if constexpr (kMode == kHistQ8Const) {
-                const unsigned int w1 = P[cell], w2 = P[kPlane + cell];
-                const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
-                accG[cc] += static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
-                            128ll * static_cast<long long>(n1 + n2);
-                accC[cc] += n1 | (n2 << 16);
             } else {
                 const unsigned int w1 = P[cell];
                 const unsigned int n1 = w1 >> 20;
@@ -266,51 +382,45 @@ __device__ __noinline__ void accumulate_unit(unsigned int* __restrict__ P, const
         }
         __syncthreads();
     }
-    // totals -> 5 planes
+    // totals over the (clear) planes: every cell of the padded layout has one owner
 #pragma unroll
     for (int cc = 0; cc < kCells; ++cc) {
         const int cell = threadIdx.x + cc * kThreads;
-        unsigned long long Hs;
-        unsigned int Cn;
-        if constexpr (T::var) {
-            Hs = static_cast<unsigned long long>(accH[cc]);
-            Cn = accC[cc];
-        } else {
-            const unsigned int c1 = accC[cc] & 0xffffu, c2 = accC[cc] >> 16;
-            Hs = static_cast<unsigned long long>(c1) * hq1 + static_cast<unsigned long long>(c2) * hq2;
-            Cn = c1 + c2;
-        }
-        const unsigned long long Gs = static_cast<unsigned long long>(accG[cc]);
-        P[cell] = static_cast<unsigned int>(Gs);
-        P[kPlane + cell] = static_cast<unsigned int>(Gs >> 32);
-        P[2 * kPlane + cell] = static_cast<unsigned int>(Hs);
-        P[3 * kPlane + cell] = static_cast<unsigned int>(Hs >> 32);
-        P[4 * kPlane + cell] = Cn;
+        const int ti = (cell & 31) * kTotPitch + (cell >> 5);
+        Gt[ti] = static_cast<unsigned long long>(accG[cc]);
+        Ht[ti] = static_cast<unsigned long long>(accH[cc]);
+        Ct[ti] = accC[cc];
     }
 }
 
+// One launch histograms every job (context, planned leaf's smaller child; or each
+// context's root) of the wave.  The work, rows x feature groups summed over the jobs, is
+// cut into equal contiguous ranges, one per cluster; a cluster walks its range as pieces
+// (job, feature group, row range), its CTAs split each piece's rows, and after a piece the
+// cluster adds its CTAs' totals through distributed shared memory and writes them out:
+// plain stores when the piece is the whole (job, feature group), 64-bit atomics when
+// other clusters share it.  A job's slot is clear before the launch.
 template <int kMode>
 __global__ void __launch_bounds__(kThreads, 1)
-    wave_hist_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src, unsigned long long* rows_counter,
-                     int unit_target) {
+    wave_hist_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src, unsigned long long* rows_counter) {
     using T = ModeTraits<kMode>;
+    using Lay = SmemLayout<kMode>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned int* P = reinterpret_cast<unsigned int*>(smem_raw);  // planes
-    int* s_ustart = reinterpret_cast<int*>(smem_raw + kPlaneBytes * kTotPlanes);  // [kMaxWaveJobs]
-    int* s_job = s_ustart + kMaxWaveJobs;                                            // ctx << 16 | exp
-    int* s_rows = s_job + kMaxWaveJobs;                                              // job row counts
-    int* s_misc = s_rows + kMaxWaveJobs;  // [0] jobs, [1] units, [2] unit rows, [3..7] reduction
+    unsigned int* P = reinterpret_cast<unsigned int*>(smem_raw);  // working planes
+    unsigned long long* Gt = reinterpret_cast<unsigned long long*>(smem_raw + Lay::tot_off);
+    unsigned long long* Ht = Gt + kTot;  // per-row hessian modes only
+    unsigned int* Ct = reinterpret_cast<unsigned int*>(Gt + (T::var ? 2 : 1) * kTot);
+    unsigned long long* s_wstart = reinterpret_cast<unsigned long long*>(smem_raw + Lay::plan_off);
     {  // private state first: it overlaps the previous kernel's tail
         uint4* z = reinterpret_cast<uint4*>(smem_raw);
-        for (int k = threadIdx.x; k < T::planes * kPlane / 4; k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
+        for (int k = threadIdx.x; k < static_cast<int>(Lay::region / 16); k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
     }
     pdl_wait();
     pdl_trigger();
 
-    // ---- unit plan (the same in every CTA) ----
+    // ---- work plan (the same in every CTA) ----
     __shared__ int s_cpref[kMaxWaveCtx + 1];
-    __shared__ unsigned long long s_red[kWarps];
-    __shared__ int s_wsum[kWarps];
+    __shared__ unsigned long long s_red[kWarps], s_rsum[kWarps];
     if (static_cast<int>(threadIdx.x) < n_ctx)
         s_cpref[threadIdx.x] = src == 0 ? (ctxs[threadIdx.x].ctl->active ? 1 : 0) : ctxs[threadIdx.x].ctl->n_exp;
     __syncthreads();
@@ -325,135 +435,139 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncthreads();
     const int n_jobs = s_cpref[n_ctx];
-    unsigned long long w = 0;
-    for (int j = threadIdx.x; j < n_jobs; j += blockDim.x) {
-        int c = 0;
-        while (c + 1 < n_ctx && s_cpref[c + 1] <= j) ++c;
-        const int e = src == 0 ? 0 : j - s_cpref[c];
-        const WaveCtx& X = ctxs[c];
-        const JobRows jr = job_rows(X, src, e);
-        const int nfg = (X.gp.n_features + kFG - 1) / kFG;
-        s_job[j] = (c << 16) | e;
-        s_rows[j] = jr.count;
-        s_ustart[j] = nfg;  // feature groups for now; units below
-        w += static_cast<unsigned long long>(jr.count) * nfg;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = w;
-    __syncthreads();
-    int unit_rows_b;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     {
-        unsigned long long tot = 0;
-        for (int k = 0; k < kWarps; ++k) tot += s_red[k];
-        const int n_cl0 = static_cast<int>(gridDim.y / cg::this_cluster().dim_blocks().y);
-        const unsigned long long target =
-            static_cast<unsigned long long>(max(1, unit_target)) * static_cast<unsigned long long>(max(1, n_cl0));
-        const unsigned long long u = (tot + target - 1) / target;
-        // a CTA's share of a unit stays below 2^16 rows: its row counts pack into 16-bit fields
-        const unsigned long long cap = 65535ull * cg::this_cluster().dim_blocks().y;
-        unit_rows_b = static_cast<int>(min(max(static_cast<unsigned long long>(kMinUnitRows), u), cap));
-    }
-    // units of each job: exclusive prefix over the jobs, a contiguous run per thread
-    {
+        // work of each job (rows x feature groups), exclusive prefix over a contiguous run
+        // of jobs per thread
         const int per = (n_jobs + kThreads - 1) / kThreads;
-        const int j0 = threadIdx.x * per, j1 = min(n_jobs, j0 + per);
-        int local = 0;
+        const int j0 = min(n_jobs, static_cast<int>(threadIdx.x) * per), j1 = min(n_jobs, j0 + per);
+        unsigned long long local = 0, lrows = 0;
         for (int j = j0; j < j1; ++j) {
-            const int r = s_rows[j];
-            const int units = r > 0 ? s_ustart[j] * ((r + unit_rows_b - 1) / unit_rows_b) : 0;
-            s_ustart[j] = units;
-            local += units;
+            int c = 0;
+            while (c + 1 < n_ctx && s_cpref[c + 1] <= j) ++c;
+            const WaveCtx& X = ctxs[c];
+            const JobRows jr = job_rows(X, src, src == 0 ? 0 : j - s_cpref[c]);
+            const unsigned long long w =
+                static_cast<unsigned long long>(jr.count) * ((X.gp.n_features + kFG - 1) / kFG);
+            s_wstart[j] = w;
+            local += w;
+            lrows += static_cast<unsigned long long>(jr.count);
         }
-        const int lane0 = threadIdx.x & 31, warp0 = threadIdx.x >> 5;
-        int incl = local;
+        unsigned long long incl = local, rs = lrows;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane0 >= o) incl += t;
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+            rs += __shfl_xor_sync(0xffffffffu, rs, o);
         }
-        if (lane0 == 31) s_wsum[warp0] = incl;
+        if (lane == 31) s_red[warp] = incl;
+        if (lane == 0) s_rsum[warp] = rs;
         __syncthreads();
-        int wbase = 0, all = 0;
+        unsigned long long wbase = 0, all = 0, rows_all = 0;
         for (int k = 0; k < kWarps; ++k) {
-            if (k < warp0) wbase += s_wsum[k];
-            all += s_wsum[k];
+            if (k < warp) wbase += s_red[k];
+            all += s_red[k];
+            rows_all += s_rsum[k];
         }
-        int run = wbase + incl - local;
+        unsigned long long run = wbase + incl - local;
         for (int j = j0; j < j1; ++j) {
-            const int units = s_ustart[j];
-            s_ustart[j] = run;
-            run += units;
+            const unsigned long long w = s_wstart[j];
+            s_wstart[j] = run;
+            run += w;
         }
         if (threadIdx.x == 0) {
-            s_misc[0] = n_jobs;
-            s_misc[1] = all;
-            s_misc[2] = unit_rows_b;
+            s_wstart[n_jobs] = all;
+            if (rows_counter != nullptr && blockIdx.y == 0) atomicAdd(rows_counter, rows_all);
         }
     }
     __syncthreads();
-    const int n_units = s_misc[1], unit_rows = s_misc[2];
     cg::cluster_group cluster = cg::this_cluster();
     const int csize = static_cast<int>(cluster.dim_blocks().y);  // CTAs per cluster: 1, 2 or 4
     const int cl = static_cast<int>(blockIdx.y) / csize;
     const int n_cl = static_cast<int>(gridDim.y) / csize;
     const unsigned int rank = cluster.block_rank();
-    for (int u = cl; u < n_units; u += n_cl) {
-        // unit -> job (binary search over the unit starts), feature group, row chunk
+    const unsigned long long w_all = s_wstart[n_jobs];
+    const unsigned long long w_end = w_all * static_cast<unsigned long long>(cl + 1) / static_cast<unsigned long long>(n_cl);
+    const unsigned long long max_piece = static_cast<unsigned long long>(kMaxShareRows) * csize;
+    for (unsigned long long w = w_all * static_cast<unsigned long long>(cl) / static_cast<unsigned long long>(n_cl);
+         w < w_end;) {
+        // the job holding w: the last j with s_wstart[j] <= w (a non-empty job)
         int lo = 0, hi = n_jobs - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (s_ustart[mid] <= u) lo = mid;
+            if (s_wstart[mid] <= w) lo = mid;
             else hi = mid - 1;
         }
         const int j = lo;
-        const int c = s_job[j] >> 16, e = s_job[j] & 0xffff;
+        int c = 0;
+        while (c + 1 < n_ctx && s_cpref[c + 1] <= j) ++c;
         const WaveCtx& X = ctxs[c];
         const int n_f = X.gp.n_features;
-        const int nfg = (n_f + kFG - 1) / kFG;
-        const int k = u - s_ustart[j];
-        const int fg = k % nfg, chunk = k / nfg;
-        const JobRows jr = job_rows(X, src, e);
-        const int R = jr.count;
-        const int n_chunks = (R + unit_rows - 1) / unit_rows;
-        const int crows = (R + n_chunks - 1) / n_chunks;
-        const int c0 = min(R, chunk * crows), c1 = min(R, c0 + crows);
-        const int qrows = (c1 - c0 + csize - 1) / csize;
-        const int r0 = min(c1, c0 + static_cast<int>(rank) * qrows), r1 = min(c1, r0 + qrows);
-        if (rows_counter != nullptr && rank == 0 && k == 0 && threadIdx.x == 0)
-            atomicAdd(rows_counter, static_cast<unsigned long long>(R));
-        const double hscale = X.st->hscale;
-        // this CTA's rows of the unit -> its totals in the 5 planes of its shared memory
-        accumulate_unit<kMode>(P, jr.rows, r0, r1, X.codes, X.gp.stride, fg * kFG, X.gq, X.hq,
-                               static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale)),
-                               static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * hscale)));
-        cluster.sync();
-        const int share = kPlane / csize;
+        const JobRows jr = job_rows(X, src, src == 0 ? 0 : j - s_cpref[c]);
+        const unsigned long long R = static_cast<unsigned long long>(jr.count);
+        const unsigned long long off = w - s_wstart[j];
+        const int fg = static_cast<int>(off / R);
+        const unsigned long long ra = off - static_cast<unsigned long long>(fg) * R;
+        const unsigned long long len = min(min(R - ra, w_end - w), max_piece);
+        const int piece0 = static_cast<int>(ra), piece1 = static_cast<int>(ra + len);
+        const int qrows = (piece1 - piece0 + csize - 1) / csize;
+        const int r0 = min(piece1, piece0 + static_cast<int>(rank) * qrows), r1 = min(piece1, r0 + qrows);
         const int fg0 = fg * kFG;
+        if constexpr (T::var)
+            accumulate_var<kMode>(P, Gt, Ht, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, X.gq, X.hq);
+        else
+            accumulate_const<kMode>(P, Gt, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, X.gq);
+        __syncthreads();
+        cluster.sync();
+        // rank k adds its share of the cells over the cluster and writes them out
+        const bool whole = piece0 == 0 && static_cast<unsigned long long>(piece1) == R;
         const int nf_here = min(kFG, n_f - fg0);
         const size_t slot_off = static_cast<size_t>(jr.slot) * static_cast<size_t>(n_f) * kBins;
-        for (int cell = rank * share + threadIdx.x; cell < static_cast<int>(rank + 1) * share; cell += kThreads) {
-            unsigned long long g = 0, hsum = 0;
-            unsigned int cn = 0;
+        const double hscale = X.st->hscale;
+        const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hscale));
+        const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * hscale));
+        const int share = (kTot + csize - 1) / csize;
+        const int i1 = min(kTot, static_cast<int>(rank + 1) * share);
+        for (int ti = static_cast<int>(rank) * share + threadIdx.x; ti < i1; ti += kThreads) {
+            const int f = ti / kTotPitch, b = ti - f * kTotPitch;
+            if (b >= kBins || f >= nf_here) continue;
+            unsigned long long g = 0, hs = 0;
+            unsigned int cn = 0, c1 = 0, c2 = 0;
             for (int kk = 0; kk < csize; ++kk) {
-                const unsigned int* rt = cluster.map_shared_rank(P, kk);
-                g += (static_cast<unsigned long long>(rt[kPlane + cell]) << 32) | rt[cell];
-                hsum += (static_cast<unsigned long long>(rt[3 * kPlane + cell]) << 32) | rt[2 * kPlane + cell];
-                cn += rt[4 * kPlane + cell];
+                g += cluster.map_shared_rank(Gt, kk)[ti];
+                const unsigned int pc = cluster.map_shared_rank(Ct, kk)[ti];
+                if constexpr (T::var) {
+                    hs += cluster.map_shared_rank(Ht, kk)[ti];
+                    cn += pc;
+                } else {
+                    c1 += pc & 0xffffu;
+                    c2 += pc >> 16;
+                }
             }
-            const int b = cell >> 5, f = cell & 31;
-            if (f >= nf_here || cn == 0u) continue;
+            if constexpr (!T::var) {
+                hs = static_cast<unsigned long long>(c1) * hq1 + static_cast<unsigned long long>(c2) * hq2;
+                cn = c1 + c2;
+            }
+            if (cn == 0u) continue;
             const size_t o = slot_off + static_cast<size_t>(fg0 + f) * kBins + b;
-            atomicAdd(reinterpret_cast<unsigned long long*>(X.G) + o, g);
-            atomicAdd(reinterpret_cast<unsigned long long*>(X.H) + o, hsum);
-            atomicAdd(X.C + o, static_cast<int>(cn));
+            if (whole) {
+                reinterpret_cast<unsigned long long*>(X.G)[o] = g;
+                reinterpret_cast<unsigned long long*>(X.H)[o] = hs;
+                X.C[o] = static_cast<int>(cn);
+            } else {
+                atomicAdd(reinterpret_cast<unsigned long long*>(X.G) + o, g);
+                atomicAdd(reinterpret_cast<unsigned long long*>(X.H) + o, hs);
+                atomicAdd(X.C + o, static_cast<int>(cn));
+            }
         }
-        cluster.sync();  // no CTA reuses its planes while others read them
+        cluster.sync();  // no CTA clears its totals while others read them
         {
-            uint4* z = reinterpret_cast<uint4*>(smem_raw);
-            for (int kk = threadIdx.x; kk < T::planes * kPlane / 4; kk += blockDim.x) z[kk] = make_uint4(0, 0, 0, 0);
+            uint4* z = reinterpret_cast<uint4*>(smem_raw + Lay::tot_off);
+            for (int k = threadIdx.x; k < static_cast<int>(Lay::tot_bytes / 16); k += kThreads)
+                z[k] = make_uint4(0, 0, 0, 0);
         }
         __syncthreads();
+        w += len;
     }
 }
 
@@ -551,7 +665,7 @@ __global__ void __launch_bounds__(kPartThreads)
         const WaveCtx& X = ctxs[tr.c];
         const int L = X.ctl->exp_leaf[tr.e];
         const DevNode& N = X.nodes[L];
-        const DevSplit& S = X.splits[L];
+        const DevSplit& S = X.ctl->expanded[L] == 2 ? X.splits_pair[L] : X.splits[L];
         const int32_t* in = (N.buf ? X.rows1 : X.rows0) + N.start;
         const int base = tr.k * kPartTile, end = min(base + kPartTile, N.count);
         int32_t row[kPartPer];
@@ -602,7 +716,7 @@ __global__ void __launch_bounds__(kPartThreads)
         const WaveCtl* ctl = X.ctl;
         const int L = ctl->exp_leaf[tr.e];
         const DevNode& N = X.nodes[L];
-        const DevSplit& S = X.splits[L];
+        const DevSplit& S = X.ctl->expanded[L] == 2 ? X.splits_pair[L] : X.splits[L];
         const int t0 = ctl->exp_tile0[tr.e], t1 = ctl->exp_tile0[tr.e + 1];
         int tot = 0, before = 0;
         for (int kk = t0 + threadIdx.x; kk < t1; kk += kPartThreads) {
@@ -829,7 +943,7 @@ void ensure_smem() {
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev >= 0 && dev < 64 && done[dev]) return;
-    set_smem(wave_hist_kernel<kMode>, kWaveSmem);
+    set_smem(wave_hist_kernel<kMode>, SmemLayout<kMode>::bytes);
     if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
@@ -841,7 +955,7 @@ void hist_launch(const WaveCtx* ctxs, int n_ctx, int src, HistTune tune, unsigne
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1, tune.clusters * tune.cluster);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = kWaveSmem;
+    cfg.dynamicSmemBytes = SmemLayout<kMode>::bytes;
     cfg.stream = s;
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -852,7 +966,7 @@ void hist_launch(const WaveCtx* ctxs, int n_ctx, int src, HistTune tune, unsigne
     attr[1].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 2;
-    check(cudaLaunchKernelEx(&cfg, kern, ctxs, n_ctx, src, rows_counter, tune.units), "wave_hist launch");
+    check(cudaLaunchKernelEx(&cfg, kern, ctxs, n_ctx, src, rows_counter), "wave_hist launch");
 }
 
 template <int kMode>
@@ -875,11 +989,11 @@ int wave_hist_clusters(int cluster) {
     ensure_smem<kHistQ8Var>();
     cluster = cluster >= 4 ? 4 : cluster >= 2 ? 2 : 1;
     if (dev >= 0 && dev < 64 && cached[dev][cluster] > 0) return cached[dev][cluster];
-    auto kern = wave_hist_kernel<kHistExactVar>;
+    auto kern = wave_hist_kernel<kHistExactConst>;  // the largest shared-memory footprint
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(1, cluster * 64, 1);
     cfg.blockDim = dim3(kThreads, 1, 1);
-    cfg.dynamicSmemBytes = kWaveSmem;
+    cfg.dynamicSmemBytes = SmemLayout<kHistExactConst>::bytes;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 1;

@@ -223,7 +223,16 @@ __global__ void __launch_bounds__(32)
                 finished = true;
                 break;
             }
-            if (!ctl->expanded[bi]) break;
+            const int ex = ctl->expanded[bi];
+            if (!ex) break;
+            // an expansion planned with bi's PAIR split while the budget lasted is void once the
+            // budget is spent (bi now takes its axis split): plan bi again
+            if (ex == 2 && !(X.pair_on && pair_used < X.max_pair) && X.splits_pair[bi].type == 1) {
+                if (lane == 0) ctl->expanded[bi] = 0;
+                __syncwarp();
+                __threadfence_block();
+                break;
+            }
             // commit: the split of bi, children ids nn, nn + 1 (grow_tree's numbering)
             const DevSplit S = split_of(bi);
             if (lane == 0) {
@@ -301,7 +310,8 @@ __global__ void __launch_bounds__(32)
                     const DevNode& N = nodes[L];
                     tiles = (N.count + kPartTile - 1) / kPartTile;
                     ctl->exp_leaf[e] = L;
-                    ctl->expanded[L] = 1;
+                    // 2: the children are partitioned by L's with-pairs split, 1: by its axis split
+                    ctl->expanded[L] = (X.pair_on && pair_used < X.max_pair) ? 2 : 1;
                     for (int sd = 0; sd < 2; ++sd) {
                         DevNode ch{};
                         ch.start = N.start;

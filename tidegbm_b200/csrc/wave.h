@@ -19,7 +19,8 @@
 //             into the other ping-pong buffer at the leaf's own row range: a leaf whose
 //             expansion is never committed keeps its rows untouched.
 //   histogram the smaller child of every planned leaf, one persistent cluster launch
-//             over all (context, leaf, feature group, row chunk) units.
+//             over all (context, leaf) jobs: rows x feature groups cut into one
+//             contiguous range per cluster.
 //   scan      both children of every planned leaf (the larger by parent - smaller,
 //             histogram.cpp:108-117) for their best split and their totals.
 //
@@ -69,7 +70,7 @@ struct WaveCtl {
     int pad[3];
     int exp_leaf[kMaxLeavesCap];
     int exp_tile0[kMaxLeavesCap + 1];
-    int expanded[kMaxNodes];
+    int expanded[kMaxNodes];  // 0 not expanded; 1, 2: children planned by the axis, with-pairs split
 };
 
 // Everything a wave kernel needs to know about one context (device resident array).
@@ -141,11 +142,10 @@ void launch_wave_quantize(int mode, const int32_t* rows, const double* g, const 
 // expansions planned by the last select.
 // Launch shape of the histogram: `cluster` CTAs per cluster (1, 2 or 4: how many private
 // histograms one flush merges through distributed shared memory), `clusters` clusters
-// (co-resident), about `units` work units per cluster.  Picked by the autotuner.
+// (co-resident).  Picked by the autotuner.
 struct HistTune {
     int cluster = 4;
     int clusters = 37;
-    int units = 2;
 };
 int wave_hist_clusters(int cluster);  // co-resident clusters of the histogram kernel
 void launch_wave_hist(int mode, const WaveCtx* ctxs, int n_ctx, int src, HistTune tune,
