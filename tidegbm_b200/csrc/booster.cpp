@@ -853,8 +853,9 @@ void FitRun::tree_end(int t) {
     double* values_t = D.values_all.p + static_cast<size_t>(t) * max_nodes;
     double* prefix_t = D.prefix_all.p + static_cast<size_t>(t) * nbk * max_nodes;
     int* cover_t = D.cover_all.p + static_cast<size_t>(t) * max_nodes;
-    launch_apply_accum(D.codes_col.p, codes_col_pitch(n), D.nodes.p, D.st.p, D.g.p, h_rows, D.chunks.p,
-                       static_cast<int>(chunks.size()), D.all_scale.p, D.nid.p, D.seg_sums.p, n_segments, B.n_bins, s);
+    launch_apply_accum(D.codes_col.p, codes_col_pitch(n), n_f, D.nodes.p, D.st.p, D.g.p, h_rows, D.chunks.p,
+                       static_cast<int>(chunks.size()), D.all_scale.p, D.nid.p, D.seg_sums.p, n_segments, B.n_bins,
+                       (any_cat ? 1 : 0) | (c.pair_splits ? 2 : 0), s);
     launch_finalize_tree(pp, D.st.p, D.seg_sums.p, D.bucket_seg_end.p, D.cuts.p, D.all_scale.p, values_t, cover_t,
                          prefix_t, s);
     if (const_h) {

@@ -17,6 +17,7 @@
 // CTAs own segment-aligned row chunks, so each CTA accumulates into one segment in
 // shared memory (32-bit atomics) and adds its totals to the segment with one global
 // 64-bit atomic per leaf and value.
+#include <atomic>
 #include "tgb_internal.h"
 
 namespace tgb {
@@ -72,23 +73,45 @@ __device__ __forceinline__ void add64s(unsigned int* lo, unsigned int* hi, int k
 
 constexpr int kApplyRows = 8;  // rows a thread walks together
 
-// The tree walk reads the column-major codes: at each level the kApplyRows rows of a
-// thread issue their code loads together, and the 32 lanes of a warp hold 32 consecutive
-// rows, so lanes at nodes with the same split feature read one 32-byte sector.  A row
-// costs about one sector share per level instead of its whole 128-byte row.
+// Staged walk: a block stages, per tile of kStageRows rows, only the columns the tree
+// splits on (each distinct split feature once, 16-byte loads of whole tile runs) in shared
+// memory and walks its rows there: a row costs one byte per distinct split feature
+// instead of one 32-byte sector share per level.  Trees over more than kMaxStaged distinct
+// columns (or more than kMaxColWords * 32 features) take the gather walk: at each level
+// the kApplyRows rows of a thread issue their column-major code loads together, and lanes
+// at nodes with the same split feature share a sector.
+constexpr int kStageRows = 512;
+constexpr int kStagePitch = kStageRows + 16;  // a tile run starts up to 15 bytes early (16-byte loads)
+constexpr int kMaxStaged = 64;
+constexpr int kMaxColWords = 256;
+constexpr size_t kApplySmem = static_cast<size_t>(kMaxStaged) * kStagePitch;
+
+// kKinds: bit 0 the tree may hold categorical splits, bit 1 pair splits; a tree of axis
+// splits only keeps neither the masks nor the second features in shared memory.
+template <int kKinds>
 __global__ void __launch_bounds__(kApplyThreads)
-    apply_accum_kernel(const uint8_t* __restrict__ col, long long pitch, const DevNode* __restrict__ nodes,
+    apply_accum_kernel(const uint8_t* __restrict__ col, long long pitch, int n_f, const DevNode* __restrict__ nodes,
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
                        const double* __restrict__ h, const int4* __restrict__ chunks,
                        const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
                        unsigned long long* __restrict__ seg_sums, int n_bins) {
+    constexpr bool kCat = (kKinds & 1) != 0, kPair = (kKinds & 2) != 0;
+    extern __shared__ __align__(16) uint8_t s_tile[];  // [kMaxStaged][kStagePitch]
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
     __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes], s_type[kMaxNodes];
-    __shared__ int16_t s_feat2[kMaxNodes];
-    __shared__ unsigned long long s_cat[kMaxNodes][4];  // left masks of categorical nodes
+    __shared__ uint8_t s_slot[kMaxNodes], s_slot2[kPair ? kMaxNodes : 1];
+    __shared__ int16_t s_feat2[kPair ? kMaxNodes : 1];
+    __shared__ unsigned long long s_cat[kCat ? kMaxNodes : 1][4];  // left masks of categorical nodes
+    __shared__ unsigned int s_bits[kMaxColWords];
+    __shared__ int s_wbase[kMaxColWords], s_uf[kMaxStaged], s_nu;
     // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
     __shared__ unsigned int aGl[kMaxNodes], aGh[kMaxNodes], aHl[kMaxNodes], aHh[kMaxNodes], aC[kMaxNodes];
     const int nn = st->n_nodes;
+    const int n_words = (n_f + 31) / 32;
+    const bool can_stage = n_words <= kMaxColWords;
+    if (can_stage)
+        for (int w = threadIdx.x; w < n_words; w += blockDim.x) s_bits[w] = 0u;
+    __syncthreads();
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         const DevNode& N = nodes[k];
         s_feat[k] = static_cast<int16_t>(N.feature);
@@ -97,52 +120,147 @@ __global__ void __launch_bounds__(kApplyThreads)
         s_thr[k] = static_cast<uint8_t>(N.threshold < 0 ? 0 : N.threshold);
         s_ml[k] = static_cast<uint8_t>(N.missing_left);
         s_type[k] = static_cast<uint8_t>(N.is_leaf ? 0 : N.type);
-        s_feat2[k] = static_cast<int16_t>(!N.is_leaf && N.type == 1 ? N.feature2 : 0);
-        for (int q = 0; q < 4; ++q) s_cat[k][q] = N.type == 2 ? N.cat[q] : 0ull;
+        if constexpr (kPair) s_feat2[k] = static_cast<int16_t>(!N.is_leaf && N.type == 1 ? N.feature2 : 0);
+        if constexpr (kCat)
+            for (int q = 0; q < 4; ++q) s_cat[k][q] = N.type == 2 ? N.cat[q] : 0ull;
         s_leaf[k] = static_cast<uint8_t>(N.is_leaf);
         aGl[k] = aGh[k] = aHl[k] = aHh[k] = aC[k] = 0u;
+        if (can_stage && !N.is_leaf) {
+            atomicOr(&s_bits[N.feature >> 5], 1u << (N.feature & 31));
+            if (kPair && N.type == 1) atomicOr(&s_bits[N.feature2 >> 5], 1u << (N.feature2 & 31));
+        }
     }
+    __syncthreads();
+    if (can_stage) {
+        // distinct split columns: ranks by an exclusive prefix of the bitmap's popcounts
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int run = 0;
+            for (int w0 = 0; w0 < n_words; w0 += 32) {
+                const int w = w0 + lane;
+                const int c = w < n_words ? __popc(s_bits[w]) : 0;
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (w < n_words) s_wbase[w] = run + incl - c;
+                run += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) s_nu = run;
+        }
+        __syncthreads();
+        if (s_nu <= kMaxStaged) {
+            for (int w = threadIdx.x; w < n_words; w += blockDim.x) {
+                unsigned int bits = s_bits[w];
+                int u = s_wbase[w];
+                while (bits != 0u) {
+                    s_uf[u++] = w * 32 + __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                }
+            }
+            auto rank = [&](int f) {
+                return s_wbase[f >> 5] + __popc(s_bits[f >> 5] & ((1u << (f & 31)) - 1u));
+            };
+            for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+                if (s_leaf[k]) continue;
+                s_slot[k] = static_cast<uint8_t>(rank(s_feat[k]));
+                if constexpr (kPair)
+                    if (s_type[k] == 1) s_slot2[k] = static_cast<uint8_t>(rank(s_feat2[k]));
+            }
+        }
+        __syncthreads();
+    }
+    const bool staged = can_stage && s_nu <= kMaxStaged;
     const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
     const double gs = sc->gscale, hs = sc->hscale;
-    __syncthreads();
-    for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
-        int r[kApplyRows], k[kApplyRows];
-        double gv[kApplyRows], hv[kApplyRows];
-#pragma unroll
-        for (int i = 0; i < kApplyRows; ++i) {
-            r[i] = base + threadIdx.x + i * kApplyThreads;
-            k[i] = 0;
-            const bool ok = r[i] < ch.z;
-            gv[i] = ok ? g[r[i]] : 0.0;  // loaded before the walk so their latency overlaps it
-            hv[i] = ok && h ? h[r[i]] : 1.0;  // h == nullptr: unit hessians
-            if (!ok) r[i] = -1;
+    if (staged) {
+        const int nu = s_nu;
+        for (int t0 = ch.y; t0 < ch.z; t0 += kStageRows) {
+            const int t1 = min(ch.z, t0 + kStageRows);
+            const int a0 = t0 & ~15;
+            const int n16 = (t1 - a0 + 15) >> 4;
+            __syncthreads();  // the previous tile's walks are done
+            for (int idx = threadIdx.x; idx < nu * n16; idx += blockDim.x) {
+                const int u = idx / n16, v = idx - u * n16;
+                *reinterpret_cast<uint4*>(s_tile + u * kStagePitch + v * 16) = __ldg(
+                    reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0 + v * 16));
+            }
+            __syncthreads();
+            for (int r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
+                const double gv = g[r];
+                const double hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
+                const int off = r - a0;
+                int k = 0;
+                while (!s_leaf[k]) {
+                    const unsigned int b = s_tile[s_slot[k] * kStagePitch + off];
+                    bool left;
+                    if constexpr (kCat || kPair) {
+                        unsigned int b2 = 0u;
+                        if constexpr (kPair)
+                            if (s_type[k] == 1) b2 = s_tile[s_slot2[k] * kStagePitch + off];
+                        left = goes_left(s_type[k], s_cat[kCat ? k : 0], s_thr[k], s_ml[k], b, b2, n_bins);
+                    } else {
+                        left = b == 0u ? s_ml[k] != 0 : static_cast<int>(b) <= s_thr[k];
+                    }
+                    k = left ? s_left[k] : s_right[k];
+                }
+                nid[r] = static_cast<int16_t>(k);
+                add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
+                add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
+                atomicAdd(&aC[k], 1u);
+            }
         }
-        for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
-            unsigned int b[kApplyRows], b2[kApplyRows];
-            bool any = false;
+    } else {
+        for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
+            int r[kApplyRows], k[kApplyRows];
+            double gv[kApplyRows], hv[kApplyRows];
 #pragma unroll
             for (int i = 0; i < kApplyRows; ++i) {
-                const bool walk = r[i] >= 0 && !s_leaf[k[i]];
-                b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
-                b2[i] = walk && s_type[k[i]] == 1 ? __ldg(col + static_cast<long long>(s_feat2[k[i]]) * pitch + r[i])
-                                                  : 0u;
-                any |= walk;
+                r[i] = base + threadIdx.x + i * kApplyThreads;
+                k[i] = 0;
+                const bool ok = r[i] < ch.z;
+                gv[i] = ok ? g[r[i]] : 0.0;  // loaded before the walk so their latency overlaps it
+                hv[i] = ok && h ? h[r[i]] : 1.0;
+                if (!ok) r[i] = -1;
             }
-            if (!any) break;
+            for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
+                unsigned int b[kApplyRows], b2[kApplyRows];
+                bool any = false;
+#pragma unroll
+                for (int i = 0; i < kApplyRows; ++i) {
+                    const bool walk = r[i] >= 0 && !s_leaf[k[i]];
+                    b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
+                    if constexpr (kPair)
+                        b2[i] = walk && s_type[k[i]] == 1
+                                    ? __ldg(col + static_cast<long long>(s_feat2[k[i]]) * pitch + r[i])
+                                    : 0u;
+                    else
+                        b2[i] = 0u;
+                    any |= walk;
+                }
+                if (!any) break;
+#pragma unroll
+                for (int i = 0; i < kApplyRows; ++i) {
+                    if (r[i] < 0 || s_leaf[k[i]]) continue;
+                    bool left;
+                    if constexpr (kCat || kPair)
+                        left = goes_left(s_type[k[i]], s_cat[kCat ? k[i] : 0], s_thr[k[i]], s_ml[k[i]], b[i], b2[i],
+                                         n_bins);
+                    else
+                        left = b[i] == 0u ? s_ml[k[i]] != 0 : static_cast<int>(b[i]) <= s_thr[k[i]];
+                    k[i] = left ? s_left[k[i]] : s_right[k[i]];
+                }
+            }
 #pragma unroll
             for (int i = 0; i < kApplyRows; ++i) {
-                if (r[i] < 0 || s_leaf[k[i]]) continue;
-                const bool left = goes_left(s_type[k[i]], s_cat[k[i]], s_thr[k[i]], s_ml[k[i]], b[i], b2[i], n_bins);
-                k[i] = left ? s_left[k[i]] : s_right[k[i]];
+                if (r[i] < 0) continue;
+                nid[r[i]] = static_cast<int16_t>(k[i]);
+                add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
+                add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
+                atomicAdd(&aC[k[i]], 1u);
             }
-        }
-#pragma unroll
-        for (int i = 0; i < kApplyRows; ++i) {
-            if (r[i] < 0) continue;
-            nid[r[i]] = static_cast<int16_t>(k[i]);
-            add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
-            add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
-            atomicAdd(&aC[k[i]], 1u);
         }
     }
     __syncthreads();
@@ -327,14 +445,26 @@ void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cud
     check(cudaGetLastError(), "all_scale_finalize launch");
 }
 
-void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
+void launch_apply_accum(const uint8_t* col, long long pitch, int n_f, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks,
                         const AllScale* sc, int16_t* nid, unsigned long long* seg_sums, int n_segments,
-                        int n_bins, cudaStream_t s) {
+                        int n_bins, int kinds, cudaStream_t s) {
     check(cudaMemsetAsync(seg_sums, 0, sizeof(unsigned long long) * 3 * kMaxNodes * n_segments, s),
           "seg sums reset");
-    apply_accum_kernel<<<n_chunks, kApplyThreads, 0, s>>>(col, pitch, nodes, st, g, h, chunks, sc, nid,
-                                                          seg_sums, n_bins);
+    auto kern = kinds == 0 ? apply_accum_kernel<0> : kinds == 1 ? apply_accum_kernel<1>
+                                                   : kinds == 2 ? apply_accum_kernel<2> : apply_accum_kernel<3>;
+    {  // static + dynamic shared memory above 48 KB needs the opt-in, once per device
+        static std::atomic<bool> done[64][4] = {};
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (dev < 0 || dev >= 64 || !done[dev][kinds & 3]) {
+            check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kApplySmem)),
+                  "apply_accum smem attr");
+            if (dev >= 0 && dev < 64) done[dev][kinds & 3] = true;
+        }
+    }
+    kern<<<n_chunks, kApplyThreads, kApplySmem, s>>>(col, pitch, n_f, nodes, st, g, h, chunks, sc, nid, seg_sums,
+                                                     n_bins);
     check(cudaGetLastError(), "apply_accum launch");
 }
 

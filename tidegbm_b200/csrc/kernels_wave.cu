@@ -30,6 +30,7 @@
 //
 // Partition (split_indices, cpp/src/tree.cpp:68-91): stable, two launches over
 // 2048-row tiles of all planned leaves (count, then scatter with in-tile ballot ranks).
+#include <atomic>
 #include <cooperative_groups.h>
 
 #include "wave.h"
@@ -939,7 +940,7 @@ void set_smem(K kern, size_t bytes) {
 // inside a stream capture: the first launches of a fit run before its graph is captured).
 template <int kMode>
 void ensure_smem() {
-    static bool done[64] = {};
+    static std::atomic<bool> done[64] = {};
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev >= 0 && dev < 64 && done[dev]) return;
@@ -978,7 +979,7 @@ void quantize_launch(const int32_t* rows, const double* g, const double* h, cons
 }  // namespace
 
 int wave_hist_clusters(int cluster) {
-    static int cached[64][5] = {};
+    static std::atomic<int> cached[64][5] = {};
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     ensure_smem<kHistExactConst>();

@@ -330,9 +330,10 @@ void launch_all_scale_finalize(AllScale* sc, int n, cudaStream_t s);
 void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
                              double* pred, const double* y, double* partials, int n_part, cudaStream_t s);
 // col: column-major codes (col[f * pitch + r], launch_codes_transpose)
-void launch_apply_accum(const uint8_t* col, long long pitch, const DevNode* nodes, const DevTreeState* st,
+void launch_apply_accum(const uint8_t* col, long long pitch, int n_f, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
-                        int16_t* nid, unsigned long long* seg_sums, int n_segments, int n_bins, cudaStream_t s);
+                        int16_t* nid, unsigned long long* seg_sums, int n_segments, int n_bins, int kinds,
+                        cudaStream_t s);
 void launch_finalize_tree(const PostParams& pp, const DevTreeState* st, const unsigned long long* seg_sums,
                           const int* bucket_seg_end, const int* cuts, const AllScale* sc, double* values,
                           int* cover, double* prefix, cudaStream_t s);
