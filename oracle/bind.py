@@ -223,6 +223,26 @@ def oracle_fit(params: dict, X, y, ts=None, entity=None, is_cat=None) -> tuple[F
     return res, h
 
 
+def oracle_codes(X, params: dict, is_cat=None) -> tuple[np.ndarray, int]:
+    """Binner::fit + transform of the oracle (binning.cpp:34-134): row-major uint8 codes of
+    X under the fit's binning parameters, and the histogram width max_bins()."""
+    L = oracle_lib()
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    n, nf = X.shape
+    cat = np.zeros(nf, np.int32) if is_cat is None else np.ascontiguousarray(is_cat, dtype=np.int32)
+    edges = np.zeros(nf * 256)
+    n_edges = np.zeros(nf, np.int32)
+    codes = np.zeros((n, nf), np.uint8)
+    L.orc_binner_fit_cat.restype = C.c_int
+    L.orc_binner_fit_cat.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    nb = L.orc_binner_fit_cat(X.ctypes.data, n, nf, cat.ctypes.data, int(params.get("max_bin", 255)),
+                              int(params.get("cat_min_count", 5)), int(params.get("bin_sample", 262144)),
+                              int(params.get("random_state", 0)) & 0xFFFFFFFF, edges.ctypes.data, n_edges.ctypes.data,
+                              codes.ctypes.data)
+    return codes, nb
+
+
 def oracle_predict(handle, X) -> np.ndarray:
     X = np.ascontiguousarray(X, dtype=np.float64)
     out = np.zeros(X.shape[0])

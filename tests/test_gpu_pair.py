@@ -9,38 +9,56 @@ Against the reference's own fit (tests/golden/fit_pairsplit.npz) and the oracle
 restatement: identical structure, split types and second features; values within 1e-9.
 """
 import os
+from types import SimpleNamespace
 
 import numpy as np
 import pytest
+from missing_bins import empty_missing_nodes
 
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def _compare(trees_g, trees_r, atol=1e-9):
+def _compare(trees_g, trees_r, codes=None, n_bins=None, atol=1e-9):
+    """Structure, split types and values; missing directions everywhere except at split
+    nodes whose missing bin holds no row of the fit (missing_bins.py says why)."""
     assert len(trees_g) == len(trees_r)
     for t, (a, b) in enumerate(zip(trees_g, trees_r)):
-        for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
-                    "split_type", "feature2"):
+        for fld in ("is_leaf", "feature", "threshold", "left", "right", "n_samples", "depth", "split_type",
+                    "feature2"):
             assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        _compare_missing(t, a, b, codes, n_bins)
         np.testing.assert_allclose(a.value, b.value, rtol=0, atol=atol)
         np.testing.assert_allclose(a.values, b.values, rtol=0, atol=atol)
         np.testing.assert_allclose(a.prefix, b.prefix, rtol=0, atol=atol)
 
 
-def test_pair_fit_matches_reference_fixture(native):
+def _compare_missing(t, a, b, codes, n_bins):
+    differ = set(np.flatnonzero(np.asarray(a.missing_left) != np.asarray(b.missing_left)).tolist())
+    if not differ:
+        return
+    assert codes is not None, (t, "missing_left", sorted(differ))
+    empty = empty_missing_nodes(b, codes, n_bins)
+    assert differ <= empty, (t, "missing_left", sorted(differ - empty))
+
+
+def test_pair_fit_matches_reference_fixture(native, oracle):
     d = np.load(os.path.join(GOLDEN, "fit_pairsplit.npz"), allow_pickle=True)
     params = eval(str(d["params"]))
     b = native.Booster(**params)
     b.fit(d["X"], d["y"], timestamps=d["ts"], entity=d["entity"])
     trees = b.trees()
     assert len(trees) == int(d["n_trees"])
+    codes, nb = oracle.oracle_codes(d["X"], params)
     n_pair = 0
     for t, tr in enumerate(trees):
-        for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth",
-                    "split_type", "feature2"):
+        for fld in ("is_leaf", "feature", "threshold", "left", "right", "n_samples", "depth", "split_type",
+                    "feature2"):
             assert np.array_equal(getattr(tr, fld), d[f"t{t}_{fld}"]), (t, fld)
+        ref_tree = SimpleNamespace(**{fld: d[f"t{t}_{fld}"] for fld in (
+            "is_leaf", "feature", "threshold", "left", "right", "missing_left", "split_type", "feature2")})
+        _compare_missing(t, tr, ref_tree, codes, nb)
         np.testing.assert_allclose(tr.values, d[f"t{t}_values"], rtol=0, atol=1e-9)
         np.testing.assert_allclose(tr.prefix, d[f"t{t}_prefix"], rtol=0, atol=1e-9)
         n_pair += int((tr.split_type == 1).sum())
@@ -71,8 +89,9 @@ def test_pair_splits_match_oracle(native, oracle, extra):
     b = native.Booster(**params)
     b.fit(X, y, timestamps=ts_arg)
     ref, h = oracle.oracle_fit(params, X, y, ts_arg)
+    codes, nb = oracle.oracle_codes(X, params)
     try:
-        _compare(b.trees(), ref.trees)
+        _compare(b.trees(), ref.trees, codes, nb)
         assert sum(int((t.split_type == 1).sum()) for t in b.trees()) > 0
         np.testing.assert_allclose(b.evals_result()["train"], ref.evals_train, rtol=1e-9, atol=1e-9)
         np.testing.assert_allclose(b.raw_predict(X[:1000]), oracle.oracle_predict(h, X[:1000]), rtol=0, atol=1e-9)
@@ -91,8 +110,9 @@ def test_pair_and_categorical_together(native, oracle):
     b = native.Booster(**params)
     b.fit(X, y, timestamps=ts, is_cat=is_cat)
     ref, h = oracle.oracle_fit(params, X, y, ts, is_cat=is_cat)
+    codes, nb = oracle.oracle_codes(X, params, is_cat)
     try:
-        _compare(b.trees(), ref.trees)
+        _compare(b.trees(), ref.trees, codes, nb)
         for a, r in zip(b.trees(), ref.trees):
             assert np.array_equal(a.cat_left, r.cat_left)
     finally:

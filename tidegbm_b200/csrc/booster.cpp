@@ -482,8 +482,9 @@ void FitRun::prepare(const void* X_in, int x_dtype, const double* y_in, int n_in
     D.g.alloc(n, s);
     if (!const_h) D.h.alloc(n, s);  // MSE hessians are implicit (unit)
     if (wave) {
-        D.gqw.alloc(static_cast<size_t>(n) * 8, s);
-        if (mode == kHistExactVar) D.hqw.alloc(static_cast<size_t>(n) * 8, s);
+        // payloads by position in either rows buffer (2 x n elements)
+        D.gqw.alloc(static_cast<size_t>(2) * n * hist_pay_bytes(mode), s);
+        if (mode == kHistExactVar) D.hqw.alloc(static_cast<size_t>(2) * n * 8, s);
     } else {
         if (const_h && c.hist_bits == 0) D.gq.alloc(n, s);
         if (c.hist_bits == 8) D.gq8.alloc(n, s);
@@ -720,6 +721,8 @@ WaveCtx FitRun::wave_ctx() const {
     w.rows1 = D.rows1.p;
     w.gq = D.gqw.p;
     w.hq = D.hqw.p;
+    w.pay_pitch = n;
+    w.pay_bytes = hist_pay_bytes(mode);
     w.nodes = D.nodes.p;
     w.splits = D.splits.p;
     w.st = D.st.p;

@@ -66,7 +66,7 @@ size_t working_set_bytes(const tgb::Config& c, int kind, long long n, long long 
     const long long slack = 64ll << 20;
     if (kind == 1) return static_cast<size_t>(n * n_f * xsz + n * stride + 8 * n + slack);
     const long long per_row = 8 * 3              // y, pred, g
-                              + (c.objective == 0 ? 8 : 16)  // gq, or h and its scratch
+                              + (c.objective == 0 ? 16 : 40)  // payloads in both row buffers (+ h)
                               + 8 + 2            // row lists, leaf ids
                               + 26;              // GOSS keys, values and flags
     const long long nodes = 2ll * c.max_leaves - 1;
@@ -601,8 +601,9 @@ int tgb_hist_build_quantized(const unsigned char* codes, int stride, int n_featu
         st.alloc(1, s);
         ctl.alloc(1, s);
         wc.alloc(1, s);
-        gq.alloc(static_cast<size_t>(std::max(1, n_max)) * 8, s);
-        if (mode == tgb::kHistExactVar) hq.alloc(static_cast<size_t>(std::max(1, n_max)) * 8, s);
+        const int n_pay = std::max({1, n_max, n_rows});  // payloads by position in the row list
+        gq.alloc(static_cast<size_t>(n_pay) * 8, s);
+        if (mode == tgb::kHistExactVar) hq.alloc(static_cast<size_t>(n_pay) * 8, s);
         tgb::DevTreeState sh{};
         sh.n_sample = n_rows;
         tgb::check(cudaMemsetAsync(ctl.p, 0, sizeof(tgb::WaveCtl), s), "control reset");
@@ -621,6 +622,8 @@ int tgb_hist_build_quantized(const unsigned char* codes, int stride, int n_featu
         w.rows0 = const_cast<int32_t*>(rows);
         w.gq = gq.p;
         w.hq = hq.p;
+        w.pay_pitch = n_pay;
+        w.pay_bytes = tgb::hist_pay_bytes(mode);
         w.st = st.p;
         w.ctl = ctl.p;
         w.G = G;

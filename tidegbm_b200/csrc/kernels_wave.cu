@@ -98,6 +98,8 @@ __device__ __forceinline__ void rotate_words(unsigned int (&w)[8], int k) {
 // Rows of one histogram job: the root's sample or a planned leaf's smaller child.
 struct JobRows {
     const int32_t* rows;
+    const void* gq;  // payloads of rows[0 ..) (same positions)
+    const void* hq;
     int count;
     int slot;
 };
@@ -106,6 +108,8 @@ __device__ __forceinline__ JobRows job_rows(const WaveCtx& X, int src, int e) {
     JobRows r;
     if (src == 0) {
         r.rows = X.rows0;
+        r.gq = X.gq;
+        r.hq = X.hq;
         r.count = X.st->n_sample;
         r.slot = 0;
         return r;
@@ -116,9 +120,27 @@ __device__ __forceinline__ JobRows job_rows(const WaveCtx& X, int src, int e) {
     const bool left_small = a.count <= b.count;  // cpp/src/tree.cpp:423
     const DevNode& c = left_small ? a : b;
     r.rows = (c.buf ? X.rows1 : X.rows0) + c.start;
+    const long long pos = static_cast<long long>(c.buf) * X.pay_pitch + c.start;
+    r.gq = static_cast<const unsigned char*>(X.gq) + pos * X.pay_bytes;
+    r.hq = X.hq != nullptr ? static_cast<const long long*>(X.hq) + pos : nullptr;
     r.count = c.count;
     r.slot = c.slot;
     return r;
+}
+
+// A row's 32 code bytes of a feature group: one 32-byte load where the row stride keeps it
+// 32-byte aligned (two_chunks: the group has 32 bytes before the row's end), else two
+// 16-byte loads (the second only when the group has 32 bytes).
+__device__ __forceinline__ void load_codes(const uint8_t* p, bool v8, bool two_chunks, uint4& a, uint4& b) {
+    if (v8) {
+        asm volatile("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                     : "l"(p));
+    } else {
+        const uint4* p4 = reinterpret_cast<const uint4*>(p);
+        a = __ldg(p4);
+        b = two_chunks ? __ldg(p4 + 1) : make_uint4(0, 0, 0, 0);
+    }
 }
 
 // A CTA's totals in a padded [feature][bin] layout, index f * kTotPitch + b: the fold
@@ -219,37 +241,31 @@ __device__ __noinline__ void accumulate_const(unsigned int* __restrict__ P, unsi
                                               const void* __restrict__ gqp) {
     using T = ModeTraits<kMode>;
     using PT = typename ConstPayload<kMode>::type;
-    const PT* __restrict__ pay = static_cast<const PT*>(gqp);
+    const PT* __restrict__ pay = static_cast<const PT*>(gqp);  // by position, like rows
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q = lane >> 2, sh = (lane & 3) * 8;
     const bool two_chunks = stride - fg0 >= 32;
+    const bool v8 = two_chunks && (stride & 31) == 0;
     constexpr int kStep = kWarps * 32;
     for (int s0 = r0; s0 < r1; s0 += T::sub) {
         const int s1 = min(r1, s0 + T::sub);
         const int k0 = s0 + warp * 32 + lane;
         int r_cur = k0 < s1 ? rows[k0] : -1;
+        PT p = k0 < s1 ? pay[k0] : PT(0);
         int r_nxt = k0 + kStep < s1 ? rows[k0 + kStep] : -1;
+        PT p_nxt = k0 + kStep < s1 ? pay[k0 + kStep] : PT(0);
         uint4 ca = make_uint4(0, 0, 0, 0), cb = make_uint4(0, 0, 0, 0);
-        PT p = 0;
-        if (r_cur >= 0) {
-            const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r_cur) * stride + fg0);
-            ca = __ldg(src4);
-            if (two_chunks) cb = __ldg(src4 + 1);
-            p = pay[r_cur];
-        }
+        if (r_cur >= 0) load_codes(codes + static_cast<size_t>(r_cur) * stride + fg0, v8, two_chunks, ca, cb);
         for (int base = s0 + warp * 32; base < s1; base += kStep) {
             const int r = r_cur;
             const uint4 xa = ca, xb = cb;
             const PT xp = p;
             r_cur = r_nxt;
+            p = p_nxt;
             const int kn = base + 2 * kStep + lane;
             r_nxt = kn < s1 ? rows[kn] : -1;
-            if (r_cur >= 0) {
-                const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r_cur) * stride + fg0);
-                ca = __ldg(src4);
-                cb = two_chunks ? __ldg(src4 + 1) : make_uint4(0, 0, 0, 0);
-                p = pay[r_cur];
-            }
+            p_nxt = kn < s1 ? pay[kn] : PT(0);
+            if (r_cur >= 0) load_codes(codes + static_cast<size_t>(r_cur) * stride + fg0, v8, two_chunks, ca, cb);
             if (r >= 0) add_row_const<kMode>(P, xp, xa, xb, lane, q, sh);
         }
         __syncthreads();
@@ -295,6 +311,7 @@ __device__ __noinline__ void accumulate_var(unsigned int* __restrict__ P, unsign
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q = lane >> 2, sh = (lane & 3) * 8;
     const bool two_chunks = stride - fg0 >= 32;
+    const bool v8 = two_chunks && (stride & 31) == 0;
     long long accG[kCells], accH[kCells];
     unsigned int accC[kCells];
 #pragma unroll
@@ -308,29 +325,29 @@ __device__ __noinline__ void accumulate_var(unsigned int* __restrict__ P, unsign
         int r_next = s0 + warp * 32 + lane < s1 ? rows[s0 + warp * 32 + lane] : -1;
         for (int base = s0 + warp * 32; base < s1; base += kWarps * 32) {
             const int r = r_next;
+            const int k = base + lane;  // the row's position: its payload's index
             const int kn = base + kWarps * 32 + lane;
             r_next = kn < s1 ? rows[kn] : -1;
             if (r < 0) continue;
             unsigned int a0 = 0, a1 = 0, a2 = 0, a3 = 0;
             if constexpr (kMode == kHistExactVar) {
-                const long long gv = static_cast<const long long*>(gqp)[r];
-                const long long hv = static_cast<const long long*>(hqp)[r];
+                const long long gv = static_cast<const long long*>(gqp)[k];
+                const long long hv = static_cast<const long long*>(hqp)[k];
                 a0 = static_cast<unsigned int>(gv) & ((1u << kLoBits) - 1u);
                 a1 = static_cast<unsigned int>(static_cast<int>(gv >> kLoBits));
                 a2 = static_cast<unsigned int>(hv) & ((1u << kLoBits) - 1u);
                 a3 = static_cast<unsigned int>(static_cast<int>(hv >> kLoBits));
             } else if constexpr (kMode == kHistQ16Var) {
-                const unsigned int p = static_cast<const unsigned int*>(gqp)[r];
+                const unsigned int p = static_cast<const unsigned int*>(gqp)[k];
                 a0 = static_cast<unsigned int>(static_cast<int>(p) >> 16);
                 a1 = p & 0xffffu;
             } else {  // kHistQ8Var
-                const unsigned int p = static_cast<const unsigned short*>(gqp)[r];
+                const unsigned int p = static_cast<const unsigned short*>(gqp)[k];
                 a0 = (1u << 20) | (p & 0xffu);
                 a1 = p >> 8;
             }
-            const uint4* src4 = reinterpret_cast<const uint4*>(codes + static_cast<size_t>(r) * stride + fg0);
-            const uint4 ca = __ldg(src4);
-            const uint4 cb = two_chunks ? __ldg(src4 + 1) : make_uint4(0, 0, 0, 0);
+            uint4 ca, cb;
+            load_codes(codes + static_cast<size_t>(r) * stride + fg0, v8, two_chunks, ca, cb);
             unsigned int wd[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
             rotate_words(wd, q);
             unsigned int Rw[8];
@@ -515,9 +532,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int r0 = min(piece1, piece0 + static_cast<int>(rank) * qrows), r1 = min(piece1, r0 + qrows);
         const int fg0 = fg * kFG;
         if constexpr (T::var)
-            accumulate_var<kMode>(P, Gt, Ht, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, X.gq, X.hq);
+            accumulate_var<kMode>(P, Gt, Ht, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, jr.gq, jr.hq);
         else
-            accumulate_const<kMode>(P, Gt, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, X.gq);
+            accumulate_const<kMode>(P, Gt, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, jr.gq);
         __syncthreads();
         cluster.sync();
         // rank k adds its share of the cells over the cluster and writes them out
@@ -588,6 +605,14 @@ __device__ __forceinline__ int block_sum(int v, int* red) {
 #pragma unroll
     for (int w = 0; w < kPartWarps; ++w) t += red[w];
     return t;
+}
+
+// One row's payloads from element `from` to element `to` of the payload arrays.
+__device__ __forceinline__ void move_payload(const WaveCtx& X, long long from, long long to) {
+    if (X.pay_bytes == 8) static_cast<long long*>(X.gq)[to] = static_cast<const long long*>(X.gq)[from];
+    else if (X.pay_bytes == 4) static_cast<int*>(X.gq)[to] = static_cast<const int*>(X.gq)[from];
+    else static_cast<short*>(X.gq)[to] = static_cast<const short*>(X.gq)[from];
+    if (X.hq != nullptr) static_cast<long long*>(X.hq)[to] = static_cast<const long long*>(X.hq)[from];
 }
 
 // Global tile t -> (context, expansion, tile within the expansion).
@@ -760,13 +785,17 @@ __global__ void __launch_bounds__(kPartThreads)
             }
             excl[i] = e;
         }
+        // the rows' payloads move with them (same positions in the other buffer)
+        const long long from0 = static_cast<long long>(N.buf) * X.pay_pitch + N.start;
+        const long long to0 = static_cast<long long>(1 - N.buf) * X.pay_pitch + N.start;
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) {
             if (row[i] < 0) continue;
             const int kk = base + i * kPartThreads + threadIdx.x;
             const int lrank = excl[i] + __popc(bal[i] & lt_mask);
-            if (left[i]) out[left0 + lrank] = row[i];
-            else out[n_left + (base - left0) + (kk - base - lrank)] = row[i];
+            const int dst = left[i] ? left0 + lrank : n_left + (base - left0) + (kk - base - lrank);
+            out[dst] = row[i];
+            move_payload(X, from0 + kk, to0 + dst);
         }
         __syncthreads();  // wc reuse
     }
@@ -889,24 +918,24 @@ __global__ void wave_quantize_kernel(const int32_t* __restrict__ rows, const dou
         }
         if constexpr (kMode == kHistExactConst) {
             const long long v = __double2ll_rn(gv * gscale);
-            static_cast<long long*>(gq)[r] = static_cast<long long>((static_cast<unsigned long long>(v) << 1) | (sc ? 1ull : 0ull));
+            static_cast<long long*>(gq)[k] = static_cast<long long>((static_cast<unsigned long long>(v) << 1) | (sc ? 1ull : 0ull));
         } else if constexpr (kMode == kHistExactVar) {
-            static_cast<long long*>(gq)[r] = __double2ll_rn(gv * gscale);
-            static_cast<long long*>(hq)[r] = __double2ll_rn(hv * hscale);
+            static_cast<long long*>(gq)[k] = __double2ll_rn(gv * gscale);
+            static_cast<long long*>(hq)[k] = __double2ll_rn(hv * hscale);
         } else if constexpr (kMode == kHistQ16Const) {
             const int qv = sround(gv * gscale, uniform01(seed, r, 0), -32767, 32767);
-            static_cast<int*>(gq)[r] = static_cast<int>((static_cast<unsigned int>(qv) << 1) | (sc ? 1u : 0u));
+            static_cast<int*>(gq)[k] = static_cast<int>((static_cast<unsigned int>(qv) << 1) | (sc ? 1u : 0u));
         } else if constexpr (kMode == kHistQ16Var) {
             const int qg = sround(gv * gscale, uniform01(seed, r, 0), -32767, 32767);
             const int qh = sround(hv * hscale, uniform01(seed, r, 1), 0, 65535);
-            static_cast<unsigned int*>(gq)[r] = (static_cast<unsigned int>(qg) << 16) | static_cast<unsigned int>(qh);
+            static_cast<unsigned int*>(gq)[k] = (static_cast<unsigned int>(qg) << 16) | static_cast<unsigned int>(qh);
         } else if constexpr (kMode == kHistQ8Const) {
             const int qv = sround(gv * gscale, uniform01(seed, r, 0), -127, 127);
-            static_cast<short*>(gq)[r] = static_cast<short>((qv * 2) | (sc ? 1 : 0));
+            static_cast<short*>(gq)[k] = static_cast<short>((qv * 2) | (sc ? 1 : 0));
         } else {
             const int qg = sround(gv * gscale, uniform01(seed, r, 0), -127, 127);
             const int qh = sround(hv * hscale, uniform01(seed, r, 1), 0, 255);
-            static_cast<unsigned short*>(gq)[r] = static_cast<unsigned short>((qg + 128) | (qh << 8));
+            static_cast<unsigned short*>(gq)[k] = static_cast<unsigned short>((qg + 128) | (qh << 8));
         }
     }
 }

@@ -523,6 +523,10 @@ __global__ void __launch_bounds__(kScanThreads) wave_pair_kernel(const WaveCtx* 
         const uint8_t* c1 = X.codes_col + static_cast<size_t>(f1) * X.col_pitch;
         const uint8_t* c2 = X.codes_col + static_cast<size_t>(f2) * X.col_pitch;
         const bool var = X.hq != nullptr;
+        // payloads by position (exact modes: 8-byte words), like the child's rows
+        const long long pos0 = static_cast<long long>(cr.N->buf) * X.pay_pitch + cr.N->start;
+        const long long* gpay = static_cast<const long long*>(X.gq) + pos0;
+        const long long* hpay = var ? static_cast<const long long*>(X.hq) + pos0 : nullptr;
         const unsigned long long hq1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.st->hscale));
         const unsigned long long hq2 = static_cast<unsigned long long>(__double2ll_rn(1.0 * X.goss_scale * X.st->hscale));
         const int count = cr.N->count;
@@ -531,10 +535,10 @@ __global__ void __launch_bounds__(kScanThreads) wave_pair_kernel(const WaveCtx* 
             const unsigned z = pair_bin(c1[r], c2[r], p.n_bins);
             unsigned long long gv, hv;
             if (var) {
-                gv = static_cast<unsigned long long>(static_cast<const long long*>(X.gq)[r]);
-                hv = static_cast<unsigned long long>(static_cast<const long long*>(X.hq)[r]);
+                gv = static_cast<unsigned long long>(gpay[i]);
+                hv = static_cast<unsigned long long>(hpay[i]);
             } else {
-                const long long pk = static_cast<const long long*>(X.gq)[r];
+                const long long pk = gpay[i];
                 gv = static_cast<unsigned long long>(pk >> 1);
                 hv = (pk & 1) ? hq2 : hq1;
             }

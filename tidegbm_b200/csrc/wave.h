@@ -55,6 +55,9 @@ inline int hist_mode(int hist_bits, bool const_h) {
     const int base = hist_bits == 16 ? kHistQ16Const : hist_bits == 8 ? kHistQ8Const : kHistExactConst;
     return base + (const_h ? 0 : 1);
 }
+// Bytes of a row's histogram payload in `mode` (the g payload; the exact per-row mode adds
+// an 8-byte h payload).
+inline int hist_pay_bytes(int mode) { return mode <= kHistExactVar ? 8 : mode <= kHistQ16Var ? 4 : 2; }
 
 // Per-tree control of one context, device resident.
 struct WaveCtl {
@@ -80,8 +83,15 @@ struct WaveCtx {
     long long col_pitch;
     int32_t* rows0;
     int32_t* rows1;
-    const void* gq;  // per-row payload (mode dependent)
-    const void* hq;  // per-row hessian payload (exact var mode)
+    // Histogram payloads by position: the payload of the row at position k of rows buffer b
+    // (rows0: b = 0, rows1: b = 1) is element b * pay_pitch + k of gq (pay_bytes bytes) and
+    // of hq (8 bytes, exact per-row hessian mode only); the partition moves them with the
+    // rows, so the histogram reads them in row-list order.
+    void* gq;
+    void* hq;
+    long long pay_pitch;
+    int pay_bytes;
+    int pad_pay;
     DevNode* nodes;
     DevSplit* splits;
     DevTreeState* st;
@@ -133,7 +143,7 @@ void launch_wave_tree_init(DevNode* nodes, DevSplit* splits, DevTreeState* st, W
 // Per-tree histogram scales of one context from the sample maxima (st) or, when the
 // sample is every row, the all-row maxima (all).
 void launch_wave_scales(DevTreeState* st, const AllScale* all, int mode, cudaStream_t s);
-// Per-row payload of the sampled rows for `mode` (rows0[0 .. st->n_sample)).
+// Payload of the sampled rows for `mode` (rows0[0 .. st->n_sample)), by position in rows0.
 void launch_wave_quantize(int mode, const int32_t* rows, const double* g, const double* h, const uint8_t* goss_flag,
                           double goss_scale, const DevTreeState* st, unsigned long long seed, void* gq, void* hq,
                           int max_rows, cudaStream_t s);
