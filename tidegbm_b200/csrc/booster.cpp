@@ -963,6 +963,7 @@ public:
             leaves += r->c.max_leaves;
             rows_ += r->n;
             pair_ = pair_ || r->c.pair_splits;
+            cat_ = cat_ || r->any_cat;
             if (r->mode != runs_[0]->mode) throw TideError("wave: all contexts of a launch share one histogram mode");
         }
         if (leaves > kMaxWaveJobs) throw TideError("wave: too many leaves over the contexts of one launch");
@@ -1097,7 +1098,7 @@ public:
             }
         };
         hist(0);
-        launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, s_);
+        launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, cat_, s_);
         if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 0, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, dflag_, 0ull, 0, s_);
         // waves, enqueued ahead; the flag written by wave w's select is read once wave w
@@ -1117,7 +1118,7 @@ public:
             }
             launch_wave_partition(ctx_.p, n_ctx_, part_grid_, s_);
             hist(1);
-            launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, s_);
+            launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, cat_, s_);
             if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 1, s_);
             launch_wave_select(ctx_.p, n_ctx_, gsync_.p, dflag_, 0ull, 0, s_);
             check(cudaEventRecord(ev_[w], s_), "event record");
@@ -1143,7 +1144,7 @@ private:
         check(cudaStreamBeginCaptureToGraph(s_, graph_, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
               "graph capture");
         launch_wave_hist(mode_, ctx_.p, n_ctx_, 0, tune_, rows_counter_, s_);
-        launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, s_);
+        launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, cat_, s_);
         if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 0, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, nullptr, handle, 1, s_);
         cudaStreamCaptureStatus cs;
@@ -1167,7 +1168,7 @@ private:
               "body capture");
         launch_wave_partition(ctx_.p, n_ctx_, part_grid_, s_);
         launch_wave_hist(mode_, ctx_.p, n_ctx_, 1, tune_, rows_counter_, s_);
-        launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, s_);
+        launch_wave_scan(ctx_.p, n_ctx_, 1, max_f_, scan_ys_, cat_, s_);
         if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 1, s_);
         launch_wave_select(ctx_.p, n_ctx_, gsync_.p, nullptr, handle, 1, s_);
         cudaGraph_t body_out = nullptr;
@@ -1180,7 +1181,7 @@ private:
     std::vector<FitRun*> runs_;
     cudaStream_t s_;
     unsigned long long* rows_counter_;
-    bool use_graph_, autotune_, ready_ = false, pair_ = false;
+    bool use_graph_, autotune_, ready_ = false, pair_ = false, cat_ = false;
     HistTune tune_;
     int n_ctx_ = 0, max_f_ = 0, max_leaves_ = 0, mode_ = 0, part_grid_ = 0, scan_ys_ = 0;
     long long rows_ = 0;

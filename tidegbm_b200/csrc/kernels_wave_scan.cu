@@ -41,7 +41,150 @@ __device__ __forceinline__ void children_prefix(const WaveCtx* ctxs, int n_ctx, 
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
+// The histogram job of one child: its node and split outputs, its candidate index, its
+// slot, and (the larger child) the parent and small-sibling slots it is derived from.
+struct ScanTarget {
+    DevNode* N;
+    DevSplit* out;
+    int ci, slot, pslot, sslot;
+    bool derive;
+};
+
+__device__ __forceinline__ ScanTarget scan_target(const WaveCtx& X, int src, int k) {
+    ScanTarget t;
+    t.pslot = t.sslot = 0;
+    t.derive = false;
+    if (src == 0) {
+        t.N = X.nodes;
+        t.out = X.splits;
+        t.ci = kRootCand;
+        t.slot = 0;
+        return t;
+    }
+    const int L = X.ctl->exp_leaf[k >> 1];
+    const int side = k & 1;
+    t.ci = 2 * L + side;
+    t.N = X.spec + t.ci;
+    t.out = X.spec_split + t.ci;
+    t.slot = t.N->slot;
+    const DevNode& A = X.spec[2 * L];
+    const DevNode& B = X.spec[2 * L + 1];
+    const int small = A.count <= B.count ? 0 : 1;  // cpp/src/tree.cpp:423
+    t.derive = side != small;
+    t.pslot = X.nodes[L].slot;
+    t.sslot = X.spec[2 * L + small].slot;
+    return t;
+}
+
+// The last feature job of a child (one warp): the best candidate over its features
+// (best_for_leaf's ascending-feature strict '>', tree.cpp:160-166), written as its split.
+__device__ __forceinline__ void finish_child(const WaveCtx& X, int ci, DevSplit* out, int lane) {
+    const GrowParams& p = X.gp;
+    __threadfence();
+    Cand b{-1e300, 0x7fffffff};
+    for (int k = lane; k < p.n_features; k += 32) {
+        const size_t cs = static_cast<size_t>(ci) * p.n_features + k;
+        const Cand cd{static_cast<volatile double*>(X.cand_gain)[cs], static_cast<volatile int*>(X.cand_key)[cs]};
+        if (better(cd, b)) b = cd;
+    }
+    b = warp_best(b);
+    if (lane == 0) {
+        DevSplit sp{};
+        sp.gain = b.gain;
+        sp.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
+        sp.feature = sp.valid ? b.key / 512 : -1;
+        sp.threshold = sp.valid ? (b.key % 512) / 2 : -1;
+        sp.missing_left = sp.valid ? (b.key & 1) : 1;
+        sp.type = 0;
+        if (sp.valid && X.is_cat != nullptr && X.is_cat[sp.feature]) {
+            // categorical: the winning feature's left mask; missing follows bin 0's side
+            const unsigned long long* m = X.cand_cat + (static_cast<size_t>(ci) * p.n_features + sp.feature) * 4;
+            sp.type = 2;
+            sp.threshold = -1;
+            for (int k = 0; k < 4; ++k) sp.cat[k] = reinterpret_cast<const volatile unsigned long long*>(m)[k];
+            sp.missing_left = static_cast<int>(sp.cat[0] & 1ull);
+        }
+        *out = sp;
+        X.tickets[ci] = 0;  // ready for the next launch
+    }
+}
+
+// Node totals from feature 0 (every feature's bins sum to the same integers) and the
+// node's value (leaf_value, cpp/include/tidegbm/tree.hpp:53-67).
+__device__ __forceinline__ void set_totals(DevNode* N, long long Gt, long long Ht, long long Ct, double inv_gs,
+                                           double inv_hs, double l2) {
+    N->G = Gt;
+    N->H = Ht;
+    N->C = Ct;
+    const double dg = static_cast<double>(Gt) * inv_gs, dh = static_cast<double>(Ht) * inv_hs;
+    N->value = -dg / (dh + l2);
+}
+
+// Numeric features, one warp per (child, feature): every child's histogram scanned by
+// scan_feature_warp (the larger child first derived as parent - smaller), the per-feature
+// bests kept as candidates, and the child's last job picks its split.  Categorical
+// features are left to wave_scan_cat_kernel; the children's tickets count both.
+constexpr int kScanWarpThreads = 256;
+
+__global__ void __launch_bounds__(kScanWarpThreads, 2)
+    wave_scan_warp_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ int s_pref[kMaxWaveCtx + 1];
+    __shared__ int s_jpref[kMaxWaveCtx + 1];
+    children_prefix(ctxs, n_ctx, src, s_pref);
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = 0; c < n_ctx; ++c) {
+            s_jpref[c] = acc;
+            acc += (s_pref[c + 1] - s_pref[c]) * ctxs[c].gp.n_features;
+        }
+        s_jpref[n_ctx] = acc;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wpb = kScanWarpThreads / 32;
+    const int total = s_jpref[n_ctx];
+    for (int jw = blockIdx.x * wpb + (threadIdx.x >> 5); jw < total; jw += gridDim.x * wpb) {
+        int c = 0;
+        while (c + 1 < n_ctx && s_jpref[c + 1] <= jw) ++c;
+        const WaveCtx& X = ctxs[c];
+        const GrowParams& p = X.gp;
+        const int rem = jw - s_jpref[c];
+        const int k = rem / p.n_features, f = rem - k * p.n_features;
+        if (X.is_cat != nullptr && X.is_cat[f]) continue;
+        const ScanTarget t = scan_target(X, src, k);
+        const size_t e = static_cast<size_t>(p.n_features) * kBins;
+        const bool eligible = t.N->depth < p.max_depth && t.N->count >= 2 * p.min_samples_leaf;
+        const double inv_gs = X.st->inv_gscale, inv_hs = X.st->inv_hscale;
+        Cand best{-1e300, 0x7fffffff};
+        if (eligible || f == 0) {
+            const size_t fo = static_cast<size_t>(f) * kBins;
+            const size_t so = static_cast<size_t>(t.slot) * e + fo, po = static_cast<size_t>(t.pslot) * e + fo,
+                         qo = static_cast<size_t>(t.sslot) * e + fo;
+            long long Gt, Ht, Ct;
+            best = scan_feature_warp(X.G + so, X.H + so, X.C + so, X.G + po, X.H + po, X.C + po, X.G + qo, X.H + qo,
+                                     X.C + qo, t.derive, eligible, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
+                                     p.min_samples_leaf, p.min_child_weight, Gt, Ht, Ct);
+            if (f == 0 && lane == 0) set_totals(t.N, Gt, Ht, Ct, inv_gs, inv_hs, p.l2);
+        }
+        int last = 0;
+        if (lane == 0) {
+            const size_t cs = static_cast<size_t>(t.ci) * p.n_features + f;
+            X.cand_gain[cs] = best.gain;
+            X.cand_key[cs] = best.key;
+            __threadfence();
+            last = atomicAdd(&X.tickets[t.ci], 1) == p.n_features - 1;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) finish_child(X, t.ci, t.out, lane);
+    }
+}
+
+// Categorical features, one CTA per (child, feature): the histogram (derived as above)
+// ranked and scanned by scan_categorical (best_categorical, histogram.cpp:195-244).
+__global__ void __launch_bounds__(kScanThreads)
+    wave_scan_cat_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src) {
     pdl_wait();
     pdl_trigger();
     __shared__ int s_pref[kMaxWaveCtx + 1];
@@ -56,99 +199,38 @@ __global__ void __launch_bounds__(kScanThreads) wave_scan_kernel(const WaveCtx* 
         while (c + 1 < n_ctx && s_pref[c + 1] <= j) ++c;
         const WaveCtx& X = ctxs[c];
         const GrowParams& p = X.gp;
-        if (f >= p.n_features) continue;  // uniform over the CTA
+        if (f >= p.n_features || X.is_cat == nullptr || !X.is_cat[f]) continue;  // uniform over the CTA
+        const ScanTarget t = scan_target(X, src, j - s_pref[c]);
         const size_t e = static_cast<size_t>(p.n_features) * kBins;
-        DevNode* N;
-        DevSplit* out;
-        int ci, slot, pslot = 0, sslot = 0;
-        bool derive = false;
-        if (src == 0) {
-            N = X.nodes;
-            out = X.splits;
-            ci = kRootCand;
-            slot = 0;
-        } else {
-            const int k = j - s_pref[c];
-            const int L = X.ctl->exp_leaf[k >> 1];
-            const int side = k & 1;
-            ci = 2 * L + side;
-            N = X.spec + ci;
-            out = X.spec_split + ci;
-            slot = N->slot;
-            const DevNode& A = X.spec[2 * L];
-            const DevNode& B = X.spec[2 * L + 1];
-            const int small = A.count <= B.count ? 0 : 1;  // cpp/src/tree.cpp:423
-            derive = side != small;
-            pslot = X.nodes[L].slot;
-            sslot = X.spec[2 * L + small].slot;
-        }
-        const bool eligible = N->depth < p.max_depth && N->count >= 2 * p.min_samples_leaf;
+        const bool eligible = t.N->depth < p.max_depth && t.N->count >= 2 * p.min_samples_leaf;
         const double inv_gs = X.st->inv_gscale, inv_hs = X.st->inv_hscale;
-        const bool cat = X.is_cat != nullptr && X.is_cat[f] != 0;
         Cand best{-1e300, 0x7fffffff};
         if (eligible || f == 0) {
             const size_t fo = static_cast<size_t>(f) * kBins;
-            const size_t so = static_cast<size_t>(slot) * e + fo, po = static_cast<size_t>(pslot) * e + fo,
-                         qo = static_cast<size_t>(sslot) * e + fo;
+            const size_t so = static_cast<size_t>(t.slot) * e + fo, po = static_cast<size_t>(t.pslot) * e + fo,
+                         qo = static_cast<size_t>(t.sslot) * e + fo;
             long long Gt, Ht, Ct;
             best = scan_feature(X.G + so, X.H + so, X.C + so, X.G + po, X.H + po, X.C + po, X.G + qo, X.H + qo,
-                                X.C + qo, derive, eligible && !cat, f, p.n_bins, inv_gs, inv_hs, p.l2,
-                                p.min_split_gain, p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
-            if (cat && eligible) {
+                                X.C + qo, t.derive, false, f, p.n_bins, inv_gs, inv_hs, p.l2, p.min_split_gain,
+                                p.min_samples_leaf, p.min_child_weight, sm, Gt, Ht, Ct);
+            if (eligible) {
                 // best_categorical over the stored (possibly just derived) histogram
                 __syncthreads();
                 best = scan_categorical(X.G + so, X.H + so, X.C + so, f, inv_gs, inv_hs, p.l2, p.min_split_gain,
                                         p.min_samples_leaf, p.min_child_weight, X.cat_smooth, Gt, Ht, Ct, csm,
-                                        X.cand_cat + (static_cast<size_t>(ci) * p.n_features + f) * 4);
+                                        X.cand_cat + (static_cast<size_t>(t.ci) * p.n_features + f) * 4);
             }
-            if (f == 0 && threadIdx.x == 0) {
-                // node totals from feature 0 (every feature's bins sum to the same integers)
-                N->G = Gt;
-                N->H = Ht;
-                N->C = Ct;
-                const double dg = static_cast<double>(Gt) * inv_gs, dh = static_cast<double>(Ht) * inv_hs;
-                N->value = -dg / (dh + p.l2);  // leaf_value, cpp/include/tidegbm/tree.hpp:53-67
-            }
+            if (f == 0 && threadIdx.x == 0) set_totals(t.N, Gt, Ht, Ct, inv_gs, inv_hs, p.l2);
         }
         if (threadIdx.x == 0) {
-            const size_t cs = static_cast<size_t>(ci) * p.n_features + f;
+            const size_t cs = static_cast<size_t>(t.ci) * p.n_features + f;
             X.cand_gain[cs] = best.gain;
             X.cand_key[cs] = best.key;
             __threadfence();
-            last = atomicAdd(&X.tickets[ci], 1) == p.n_features - 1;
+            last = atomicAdd(&X.tickets[t.ci], 1) == p.n_features - 1;
         }
         __syncthreads();
-        if (last && threadIdx.x < 32) {
-            const int lane = threadIdx.x;
-            __threadfence();
-            Cand b{-1e300, 0x7fffffff};
-            for (int k = lane; k < p.n_features; k += 32) {
-                const size_t cs = static_cast<size_t>(ci) * p.n_features + k;
-                const Cand cd{static_cast<volatile double*>(X.cand_gain)[cs], static_cast<volatile int*>(X.cand_key)[cs]};
-                if (better(cd, b)) b = cd;
-            }
-            b = warp_best(b);
-            if (lane == 0) {
-                DevSplit sp{};
-                sp.gain = b.gain;
-                sp.valid = (b.key != 0x7fffffff) && b.gain >= p.min_split_gain;
-                sp.feature = sp.valid ? b.key / 512 : -1;
-                sp.threshold = sp.valid ? (b.key % 512) / 2 : -1;
-                sp.missing_left = sp.valid ? (b.key & 1) : 1;
-                sp.type = 0;
-                if (sp.valid && X.is_cat != nullptr && X.is_cat[sp.feature]) {
-                    // categorical: the winning feature's left mask; missing follows bin 0's side
-                    const unsigned long long* m =
-                        X.cand_cat + (static_cast<size_t>(ci) * p.n_features + sp.feature) * 4;
-                    sp.type = 2;
-                    sp.threshold = -1;
-                    for (int k = 0; k < 4; ++k) sp.cat[k] = reinterpret_cast<const volatile unsigned long long*>(m)[k];
-                    sp.missing_left = static_cast<int>(sp.cat[0] & 1ull);
-                }
-                *out = sp;
-                X.tickets[ci] = 0;  // ready for the next launch
-            }
-        }
+        if (last && threadIdx.x < 32) finish_child(X, t.ci, t.out, static_cast<int>(threadIdx.x));
         __syncthreads();  // shared state reuse
     }
 }
@@ -179,6 +261,10 @@ __global__ void __launch_bounds__(32)
     const int lane = threadIdx.x;
     __shared__ double s_gain[kMaxLeavesCap + 1];
     __shared__ int s_id[kMaxLeavesCap + 1];
+    // every node's selection state, staged once: its split's gain and whether it is a
+    // candidate (restaged when the pair budget runs out and the splits change)
+    __shared__ double s_ng[kMaxNodes];
+    __shared__ unsigned char s_nc[kMaxNodes];
     int active = 0;
     if (ctl->active) {
         const int budget = p.max_leaves - 1;
@@ -194,6 +280,13 @@ __global__ void __launch_bounds__(32)
         auto split_of = [&](int k) -> DevSplit {
             return (X.pair_on && pair_used < X.max_pair) ? X.splits_pair[k] : splits[k];
         };
+        auto stage = [&](int k) {
+            const DevSplit S = split_of(k);
+            s_nc[k] = candidate(p, nodes[k], S) ? 1 : 0;
+            s_ng[k] = S.gain;
+        };
+        for (int k = lane; k < nn; k += 32) stage(k);
+        __syncwarp();
         bool finished = false;
         while (true) {
             if (done_splits >= budget || runaway) {
@@ -203,10 +296,9 @@ __global__ void __launch_bounds__(32)
             double bg = 0.0;
             int bi = 0x7fffffff;
             for (int k = lane; k < nn; k += 32) {
-                const DevSplit S = split_of(k);
-                if (!candidate(p, nodes[k], S)) continue;
-                if (bi == 0x7fffffff || better_leaf(S.gain, k, bg, bi)) {
-                    bg = S.gain;
+                if (!s_nc[k]) continue;
+                if (bi == 0x7fffffff || better_leaf(s_ng[k], k, bg, bi)) {
+                    bg = s_ng[k];
                     bi = k;
                 }
             }
@@ -260,9 +352,17 @@ __global__ void __launch_bounds__(32)
             }
             __syncwarp();
             __threadfence_block();
+            const bool pairs_before = X.pair_on && pair_used < X.max_pair;
             nn += 2;
             done_splits += 1;
             if (S.type == 1) pair_used += 1;
+            if (pairs_before != (X.pair_on && pair_used < X.max_pair)) {
+                for (int k = lane; k < nn; k += 32) stage(k);  // the budget ran out: axis splits from here
+            } else {
+                if (lane == 0) s_nc[bi] = 0;
+                if (lane < 2) stage(nn - 2 + lane);
+            }
+            __syncwarp();
         }
         int n_exp = 0;
         if (!finished) {
@@ -273,9 +373,8 @@ __global__ void __launch_bounds__(32)
                 bool is_c = false;
                 double gk = 0.0;
                 if (k < nn) {
-                    const DevSplit S = split_of(k);
-                    is_c = candidate(p, nodes[k], S);
-                    gk = S.gain;
+                    is_c = s_nc[k] != 0;
+                    gk = s_ng[k];
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, is_c);
                 if (is_c) {
@@ -596,8 +695,12 @@ void launch_wave_pair(const WaveCtx* ctxs, int n_ctx, int src, cudaStream_t s) {
     launch_pdl(wave_pair_kernel, dim3(kMaxPairs, 32), dim3(kScanThreads), 0, s, "wave_pair launch", ctxs, n_ctx, src);
 }
 
-void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, cudaStream_t s) {
-    launch_pdl(wave_scan_kernel, dim3(max_f, ys), dim3(kScanThreads), 0, s, "wave_scan launch", ctxs, n_ctx, src);
+void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, bool any_cat, cudaStream_t s) {
+    launch_pdl(wave_scan_warp_kernel, dim3(148 * 2), dim3(kScanWarpThreads), 0, s, "wave_scan launch", ctxs, n_ctx,
+               src);
+    if (any_cat)
+        launch_pdl(wave_scan_cat_kernel, dim3(max_f, ys), dim3(kScanThreads), 0, s, "wave_scan_cat launch", ctxs, n_ctx,
+                   src);
 }
 
 void launch_wave_select(const WaveCtx* ctxs, int n_ctx, int* gsync, unsigned* host_flag, unsigned long long cond,

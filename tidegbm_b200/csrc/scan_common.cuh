@@ -126,6 +126,117 @@ __device__ __forceinline__ Cand scan_feature(long long* __restrict__ Gf, long lo
     return best;
 }
 
+// One warp scans one feature: lane l owns bins [8l, 8l + 8) (the same arithmetic, in the
+// same order, as scan_feature, without block barriers).  Returns the warp's best candidate
+// and the feature's totals in every lane.
+__device__ __forceinline__ Cand scan_feature_warp(long long* __restrict__ Gf, long long* __restrict__ Hf,
+                                                  int* __restrict__ Cf, const long long* __restrict__ PGf,
+                                                  const long long* __restrict__ PHf, const int* __restrict__ PCf,
+                                                  const long long* __restrict__ SGf, const long long* __restrict__ SHf,
+                                                  const int* __restrict__ SCf, bool derive, bool scan, int f, int n_bins,
+                                                  double inv_gs, double inv_hs, double lam, double gamma, int min_leaf,
+                                                  double min_hess, long long& Gt, long long& Ht, long long& Ct) {
+    constexpr int kPer = kBins / 32;
+    const int lane = threadIdx.x & 31, b0 = lane * kPer;
+    long long g[kPer], hh[kPer], c[kPer];
+    {
+        const longlong2* g2 = reinterpret_cast<const longlong2*>((derive ? PGf : Gf) + b0);
+        const longlong2* h2 = reinterpret_cast<const longlong2*>((derive ? PHf : Hf) + b0);
+        const int4* c4 = reinterpret_cast<const int4*>((derive ? PCf : Cf) + b0);
+#pragma unroll
+        for (int i = 0; i < kPer / 2; ++i) {
+            const longlong2 a = g2[i], b = h2[i];
+            g[2 * i] = a.x;
+            g[2 * i + 1] = a.y;
+            hh[2 * i] = b.x;
+            hh[2 * i + 1] = b.y;
+        }
+#pragma unroll
+        for (int i = 0; i < kPer / 4; ++i) {
+            const int4 a = c4[i];
+            c[4 * i] = a.x;
+            c[4 * i + 1] = a.y;
+            c[4 * i + 2] = a.z;
+            c[4 * i + 3] = a.w;
+        }
+    }
+    if (derive) {
+        const longlong2* g2 = reinterpret_cast<const longlong2*>(SGf + b0);
+        const longlong2* h2 = reinterpret_cast<const longlong2*>(SHf + b0);
+        const int4* c4 = reinterpret_cast<const int4*>(SCf + b0);
+#pragma unroll
+        for (int i = 0; i < kPer / 2; ++i) {
+            const longlong2 a = g2[i], b = h2[i];
+            g[2 * i] -= a.x;
+            g[2 * i + 1] -= a.y;
+            hh[2 * i] -= b.x;
+            hh[2 * i + 1] -= b.y;
+        }
+#pragma unroll
+        for (int i = 0; i < kPer / 4; ++i) {
+            const int4 a = c4[i];
+            c[4 * i] -= a.x;
+            c[4 * i + 1] -= a.y;
+            c[4 * i + 2] -= a.z;
+            c[4 * i + 3] -= a.w;
+        }
+        longlong2* go = reinterpret_cast<longlong2*>(Gf + b0);
+        longlong2* ho = reinterpret_cast<longlong2*>(Hf + b0);
+        int4* co = reinterpret_cast<int4*>(Cf + b0);
+#pragma unroll
+        for (int i = 0; i < kPer / 2; ++i) {
+            go[i] = make_longlong2(g[2 * i], g[2 * i + 1]);
+            ho[i] = make_longlong2(hh[2 * i], hh[2 * i + 1]);
+        }
+#pragma unroll
+        for (int i = 0; i < kPer / 4; ++i)
+            co[i] = make_int4(static_cast<int>(c[4 * i]), static_cast<int>(c[4 * i + 1]), static_cast<int>(c[4 * i + 2]),
+                              static_cast<int>(c[4 * i + 3]));
+    }
+    long long tg = 0, th = 0, tc = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        tg += g[i];
+        th += hh[i];
+        tc += c[i];
+    }
+    const long long ig = warp_incl_scan(tg, lane), ih = warp_incl_scan(th, lane), ic = warp_incl_scan(tc, lane);
+    Gt = __shfl_sync(0xffffffffu, ig, 31);
+    Ht = __shfl_sync(0xffffffffu, ih, 31);
+    Ct = __shfl_sync(0xffffffffu, ic, 31);
+    const long long G0 = __shfl_sync(0xffffffffu, g[0], 0), H0 = __shfl_sync(0xffffffffu, hh[0], 0),
+                    C0 = __shfl_sync(0xffffffffu, c[0], 0);
+    Cand best{-1e300, 0x7fffffff};
+    if (scan) {
+        const double dGt = static_cast<double>(Gt) * inv_gs, dHt = static_cast<double>(Ht) * inv_hs;
+        const double parent = (dGt * dGt) / (dHt + lam);
+        long long rg = ig - tg, rh = ih - th, rc = ic - tc;  // bins before this lane's
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            rg += g[i];
+            rh += hh[i];
+            rc += c[i];
+            const int b = b0 + i;
+            if (b < 1 || b > n_bins - 2 || c[i] == 0) continue;
+            const long long GL = rg - G0, HL = rh - H0, CL = rc - C0;  // bins 1..b
+#pragma unroll
+            for (int ml = 0; ml <= 1; ++ml) {
+                const long long gL = GL + (ml ? G0 : 0), hL = HL + (ml ? H0 : 0), cL = CL + (ml ? C0 : 0);
+                const long long cR = Ct - cL;
+                if (cL < min_leaf || cR < min_leaf) continue;
+                const double dgL = static_cast<double>(gL) * inv_gs, dhL = static_cast<double>(hL) * inv_hs;
+                const double dgR = static_cast<double>(Gt - gL) * inv_gs, dhR = static_cast<double>(Ht - hL) * inv_hs;
+                if (dhL < min_hess || dhR < min_hess) continue;
+                const double gain = 0.5 * ((dgL * dgL) / (dhL + lam) + (dgR * dgR) / (dhR + lam) - parent) - gamma;
+                const Cand cand{gain, f * 512 + b * 2 + ml};
+                if (better(cand, best)) best = cand;
+            }
+        }
+        best = warp_best(best);
+    }
+    return best;
+}
+
 // ---- categorical features ---------------------------------------------------------------
 //
 // std::sort of libstdc++ (introsort: median-of-three quicksort down to runs of 16, heap

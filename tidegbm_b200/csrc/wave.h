@@ -160,7 +160,7 @@ struct HistTune {
 int wave_hist_clusters(int cluster);  // co-resident clusters of the histogram kernel
 void launch_wave_hist(int mode, const WaveCtx* ctxs, int n_ctx, int src, HistTune tune,
                       unsigned long long* rows_counter, cudaStream_t s);
-void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, cudaStream_t s);
+void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, bool any_cat, cudaStream_t s);
 // gsync: 2 device ints (flag, ticket), zero.  host_flag: mapped host word or nullptr;
 // cond / use_cond: the graph's loop condition (set to "any context still growing").
 void launch_wave_select(const WaveCtx* ctxs, int n_ctx, int* gsync, unsigned* host_flag,
