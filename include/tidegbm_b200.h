@@ -125,7 +125,9 @@ TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
  * sort), "timed_selects" (wave selects run in the timed range: with batched growth a tree
  * runs 3 + 5 x (selects - 1) kernels in its waves), "graph_used" (1 when the waves ran as
  * a CUDA graph), "hist_cluster" / "hist_clusters" (the tuned launch shape of the
- * histogram: CTAs per cluster, clusters launched).  Unknown names return -1. */
+ * histogram: CTAs per cluster, clusters launched), "driver" (set-up of the batched
+ * growth), "finish_sync" (from the tree loop's end to the GOSS sampler's stop).  Unknown
+ * names return -1. */
 TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);
 
 /* Host part of Binner::fit (cpp/src/binning.cpp:14-102), numeric features, no mask:

@@ -878,12 +878,14 @@ void FitRun::tree_end(int t) {
 }
 
 bool FitRun::finish() {
+    const double tf = now();
     check(cudaStreamSynchronize(s), "tree loop");
     if (sampler) {
         sampler->stop();
         st.t_producer = sampler->producer_seconds();
         sampler.reset();
     }
+    st.t_finish_sync = now() - tf;
     const double td = now();
     std::vector<DevNode> nodes_h(static_cast<size_t>(T) * max_nodes);
     std::vector<DevTreeState> st_h(T);
@@ -1221,8 +1223,10 @@ void fit_runs(std::vector<FitRun*>& runs, cudaStream_t s) {
     }
     std::unique_ptr<WaveDriver> drv;
     if (wave) {
+        const double td = now();
         std::vector<FitRun*> rr(runs.begin(), runs.end());
         drv = std::make_unique<WaveDriver>(rr, s, c.graph != 0, c.hist_tune != 0, r0.rows_counter.p);
+        for (auto* r : runs) r->st.t_driver = now() - td;
     }
     const double ttree = now();
     for (int t = 0; t < T; ++t) {

@@ -104,6 +104,7 @@ struct FitStats {
     double t_total = 0, t_sort = 0, t_binfit = 0, t_upload = 0, t_transform = 0, t_trees = 0, t_download = 0;
     double t_rng = 0;
     double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
+    double t_driver = 0, t_finish_sync = 0;  // wave driver set-up; tree loop's tail to the sampler's stop
     double t_bin_counts = 0, t_bin_draws = 0, t_bin_edges = 0;  // stages of the device binner
     int goss_refits = 0;  // 1 when the fit was repeated with the 64-bit GOSS sort
     double t_pre_upload = 0, t_prep = 0;  // host set-up before the upload and before the tree loop

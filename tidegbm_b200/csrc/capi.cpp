@@ -435,6 +435,8 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "graph_used") *out = s.graph_used;
         else if (k == "hist_cluster") *out = s.hist_cluster;
         else if (k == "hist_clusters") *out = s.hist_clusters;
+        else if (k == "driver") *out = s.t_driver;
+        else if (k == "finish_sync") *out = s.t_finish_sync;
         else if (k == "pre_upload") *out = s.t_pre_upload;
         else if (k == "prep") *out = s.t_prep;
         else throw tgb::TideError("unknown fit stat: " + k);

@@ -607,12 +607,16 @@ __device__ __forceinline__ int block_sum(int v, int* red) {
     return t;
 }
 
-// One row's payloads from element `from` to element `to` of the payload arrays.
-__device__ __forceinline__ void move_payload(const WaveCtx& X, long long from, long long to) {
-    if (X.pay_bytes == 8) static_cast<long long*>(X.gq)[to] = static_cast<const long long*>(X.gq)[from];
-    else if (X.pay_bytes == 4) static_cast<int*>(X.gq)[to] = static_cast<const int*>(X.gq)[from];
-    else static_cast<short*>(X.gq)[to] = static_cast<const short*>(X.gq)[from];
-    if (X.hq != nullptr) static_cast<long long*>(X.hq)[to] = static_cast<const long long*>(X.hq)[from];
+// A row's g payload (element i of the payload array), widened to 64 bits, and back.
+__device__ __forceinline__ long long load_payload(const WaveCtx& X, long long i) {
+    if (X.pay_bytes == 8) return static_cast<const long long*>(X.gq)[i];
+    if (X.pay_bytes == 4) return static_cast<const int*>(X.gq)[i];
+    return static_cast<const short*>(X.gq)[i];
+}
+__device__ __forceinline__ void store_payload(const WaveCtx& X, long long i, long long v) {
+    if (X.pay_bytes == 8) static_cast<long long*>(X.gq)[i] = v;
+    else if (X.pay_bytes == 4) static_cast<int*>(X.gq)[i] = static_cast<int>(v);
+    else static_cast<short*>(X.gq)[i] = static_cast<short>(v);
 }
 
 // Global tile t -> (context, expansion, tile within the expansion).
@@ -766,6 +770,17 @@ __global__ void __launch_bounds__(kPartThreads)
         int32_t row[kPartPer];
         bool left[kPartPer];
         load_tile(X, in, S, base, end, row, left);
+        // the rows' payloads move with them (same positions in the other buffer); loaded
+        // here so that their latency overlaps the ranks below
+        const long long from0 = static_cast<long long>(N.buf) * X.pay_pitch + N.start;
+        const long long to0 = static_cast<long long>(1 - N.buf) * X.pay_pitch + N.start;
+        long long pg[kPartPer], ph[kPartPer];
+#pragma unroll
+        for (int i = 0; i < kPartPer; ++i) {
+            const int kk = base + i * kPartThreads + threadIdx.x;
+            pg[i] = row[i] >= 0 ? load_payload(X, from0 + kk) : 0;
+            ph[i] = row[i] >= 0 && X.hq != nullptr ? static_cast<const long long*>(X.hq)[from0 + kk] : 0;
+        }
         unsigned bal[kPartPer];
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) {
@@ -785,9 +800,6 @@ __global__ void __launch_bounds__(kPartThreads)
             }
             excl[i] = e;
         }
-        // the rows' payloads move with them (same positions in the other buffer)
-        const long long from0 = static_cast<long long>(N.buf) * X.pay_pitch + N.start;
-        const long long to0 = static_cast<long long>(1 - N.buf) * X.pay_pitch + N.start;
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) {
             if (row[i] < 0) continue;
@@ -795,7 +807,8 @@ __global__ void __launch_bounds__(kPartThreads)
             const int lrank = excl[i] + __popc(bal[i] & lt_mask);
             const int dst = left[i] ? left0 + lrank : n_left + (base - left0) + (kk - base - lrank);
             out[dst] = row[i];
-            move_payload(X, from0 + kk, to0 + dst);
+            store_payload(X, to0 + dst, pg[i]);
+            if (X.hq != nullptr) static_cast<long long*>(X.hq)[to0 + dst] = ph[i];
         }
         __syncthreads();  // wc reuse
     }

@@ -261,10 +261,15 @@ __global__ void __launch_bounds__(32)
     const int lane = threadIdx.x;
     __shared__ double s_gain[kMaxLeavesCap + 1];
     __shared__ int s_id[kMaxLeavesCap + 1];
-    // every node's selection state, staged once: its split's gain and whether it is a
-    // candidate (restaged when the pair budget runs out and the splits change)
+    // Selection state staged once, so that the commit loop reads no global memory: per
+    // node its current split's gain, candidacy, type and with-pairs type, and whether it
+    // is expanded; per expanded node the same for its two planned children.  Restaged
+    // from the node table when the pair budget runs out (the splits change).
     __shared__ double s_ng[kMaxNodes];
-    __shared__ unsigned char s_nc[kMaxNodes];
+    __shared__ unsigned char s_nc[kMaxNodes], s_ex[kMaxNodes], s_ty[kMaxNodes], s_pty[kMaxNodes];
+    __shared__ double s_cg[2 * kMaxNodes];
+    __shared__ unsigned char s_cc[2 * kMaxNodes], s_cty[2 * kMaxNodes], s_cpty[2 * kMaxNodes];
+    __shared__ int s_commit[kMaxLeavesCap];
     int active = 0;
     if (ctl->active) {
         const int budget = p.max_leaves - 1;
@@ -277,16 +282,65 @@ __global__ void __launch_bounds__(32)
         int pair_used = ctl->pair_used;
         // the split a leaf takes: with the PAIR candidates while the tree's pair budget lasts
         // (tree.cpp:214-218, re-scored after every pair split, tree.cpp:393-396)
-        auto split_of = [&](int k) -> DevSplit {
-            return (X.pair_on && pair_used < X.max_pair) ? X.splits_pair[k] : splits[k];
+        auto pairs_on = [&]() { return X.pair_on && pair_used < X.max_pair; };
+        auto stage_all = [&]() {
+            const bool pr = pairs_on();
+            for (int k = lane; k < nn; k += 32) {
+                const DevSplit S = pr ? X.splits_pair[k] : splits[k];
+                s_nc[k] = candidate(p, nodes[k], S) ? 1 : 0;
+                s_ng[k] = S.gain;
+                s_ty[k] = static_cast<unsigned char>(S.type);
+                s_pty[k] = X.pair_on ? static_cast<unsigned char>(X.splits_pair[k].type) : 0;
+                const int ex = ctl->expanded[k];
+                s_ex[k] = static_cast<unsigned char>(ex);
+                if (ex) {
+                    for (int sd = 0; sd < 2; ++sd) {
+                        const int ci = 2 * k + sd;
+                        const DevSplit C = pr ? X.spec_split_pair[ci] : X.spec_split[ci];
+                        s_cc[ci] = candidate(p, X.spec[ci], C) ? 1 : 0;
+                        s_cg[ci] = C.gain;
+                        s_cty[ci] = static_cast<unsigned char>(C.type);
+                        s_cpty[ci] = X.pair_on ? static_cast<unsigned char>(X.spec_split_pair[ci].type) : 0;
+                    }
+                }
+            }
+            __syncwarp();
         };
-        auto stage = [&](int k) {
-            const DevSplit S = split_of(k);
-            s_nc[k] = candidate(p, nodes[k], S) ? 1 : 0;
-            s_ng[k] = S.gain;
+        // the node-table writes of the pending commits (children ids nn_first + 2i, + 1 for
+        // the i-th), issued in parallel; `pr`: the pair state they were committed under
+        int n_commit = 0, nn_first = nn;
+        auto flush = [&](bool pr) {
+            for (int i = lane; i < n_commit; i += 32) {
+                const int bi = s_commit[i], nc = nn_first + 2 * i;
+                const DevSplit S = pr ? X.splits_pair[bi] : splits[bi];
+                DevNode& P = nodes[bi];
+                P.is_leaf = 0;
+                P.feature = S.feature;
+                P.threshold = S.threshold;
+                P.missing_left = S.missing_left;
+                P.gain = S.gain;
+                P.type = S.type;
+                P.feature2 = S.type == 1 ? S.feature2 : -1;
+                for (int k = 0; k < 4; ++k) P.cat[k] = S.cat[k];
+                P.left = nc;
+                P.right = nc + 1;
+                nodes[nc] = X.spec[2 * bi];
+                nodes[nc + 1] = X.spec[2 * bi + 1];
+                splits[nc] = X.spec_split[2 * bi];
+                splits[nc + 1] = X.spec_split[2 * bi + 1];
+                if (X.pair_on) {
+                    X.splits_pair[nc] = X.spec_split_pair[2 * bi];
+                    X.splits_pair[nc + 1] = X.spec_split_pair[2 * bi + 1];
+                }
+                ctl->expanded[nc] = 0;
+                ctl->expanded[nc + 1] = 0;
+            }
+            __syncwarp();
+            __threadfence_block();
+            n_commit = 0;
+            nn_first = nn;
         };
-        for (int k = lane; k < nn; k += 32) stage(k);
-        __syncwarp();
+        stage_all();
         bool finished = false;
         while (true) {
             if (done_splits >= budget || runaway) {
@@ -315,55 +369,46 @@ __global__ void __launch_bounds__(32)
                 finished = true;
                 break;
             }
-            const int ex = ctl->expanded[bi];
+            const int ex = s_ex[bi];
             if (!ex) break;
             // an expansion planned with bi's PAIR split while the budget lasted is void once the
             // budget is spent (bi now takes its axis split): plan bi again
-            if (ex == 2 && !(X.pair_on && pair_used < X.max_pair) && X.splits_pair[bi].type == 1) {
-                if (lane == 0) ctl->expanded[bi] = 0;
+            if (ex == 2 && !pairs_on() && s_pty[bi] == 1) {
+                if (lane == 0) {
+                    ctl->expanded[bi] = 0;
+                    s_ex[bi] = 0;
+                }
                 __syncwarp();
                 __threadfence_block();
                 break;
             }
             // commit: the split of bi, children ids nn, nn + 1 (grow_tree's numbering)
-            const DevSplit S = split_of(bi);
+            const bool pr_before = pairs_on();
+            const int ty = s_ty[bi];
             if (lane == 0) {
-                DevNode& P = nodes[bi];
-                P.is_leaf = 0;
-                P.feature = S.feature;
-                P.threshold = S.threshold;
-                P.missing_left = S.missing_left;
-                P.gain = S.gain;
-                P.type = S.type;
-                P.feature2 = S.type == 1 ? S.feature2 : -1;
-                for (int k = 0; k < 4; ++k) P.cat[k] = S.cat[k];
-                P.left = nn;
-                P.right = nn + 1;
-                nodes[nn] = X.spec[2 * bi];
-                nodes[nn + 1] = X.spec[2 * bi + 1];
-                splits[nn] = X.spec_split[2 * bi];
-                splits[nn + 1] = X.spec_split[2 * bi + 1];
-                if (X.pair_on) {
-                    X.splits_pair[nn] = X.spec_split_pair[2 * bi];
-                    X.splits_pair[nn + 1] = X.spec_split_pair[2 * bi + 1];
-                }
-                ctl->expanded[nn] = 0;
-                ctl->expanded[nn + 1] = 0;
+                s_commit[n_commit] = bi;
+                s_nc[bi] = 0;
+            }
+            if (lane < 2) {
+                const int k = nn + lane, ci = 2 * bi + lane;
+                s_nc[k] = s_cc[ci];
+                s_ng[k] = s_cg[ci];
+                s_ex[k] = 0;
+                s_ty[k] = s_cty[ci];
+                s_pty[k] = s_cpty[ci];
             }
             __syncwarp();
-            __threadfence_block();
-            const bool pairs_before = X.pair_on && pair_used < X.max_pair;
+            n_commit += 1;
             nn += 2;
             done_splits += 1;
-            if (S.type == 1) pair_used += 1;
-            if (pairs_before != (X.pair_on && pair_used < X.max_pair)) {
-                for (int k = lane; k < nn; k += 32) stage(k);  // the budget ran out: axis splits from here
-            } else {
-                if (lane == 0) s_nc[bi] = 0;
-                if (lane < 2) stage(nn - 2 + lane);
+            if (ty == 1) pair_used += 1;
+            if (pr_before != pairs_on()) {
+                // the budget ran out: write the commits so far, then axis splits from here
+                flush(pr_before);
+                stage_all();
             }
-            __syncwarp();
         }
+        flush(pairs_on());
         int n_exp = 0;
         if (!finished) {
             // candidates of the new state, best first
