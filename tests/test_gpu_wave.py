@@ -70,6 +70,26 @@ def test_waves_equal_one_split_loop(native, name):
     _same(_fit(native, p, grow=1, **params), _fit(native, p, grow=0, **params))
 
 
+@pytest.mark.parametrize("cap", [1, 2, 5])
+def test_expansion_cap_grows_the_same_trees(native, cap):
+    """wave_expand caps the speculative expansions a wave plans (1: only the best leaf,
+    the one-split order in waves); every cap grows the same trees, with more waves and
+    fewer expansions than the uncapped default."""
+    from tidegbm_b200 import panels
+
+    p = panels.panel_scale(n_dates=60, n_entities=1500, n_features=20)
+    params = dict(n_estimators=6, learning_rate=0.1, max_depth=8, horizon=1, objective="mse", goss=1,
+                  pair_splits=False, grow=1, timing_from=0)
+    a = _fit(native, p, wave_expand=cap, **params)
+    b = _fit(native, p, **params)
+    _same(a, b)
+    sa, sb = a.fit_stats(), b.fit_stats()
+    assert sa["expansions"] <= sb["expansions"]
+    assert sa["timed_selects"] >= sb["timed_selects"]
+    if cap == 1:  # one expansion per select: every expansion is committed
+        assert sa["expansions"] == sum(int((~t.is_leaf.astype(bool)).sum()) for t in a.trees())
+
+
 def test_graph_loop_equals_host_waves(native):
     from tidegbm_b200 import panels
 

@@ -93,6 +93,7 @@ void Config::validate() const {
     if (goss_top <= 0.0) throw TideError("GPU path: goss_top must be > 0");
     if (hist_bits != 0 && hist_bits != 8 && hist_bits != 16)
         throw TideError("hist_bits must be 0 (exact), 16 or 8 (quantised gradients)");
+    if (wave_expand < 0) throw TideError("wave_expand must be >= 0 (0: every candidate within the budget)");
 }
 
 namespace {
@@ -740,6 +741,7 @@ WaveCtx FitRun::wave_ctx() const {
     w.goss_scale = use_goss ? goss_scale : 1.0;
     w.n_slots = n_slots;
     w.max_tiles = max_tiles;
+    w.max_expand = c.wave_expand;
     w.is_cat = D.is_cat.p;
     w.cand_cat = D.cand_cat.p;
     w.cat_smooth = c.cat_smooth;
@@ -903,7 +905,11 @@ bool FitRun::finish() {
         check(cudaMemcpyAsync(&overflow, D.goss_overflow.p, sizeof(int), cudaMemcpyDeviceToHost, s), "overflow flag");
     if (c.grow != 0)
         check(cudaMemcpyAsync(&wave_error, &D.ctl.p->error, sizeof(int), cudaMemcpyDeviceToHost, s), "wave error flag");
+    int exp_total = 0;
+    if (c.grow != 0)
+        check(cudaMemcpyAsync(&exp_total, &D.ctl.p->exp_total, sizeof(int), cudaMemcpyDeviceToHost, s), "expansions");
     check(cudaStreamSynchronize(s), "D2H");
+    st.expansions = exp_total;
     if (wave_error) throw TideError("GPU path: a wave outgrew its histogram slots or partition tiles");
     B.trees.assign(T, HostTree());
     for (int t = 0; t < T; ++t) {

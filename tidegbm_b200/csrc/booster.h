@@ -75,6 +75,9 @@ struct Config {
     // Batched growth: tune the histogram's launch shape on the first tree (1), or use the
     // default (0); the choice is kept per shape of the work for the process.
     int hist_tune = 1;
+    // Batched growth: expansions a wave may plan (0: every leaf ranked within the splits
+    // left, the widest speculation; k: the k best).  Any value grows the same tree.
+    int wave_expand = 0;
     // Measurement hooks (no effect on results): CUDA events around trees
     // [timing_from, timing_to) (timing_to < 0: through the last tree), and per-launch
     // events around every histogram kernel in that range.
@@ -105,6 +108,7 @@ struct FitStats {
     double t_rng = 0;
     double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
     double t_driver = 0, t_finish_sync = 0;  // wave driver set-up; tree loop's tail to the sampler's stop
+    long long expansions = 0;                // leaves expanded (children histogrammed) over the fit's trees
     double t_bin_counts = 0, t_bin_draws = 0, t_bin_edges = 0;  // stages of the device binner
     int goss_refits = 0;  // 1 when the fit was repeated with the 64-bit GOSS sort
     double t_pre_upload = 0, t_prep = 0;  // host set-up before the upload and before the tree loop

@@ -149,6 +149,7 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "grow") c.grow = static_cast<int>(v);
         else if (k == "graph") c.graph = static_cast<int>(v);
         else if (k == "hist_tune") c.hist_tune = static_cast<int>(v);
+        else if (k == "wave_expand") c.wave_expand = static_cast<int>(v);
         else if (k == "cat_min_count") c.cat_min_count = static_cast<int>(v);
         else if (k == "pair_top_k") c.pair_top_k = static_cast<int>(v);
         else if (k == "max_pair_splits_per_tree") c.max_pair_splits_per_tree = static_cast<int>(v);
@@ -436,6 +437,7 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "hist_cluster") *out = s.hist_cluster;
         else if (k == "hist_clusters") *out = s.hist_clusters;
         else if (k == "driver") *out = s.t_driver;
+        else if (k == "expansions") *out = static_cast<double>(s.expansions);
         else if (k == "finish_sync") *out = s.t_finish_sync;
         else if (k == "pre_upload") *out = s.t_pre_upload;
         else if (k == "prep") *out = s.t_prep;

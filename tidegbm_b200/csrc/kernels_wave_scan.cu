@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(32)
                     int rank = 0;
                     for (int q = 0; q < nc; ++q)
                         if (q != i && better_leaf(s_gain[q], s_id[q], s_gain[i], s_id[i])) ++rank;
-                    take = rank < B && !ctl->expanded[s_id[i]];
+                    take = rank < B && (X.max_expand <= 0 || rank < X.max_expand) && !ctl->expanded[s_id[i]];
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, take);
                 int tiles = 0;
@@ -490,6 +490,7 @@ __global__ void __launch_bounds__(32)
                 ctl->tiles_total = base_tiles;
                 ctl->slot0 = slot_first;
                 ctl->exp_counter += n_exp;
+                ctl->exp_total += n_exp;
                 if (slot_first + 2 * n_exp > X.n_slots || base_tiles > X.max_tiles) ctl->error = 1;
             }
             active = n_exp > 0 && slot_first + 2 * n_exp <= X.n_slots && base_tiles <= X.max_tiles;

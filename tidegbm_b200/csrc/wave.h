@@ -70,7 +70,8 @@ struct WaveCtl {
     int error;        // a slot, buffer or wave-count bound was hit (never expected)
     int waves;        // selects run for this tree (bounded: a tree needs at most max_leaves)
     int pair_used;    // PAIR splits committed in this tree
-    int pad[3];
+    int exp_total;    // expansions planned over all trees of the fit (not reset per tree)
+    int pad[2];
     int exp_leaf[kMaxLeavesCap];
     int exp_tile0[kMaxLeavesCap + 1];
     int expanded[kMaxNodes];  // 0 not expanded; 1, 2: children planned by the axis, with-pairs split
@@ -109,6 +110,8 @@ struct WaveCtx {
     double goss_scale;
     int n_slots;
     int max_tiles;
+    int max_expand;  // expansions a select may plan (0: every candidate ranked within the budget)
+    int pad_expand;
     // categorical features (nullptr: none): flags per feature, the left masks of the scan
     // candidates [(2 * kMaxNodes + 1)][F][4], and the ranking's smoothing (cat_smooth)
     const uint8_t* is_cat;
