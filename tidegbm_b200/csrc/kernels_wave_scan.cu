@@ -247,7 +247,9 @@ __device__ __forceinline__ bool better_leaf(double ga, int ia, double gb, int ib
     return ga > gb || (ga == gb && ia < ib);
 }
 
-__global__ void __launch_bounds__(32)
+constexpr int kSelectThreads = 256;  // all stage the selection state; warp 0 then selects
+
+__global__ void __launch_bounds__(kSelectThreads)
     wave_select_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int* gsync, unsigned* host_flag,
                        cudaGraphConditionalHandle cond, int use_cond) {
     pdl_wait();
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(32)
     DevTreeState* st = X.st;
     DevNode* nodes = X.nodes;
     DevSplit* splits = X.splits;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     __shared__ double s_gain[kMaxLeavesCap + 1];
     __shared__ int s_id[kMaxLeavesCap + 1];
     // Selection state staged once, so that the commit loop reads no global memory: per
@@ -276,16 +278,15 @@ __global__ void __launch_bounds__(32)
         // every select commits at least one split or ends the tree, so a tree takes at most
         // max_leaves of them; past that bound the tree is ended with the error flag set
         const bool runaway = ctl->waves > p.max_leaves + 1;
-        if (lane == 0) ctl->waves += 1;
         int nn = st->n_nodes;
         int done_splits = ctl->splits_done;
         int pair_used = ctl->pair_used;
         // the split a leaf takes: with the PAIR candidates while the tree's pair budget lasts
         // (tree.cpp:214-218, re-scored after every pair split, tree.cpp:393-396)
         auto pairs_on = [&]() { return X.pair_on && pair_used < X.max_pair; };
-        auto stage_all = [&]() {
+        auto stage_all = [&](int t, int step) {
             const bool pr = pairs_on();
-            for (int k = lane; k < nn; k += 32) {
+            for (int k = t; k < nn; k += step) {
                 const DevSplit S = pr ? X.splits_pair[k] : splits[k];
                 s_nc[k] = candidate(p, nodes[k], S) ? 1 : 0;
                 s_ng[k] = S.gain;
@@ -304,7 +305,6 @@ __global__ void __launch_bounds__(32)
                     }
                 }
             }
-            __syncwarp();
         };
         // the node-table writes of the pending commits (children ids nn_first + 2i, + 1 for
         // the i-th), issued in parallel; `pr`: the pair state they were committed under
@@ -340,7 +340,10 @@ __global__ void __launch_bounds__(32)
             n_commit = 0;
             nn_first = nn;
         };
-        stage_all();
+        stage_all(static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x));
+        __syncthreads();
+        if (threadIdx.x >= 32) return;  // warp 0 selects
+        if (lane == 0) ctl->waves += 1;
         bool finished = false;
         while (true) {
             if (done_splits >= budget || runaway) {
@@ -405,7 +408,8 @@ __global__ void __launch_bounds__(32)
             if (pr_before != pairs_on()) {
                 // the budget ran out: write the commits so far, then axis splits from here
                 flush(pr_before);
-                stage_all();
+                stage_all(lane, 32);
+                __syncwarp();
             }
         }
         flush(pairs_on());
@@ -509,7 +513,7 @@ __global__ void __launch_bounds__(32)
         }
     }
     // launch-loop condition: any context still growing (the last context to finish sets it)
-    if (lane == 0) {
+    if (threadIdx.x == 0) {
         if (active) atomicOr(&gsync[0], 1);
         __threadfence();
         const int t = atomicAdd(&gsync[1], 1);
@@ -751,7 +755,8 @@ void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys
 
 void launch_wave_select(const WaveCtx* ctxs, int n_ctx, int* gsync, unsigned* host_flag, unsigned long long cond,
                         int use_cond, cudaStream_t s) {
-    launch_pdl(wave_select_kernel, dim3(n_ctx), dim3(32), 0, s, "wave_select launch", ctxs, n_ctx, gsync, host_flag,
+    launch_pdl(wave_select_kernel, dim3(n_ctx), dim3(kSelectThreads), 0, s, "wave_select launch", ctxs, n_ctx, gsync,
+               host_flag,
                static_cast<cudaGraphConditionalHandle>(cond), use_cond);
 }
 
