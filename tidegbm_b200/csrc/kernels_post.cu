@@ -81,20 +81,10 @@ constexpr int kApplyRows = 8;  // rows a thread walks together
 // the kApplyRows rows of a thread issue their column-major code loads together, and lanes
 // at nodes with the same split feature share a sector.
 constexpr int kStageRows = 512;
-constexpr int kStagePitch = kStageRows + 16;  // a tile run starts up to 15 bytes early (16-byte copies)
+constexpr int kStagePitch = kStageRows + 16;  // a tile run starts up to 15 bytes early (16-byte loads)
 constexpr int kMaxStaged = 64;
 constexpr int kMaxColWords = 256;
-constexpr size_t kStageBytes = static_cast<size_t>(kMaxStaged) * kStagePitch;
-constexpr size_t kApplySmem = 2 * kStageBytes;  // double-buffered: the next tile streams in during the walk
-
-// 16-byte asynchronous global -> shared copy (completion per thread through commit groups).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(smem))),
-                 "l"(gmem)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+constexpr size_t kApplySmem = static_cast<size_t>(kMaxStaged) * kStagePitch;
 
 // kKinds: bit 0 the tree may hold categorical splits, bit 1 pair splits; a tree of axis
 // splits only keeps neither the masks nor the second features in shared memory.
@@ -187,41 +177,29 @@ __global__ void __launch_bounds__(kApplyThreads)
     const double gs = sc->gscale, hs = sc->hscale;
     if (staged) {
         const int nu = s_nu;
-        // tile [t0, t0 + kStageRows) of every staged column into buffer `buf` (16-byte copies
-        // of the 16-aligned run covering it)
-        auto issue = [&](int t0, int buf) {
+        for (int t0 = ch.y; t0 < ch.z; t0 += kStageRows) {
             const int t1 = min(ch.z, t0 + kStageRows);
             const int a0 = t0 & ~15;
             const int n16 = (t1 - a0 + 15) >> 4;
-            uint8_t* dst = s_tile + buf * kStageBytes;
+            __syncthreads();  // the previous tile's walks are done
             for (int idx = threadIdx.x; idx < nu * n16; idx += blockDim.x) {
                 const int u = idx / n16, v = idx - u * n16;
-                cp_async16(dst + u * kStagePitch + v * 16, col + static_cast<long long>(s_uf[u]) * pitch + a0 + v * 16);
+                *reinterpret_cast<uint4*>(s_tile + u * kStagePitch + v * 16) = __ldg(
+                    reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0 + v * 16));
             }
-            cp_async_commit();
-        };
-        issue(ch.y, 0);
-        int it = 0;
-        for (int t0 = ch.y; t0 < ch.z; t0 += kStageRows, ++it) {
-            const int t1 = min(ch.z, t0 + kStageRows);
-            const int a0 = t0 & ~15;
-            if (t1 < ch.z) issue(t1, (it + 1) & 1);
-            else cp_async_commit();  // an empty group: every iteration waits on the same count
-            cp_async_wait_prev();    // this thread's copies of the current tile are done
-            __syncthreads();         // and every thread's
-            const uint8_t* tile = s_tile + (it & 1) * kStageBytes;
+            __syncthreads();
             for (int r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
                 const double gv = g[r];
                 const double hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
                 const int off = r - a0;
                 int k = 0;
                 while (!s_leaf[k]) {
-                    const unsigned int b = tile[s_slot[k] * kStagePitch + off];
+                    const unsigned int b = s_tile[s_slot[k] * kStagePitch + off];
                     bool left;
                     if constexpr (kCat || kPair) {
                         unsigned int b2 = 0u;
                         if constexpr (kPair)
-                            if (s_type[k] == 1) b2 = tile[s_slot2[k] * kStagePitch + off];
+                            if (s_type[k] == 1) b2 = s_tile[s_slot2[k] * kStagePitch + off];
                         left = goes_left(s_type[k], s_cat[kCat ? k : 0], s_thr[k], s_ml[k], b, b2, n_bins);
                     } else {
                         left = b == 0u ? s_ml[k] != 0 : static_cast<int>(b) <= s_thr[k];
@@ -233,7 +211,6 @@ __global__ void __launch_bounds__(kApplyThreads)
                 add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
                 atomicAdd(&aC[k], 1u);
             }
-            __syncthreads();  // the walks of this tile are done before its buffer is refilled
         }
     } else {
         for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
