@@ -89,7 +89,7 @@ constexpr size_t kApplySmem = static_cast<size_t>(kMaxStaged) * kStagePitch;
 // kKinds: bit 0 the tree may hold categorical splits, bit 1 pair splits; a tree of axis
 // splits only keeps neither the masks nor the second features in shared memory.
 template <int kKinds>
-__global__ void __launch_bounds__(kApplyThreads)
+__global__ void __launch_bounds__(kApplyThreads, 3)
     apply_accum_kernel(const uint8_t* __restrict__ col, long long pitch, int n_f, const DevNode* __restrict__ nodes,
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
                        const double* __restrict__ h, const int4* __restrict__ chunks,
@@ -99,11 +99,13 @@ __global__ void __launch_bounds__(kApplyThreads)
     extern __shared__ __align__(16) uint8_t s_tile[];  // [kMaxStaged][kStagePitch]
     __shared__ int16_t s_feat[kMaxNodes], s_left[kMaxNodes], s_right[kMaxNodes];
     __shared__ uint8_t s_thr[kMaxNodes], s_ml[kMaxNodes], s_leaf[kMaxNodes], s_type[kMaxNodes];
-    __shared__ uint8_t s_slot[kMaxNodes], s_slot2[kPair ? kMaxNodes : 1];
     __shared__ int16_t s_feat2[kPair ? kMaxNodes : 1];
     __shared__ unsigned long long s_cat[kCat ? kMaxNodes : 1][4];  // left masks of categorical nodes
     __shared__ unsigned int s_bits[kMaxColWords];
     __shared__ int s_wbase[kMaxColWords], s_uf[kMaxStaged], s_nu;
+    // staged walk: a node in one word (left 0-15, right 16-31, threshold 32-39, staged column
+    // 40-47, missing_left 48, is_leaf 49, split type 50-51, second staged column 52-59)
+    __shared__ unsigned long long s_word[kMaxNodes];
     // 64-bit sums as (low, high) 32-bit words: shared atomics stay single 32-bit operations.
     __shared__ unsigned int aGl[kMaxNodes], aGh[kMaxNodes], aHl[kMaxNodes], aHh[kMaxNodes], aC[kMaxNodes];
     const int nn = st->n_nodes;
@@ -164,10 +166,18 @@ __global__ void __launch_bounds__(kApplyThreads)
                 return s_wbase[f >> 5] + __popc(s_bits[f >> 5] & ((1u << (f & 31)) - 1u));
             };
             for (int k = threadIdx.x; k < nn; k += blockDim.x) {
-                if (s_leaf[k]) continue;
-                s_slot[k] = static_cast<uint8_t>(rank(s_feat[k]));
-                if constexpr (kPair)
-                    if (s_type[k] == 1) s_slot2[k] = static_cast<uint8_t>(rank(s_feat2[k]));
+                unsigned long long w = static_cast<unsigned long long>(static_cast<uint16_t>(s_left[k])) |
+                                       static_cast<unsigned long long>(static_cast<uint16_t>(s_right[k])) << 16 |
+                                       static_cast<unsigned long long>(s_thr[k]) << 32 |
+                                       static_cast<unsigned long long>(s_ml[k] & 1) << 48 |
+                                       static_cast<unsigned long long>(s_leaf[k] & 1) << 49 |
+                                       static_cast<unsigned long long>(s_type[k] & 3) << 50;
+                if (!s_leaf[k]) {
+                    w |= static_cast<unsigned long long>(rank(s_feat[k])) << 40;
+                    if constexpr (kPair)
+                        if (s_type[k] == 1) w |= static_cast<unsigned long long>(rank(s_feat2[k])) << 52;
+                }
+                s_word[k] = w;
             }
         }
         __syncthreads();
@@ -182,33 +192,41 @@ __global__ void __launch_bounds__(kApplyThreads)
             const int a0 = t0 & ~15;
             const int n16 = (t1 - a0 + 15) >> 4;
             __syncthreads();  // the previous tile's walks are done
-            for (int idx = threadIdx.x; idx < nu * n16; idx += blockDim.x) {
-                const int u = idx / n16, v = idx - u * n16;
-                *reinterpret_cast<uint4*>(s_tile + u * kStagePitch + v * 16) = __ldg(
-                    reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0 + v * 16));
+            {  // a warp per staged column, a lane per 16 bytes of its run
+                const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+                for (int u = threadIdx.x >> 5; u < nu; u += nw) {
+                    const uint4* src = reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0);
+                    uint4* dst = reinterpret_cast<uint4*>(s_tile + u * kStagePitch);
+                    for (int v = lane; v < n16; v += 32) dst[v] = __ldg(src + v);
+                }
             }
             __syncthreads();
             for (int r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
                 const double gv = g[r];
                 const double hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
-                const int off = r - a0;
+                const uint8_t* trow = s_tile + (r - a0);
                 int k = 0;
-                while (!s_leaf[k]) {
-                    const unsigned int b = s_tile[s_slot[k] * kStagePitch + off];
+                unsigned long long w = s_word[0];
+                while (!((w >> 49) & 1ull)) {
+                    const unsigned int b = trow[((w >> 40) & 0xffu) * kStagePitch];
+                    const unsigned int thr = static_cast<unsigned int>(w >> 32) & 0xffu;
+                    const bool ml = (w >> 48) & 1ull;
                     bool left;
                     if constexpr (kCat || kPair) {
+                        const int type = static_cast<int>(w >> 50) & 3;
                         unsigned int b2 = 0u;
                         if constexpr (kPair)
-                            if (s_type[k] == 1) b2 = s_tile[s_slot2[k] * kStagePitch + off];
-                        left = goes_left(s_type[k], s_cat[kCat ? k : 0], s_thr[k], s_ml[k], b, b2, n_bins);
+                            if (type == 1) b2 = trow[((w >> 52) & 0xffu) * kStagePitch];
+                        left = goes_left(type, s_cat[kCat ? k : 0], static_cast<int>(thr), ml, b, b2, n_bins);
                     } else {
-                        left = b == 0u ? s_ml[k] != 0 : static_cast<int>(b) <= s_thr[k];
+                        left = b == 0u ? ml : b <= thr;
                     }
-                    k = left ? s_left[k] : s_right[k];
+                    k = left ? static_cast<int>(w & 0xffffu) : static_cast<int>((w >> 16) & 0xffffu);
+                    w = s_word[k];
                 }
                 nid[r] = static_cast<int16_t>(k);
                 add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
-                add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
+                if (h != nullptr) add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
                 atomicAdd(&aC[k], 1u);
             }
         }
@@ -258,17 +276,21 @@ __global__ void __launch_bounds__(kApplyThreads)
                 if (r[i] < 0) continue;
                 nid[r[i]] = static_cast<int16_t>(k[i]);
                 add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
-                add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
+                if (h != nullptr)
+                    add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
                 atomicAdd(&aC[k[i]], 1u);
             }
         }
     }
     __syncthreads();
     unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
+    // unit hessians (h == nullptr): every row adds the same fixed-point 1, so H = count x that
+    const unsigned long long h1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hs));
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         if (aC[k] == 0u) continue;
         atomicAdd(out + 3 * k, (static_cast<unsigned long long>(aGh[k]) << 32) | aGl[k]);
-        atomicAdd(out + 3 * k + 1, (static_cast<unsigned long long>(aHh[k]) << 32) | aHl[k]);
+        atomicAdd(out + 3 * k + 1, h != nullptr ? (static_cast<unsigned long long>(aHh[k]) << 32) | aHl[k]
+                                                : static_cast<unsigned long long>(aC[k]) * h1);
         atomicAdd(out + 3 * k + 2, static_cast<unsigned long long>(aC[k]));
     }
 }
