@@ -622,7 +622,8 @@ def run_ours(args) -> None:
            "d2h_bytes_per_step": int(d2h / n_est), "fit_wall_s": e2e_wall, "trees": n_est,
            "breakdown_s": {k: st[k] for k in ("total", "sort", "pre_upload", "bin_fit", "bin_counts", "bin_draws",
                                               "bin_edges", "upload_transform", "alloc", "h2d", "transpose", "prep",
-                                              "driver", "trees", "finish_sync", "download", "host_rng",
+                                              "driver", "trees", "driver_free", "finish_sync", "download", "release",
+                                              "host_rng",
                                               "goss_producer", "goss_refits")},
            "cold_first_fit": {"trees": 2, "wall_s": cold_wall,
                               "note": "first full-size fit of the process (warm-up): first-touch device allocations",

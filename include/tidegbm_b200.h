@@ -126,7 +126,8 @@ TGB_API int tgb_fit_stats(tgb_booster* b, double* out18);
  * runs 3 + 5 x (selects - 1) kernels in its waves), "graph_used" (1 when the waves ran as
  * a CUDA graph), "hist_cluster" / "hist_clusters" (the tuned launch shape of the
  * histogram: CTAs per cluster, clusters launched), "driver" (set-up of the batched
- * growth), "finish_sync" (from the tree loop's end to the GOSS sampler's stop),
+ * growth), "driver_free" (its release after the tree loop), "finish_sync" (from the tree
+ * loop's end to the GOSS sampler's stop), "release" (the fit's buffers back to the pool),
  * "expansions" (leaves whose children were histogrammed, over all trees; a tree commits
  * max_leaves - 1 of them at most, the rest were speculative).  Unknown names return -1. */
 TGB_API int tgb_fit_stat(tgb_booster* b, const char* key, double* out);

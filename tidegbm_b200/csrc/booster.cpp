@@ -943,8 +943,10 @@ bool FitRun::finish() {
     D.trees_flat = 0;
     // The fit's working buffers go back to the pool (ordered on the stream); a fitted model
     // keeps only its host-side trees and edges, and predict allocates what it needs.
+    const double trl = now();
     rows_counter.release();
     D.release_fit_buffers();
+    st.t_release = now() - trl;
     st.gpu_launches = static_cast<int>(g_kernel_launches.load() - launches0);
     st.t_total = now() - t0;
     return overflow != 0;
@@ -1290,6 +1292,9 @@ void fit_runs(std::vector<FitRun*>& runs, cudaStream_t s) {
         cudaEventDestroy(ev_begin);
         cudaEventDestroy(ev_end);
     }
+    const double tdf = now();
+    drv.reset();  // the tree graph, the mapped loop flag and the contexts
+    for (auto* r : runs) r->st.t_driver_free = now() - tdf;
 }
 
 void GpuBooster::fit(const void* X_in, int x_dtype, const double* y_in, int n, int n_f, const int64_t* ts_in,

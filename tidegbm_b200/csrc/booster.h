@@ -108,6 +108,8 @@ struct FitStats {
     double t_rng = 0;
     double t_alloc = 0, t_h2d = 0, t_transpose = 0, t_producer = 0;
     double t_driver = 0, t_finish_sync = 0;  // wave driver set-up; tree loop's tail to the sampler's stop
+    double t_driver_free = 0;                // wave driver release after the tree loop
+    double t_release = 0;                    // the fit's working buffers back to the pool
     long long expansions = 0;                // leaves expanded (children histogrammed) over the fit's trees
     double t_bin_counts = 0, t_bin_draws = 0, t_bin_edges = 0;  // stages of the device binner
     int goss_refits = 0;  // 1 when the fit was repeated with the 64-bit GOSS sort

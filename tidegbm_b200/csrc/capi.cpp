@@ -439,6 +439,8 @@ int tgb_fit_stat(tgb_booster* hb, const char* key, double* out) {
         else if (k == "driver") *out = s.t_driver;
         else if (k == "expansions") *out = static_cast<double>(s.expansions);
         else if (k == "finish_sync") *out = s.t_finish_sync;
+        else if (k == "driver_free") *out = s.t_driver_free;
+        else if (k == "release") *out = s.t_release;
         else if (k == "pre_upload") *out = s.t_pre_upload;
         else if (k == "prep") *out = s.t_prep;
         else throw tgb::TideError("unknown fit stat: " + k);

@@ -279,7 +279,7 @@ class Booster:
                 "transpose", "goss_producer"]
         res = dict(zip(keys, o.tolist()))
         for k in ("bin_counts", "bin_draws", "bin_edges", "goss_refits", "pre_upload", "prep", "timed_selects",
-                  "graph_used", "hist_cluster", "hist_clusters", "driver", "finish_sync", "expansions"):
+                  "graph_used", "hist_cluster", "hist_clusters", "driver", "finish_sync", "driver_free", "release", "expansions"):
             v = C.c_double()
             check(lib().tgb_fit_stat(self._h, k.encode(), C.byref(v)))
             res[k] = v.value
