@@ -309,8 +309,11 @@ int binner_fit_from_plan(const BinPlan& plan, const void* Xd, int x_dtype, int n
         launch_keep_bits(keep_d, bin_sample, n_f, take_d, bits, words, s);
     }
     int* fill = scratch.get<int>(n_f);
-    check(cudaMemsetAsync(fill, 0, sizeof(int) * n_f, s), "fill reset");
-    launch_sample_gather(Xd, x_dtype, n, n_f, base_d, bits, words, take_d, smp_a, cap, fill, s);
+    long long* m_d = scratch.get<long long>(n_f);
+    check(cudaMemcpyAsync(m_d, plan.m.data(), sizeof(long long) * n_f, cudaMemcpyHostToDevice, s), "totals upload");
+    int* kc_d = scratch.get<int>(nc);
+    int* kbase_d = scratch.get<int>(nc);
+    launch_sample_gather(Xd, x_dtype, n, n_f, base_d, m_d, bits, words, take_d, smp_a, cap, kc_d, kbase_d, fill, s);
     std::vector<int> seg(2 * static_cast<size_t>(n_f));
     for (int f = 0; f < n_f; ++f) {
         seg[f] = static_cast<int>(f * cap);

@@ -960,6 +960,38 @@ bool FitRun::finish() {
 // node repeats the wave body while select leaves the loop condition at 1, so a tree costs
 // one graph launch and no host round trip.  Without it the host enqueues waves ahead of
 // the device and stops two waves after a mapped flag says every tree is done.
+// Mapped host flags of the host-driven wave loop, kept for the process: allocating and
+// freeing mapped pinned memory can take tens to hundreds of milliseconds, which every fit
+// would otherwise pay.  Portable, so any device may use a flag.
+struct WaveFlagPool {
+    std::mutex mu;
+    std::vector<unsigned*> free;
+};
+WaveFlagPool& wave_flag_pool() {
+    static WaveFlagPool* p = new WaveFlagPool();  // outlives every booster (never destroyed)
+    return *p;
+}
+unsigned* take_wave_flag() {
+    WaveFlagPool& p = wave_flag_pool();
+    {
+        std::lock_guard<std::mutex> lk(p.mu);
+        if (!p.free.empty()) {
+            unsigned* f = p.free.back();
+            p.free.pop_back();
+            return f;
+        }
+    }
+    unsigned* f = nullptr;
+    check(cudaHostAlloc(reinterpret_cast<void**>(&f), sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable),
+          "cudaHostAlloc (wave flag)");
+    return f;
+}
+void give_wave_flag(unsigned* f) {
+    WaveFlagPool& p = wave_flag_pool();
+    std::lock_guard<std::mutex> lk(p.mu);
+    p.free.push_back(f);
+}
+
 class WaveDriver {
 public:
     WaveDriver(std::vector<FitRun*> runs, cudaStream_t s, bool use_graph, bool tune, unsigned long long* rows_counter)
@@ -986,10 +1018,6 @@ public:
         check(cudaMemcpyAsync(ctx_.p, h.data(), sizeof(WaveCtx) * n_ctx_, cudaMemcpyHostToDevice, s_), "contexts");
         gsync_.alloc(3, s_);
         check(cudaMemsetAsync(gsync_.p, 0, 3 * sizeof(int), s_), "gsync reset");
-        check(cudaHostAlloc(reinterpret_cast<void**>(&hflag_), sizeof(unsigned), cudaHostAllocMapped),
-              "cudaHostAlloc (wave flag)");
-        check(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dflag_), hflag_, 0), "wave flag pointer");
-        *hflag_ = 1u;
         part_grid_ = 148 * 8;
         scan_ys_ = std::min(64, std::max(2, 2 * max_leaves_ * n_ctx_ / 4));
     }
@@ -997,9 +1025,9 @@ public:
     const HistTune& tune() const { return tune_; }
 
     // Launch shape of the histogram, tuned once per (device, payload mode, contexts, feature
-    // count, rows bucket) in the process: every candidate (1, 2 or 4 CTAs per cluster x 1, 2
-    // or 4 units per cluster) builds the first tree's root histograms, timed with CUDA
-    // events (a warm-up run, then the better of two), and the fastest is kept.  The root
+    // count, rows bucket) in the process: every candidate (1, 2 or 4 CTAs per cluster)
+    // builds the first tree's root histograms, timed with CUDA events (a warm-up run, then
+    // the better of two), and the fastest is kept.  The root
     // slots are cleared before each run and after the last, so the tree starts afresh.
     void autotune() {
         int dev = 0;
@@ -1085,7 +1113,7 @@ public:
     ~WaveDriver() {
         if (exec_) cudaGraphExecDestroy(exec_);
         if (graph_) cudaGraphDestroy(graph_);
-        if (hflag_) cudaFreeHost(hflag_);
+        if (hflag_) give_wave_flag(hflag_);
         for (auto& e : ev_) cudaEventDestroy(e);
     }
 
@@ -1107,6 +1135,11 @@ public:
                 *hist_used += 2;
             }
         };
+        if (hflag_ == nullptr) {  // the loop flag of the host-driven waves (mapped host memory)
+            hflag_ = take_wave_flag();
+            check(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dflag_), hflag_, 0), "wave flag pointer");
+            *reinterpret_cast<volatile unsigned*>(hflag_) = 1u;
+        }
         hist(0);
         launch_wave_scan(ctx_.p, n_ctx_, 0, max_f_, scan_ys_, cat_, s_);
         if (pair_) launch_wave_pair(ctx_.p, n_ctx_, 0, s_);

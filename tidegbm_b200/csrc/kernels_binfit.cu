@@ -13,7 +13,11 @@
 //                           the head of the exact shuffle prefix (sampling.h)
 //   shuffle_tail_kernel     the shuffle's remaining draws (kernels_shuffle.cu)
 //   keep_bits_kernel        kept ranks -> one bit per non-NaN rank and feature
-//   sample_gather_kernel    X once more; each kept value is appended to its feature
+//   kept_counts_kernel      kept values per (chunk, feature): a popcount of the chunk's
+//                           rank range of the feature's kept bits
+//   kept_scan_kernel        their exclusive prefix over the chunks of each feature
+//   sample_gather_kernel    X once more; each kept value goes to its feature's sample at
+//                           its chunk's prefix plus its rank among the chunk's kept values
 //   CUB segmented sort      every feature's sample ascending
 //   quantile_edges_kernel   unique values, then the interpolated edges in the
 //                           reference's FP64 statement order (this file is compiled
@@ -73,11 +77,73 @@ __global__ void keep_bits_kernel(const int32_t* __restrict__ keep, int bin_sampl
     }
 }
 
+// One warp per (chunk, feature): the kept values among the feature's non-NaN ranks
+// [base[c][f], base[c + 1][f]) (the last chunk ends at the feature's total m[f]).
+__global__ void kept_counts_kernel(const long long* __restrict__ base, const long long* __restrict__ m, int n_chunks,
+                                   int n_f, const uint32_t* __restrict__ bits, long long words,
+                                   const uint8_t* __restrict__ take_all, int* __restrict__ kc) {
+    const int lane = threadIdx.x & 31;
+    const long long n_pairs = static_cast<long long>(n_chunks) * n_f;
+    for (long long pr = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5; pr < n_pairs;
+         pr += (static_cast<long long>(gridDim.x) * blockDim.x) >> 5) {
+        const int c = static_cast<int>(pr / n_f), f = static_cast<int>(pr - static_cast<long long>(c) * n_f);
+        const long long lo = base[pr];
+        const long long hi = c + 1 < n_chunks ? base[pr + n_f] : m[f];
+        int cnt = 0;
+        if (take_all[f]) {
+            cnt = static_cast<int>(hi - lo);
+        } else if (hi > lo) {
+            const uint32_t* fb = bits + f * words;
+            for (long long w = (lo >> 5) + lane; w <= ((hi - 1) >> 5); w += 32) {
+                uint32_t v = fb[w];
+                const long long b0 = w << 5;
+                if (b0 < lo) v &= ~0u << (lo - b0);                       // drop ranks below lo
+                if (b0 + 32 > hi) v &= (hi - b0 >= 32) ? ~0u : ((1u << (hi - b0)) - 1u);  // and from hi on
+                cnt += __popc(v);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        if (lane == 0) kc[pr] = cnt;
+    }
+}
+
+// One CTA per feature: kbase[c][f] = sum of kc[c'][f] over c' < c; total[f] = the sum.
+__global__ void __launch_bounds__(256) kept_scan_kernel(const int* __restrict__ kc, int n_chunks, int n_f,
+                                                       int* __restrict__ kbase, int* __restrict__ total) {
+    const int f = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int s_w[8];
+    int run = 0;
+    for (int c0 = 0; c0 < n_chunks; c0 += 256) {
+        const int c = c0 + static_cast<int>(threadIdx.x);
+        const int v = c < n_chunks ? kc[static_cast<size_t>(c) * n_f + f] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        int wb = 0, all = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k < warp) wb += s_w[k];
+            all += s_w[k];
+        }
+        if (c < n_chunks) kbase[static_cast<size_t>(c) * n_f + f] = run + wb + incl - v;
+        run += all;
+        __syncthreads();  // s_w reuse
+    }
+    if (threadIdx.x == 0) total[f] = run;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kWalkThreads)
     sample_gather_kernel(const T* __restrict__ X, int n, int n_f, const long long* __restrict__ base,
                          const uint32_t* __restrict__ bits, long long words, const uint8_t* __restrict__ take_all,
-                         T* __restrict__ sample, long long cap, int* __restrict__ fill) {
+                         T* __restrict__ sample, long long cap, const int* __restrict__ kbase) {
     const int f = blockIdx.y * kWalkThreads + threadIdx.x;
     if (f >= n_f) return;
     const int r0 = blockIdx.x * kFitChunk;
@@ -86,12 +152,12 @@ __global__ void __launch_bounds__(kWalkThreads)
     long long rank = base[static_cast<size_t>(blockIdx.x) * n_f + f];
     const bool all = take_all[f] != 0;
     const uint32_t* fb = bits + f * words;
-    T* out = sample + f * cap;
-    int* fl = fill + f;
+    T* out = sample + f * cap + kbase[static_cast<size_t>(blockIdx.x) * n_f + f];
+    int k_out = 0;
     auto visit = [&](T v) {
         if (!not_nan(v)) return;
         const bool kept = all || ((fb[rank >> 5] >> (rank & 31)) & 1u);
-        if (kept) out[atomicAdd(fl, 1)] = v;
+        if (kept) out[k_out++] = v;
         ++rank;
     };
     int r = r0;
@@ -203,9 +269,9 @@ void launch_walk_count(const T* X, int n, int n_f, int* counts, cudaStream_t s) 
 
 template <typename T>
 void launch_walk_gather(const T* X, int n, int n_f, const long long* base, const uint32_t* bits, long long words,
-                        const uint8_t* take_all, T* sample, long long cap, int* fill, cudaStream_t s) {
+                        const uint8_t* take_all, T* sample, long long cap, const int* kbase, cudaStream_t s) {
     dim3 grid((n + kFitChunk - 1) / kFitChunk, (n_f + kWalkThreads - 1) / kWalkThreads);
-    sample_gather_kernel<T><<<grid, kWalkThreads, 0, s>>>(X, n, n_f, base, bits, words, take_all, sample, cap, fill);
+    sample_gather_kernel<T><<<grid, kWalkThreads, 0, s>>>(X, n, n_f, base, bits, words, take_all, sample, cap, kbase);
     check(cudaGetLastError(), "sample_gather launch");
 }
 
@@ -236,16 +302,23 @@ void launch_keep_bits(const int32_t* keep, int bin_sample, int n_f, const uint8_
     check(cudaGetLastError(), "keep_bits launch");
 }
 
-void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const uint32_t* bits,
-                          long long words, const uint8_t* take_all, void* sample, long long cap, int* fill,
-                          cudaStream_t s) {
+void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const long long* m,
+                          const uint32_t* bits, long long words, const uint8_t* take_all, void* sample, long long cap,
+                          int* kc, int* kbase, int* total, cudaStream_t s) {
     if (n <= 0 || n_f <= 0) return;
+    const int n_chunks = (n + kFitChunk - 1) / kFitChunk;
+    const long long pairs = static_cast<long long>(n_chunks) * n_f;
+    const int blocks = static_cast<int>(std::min<long long>(148 * 16, (pairs * 32 + 255) / 256));
+    kept_counts_kernel<<<blocks, 256, 0, s>>>(base, m, n_chunks, n_f, bits, words, take_all, kc);
+    check(cudaGetLastError(), "kept_counts launch");
+    kept_scan_kernel<<<n_f, 256, 0, s>>>(kc, n_chunks, n_f, kbase, total);
+    check(cudaGetLastError(), "kept_scan launch");
     if (x_dtype == 0)
         launch_walk_gather(static_cast<const float*>(X), n, n_f, base, bits, words, take_all,
-                           static_cast<float*>(sample), cap, fill, s);
+                           static_cast<float*>(sample), cap, kbase, s);
     else
         launch_walk_gather(static_cast<const double*>(X), n, n_f, base, bits, words, take_all,
-                           static_cast<double*>(sample), cap, fill, s);
+                           static_cast<double*>(sample), cap, kbase, s);
 }
 
 size_t sample_sort_bytes(int x_dtype, long long total, int n_f) {

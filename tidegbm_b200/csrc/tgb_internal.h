@@ -228,9 +228,10 @@ void launch_keep_bits(const int32_t* keep, int bin_sample, int n_f, const uint8_
 // range runs past its refill limit.
 void launch_shuffle_prefix(const uint32_t* seeds, const long long* ms, int n_ranges, int keep, int32_t* out,
                            int32_t* head, int32_t* cnt, int32_t* items, int* err, cudaStream_t s);
-void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const uint32_t* bits,
-                          long long words, const uint8_t* take_all, void* sample, long long cap, int* fill,
-                          cudaStream_t s);
+// kc, kbase: scratch of (chunks x n_f) ints; total[f]: the values gathered for feature f.
+void launch_sample_gather(const void* X, int x_dtype, int n, int n_f, const long long* base, const long long* m,
+                          const uint32_t* bits, long long words, const uint8_t* take_all, void* sample, long long cap,
+                          int* kc, int* kbase, int* total, cudaStream_t s);
 size_t sample_sort_bytes(int x_dtype, long long total, int n_f);
 void launch_sample_sort(int x_dtype, const void* in, void* out, long long total, int n_f, const int* seg_begin,
                         const int* seg_end, void* tmp, size_t tmp_bytes, cudaStream_t s);
