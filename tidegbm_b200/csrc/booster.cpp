@@ -253,6 +253,7 @@ struct FitRun {
     int n = 0, n_f = 0, stride = 0, T = 0, max_nodes = 0, nbk = 1;
     int n_threads = 1;
     bool use_goss = false, const_h = true, any_cat = false;
+    bool g_ready = false;  // the previous tree's sweep wrote this tree's mse gradient
     int n_top = 0, n_other = 0;
     double goss_scale = 1.0;
     std::unique_ptr<GossSampler> sampler;
@@ -765,7 +766,8 @@ WaveCtx FitRun::wave_ctx() const {
 void FitRun::tree_begin(int t) {
     const bool wave = c.grow != 0;
     if (const_h) {
-        launch_grad_mse_fused(D.y.p, D.pred.p, n, D.g.p, D.all_scale.p, s);
+        if (!g_ready) launch_grad_mse_fused(D.y.p, D.pred.p, n, D.g.p, D.all_scale.p, s);
+        g_ready = false;
         launch_all_scale_finalize(D.all_scale.p, n, s);
     } else {
         launch_grad_pairwise(D.y.p, D.pred.p, D.run_start.p, D.run_len.p, order_d, n_runs, n, D.g.p, D.h.p, s);
@@ -864,7 +866,10 @@ void FitRun::tree_end(int t) {
     launch_finalize_tree(pp, D.st.p, D.seg_sums.p, D.bucket_seg_end.p, D.cuts.p, D.all_scale.p, values_t, cover_t,
                          prefix_t, s);
     if (const_h) {
-        launch_pred_update_loss(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, D.y.p, D.loss_part.p, 2368, s);
+        // the next tree's gradient from the same pass (not after the last tree)
+        g_ready = t + 1 < T;
+        launch_pred_update_loss(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, D.y.p, D.loss_part.p, 2368,
+                                g_ready ? D.g.p : nullptr, g_ready ? D.all_scale.p : nullptr, s);
         launch_loss_finalize(0, D.loss_part.p, nullptr, 2368, n, D.losses.p + t, s);
     } else {
         launch_pred_update(pp, D.nid.p, prefix_t, D.st.p, D.pred.p, s);

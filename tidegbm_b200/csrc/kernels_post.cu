@@ -358,13 +358,17 @@ __global__ void pred_update_kernel(PostParams pp, const int16_t* __restrict__ ni
 
 // pred update fused with the MSE training loss on the updated predictions
 // (booster.cpp:655-664 then 704-706): per-block partial sums of (pred - y)^2.
+// g != nullptr: also the next tree's mse gradient g = 1 * (pred - y) (objective.cpp:105-118,
+// the same double the gradient kernel computes) and its largest |g| into sc (reset by the
+// caller), so that the next tree needs no separate pass over pred and y.
 __global__ void pred_update_loss_kernel(PostParams pp, const int16_t* __restrict__ nid,
                                         const double* __restrict__ prefix, const DevTreeState* __restrict__ st,
                                         double* __restrict__ pred, const double* __restrict__ y,
-                                        double* __restrict__ partials) {
+                                        double* __restrict__ partials, double* __restrict__ g,
+                                        AllScale* __restrict__ sc) {
     const int nn = st->n_nodes;
     const int n = pp.n;
-    double acc = 0.0;
+    double acc = 0.0, mg = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int b = 0;
         if (!pp.iid_mode) {
@@ -375,6 +379,19 @@ __global__ void pred_update_loss_kernel(PostParams pp, const int16_t* __restrict
         pred[i] = p;
         const double d = p - y[i];
         acc += 1.0 * d * d;
+        if (g != nullptr) {
+            const double gv = 1.0 * d;
+            g[i] = gv;
+            mg = fmax(mg, fabs(gv));
+        }
+    }
+    if (g != nullptr) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mg = fmax(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+        if ((threadIdx.x & 31) == 0)
+            atomicMax(&sc->maxg_bits, static_cast<unsigned long long>(__double_as_longlong(mg)));
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            atomicMax(&sc->maxh_bits, static_cast<unsigned long long>(__double_as_longlong(1.0)));
     }
     __shared__ double ws[32];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -449,8 +466,10 @@ void launch_predict_trees(const uint8_t* codes, int stride, int n, const int16_t
 }
 
 void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
-                             double* pred, const double* y, double* partials, int n_part, cudaStream_t s) {
-    pred_update_loss_kernel<<<n_part, 256, 0, s>>>(pp, nid, prefix, st, pred, y, partials);
+                             double* pred, const double* y, double* partials, int n_part, double* g, AllScale* sc,
+                             cudaStream_t s) {
+    if (g != nullptr) check(cudaMemsetAsync(sc, 0, 2 * sizeof(unsigned long long), s), "all scale reset");
+    pred_update_loss_kernel<<<n_part, 256, 0, s>>>(pp, nid, prefix, st, pred, y, partials, g, sc);
     check(cudaGetLastError(), "pred_update_loss launch");
 }
 

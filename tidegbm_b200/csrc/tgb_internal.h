@@ -328,8 +328,10 @@ void launch_goss_select(const double* g, const double* h, int n, int n_top, int 
 void launch_all_scale(const double* g, const double* h, int n, AllScale* sc, cudaStream_t s);
 void launch_all_scale_finalize(AllScale* sc, int n, cudaStream_t s);
 // pred += lr * prefix[bucket][leaf] and per-block sums of (pred - y)^2 into partials[n_part].
+// g, sc (mse only, may be null): the next tree's gradient and its maxima from the same pass.
 void launch_pred_update_loss(const PostParams& pp, const int16_t* nid, const double* prefix, const DevTreeState* st,
-                             double* pred, const double* y, double* partials, int n_part, cudaStream_t s);
+                             double* pred, const double* y, double* partials, int n_part, double* g, AllScale* sc,
+                             cudaStream_t s);
 // col: column-major codes (col[f * pitch + r], launch_codes_transpose)
 void launch_apply_accum(const uint8_t* col, long long pitch, int n_f, const DevNode* nodes, const DevTreeState* st,
                         const double* g, const double* h, const int4* chunks, int n_chunks, const AllScale* sc,
