@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kApplyThreads, 3)
     apply_accum_kernel(const uint8_t* __restrict__ col, long long pitch, int n_f, const DevNode* __restrict__ nodes,
                        const DevTreeState* __restrict__ st, const double* __restrict__ g,
                        const double* __restrict__ h, const int4* __restrict__ chunks,
-                       const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
+                       int n_chunks, const AllScale* __restrict__ sc, int16_t* __restrict__ nid,
                        unsigned long long* __restrict__ seg_sums, int n_bins) {
     constexpr bool kCat = (kKinds & 1) != 0, kPair = (kKinds & 2) != 0;
     extern __shared__ __align__(16) uint8_t s_tile[];  // [kMaxStaged][kStagePitch]
@@ -183,115 +183,120 @@ __global__ void __launch_bounds__(kApplyThreads, 3)
         __syncthreads();
     }
     const bool staged = can_stage && s_nu <= kMaxStaged;
-    const int4 ch = chunks[blockIdx.x];  // {segment, row start, row end, unused}
     const double gs = sc->gscale, hs = sc->hscale;
-    if (staged) {
-        const int nu = s_nu;
-        for (int t0 = ch.y; t0 < ch.z; t0 += kStageRows) {
-            const int t1 = min(ch.z, t0 + kStageRows);
-            const int a0 = t0 & ~15;
-            const int n16 = (t1 - a0 + 15) >> 4;
-            __syncthreads();  // the previous tile's walks are done
-            {  // a warp per staged column, a lane per 16 bytes of its run
-                const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-                for (int u = threadIdx.x >> 5; u < nu; u += nw) {
-                    const uint4* src = reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0);
-                    uint4* dst = reinterpret_cast<uint4*>(s_tile + u * kStagePitch);
-                    for (int v = lane; v < n16; v += 32) dst[v] = __ldg(src + v);
-                }
-            }
-            __syncthreads();
-            for (int r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
-                const double gv = g[r];
-                const double hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
-                const uint8_t* trow = s_tile + (r - a0);
-                int k = 0;
-                unsigned long long w = s_word[0];
-                while (!((w >> 49) & 1ull)) {
-                    const unsigned int b = trow[((w >> 40) & 0xffu) * kStagePitch];
-                    const unsigned int thr = static_cast<unsigned int>(w >> 32) & 0xffu;
-                    const bool ml = (w >> 48) & 1ull;
-                    bool left;
-                    if constexpr (kCat || kPair) {
-                        const int type = static_cast<int>(w >> 50) & 3;
-                        unsigned int b2 = 0u;
-                        if constexpr (kPair)
-                            if (type == 1) b2 = trow[((w >> 52) & 0xffu) * kStagePitch];
-                        left = goes_left(type, s_cat[kCat ? k : 0], static_cast<int>(thr), ml, b, b2, n_bins);
-                    } else {
-                        left = b == 0u ? ml : b <= thr;
-                    }
-                    k = left ? static_cast<int>(w & 0xffffu) : static_cast<int>((w >> 16) & 0xffffu);
-                    w = s_word[k];
-                }
-                nid[r] = static_cast<int16_t>(k);
-                add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
-                if (h != nullptr) add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
-                atomicAdd(&aC[k], 1u);
-            }
-        }
-    } else {
-        for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
-            int r[kApplyRows], k[kApplyRows];
-            double gv[kApplyRows], hv[kApplyRows];
-#pragma unroll
-            for (int i = 0; i < kApplyRows; ++i) {
-                r[i] = base + threadIdx.x + i * kApplyThreads;
-                k[i] = 0;
-                const bool ok = r[i] < ch.z;
-                gv[i] = ok ? g[r[i]] : 0.0;  // loaded before the walk so their latency overlaps it
-                hv[i] = ok && h ? h[r[i]] : 1.0;
-                if (!ok) r[i] = -1;
-            }
-            for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
-                unsigned int b[kApplyRows], b2[kApplyRows];
-                bool any = false;
-#pragma unroll
-                for (int i = 0; i < kApplyRows; ++i) {
-                    const bool walk = r[i] >= 0 && !s_leaf[k[i]];
-                    b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
-                    if constexpr (kPair)
-                        b2[i] = walk && s_type[k[i]] == 1
-                                    ? __ldg(col + static_cast<long long>(s_feat2[k[i]]) * pitch + r[i])
-                                    : 0u;
-                    else
-                        b2[i] = 0u;
-                    any |= walk;
-                }
-                if (!any) break;
-#pragma unroll
-                for (int i = 0; i < kApplyRows; ++i) {
-                    if (r[i] < 0 || s_leaf[k[i]]) continue;
-                    bool left;
-                    if constexpr (kCat || kPair)
-                        left = goes_left(s_type[k[i]], s_cat[kCat ? k[i] : 0], s_thr[k[i]], s_ml[k[i]], b[i], b2[i],
-                                         n_bins);
-                    else
-                        left = b[i] == 0u ? s_ml[k[i]] != 0 : static_cast<int>(b[i]) <= s_thr[k[i]];
-                    k[i] = left ? s_left[k[i]] : s_right[k[i]];
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < kApplyRows; ++i) {
-                if (r[i] < 0) continue;
-                nid[r[i]] = static_cast<int16_t>(k[i]);
-                add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
-                if (h != nullptr)
-                    add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
-                atomicAdd(&aC[k[i]], 1u);
-            }
-        }
-    }
-    __syncthreads();
-    unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
     // unit hessians (h == nullptr): every row adds the same fixed-point 1, so H = count x that
     const unsigned long long h1 = static_cast<unsigned long long>(__double2ll_rn(1.0 * hs));
-    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
-        if (aC[k] == 0u) continue;
-        atomicAdd(out + 3 * k, (static_cast<unsigned long long>(aGh[k]) << 32) | aGl[k]);
-        atomicAdd(out + 3 * k + 1, h != nullptr ? (static_cast<unsigned long long>(aHh[k]) << 32) | aHl[k]
-                                                : static_cast<unsigned long long>(aC[k]) * h1);
-        atomicAdd(out + 3 * k + 2, static_cast<unsigned long long>(aC[k]));
+    // a CTA takes chunks in turn (the node tables above are staged once per CTA)
+    for (int ci = blockIdx.x; ci < n_chunks; ci += gridDim.x) {
+        const int4 ch = chunks[ci];  // {segment, row start, row end, unused}
+        if (staged) {
+            const int nu = s_nu;
+            for (int t0 = ch.y; t0 < ch.z; t0 += kStageRows) {
+                const int t1 = min(ch.z, t0 + kStageRows);
+                const int a0 = t0 & ~15;
+                const int n16 = (t1 - a0 + 15) >> 4;
+                __syncthreads();  // the previous tile's walks are done
+                {  // a warp per staged column, a lane per 16 bytes of its run
+                    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+                    for (int u = threadIdx.x >> 5; u < nu; u += nw) {
+                        const uint4* src = reinterpret_cast<const uint4*>(col + static_cast<long long>(s_uf[u]) * pitch + a0);
+                        uint4* dst = reinterpret_cast<uint4*>(s_tile + u * kStagePitch);
+                        for (int v = lane; v < n16; v += 32) dst[v] = __ldg(src + v);
+                    }
+                }
+                __syncthreads();
+                for (int r = t0 + threadIdx.x; r < t1; r += blockDim.x) {
+                    const double gv = g[r];
+                    const double hv = h ? h[r] : 1.0;  // h == nullptr: unit hessians
+                    const uint8_t* trow = s_tile + (r - a0);
+                    int k = 0;
+                    unsigned long long w = s_word[0];
+                    while (!((w >> 49) & 1ull)) {
+                        const unsigned int b = trow[((w >> 40) & 0xffu) * kStagePitch];
+                        const unsigned int thr = static_cast<unsigned int>(w >> 32) & 0xffu;
+                        const bool ml = (w >> 48) & 1ull;
+                        bool left;
+                        if constexpr (kCat || kPair) {
+                            const int type = static_cast<int>(w >> 50) & 3;
+                            unsigned int b2 = 0u;
+                            if constexpr (kPair)
+                                if (type == 1) b2 = trow[((w >> 52) & 0xffu) * kStagePitch];
+                            left = goes_left(type, s_cat[kCat ? k : 0], static_cast<int>(thr), ml, b, b2, n_bins);
+                        } else {
+                            left = b == 0u ? ml : b <= thr;
+                        }
+                        k = left ? static_cast<int>(w & 0xffffu) : static_cast<int>((w >> 16) & 0xffffu);
+                        w = s_word[k];
+                    }
+                    nid[r] = static_cast<int16_t>(k);
+                    add64s(aGl, aGh, k, static_cast<unsigned long long>(__double2ll_rn(gv * gs)));
+                    if (h != nullptr) add64s(aHl, aHh, k, static_cast<unsigned long long>(__double2ll_rn(hv * hs)));
+                    atomicAdd(&aC[k], 1u);
+                }
+            }
+        } else {
+            for (int base = ch.y; base < ch.z; base += kApplyThreads * kApplyRows) {
+                int r[kApplyRows], k[kApplyRows];
+                double gv[kApplyRows], hv[kApplyRows];
+    #pragma unroll
+                for (int i = 0; i < kApplyRows; ++i) {
+                    r[i] = base + threadIdx.x + i * kApplyThreads;
+                    k[i] = 0;
+                    const bool ok = r[i] < ch.z;
+                    gv[i] = ok ? g[r[i]] : 0.0;  // loaded before the walk so their latency overlaps it
+                    hv[i] = ok && h ? h[r[i]] : 1.0;
+                    if (!ok) r[i] = -1;
+                }
+                for (int level = 0; level < kMaxNodes; ++level) {  // a path has fewer than kMaxNodes nodes
+                    unsigned int b[kApplyRows], b2[kApplyRows];
+                    bool any = false;
+    #pragma unroll
+                    for (int i = 0; i < kApplyRows; ++i) {
+                        const bool walk = r[i] >= 0 && !s_leaf[k[i]];
+                        b[i] = walk ? __ldg(col + static_cast<long long>(s_feat[k[i]]) * pitch + r[i]) : 0u;
+                        if constexpr (kPair)
+                            b2[i] = walk && s_type[k[i]] == 1
+                                        ? __ldg(col + static_cast<long long>(s_feat2[k[i]]) * pitch + r[i])
+                                        : 0u;
+                        else
+                            b2[i] = 0u;
+                        any |= walk;
+                    }
+                    if (!any) break;
+    #pragma unroll
+                    for (int i = 0; i < kApplyRows; ++i) {
+                        if (r[i] < 0 || s_leaf[k[i]]) continue;
+                        bool left;
+                        if constexpr (kCat || kPair)
+                            left = goes_left(s_type[k[i]], s_cat[kCat ? k[i] : 0], s_thr[k[i]], s_ml[k[i]], b[i], b2[i],
+                                             n_bins);
+                        else
+                            left = b[i] == 0u ? s_ml[k[i]] != 0 : static_cast<int>(b[i]) <= s_thr[k[i]];
+                        k[i] = left ? s_left[k[i]] : s_right[k[i]];
+                    }
+                }
+    #pragma unroll
+                for (int i = 0; i < kApplyRows; ++i) {
+                    if (r[i] < 0) continue;
+                    nid[r[i]] = static_cast<int16_t>(k[i]);
+                    add64s(aGl, aGh, k[i], static_cast<unsigned long long>(__double2ll_rn(gv[i] * gs)));
+                    if (h != nullptr)
+                        add64s(aHl, aHh, k[i], static_cast<unsigned long long>(__double2ll_rn(hv[i] * hs)));
+                    atomicAdd(&aC[k[i]], 1u);
+                }
+            }
+        }
+        __syncthreads();
+        unsigned long long* out = seg_sums + static_cast<size_t>(ch.x) * kMaxNodes * 3;
+        for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+            if (aC[k] == 0u) continue;
+            atomicAdd(out + 3 * k, (static_cast<unsigned long long>(aGh[k]) << 32) | aGl[k]);
+            atomicAdd(out + 3 * k + 1, h != nullptr ? (static_cast<unsigned long long>(aHh[k]) << 32) | aHl[k]
+                                                    : static_cast<unsigned long long>(aC[k]) * h1);
+            atomicAdd(out + 3 * k + 2, static_cast<unsigned long long>(aC[k]));
+            aGl[k] = aGh[k] = aHl[k] = aHh[k] = aC[k] = 0u;  // clear for the CTA's next chunk
+        }
+        __syncthreads();
     }
 }
 
@@ -504,8 +509,15 @@ void launch_apply_accum(const uint8_t* col, long long pitch, int n_f, const DevN
             if (dev >= 0 && dev < 64) done[dev][kinds & 3] = true;
         }
     }
-    kern<<<n_chunks, kApplyThreads, kApplySmem, s>>>(col, pitch, n_f, nodes, st, g, h, chunks, sc, nid, seg_sums,
-                                                     n_bins);
+    // a persistent grid: 3 CTAs per SM (its register and shared-memory budget), chunks in turn
+    int sms = 148;
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int grid = std::max(1, std::min(n_chunks, 3 * sms));
+    kern<<<grid, kApplyThreads, kApplySmem, s>>>(col, pitch, n_f, nodes, st, g, h, chunks, n_chunks, sc, nid,
+                                                 seg_sums, n_bins);
     check(cudaGetLastError(), "apply_accum launch");
 }
 
