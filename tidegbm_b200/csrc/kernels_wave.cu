@@ -688,14 +688,16 @@ __global__ void __launch_bounds__(kPartThreads)
     pdl_trigger();
     __shared__ int s_pref[kMaxWaveCtx + 1];
     __shared__ int red[kPartWarps];
+    __shared__ int s_last;
     load_tile_prefix(ctxs, n_ctx, s_pref);
     const int total = s_pref[n_ctx];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const TileRef tr = find_tile(ctxs, s_pref, n_ctx, t);
         const WaveCtx& X = ctxs[tr.c];
-        const int L = X.ctl->exp_leaf[tr.e];
+        WaveCtl* ctl = X.ctl;
+        const int L = ctl->exp_leaf[tr.e];
         const DevNode& N = X.nodes[L];
-        const DevSplit& S = X.ctl->expanded[L] == 2 ? X.splits_pair[L] : X.splits[L];
+        const DevSplit& S = ctl->expanded[L] == 2 ? X.splits_pair[L] : X.splits[L];
         const int32_t* in = (N.buf ? X.rows1 : X.rows0) + N.start;
         const int base = tr.k * kPartTile, end = min(base + kPartTile, N.count);
         int32_t row[kPartPer];
@@ -705,7 +707,47 @@ __global__ void __launch_bounds__(kPartThreads)
 #pragma unroll
         for (int i = 0; i < kPartPer; ++i) cnt += left[i] ? 1 : 0;
         cnt = block_sum(cnt, red);
-        if (threadIdx.x == 0) X.tile_counts[tr.lt] = cnt;
+        const int t0 = ctl->exp_tile0[tr.e], t1 = ctl->exp_tile0[tr.e + 1];
+        if (threadIdx.x == 0) {
+            X.tile_counts[tr.lt] = cnt;
+            __threadfence();
+            s_last = atomicAdd(&ctl->part_ticket[tr.e], 1) == t1 - t0 - 1;
+        }
+        __syncthreads();
+        if (s_last) {
+            // the leaf's last tile: its tiles' counts -> exclusive prefixes (in place), and the
+            // leaf's left total, for the scatter
+            __threadfence();
+            volatile int* tc = X.tile_counts;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            int run = 0;
+            for (int k0 = t0; k0 < t1; k0 += kPartThreads) {
+                const int k = k0 + static_cast<int>(threadIdx.x);
+                const int v = k < t1 ? tc[k] : 0;
+                int incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += u;
+                }
+                if (lane == 31) red[warp] = incl;
+                __syncthreads();
+                int wb = 0, all = 0;
+#pragma unroll
+                for (int w = 0; w < kPartWarps; ++w) {
+                    if (w < warp) wb += red[w];
+                    all += red[w];
+                }
+                if (k < t1) tc[k] = run + wb + incl - v;
+                run += all;
+                __syncthreads();  // red reuse
+            }
+            if (threadIdx.x == 0) {
+                ctl->exp_left[tr.e] = run;
+                ctl->part_ticket[tr.e] = 0;  // ready for the next wave
+            }
+        }
+        __syncthreads();  // s_last reuse
     }
     // Clear the histogram slots of this wave's children (2 per expansion, consecutive):
     // the smaller child's is accumulated into by the histogram launch.
@@ -747,15 +789,8 @@ __global__ void __launch_bounds__(kPartThreads)
         const int L = ctl->exp_leaf[tr.e];
         const DevNode& N = X.nodes[L];
         const DevSplit& S = X.ctl->expanded[L] == 2 ? X.splits_pair[L] : X.splits[L];
-        const int t0 = ctl->exp_tile0[tr.e], t1 = ctl->exp_tile0[tr.e + 1];
-        int tot = 0, before = 0;
-        for (int kk = t0 + threadIdx.x; kk < t1; kk += kPartThreads) {
-            const int v = X.tile_counts[kk];
-            tot += v;
-            if (kk < tr.lt) before += v;
-        }
-        const int n_left = block_sum(tot, red);
-        const int left0 = block_sum(before, red);
+        const int n_left = ctl->exp_left[tr.e];   // the leaf's left rows (count launch)
+        const int left0 = X.tile_counts[tr.lt];  // left rows of the leaf's earlier tiles
         if (tr.k == 0 && threadIdx.x == 0) {
             DevNode& A = X.spec[2 * L];
             DevNode& B = X.spec[2 * L + 1];

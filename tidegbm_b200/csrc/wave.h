@@ -74,6 +74,8 @@ struct WaveCtl {
     int pad[2];
     int exp_leaf[kMaxLeavesCap];
     int exp_tile0[kMaxLeavesCap + 1];
+    int exp_left[kMaxLeavesCap];     // rows of the planned leaf going left (partition count)
+    int part_ticket[kMaxLeavesCap];  // count tiles done per planned leaf (zero between launches)
     int expanded[kMaxNodes];  // 0 not expanded; 1, 2: children planned by the axis, with-pairs split
 };
 
