@@ -776,7 +776,6 @@ __global__ void __launch_bounds__(kPartThreads)
     pdl_wait();
     pdl_trigger();
     __shared__ int s_pref[kMaxWaveCtx + 1];
-    __shared__ int red[kPartWarps];
     __shared__ int wc[kPartPer * kPartWarps];
     load_tile_prefix(ctxs, n_ctx, s_pref);
     const int total = s_pref[n_ctx];
