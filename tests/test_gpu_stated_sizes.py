@@ -14,19 +14,25 @@ from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import pytest
+from missing_bins import empty_missing_nodes
 
 torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
 
-def _compare(gpu, ref, atol=1e-9, n_trees=None):
+def _compare(gpu, ref, codes, n_bins, atol=1e-9, n_trees=None):
+    """Structure and values; missing directions at every split node whose missing bin holds
+    rows (missing_bins.py: an empty missing bin's direction is FP64 residue in the reference)."""
     trees_g = gpu.trees()[:n_trees] if n_trees else gpu.trees()
     trees_r = ref.trees[:n_trees] if n_trees else ref.trees
     assert len(trees_g) == len(trees_r)
     for t, (a, b) in enumerate(zip(trees_g, trees_r)):
-        for fld in ("is_leaf", "feature", "threshold", "left", "right", "missing_left", "n_samples", "depth"):
+        for fld in ("is_leaf", "feature", "threshold", "left", "right", "n_samples", "depth"):
             assert np.array_equal(getattr(a, fld), getattr(b, fld)), (t, fld)
+        differ = set(np.flatnonzero(np.asarray(a.missing_left) != np.asarray(b.missing_left)).tolist())
+        if differ:
+            assert differ <= empty_missing_nodes(b, codes, n_bins), (t, "missing_left", sorted(differ))
         assert np.array_equal(a.cover, b.cover), t
         np.testing.assert_allclose(a.value, b.value, rtol=0, atol=atol)
         np.testing.assert_allclose(a.values, b.values, rtol=0, atol=atol)
@@ -43,8 +49,9 @@ def test_pairwise_2000_dates_matches_oracle(native, oracle):
     gpu = native.Booster(**params)
     gpu.fit(p.X, p.y, timestamps=p.ts, entity=p.entity)
     ref, h = oracle.oracle_fit(params, p.X.astype(np.float64), p.y, p.ts, p.entity)
+    codes, nb = oracle.oracle_codes(p.X, params)
     try:
-        _compare(gpu, ref)
+        _compare(gpu, ref, codes, nb)
         np.testing.assert_allclose(gpu.evals_result()["train"], ref.evals_train, rtol=1e-9, atol=1e-9)
     finally:
         oracle.oracle_free(h)
@@ -97,6 +104,6 @@ def test_scale_10m_codes_and_first_tree_match_oracle(native, oracle):
     # tree 0 against the oracle's fit of one tree (GOSS sample of 3M rows)
     ref, h = oracle.oracle_fit(params, p.X.astype(np.float64), p.y, p.ts, p.entity)
     try:
-        _compare(gpu, ref, n_trees=1)
+        _compare(gpu, ref, codes, ref.n_bins, n_trees=1)
     finally:
         oracle.oracle_free(h)
