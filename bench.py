@@ -792,9 +792,13 @@ def main() -> None:
                     help="serve an N-request trace of the serving workload (p50/p99 latency); 0: skip")
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="0: host-driven waves, every kernel its own launch (for per-kernel launch lists)")
+    ap.add_argument("--hist-stage", type=int, default=1, choices=[0, 1],
+                    help="0: histogram code rows loaded lane by lane instead of staged by TMA gathers")
     args = ap.parse_args()
     if args.graph == 0:
         PARAMS["graph"] = 0
+    if args.hist_stage == 0:
+        PARAMS["hist_stage"] = 0
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -94,6 +94,7 @@ void Config::validate() const {
     if (hist_bits != 0 && hist_bits != 8 && hist_bits != 16)
         throw TideError("hist_bits must be 0 (exact), 16 or 8 (quantised gradients)");
     if (wave_expand < 0) throw TideError("wave_expand must be >= 0 (0: every candidate within the budget)");
+    if (hist_stage != 0 && hist_stage != 1) throw TideError("hist_stage must be 0 (direct loads) or 1 (TMA gathers)");
 }
 
 namespace {
@@ -743,6 +744,7 @@ WaveCtx FitRun::wave_ctx() const {
     w.n_slots = n_slots;
     w.max_tiles = max_tiles;
     w.max_expand = c.wave_expand;
+    w.codes_map_ok = c.hist_stage != 0 && encode_codes_map(&w.codes_map, D.codes.p, n, stride) ? 1 : 0;
     w.is_cat = D.is_cat.p;
     w.cand_cat = D.cand_cat.p;
     w.cat_smooth = c.cat_smooth;
@@ -915,6 +917,7 @@ bool FitRun::finish() {
         check(cudaMemcpyAsync(&exp_total, &D.ctl.p->exp_total, sizeof(int), cudaMemcpyDeviceToHost, s), "expansions");
     check(cudaStreamSynchronize(s), "D2H");
     st.expansions = exp_total;
+    if (wave_error == 3) throw TideError("GPU path: a histogram's TMA staging wait gave up");
     if (wave_error) throw TideError("GPU path: a wave outgrew its histogram slots or partition tiles");
     B.trees.assign(T, HostTree());
     for (int t = 0; t < T; ++t) {

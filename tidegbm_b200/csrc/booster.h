@@ -78,6 +78,9 @@ struct Config {
     // Batched growth: expansions a wave may plan (0: every leaf ranked within the splits
     // left, the widest speculation; k: the k best).  Any value grows the same tree.
     int wave_expand = 0;
+    // Histogram code rows (constant-hessian modes): staged into shared memory by TMA gathers
+    // (1), or loaded by each lane from global memory (0).  Same results either way.
+    int hist_stage = 1;
     // Measurement hooks (no effect on results): CUDA events around trees
     // [timing_from, timing_to) (timing_to < 0: through the last tree), and per-launch
     // events around every histogram kernel in that range.

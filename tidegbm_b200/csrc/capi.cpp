@@ -150,6 +150,7 @@ int tgb_set_int(tgb_booster* hb, const char* key, long long v) {
         else if (k == "graph") c.graph = static_cast<int>(v);
         else if (k == "hist_tune") c.hist_tune = static_cast<int>(v);
         else if (k == "wave_expand") c.wave_expand = static_cast<int>(v);
+        else if (k == "hist_stage") c.hist_stage = static_cast<int>(v);
         else if (k == "cat_min_count") c.cat_min_count = static_cast<int>(v);
         else if (k == "pair_top_k") c.pair_top_k = static_cast<int>(v);
         else if (k == "max_pair_splits_per_tree") c.max_pair_splits_per_tree = static_cast<int>(v);
@@ -638,12 +639,16 @@ int tgb_hist_build_quantized(const unsigned char* codes, int stride, int n_featu
         w.gp.n_features = n_features;
         w.gp.stride = stride;
         w.goss_scale = 1.0;
+        w.codes_map_ok = tgb::encode_codes_map(&w.codes_map, codes, n_max, stride) ? 1 : 0;
         tgb::check(cudaMemcpyAsync(wc.p, &w, sizeof(w), cudaMemcpyHostToDevice, s), "context upload");
         tgb::HistTune tune;
         tune.clusters = tgb::wave_hist_clusters(tune.cluster);
         tgb::launch_wave_hist(mode, wc.p, 1, 0, tune, nullptr, s);
         tgb::check(cudaMemcpyAsync(&sh, st.p, sizeof(sh), cudaMemcpyDeviceToHost, s), "state download");
+        int err = 0;
+        tgb::check(cudaMemcpyAsync(&err, &ctl.p->error, sizeof(int), cudaMemcpyDeviceToHost, s), "error flag");
         tgb::check(cudaStreamSynchronize(s), "quantised histogram");
+        if (err != 0) throw tgb::TideError("GPU path: the histogram's TMA staging wait gave up");
         scales_out[0] = sh.inv_gscale;
         scales_out[1] = sh.inv_hscale;
     });

@@ -31,6 +31,8 @@
 // Partition (split_indices, cpp/src/tree.cpp:68-91): stable, two launches over
 // 2048-row tiles of all planned leaves (count, then scatter with in-tile ballot ranks).
 #include <atomic>
+#include <cstdint>
+#include <cstring>
 #include <cooperative_groups.h>
 
 #include "wave.h"
@@ -298,6 +300,176 @@ __device__ __noinline__ void accumulate_const(unsigned int* __restrict__ P, unsi
     }
 }
 
+// ---- code rows staged by TMA (constant-hessian modes) ---------------------------------
+// A warp owns two 1 KB staging slots (its batch of 32 rows x the group's 32 code bytes)
+// and an mbarrier per slot.  Lanes 0-7 each gather four rows of a batch with one
+// cp.async.bulk.tensor tile::gather4 (box: 32 bytes of one row), two batches ahead of the
+// one the warp accumulates; a lane then reads its row from the slot with two conflict-free
+// 16-byte shared loads.  The direct loads cost 32 scattered sectors per warp and row batch
+// on the L1 data path that the shared reductions also use; the gathers leave it to them.
+constexpr int kSlotBytes = 32 * kFG;                 // one warp's batch
+constexpr int kSlotStride = kWarps * kSlotBytes;     // slot 1 of every warp after slot 0 of all
+constexpr int kStageBytes = 2 * kSlotStride;         // 64 KB, over the 64-bit totals
+constexpr int kSpinLimit = 1 << 18;                  // polls of one mbarrier wait
+constexpr int kErrStaging = 3;                       // ctl->error: a staging wait gave up
+static_assert(kStageBytes + 128 <= kTot * 8, "the staging slots lie inside the G totals");
+
+__device__ __forceinline__ unsigned int smem_u32(const void* p) {
+    return static_cast<unsigned int>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned int bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned int bar, unsigned int bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Polls phase `parity` of the barrier at most kSpinLimit times; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned int bar, unsigned int parity) {
+    for (int it = 0; it < kSpinLimit; ++it) {
+        unsigned int done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// Rows y0..y3, bytes [x, x + 32) of each, to dst (4 x 32 bytes), completing on bar.
+__device__ __forceinline__ void tma_gather4(unsigned int dst, const CUtensorMap* map, int x, int y0, int y1, int y2,
+                                            int y3, unsigned int bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3), "r"(bar)
+        : "memory");
+}
+
+// accumulate_const with the code rows staged by TMA.  The 64-bit G totals are kept in
+// registers (a thread owns the same cells as in the fold) and written to Gt at the end: the
+// staging slots lie over Gt meanwhile; the counts fold into Ct as before.  `phase` holds the
+// parity of each of the warp's two barriers across calls; returned updated.  A wait that
+// gives up sets ctl->error and ends the staging for the rest of the call (no new gathers,
+// no further waits but one bounded wait per gather still in flight).
+template <int kMode>
+__device__ __noinline__ unsigned int accumulate_const_tma(unsigned int* __restrict__ P,
+                                                          unsigned long long* __restrict__ Gt,
+                                                          unsigned int* __restrict__ Ct, unsigned char* stage,
+                                                          unsigned long long* bars, unsigned int phase,
+                                                          const int32_t* __restrict__ rows, int r0, int r1,
+                                                          const CUtensorMap* map, int fg0,
+                                                          const void* __restrict__ gqp, int* err) {
+    using T = ModeTraits<kMode>;
+    using PT = typename ConstPayload<kMode>::type;
+    constexpr int kStep = kWarps * 32;
+    constexpr int kFoldRounds = T::sub / kStep;
+    static_assert(T::sub % kStep == 0, "a sub-chunk is whole rounds of the CTA");
+    const PT* __restrict__ pay = static_cast<const PT*>(gqp);  // by position, like rows
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int q = lane >> 2, sh = (lane & 3) * 8;
+    const unsigned int slot0 = smem_u32(stage) + warp * kSlotBytes;
+    const unsigned int bar0 = smem_u32(bars + 2 * warp);
+    long long accG[kCells];
+#pragma unroll
+    for (int cc = 0; cc < kCells; ++cc) accG[cc] = 0;
+    // the staging area's generic writes (zeroing, the previous piece's totals) before the
+    // gathers' asynchronous ones; the descriptor was written by a host copy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane < 8) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+    __syncthreads();
+    bool ok = true;
+    unsigned int pending = 0u;  // slots with gathers in flight
+    // Gathers batch k of this warp into slot s; returns the lane's payload of it.
+    auto issue = [&](int k, int s) -> PT {
+        const int base = r0 + k * kStep + warp * 32;
+        if (!ok || base >= r1) return PT(0);
+        const int kk = base + lane;
+        const bool v = kk < r1;
+        const int row = rows[v ? kk : base];  // the batch's first row pads a short batch
+        const PT p = v ? pay[kk] : PT(0);
+        const int y0 = __shfl_sync(0xffffffffu, row, (4 * lane) & 31);
+        const int y1 = __shfl_sync(0xffffffffu, row, (4 * lane + 1) & 31);
+        const int y2 = __shfl_sync(0xffffffffu, row, (4 * lane + 2) & 31);
+        const int y3 = __shfl_sync(0xffffffffu, row, (4 * lane + 3) & 31);
+        const unsigned int bar = bar0 + 8u * s;
+        if (lane == 0) mbar_expect_tx(bar, kSlotBytes);
+        __syncwarp();
+        if (lane < 8) tma_gather4(slot0 + s * kSlotStride + lane * 128, map, fg0, y0, y1, y2, y3, bar);
+        pending |= 1u << s;
+        return p;
+    };
+    const int n_rounds = r1 > r0 ? (r1 - r0 + kStep - 1) / kStep : 0;
+    PT p0 = issue(0, 0);
+    PT p1 = issue(1, 1);
+    const int h = (lane >> 2) & 1;  // lanes 4-7 of each 8 read their second half first
+    for (int i = 0; i < n_rounds; ++i) {
+        const int s = i & 1;
+        const int base = r0 + i * kStep + warp * 32;
+        if (base < r1) {
+            if (ok) {
+                ok = __all_sync(0xffffffffu, mbar_wait(bar0 + 8u * s, (phase >> s) & 1u));
+                if (ok) {
+                    phase ^= 1u << s;
+                    pending &= ~(1u << s);
+                } else if (lane == 0) {
+                    atomicExch(err, kErrStaging);
+                }
+            }
+            const unsigned char* rp = stage + s * kSlotStride + warp * kSlotBytes + lane * 32;
+            const uint4 c0 = *reinterpret_cast<const uint4*>(rp + 16 * h);
+            const uint4 c1 = *reinterpret_cast<const uint4*>(rp + 16 * (h ^ 1));
+            const uint4 ca = h ? c1 : c0, cb = h ? c0 : c1;
+            const PT p = s ? p1 : p0;
+            __syncwarp();  // every lane has read the slot before it is refilled
+            const PT pn = issue(i + 2, s);
+            if (s) p1 = pn;
+            else p0 = pn;
+            if (base + lane < r1) add_row_const<kMode>(P, p, ca, cb, lane, q, sh);
+        }
+        if ((i + 1) % kFoldRounds == 0 || i + 1 == n_rounds) {
+            __syncthreads();
+            // fold the sub-chunk: G into registers, counts into Ct; clear the planes
+#pragma unroll
+            for (int cc = 0; cc < kCells; ++cc) {
+                const int cell = threadIdx.x + cc * kThreads;
+                const int ti = (cell & 31) * kTotPitch + (cell >> 5);
+                long long dg;
+                unsigned int dc;
+                if constexpr (kMode == kHistExactConst) {
+                    dg = static_cast<long long>(static_cast<int>(P[kPlane + cell])) * (1ll << kLoBits) + P[cell];
+                    dc = P[2 * kPlane + cell];
+                } else if constexpr (kMode == kHistQ16Const) {
+                    dg = static_cast<int>(P[cell]);
+                    dc = P[kPlane + cell];
+                } else {
+                    const unsigned int w1 = P[cell], w2 = P[kPlane + cell];
+                    const unsigned int n1 = w1 >> 20, n2 = w2 >> 20;
+                    dg = static_cast<long long>(w1 & 0xfffffu) + static_cast<long long>(w2 & 0xfffffu) -
+                         128ll * static_cast<long long>(n1 + n2);
+                    dc = n1 | (n2 << 16);
+                }
+                accG[cc] += dg;
+                Ct[ti] += dc;
+#pragma unroll
+                for (int pl = 0; pl < T::planes; ++pl) P[pl * kPlane + cell] = 0u;
+            }
+            __syncthreads();
+        }
+    }
+    if (!ok)  // warp-uniform
+        for (int s = 0; s < 2; ++s)
+            if (((pending >> s) & 1u) && __all_sync(0xffffffffu, mbar_wait(bar0 + 8u * s, (phase >> s) & 1u)))
+                phase ^= 1u << s;
+    // every warp is past its last slot read (the last round's fold): the totals over them
+#pragma unroll
+    for (int cc = 0; cc < kCells; ++cc) {
+        const int cell = threadIdx.x + cc * kThreads;
+        Gt[(cell & 31) * kTotPitch + (cell >> 5)] = static_cast<unsigned long long>(accG[cc]);
+    }
+    return phase;
+}
+
 // The rows [r0, r1) of a CTA's share of one piece, per-row hessian modes: the same lane-
 // per-row reductions, folded into per-thread 64-bit registers every sub-chunk; the totals
 // are written over the (then clear) working planes at the end.
@@ -423,15 +595,26 @@ __global__ void __launch_bounds__(kThreads, 1)
     wave_hist_kernel(const WaveCtx* __restrict__ ctxs, int n_ctx, int src, unsigned long long* rows_counter) {
     using T = ModeTraits<kMode>;
     using Lay = SmemLayout<kMode>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned int* P = reinterpret_cast<unsigned int*>(smem_raw);  // working planes
     unsigned long long* Gt = reinterpret_cast<unsigned long long*>(smem_raw + Lay::tot_off);
     unsigned long long* Ht = Gt + kTot;  // per-row hessian modes only
     unsigned int* Ct = reinterpret_cast<unsigned int*>(Gt + (T::var ? 2 : 1) * kTot);
     unsigned long long* s_wstart = reinterpret_cast<unsigned long long*>(smem_raw + Lay::plan_off);
+    // TMA staging (constant-hessian modes): slots over Gt from its first 128-byte boundary,
+    // two mbarriers per warp, their parities
+    __shared__ __align__(8) unsigned long long s_bars[2 * kWarps];
+    unsigned char* stage = smem_raw + Lay::tot_off;
+    stage += (128u - (smem_u32(stage) & 127u)) & 127u;
+    unsigned int phase = 0u;
     {  // private state first: it overlaps the previous kernel's tail
         uint4* z = reinterpret_cast<uint4*>(smem_raw);
         for (int k = threadIdx.x; k < static_cast<int>(Lay::region / 16); k += blockDim.x) z[k] = make_uint4(0, 0, 0, 0);
+    }
+    if (!T::var && (threadIdx.x & 31) == 0) {
+        mbar_init(smem_u32(&s_bars[2 * (threadIdx.x >> 5)]));
+        mbar_init(smem_u32(&s_bars[2 * (threadIdx.x >> 5) + 1]));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     pdl_wait();
     pdl_trigger();
@@ -533,6 +716,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int fg0 = fg * kFG;
         if constexpr (T::var)
             accumulate_var<kMode>(P, Gt, Ht, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, jr.gq, jr.hq);
+        else if (X.codes_map_ok)
+            phase = accumulate_const_tma<kMode>(P, Gt, Ct, stage, s_bars, phase, jr.rows, r0, r1, &X.codes_map, fg0,
+                                                jr.gq, &X.ctl->error);
         else
             accumulate_const<kMode>(P, Gt, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, jr.gq);
         __syncthreads();
@@ -1085,6 +1271,39 @@ int wave_hist_clusters(int cluster) {
     }
     if (dev >= 0 && dev < 64) cached[dev][cluster] = clusters;
     return clusters;
+}
+
+bool encode_codes_map(CUtensorMap* map, const uint8_t* codes, long long n_rows, int stride) {
+    std::memset(map, 0, sizeof(*map));
+    if (codes == nullptr || n_rows <= 0 || n_rows > 0x7fffffffll || stride < kFG || stride % 16 != 0 ||
+        (reinterpret_cast<uintptr_t>(codes) & 15u) != 0)
+        return false;
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static const Encode encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            return static_cast<Encode>(nullptr);
+        }
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (encode == nullptr) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(stride), static_cast<cuuint64_t>(n_rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(stride)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kFG), 1u};  // gather4: one row high
+    const cuuint32_t elem[2] = {1u, 1u};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(codes), dims, strides, box,
+                              elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        std::memset(map, 0, sizeof(*map));
+        return false;
+    }
+    return true;
 }
 
 void launch_wave_hist(int mode, const WaveCtx* ctxs, int n_ctx, int src, HistTune tune,

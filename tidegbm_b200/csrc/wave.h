@@ -30,6 +30,8 @@
 // most once, so 4 * max_leaves - 1 slots always suffice.
 #pragma once
 
+#include <cuda.h>
+
 #include "tgb_internal.h"
 
 namespace tgb {
@@ -81,6 +83,9 @@ struct WaveCtl {
 
 // Everything a wave kernel needs to know about one context (device resident array).
 struct WaveCtx {
+    // TMA descriptor of codes (uint8 [n][stride], box: 32 bytes of one row) for the
+    // histogram's gathers; used when codes_map_ok (encode_codes_map succeeded)
+    CUtensorMap codes_map;
     const uint8_t* codes;      // row-major [n][stride]
     const uint8_t* codes_col;  // column-major [F][col_pitch]
     long long col_pitch;
@@ -113,7 +118,7 @@ struct WaveCtx {
     int n_slots;
     int max_tiles;
     int max_expand;  // expansions a select may plan (0: every candidate ranked within the budget)
-    int pad_expand;
+    int codes_map_ok;
     // categorical features (nullptr: none): flags per feature, the left masks of the scan
     // candidates [(2 * kMaxNodes + 1)][F][4], and the ranking's smoothing (cat_smooth)
     const uint8_t* is_cat;
@@ -163,6 +168,10 @@ struct HistTune {
     int clusters = 37;
 };
 int wave_hist_clusters(int cluster);  // co-resident clusters of the histogram kernel
+// codes_map for a row-major uint8 code matrix [n_rows][stride]: false (map zeroed) where
+// TMA cannot address it (stride not a multiple of 16 or below 32 bytes, base not 16-byte
+// aligned, no driver entry point); the histogram then loads code rows directly.
+bool encode_codes_map(CUtensorMap* map, const uint8_t* codes, long long n_rows, int stride);
 void launch_wave_hist(int mode, const WaveCtx* ctxs, int n_ctx, int src, HistTune tune,
                       unsigned long long* rows_counter, cudaStream_t s);
 void launch_wave_scan(const WaveCtx* ctxs, int n_ctx, int src, int max_f, int ys, bool any_cat, cudaStream_t s);

@@ -109,7 +109,7 @@ def _ptr(a) -> C.c_void_p | None:
 _INT_KEYS = {"n_estimators", "max_depth", "max_leaves", "min_samples_leaf", "max_bin", "n_time_buckets",
              "random_state", "n_jobs", "iid_mode", "halo", "pair_splits", "horizon", "embargo", "goss",
              "bin_sample", "finer_torb", "causal_bins", "causal_structure", "verbose", "col_major_hist",
-             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune", "wave_expand",
+             "cat_min_count", "timing_from", "timing_to", "profile_hist", "hist_bits", "grow", "graph", "hist_tune", "wave_expand", "hist_stage",
              "pair_top_k", "max_pair_splits_per_tree"}
 _DOUBLE_KEYS = {"cat_smooth", "pair_trigger", "pair_l2", "learning_rate", "l2", "l1", "min_child_weight", "min_split_gain", "subsample", "colsample",
                 "colsample_bynode", "goss_top", "goss_other", "torb_min_cover", "max_delta_step", "time_decay",
