@@ -380,14 +380,20 @@ __device__ __noinline__ unsigned int accumulate_const_tma(unsigned int* __restri
     __syncthreads();
     bool ok = true;
     unsigned int pending = 0u;  // slots with gathers in flight
-    // Gathers batch k of this warp into slot s; returns the lane's payload of it.
-    auto issue = [&](int k, int s) -> PT {
+    // The lane's row of batch k of this warp (the batch's first row pads a short batch),
+    // loaded a round before its gather is issued.
+    auto row_of = [&](int k) -> int {
+        const int base = r0 + k * kStep + warp * 32;
+        if (base >= r1) return 0;
+        const int kk = base + lane;
+        return rows[kk < r1 ? kk : base];
+    };
+    // Gathers batch k of this warp (lane rows `row`) into slot s; returns the lane's payload.
+    auto issue = [&](int k, int s, int row) -> PT {
         const int base = r0 + k * kStep + warp * 32;
         if (!ok || base >= r1) return PT(0);
         const int kk = base + lane;
-        const bool v = kk < r1;
-        const int row = rows[v ? kk : base];  // the batch's first row pads a short batch
-        const PT p = v ? pay[kk] : PT(0);
+        const PT p = kk < r1 ? pay[kk] : PT(0);
         const int y0 = __shfl_sync(0xffffffffu, row, (4 * lane) & 31);
         const int y1 = __shfl_sync(0xffffffffu, row, (4 * lane + 1) & 31);
         const int y2 = __shfl_sync(0xffffffffu, row, (4 * lane + 2) & 31);
@@ -400,8 +406,9 @@ __device__ __noinline__ unsigned int accumulate_const_tma(unsigned int* __restri
         return p;
     };
     const int n_rounds = r1 > r0 ? (r1 - r0 + kStep - 1) / kStep : 0;
-    PT p0 = issue(0, 0);
-    PT p1 = issue(1, 1);
+    PT p0 = issue(0, 0, row_of(0));
+    PT p1 = issue(1, 1, row_of(1));
+    int rq = row_of(2);
     const int h = (lane >> 2) & 1;  // lanes 4-7 of each 8 read their second half first
     for (int i = 0; i < n_rounds; ++i) {
         const int s = i & 1;
@@ -422,7 +429,8 @@ __device__ __noinline__ unsigned int accumulate_const_tma(unsigned int* __restri
             const uint4 ca = h ? c1 : c0, cb = h ? c0 : c1;
             const PT p = s ? p1 : p0;
             __syncwarp();  // every lane has read the slot before it is refilled
-            const PT pn = issue(i + 2, s);
+            const PT pn = issue(i + 2, s, rq);
+            rq = row_of(i + 3);
             if (s) p1 = pn;
             else p0 = pn;
             if (base + lane < r1) add_row_const<kMode>(P, p, ca, cb, lane, q, sh);
