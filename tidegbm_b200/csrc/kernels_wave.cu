@@ -336,6 +336,15 @@ __device__ __forceinline__ bool mbar_wait(unsigned int bar, unsigned int parity)
     }
     return false;
 }
+// 16 bytes of shared memory at a 32-bit shared address (after the slot's barrier wait).
+__device__ __forceinline__ uint4 lds16(unsigned int addr) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
 // Rows y0..y3, bytes [x, x + 32) of each, to dst (4 x 32 bytes), completing on bar.
 __device__ __forceinline__ void tma_gather4(unsigned int dst, const CUtensorMap* map, int x, int y0, int y1, int y2,
                                             int y3, unsigned int bar) {
@@ -423,9 +432,9 @@ __device__ __noinline__ unsigned int accumulate_const_tma(unsigned int* __restri
                     atomicExch(err, kErrStaging);
                 }
             }
-            const unsigned char* rp = stage + s * kSlotStride + warp * kSlotBytes + lane * 32;
-            const uint4 c0 = *reinterpret_cast<const uint4*>(rp + 16 * h);
-            const uint4 c1 = *reinterpret_cast<const uint4*>(rp + 16 * (h ^ 1));
+            const unsigned int rp = slot0 + s * kSlotStride + lane * 32;
+            const uint4 c0 = lds16(rp + 16 * h);
+            const uint4 c1 = lds16(rp + 16 * (h ^ 1));
             const uint4 ca = h ? c1 : c0, cb = h ? c0 : c1;
             const PT p = s ? p1 : p0;
             __syncwarp();  // every lane has read the slot before it is refilled
