@@ -55,8 +55,9 @@ TGB_API void tgb_booster_free(tgb_booster* b);
  * launch sequence; hist_bits 0, or 8 with objective mse); "graph" = 1 (default: a tree's
  * waves run as one CUDA graph with a device-side loop) or 0 (enqueued by the host);
  * "hist_tune" = 1 (default: the histogram's launch shape is tuned on the first tree and
- * kept for the process) or 0; "wave_expand" = 0 (default: a wave plans every leaf ranked
- * within the splits left) or k > 0 (the k best; the same trees either way); "hist_stage" =
+ * kept for the process) or 0; "wave_expand" = 8 (default: a wave plans the 8 best leaves
+ * ranked within the splits left), k > 0 (the k best) or 0 (all of them; the same trees
+ * whatever the value); "hist_stage" =
  * 1 (default: the constant-hessian histograms stage code rows in shared memory with TMA
  * gathers) or 0 (each lane loads its rows' codes from global memory; the same results). */
 TGB_API int tgb_set_int(tgb_booster* b, const char* key, long long value);
