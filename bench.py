@@ -794,7 +794,11 @@ def main() -> None:
                     help="0: host-driven waves, every kernel its own launch (for per-kernel launch lists)")
     ap.add_argument("--hist-stage", type=int, default=1, choices=[0, 1],
                     help="0: histogram code rows loaded lane by lane instead of staged by TMA gathers")
+    ap.add_argument("--wave-expand", type=int, default=None, metavar="K",
+                    help="expansions a wave may plan (the library's default when absent; 0: uncapped)")
     args = ap.parse_args()
+    if args.wave_expand is not None:
+        PARAMS["wave_expand"] = args.wave_expand
     if args.graph == 0:
         PARAMS["graph"] = 0
     if args.hist_stage == 0:
