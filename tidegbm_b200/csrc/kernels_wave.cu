@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int fg0 = fg * kFG;
         if constexpr (T::var)
             accumulate_var<kMode>(P, Gt, Ht, Ct, jr.rows, r0, r1, X.codes, X.gp.stride, fg0, jr.gq, jr.hq);
-        else if (X.codes_map_ok)
+        else if (X.codes_map_ok && (reinterpret_cast<uintptr_t>(&X.codes_map) & 63u) == 0)  // TMA wants 64 B
             phase = accumulate_const_tma<kMode>(P, Gt, Ct, stage, s_bars, phase, jr.rows, r0, r1, &X.codes_map, fg0,
                                                 jr.gq, &X.ctl->error);
         else
