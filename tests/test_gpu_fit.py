@@ -210,6 +210,16 @@ def test_fit_int8_pairwise_needs_batched_growth(native):
     assert len(b.trees()) == 3
 
 
+@pytest.mark.parametrize("key,value", [("hist_stage", 2), ("hist_stage", -1), ("wave_expand", -1)])
+def test_fit_rejects_invalid_growth_keys(native, key, value):
+    """hist_stage is 0 or 1 and wave_expand is at least 0; anything else is an error at fit
+    time, never a silent default."""
+    X = np.random.default_rng(2).standard_normal((500, 4)).astype(np.float32)
+    y = X[:, 0].astype(np.float64)
+    with pytest.raises(native.TideError, match=key):
+        native.Booster(iid_mode=1, pair_splits=False, n_estimators=2, **{key: value}).fit(X, y)
+
+
 def test_fit_iid_float64_input(native, oracle):
     """iid mode (no TORB), float64 X, max_leaves 15, depth 4."""
     rng = np.random.default_rng(5)
