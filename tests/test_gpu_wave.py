@@ -157,13 +157,15 @@ def test_quantised_histograms_track_exact(native, bits, objective):
     assert abs(ic(q.raw_predict(ho.X), ho) - ic(ex.raw_predict(ho.X), ho)) <= 0.02
 
 
-@pytest.mark.parametrize("n_features,hist_bits,goss", [(40, 0, 1), (128, 0, 0), (20, 16, 1), (72, 8, 1), (8, 0, 1)])
+@pytest.mark.parametrize("n_features,hist_bits,goss", [(40, 0, 1), (128, 0, 0), (20, 16, 1), (72, 8, 1), (8, 0, 1),
+                                                       (33, 16, 1), (256, 0, 0)])
 def test_tma_staging_grows_the_same_trees(native, n_features, hist_bits, goss):
     """hist_stage 1 stages the code rows of the constant-hessian histograms in shared
     memory by TMA gathers (32 bytes of each of 4 rows per gather, a feature group past
     the row's last code filled with zeros), 0 loads them lane by lane: the same integer
-    sums, so the same trees bit for bit.  40 and 72 features end in a partial group;
-    8 features (16-byte rows) cannot be addressed by the gathers and load directly."""
+    sums, so the same trees bit for bit.  40, 72 and 33 features end in a partial group
+    (33: one feature in a 48-byte row); 256 features are eight groups; 8 features
+    (16-byte rows) cannot be addressed by the gathers and load directly."""
     from tidegbm_b200 import panels
 
     p = panels.panel_small(n_dates=120, n_entities=300, n_features=n_features, seed=11)
