@@ -8,8 +8,9 @@
 // features, summed over the jobs) is cut into one contiguous range per cluster, walked as
 // pieces (job, feature group, rows) whose rows the cluster's CTAs split.  Inside a CTA the
 // accumulation is the lane-per-row scheme:
-// a warp takes 32 rows, lane l loads its row's 32 code bytes of the group with two
-// 16-byte loads and rotates them by l bytes in registers, so step j of the 32-step loop
+// a warp takes 32 rows, lane l holds its row's 32 code bytes of the group (staged in shared
+// memory by TMA gathers in the constant-hessian modes, else loaded from global memory) and
+// rotates them by l bytes in registers, so step j of the 32-step loop
 // touches feature (j + l) & 31: 32 lanes, 32 features, 32 banks of the [bin][feature]
 // layout, conflict-free whatever the codes.  Every code costs fire-and-forget 32-bit
 // shared reductions only (their count depends on the payload mode, below), exact over a
